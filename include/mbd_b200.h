@@ -1,0 +1,144 @@
+/*
+ * mbd_b200.h -- C ABI of the B200-native MBD@rsSCS engine.
+ *
+ * Drop-in for the pmbd.x hot path of 000Justin000/MBD.  The reference enters
+ * its physics through one in-process seam, MBD_rsSCS.f90:218-221
+ *     CALL init_blacs(); CALL MBD_at_rsSCS(ene_mbd_rsSCS)
+ * where MBD_at_rsSCS (UTILS.f90:153-349) reads module globals (coords,
+ * atom_name, hirshfeld_volume, lattice_vector, cut-offs, vacuum axes, flag_xc)
+ * and leaves the energy, alpha_eff, C6_eff and coupled_atom_pol behind.  The
+ * calls below take the same data explicitly.  Every pointer is HOST memory
+ * owned by the caller (except in mbd_rsscs_compute_resident's device path),
+ * arrays follow Fortran column-major order, and every argument type maps to
+ * iso_c_binding (c_int, c_double, c_ptr, c_char).
+ *
+ * Threading: one context per host thread.  A context owns its device
+ * buffers, streams and kernels' workspaces.
+ */
+#ifndef MBD_B200_H
+#define MBD_B200_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes (replace the reference's STOP / ignored INFO) ---------- */
+enum {
+    MBD_OK = 0,
+    MBD_ERR_ARG = 1,              /* bad argument (null pointer, n_atoms < 1, ...) */
+    MBD_ERR_UNKNOWN_ELEMENT = 2,  /* get_vdw_param 'case default' STOP, UTILS.f90:1693-1699 */
+    MBD_ERR_RELAY_NOT_SPD = 3,    /* PDPOTRF info > 0, never checked at UTILS.f90:469 */
+    MBD_ERR_NONPOSITIVE_ALPHA = 4,/* screened alpha_eff <= 0: (alpha/alpha0)^(1/3) undefined, UTILS.f90:737 */
+    MBD_ERR_EIGENSOLVER = 5,      /* PDSYEV info != 0, UTILS.f90:845,864-866 */
+    MBD_ERR_DEVICE = 6,           /* CUDA runtime error / no sm_100 device */
+    MBD_ERR_TIMEOUT = 7,          /* a bounded device-side wait ran out */
+    MBD_ERR_OUT_OF_MEMORY = 8,
+    MBD_ERR_REFINEMENT = 9,       /* mixed mode: refinement did not reach the residual gate
+                                     (informational: the direct FP64 fallback then ran) */
+    MBD_ERR_NOT_BUILT = 10        /* requested mode is not available in this build */
+};
+
+/* ---- compute modes ------------------------------------------------------- */
+enum {
+    MBD_MODE_PLAIN_FP64 = 0,      /* FP64 tensor build, FP64 Cholesky, FP64 eigensolve */
+    MBD_MODE_MIXED = 1,           /* FP32 relay copy factorised on tcgen05 tensor cores
+                                     (3xTF32), FP64 iterative refinement to 1e-10 */
+    MBD_MODE_MIXED_LEARNED = 2    /* MIXED + learned block preconditioner / warm start
+                                     for a block-CG relay solve, direct-solve fallback */
+};
+
+#define MBD_N_FREQ 21             /* omega = 0 plus 20 Gauss-Legendre points, UTILS.f90:1188-1211 */
+
+typedef struct mbd_ctx mbd_ctx;
+
+/* One geometry plus its settings (the module globals of UTILS.f90:18-49). */
+typedef struct {
+    int n_atoms;
+    const int* z;                 /* [n_atoms] atomic numbers (get_vdw_param's atom_name) */
+    const double* coords_bohr;    /* [3*n_atoms] column-major coords(3,N), bohr (after MBD_rsSCS.f90:211) */
+    const double* hirshfeld;      /* [n_atoms] Hirshfeld volume ratios */
+    int n_periodic;               /* 0 = cluster, >0 = periodic (MBD_rsSCS.f90:83) */
+    const double* lattice_bohr;   /* [9] column-major lattice_vector(3,3), columns = vectors, bohr;
+                                     ignored when n_periodic == 0 (may be NULL) */
+    double scs_cut_A;             /* mbd_scs_dip_cutoff, Angstrom (default 120) */
+    double cfdm_cut_A;            /* mbd_cfdm_dip_cutoff, Angstrom (default 100) */
+    double sc_cut_A;              /* mbd_supercell_cutoff, Angstrom (default 25) */
+    int vacuum[3];                /* mbd_scs_vacuum_axis, 0/1 */
+    int xc;                       /* flag_xc: 1 PBE, 2 PBE0, 3 HSE, other -> beta = 1 */
+} mbd_geom;
+
+/* Results of one geometry.  Array pointers are caller-owned and may be NULL
+ * (that output is then skipped). */
+typedef struct {
+    double energy_Ha;             /* MBD@rsSCS energy, UTILS.f90:858 */
+    double c6_mol;                /* system C6, UTILS.f90:288 */
+    int nimag;                    /* number of negative CFDM eigenvalues, UTILS.f90:850-863 */
+    int status;                   /* MBD_OK or an error code for this geometry */
+    int supercell[3];             /* supercell multiplicities, UTILS.f90:1252-1283 */
+    int refine_iters;             /* mixed modes: refinement / CG iterations taken (max over freqs) */
+    double err_est[3];            /* [0] max relative relay residual ||b-Ax||/||b|| over freqs (FP64),
+                                     [1] estimated relative error of alpha_eff,
+                                     [2] estimated relative error of C6 */
+    double* alpha_eff;            /* [n_atoms] screened static polarizability, UTILS.f90:263 */
+    double* c6_eff;               /* [n_atoms] screened C6, UTILS.f90:313 */
+    double* alpha_iw;             /* [21*n_atoms] column-major alpha(f,i); row f=0 is alpha_eff,
+                                     rows 1..20 are coupled_atom_pol(1:20,:) of UTILS.f90:265 */
+    double* molpol_eig;           /* [21*3] column-major eig(f,k) of the molecular polarizability
+                                     tensor (DSYEV('V','U'), UTILS.f90:273) */
+} mbd_result;
+
+/* Create a context on CUDA device `device`.  Replaces start_mpi/init_blacs
+ * (UTILS.f90:97-135): there is no process grid.  Returns MBD_OK or
+ * MBD_ERR_DEVICE when the device is not an sm_100 GPU. */
+int mbd_rsscs_create(mbd_ctx** ctx, int device);
+
+/* Destroy a context and free its device memory. */
+void mbd_rsscs_destroy(mbd_ctx* ctx);
+
+/* One geometry, host buffers in and out: MBD_at_rsSCS (UTILS.f90:153-349).
+ * Returns the same code as out->status. */
+int mbd_rsscs_energy(mbd_ctx* ctx, const mbd_geom* geom, int mode, mbd_result* out);
+
+/* Many geometries of uneven size in one call (no reference counterpart: the
+ * reference handles one geometry per process launch, MBD_rsSCS.f90:1-239).
+ * Returns MBD_OK when every geometry succeeded, else the first failing code;
+ * per-geometry codes are in out[g].status. */
+int mbd_rsscs_energy_batch(mbd_ctx* ctx, int n_geom, const mbd_geom* geoms, int mode,
+                           mbd_result* out);
+
+/* Split form of mbd_rsscs_energy_batch for callers that keep inputs resident:
+ *   upload   copies the geometries to device memory and prepares the work;
+ *   compute  runs every kernel on the resident inputs (no host<->device copy);
+ *   download copies results into the mbd_result array.
+ * The three calls together equal mbd_rsscs_energy_batch. */
+int mbd_rsscs_upload(mbd_ctx* ctx, int n_geom, const mbd_geom* geoms);
+int mbd_rsscs_compute(mbd_ctx* ctx, int mode);
+int mbd_rsscs_download(mbd_ctx* ctx, mbd_result* out);
+
+/* Fortran-friendly helpers. */
+int mbd_rsscs_element_z(const char* symbol);   /* "C" -> 6; 0 if no vdW parameters (UTILS.f90:1336-1701) */
+const char* mbd_rsscs_strerror(int code);
+/* Free-atom table entry: alpha0, C6, R0 as the reference stores them
+ * (REAL*4 literals widened to double).  Returns MBD_ERR_UNKNOWN_ELEMENT for
+ * elements without parameters. */
+int mbd_rsscs_vdw_params(int z, double* alpha0, double* c6, double* r0);
+
+/* Device time in milliseconds of the last mbd_rsscs_compute, per stage:
+ * [0] total, [1] atom/frequency setup, [2] relay tensor build, [3] relay
+ * factorisation, [4] relay solve/refinement + epilogue, [5] CFDM build,
+ * [6] tridiagonal reduction, [7] eigenvalues + energy.  n must be >= 8. */
+int mbd_rsscs_last_timings(mbd_ctx* ctx, double* ms, int n);
+
+/* Counters of the last upload/compute/download: [0] kernel launches issued
+ * by mbd_rsscs_compute, [1] host->device bytes copied by mbd_rsscs_upload,
+ * [2] device->host bytes copied by mbd_rsscs_download.  n must be >= 3. */
+int mbd_rsscs_last_stats(mbd_ctx* ctx, double* out, int n);
+
+/* The CUDA stream (cudaStream_t) every kernel of this context runs on, so a
+ * caller can record its own events around mbd_rsscs_compute. */
+void* mbd_rsscs_stream(mbd_ctx* ctx);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* MBD_B200_H */

@@ -1,0 +1,553 @@
+// C ABI of the engine (include/mbd_b200.h): context, upload / compute /
+// download, and the orchestration of the kernels for one batch of
+// geometries.  Replaces MBD_at_rsSCS (UTILS.f90:153-349) and the BLACS /
+// MPI plumbing around it (UTILS.f90:97-149, 499-529) with one GPU.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <memory>
+#include <vector>
+
+#include "kernels.h"
+#include "mbd_internal.h"
+
+namespace mbd {
+
+// Raw device allocation owned by the context (grow-only).
+struct DevBuf {
+  void* p = nullptr;
+  size_t bytes = 0;
+  ~DevBuf() {
+    if (p) cudaFree(p);
+  }
+  cudaError_t reserve(size_t b) {
+    if (b <= bytes) return cudaSuccess;
+    if (p) cudaFree(p);
+    p = nullptr;
+    bytes = 0;
+    cudaError_t e = cudaMalloc(&p, b);
+    if (e == cudaSuccess) bytes = b;
+    return e;
+  }
+  template <class T>
+  T* as() const { return static_cast<T*>(p); }
+};
+
+// Per-geometry device state that must survive until download.
+struct GeomDev {
+  GeomPlan plan;
+  DevBuf inputs;     // coords, alpha0, c6free, r0, hirsh, shifts, diff data
+  DevBuf results;    // alpha_w, sgm, rvdw_iso, alpha_iw, molpol, c6_eff, alpha_eff, omega, rvdw_eff, scalars, energy, info, d, e, ev
+  // offsets into inputs (doubles unless noted)
+  const double *coords, *alpha0, *c6free, *r0, *hirsh, *scs_shifts, *cfdm_shifts, *diff_shift;
+  const int *diff_is_zero, *place_offset, *place_rc, *place_cc;
+  // results
+  double *alpha_w, *sgm, *rvdw_iso, *alpha_iw, *molpol, *c6_eff, *alpha_eff, *omega, *rvdw_eff;
+  double *scalars, *energy, *d, *e, *ev;
+  int* info;
+  int status_host = MBD_OK;
+};
+
+struct Stage {
+  enum { kTotal = 0, kSetup, kBuild, kFactor, kSolve, kCfdm, kTridiag, kEig, kCount };
+};
+
+}  // namespace mbd
+
+struct mbd_ctx {
+  int device = 0;
+  int num_sms = 0;
+  int trd_ctas_per_sm = 1;
+  cudaStream_t stream = nullptr;
+  std::vector<std::unique_ptr<mbd::GeomDev>> geoms;
+  // shared workspaces, sized for the largest geometry of the batch
+  mbd::DevBuf relay64, linv, rhs, tridiag_ws, hmat, misc;
+  double* weights_dev = nullptr;
+  int* err_flag = nullptr;
+  mbd::TridiagJob* job_dev = nullptr;
+  std::vector<cudaEvent_t> events;
+  double last_ms[mbd::Stage::kCount] = {0};
+  double launches = 0, h2d_bytes = 0, d2h_bytes = 0;
+  int last_mode = 0;
+  bool have_batch = false;
+};
+
+namespace mbd {
+namespace {
+
+int cuda_status(cudaError_t e) {
+  if (e == cudaSuccess) return MBD_OK;
+  if (e == cudaErrorMemoryAllocation) return MBD_ERR_OUT_OF_MEMORY;
+  return MBD_ERR_DEVICE;
+}
+
+#define MBD_CUDA(x)                          \
+  do {                                       \
+    cudaError_t _e = (x);                    \
+    if (_e != cudaSuccess) return cuda_status(_e); \
+  } while (0)
+
+template <class T>
+size_t bytes_of(size_t n) {
+  return ((n * sizeof(T)) + 255) & ~size_t(255);
+}
+
+// Symmetric 3x3 eigenvalues from the upper triangle (DSYEV('V','U'), UTILS.f90:273),
+// cyclic Jacobi in FP64, ascending.
+void sym3_eigenvalues_upper(const double* M, double out[3]) {
+  double a[3][3];
+  for (int r = 0; r < 3; ++r)
+    for (int c = 0; c < 3; ++c) a[r][c] = (r <= c) ? M[3 * r + c] : M[3 * c + r];
+  for (int sweep = 0; sweep < 50; ++sweep) {
+    double off = std::fabs(a[0][1]) + std::fabs(a[0][2]) + std::fabs(a[1][2]);
+    if (off == 0.0) break;
+    for (int p = 0; p < 2; ++p)
+      for (int q = p + 1; q < 3; ++q) {
+        if (a[p][q] == 0.0) continue;
+        double theta = (a[q][q] - a[p][p]) / (2.0 * a[p][q]);
+        double t = (theta >= 0 ? 1.0 : -1.0) / (std::fabs(theta) + std::sqrt(theta * theta + 1.0));
+        double c = 1.0 / std::sqrt(t * t + 1.0), s = t * c;
+        for (int k = 0; k < 3; ++k) {
+          double akp = a[k][p], akq = a[k][q];
+          a[k][p] = c * akp - s * akq;
+          a[k][q] = s * akp + c * akq;
+        }
+        for (int k = 0; k < 3; ++k) {
+          double apk = a[p][k], aqk = a[q][k];
+          a[p][k] = c * apk - s * aqk;
+          a[q][k] = s * apk + c * aqk;
+        }
+      }
+  }
+  out[0] = a[0][0];
+  out[1] = a[1][1];
+  out[2] = a[2][2];
+  std::sort(out, out + 3);
+}
+
+int upload_geometry(mbd_ctx* ctx, const mbd_geom& g, GeomDev* gd) {
+  int st = build_plan(g, &gd->plan);
+  if (st != MBD_OK) return st;
+  const GeomPlan& p = gd->plan;
+  const int N = p.N;
+  const int nshift_s = (int)p.scs_shifts.size() / 3, nshift_c = (int)p.cfdm_shifts.size() / 3;
+  const int ndiff = (int)p.diff_is_zero.size();
+  const int nplace = (int)p.place_rc.size();
+  // inputs
+  size_t off = 0;
+  std::vector<size_t> offs;
+  auto add = [&](size_t b) { offs.push_back(off); off += b; };
+  add(bytes_of<double>(3 * N));             // coords
+  add(bytes_of<double>(N));                 // alpha0
+  add(bytes_of<double>(N));                 // c6free
+  add(bytes_of<double>(N));                 // r0
+  add(bytes_of<double>(N));                 // hirsh
+  add(bytes_of<double>(3 * nshift_s));
+  add(bytes_of<double>(3 * nshift_c));
+  add(bytes_of<double>(3 * ndiff));
+  add(bytes_of<int>(ndiff));
+  add(bytes_of<int>(ndiff + 1));
+  add(bytes_of<int>(nplace));
+  add(bytes_of<int>(nplace));
+  MBD_CUDA(gd->inputs.reserve(off));
+  char* base = gd->inputs.as<char>();
+  std::vector<char> host(off, 0);
+  auto put = [&](int idx, const void* src, size_t b) { std::memcpy(host.data() + offs[idx], src, b); };
+  put(0, p.coords.data(), sizeof(double) * 3 * N);
+  put(1, p.alpha0.data(), sizeof(double) * N);
+  put(2, p.c6free.data(), sizeof(double) * N);
+  put(3, p.r0.data(), sizeof(double) * N);
+  put(4, p.hirsh.data(), sizeof(double) * N);
+  put(5, p.scs_shifts.data(), sizeof(double) * 3 * nshift_s);
+  put(6, p.cfdm_shifts.data(), sizeof(double) * 3 * nshift_c);
+  put(7, p.diff_shift.data(), sizeof(double) * 3 * ndiff);
+  put(8, p.diff_is_zero.data(), sizeof(int) * ndiff);
+  put(9, p.place_offset.data(), sizeof(int) * (ndiff + 1));
+  put(10, p.place_rc.data(), sizeof(int) * nplace);
+  put(11, p.place_cc.data(), sizeof(int) * nplace);
+  MBD_CUDA(cudaMemcpyAsync(base, host.data(), off, cudaMemcpyHostToDevice, ctx->stream));
+  ctx->h2d_bytes += (double)off;
+  gd->coords = reinterpret_cast<const double*>(base + offs[0]);
+  gd->alpha0 = reinterpret_cast<const double*>(base + offs[1]);
+  gd->c6free = reinterpret_cast<const double*>(base + offs[2]);
+  gd->r0 = reinterpret_cast<const double*>(base + offs[3]);
+  gd->hirsh = reinterpret_cast<const double*>(base + offs[4]);
+  gd->scs_shifts = reinterpret_cast<const double*>(base + offs[5]);
+  gd->cfdm_shifts = reinterpret_cast<const double*>(base + offs[6]);
+  gd->diff_shift = reinterpret_cast<const double*>(base + offs[7]);
+  gd->diff_is_zero = reinterpret_cast<const int*>(base + offs[8]);
+  gd->place_offset = reinterpret_cast<const int*>(base + offs[9]);
+  gd->place_rc = reinterpret_cast<const int*>(base + offs[10]);
+  gd->place_cc = reinterpret_cast<const int*>(base + offs[11]);
+  // results
+  off = 0;
+  offs.clear();
+  add(bytes_of<double>(21 * N));   // 0 alpha_w
+  add(bytes_of<double>(21 * N));   // 1 sgm
+  add(bytes_of<double>(N));        // 2 rvdw_iso
+  add(bytes_of<double>(21 * N));   // 3 alpha_iw
+  add(bytes_of<double>(21 * 9));   // 4 molpol
+  add(bytes_of<double>(N));        // 5 c6_eff
+  add(bytes_of<double>(N));        // 6 alpha_eff
+  add(bytes_of<double>(N));        // 7 omega
+  add(bytes_of<double>(N));        // 8 rvdw_eff
+  add(bytes_of<double>(8));        // 9 scalars
+  add(bytes_of<double>(8));        // 10 energy
+  add(bytes_of<double>(p.nH));     // 11 d
+  add(bytes_of<double>(p.nH));     // 12 e
+  add(bytes_of<double>(p.nH));     // 13 ev
+  add(bytes_of<int>(32));          // 14 info
+  MBD_CUDA(gd->results.reserve(off));
+  base = gd->results.as<char>();
+  MBD_CUDA(cudaMemsetAsync(base, 0, off, ctx->stream));
+  gd->alpha_w = reinterpret_cast<double*>(base + offs[0]);
+  gd->sgm = reinterpret_cast<double*>(base + offs[1]);
+  gd->rvdw_iso = reinterpret_cast<double*>(base + offs[2]);
+  gd->alpha_iw = reinterpret_cast<double*>(base + offs[3]);
+  gd->molpol = reinterpret_cast<double*>(base + offs[4]);
+  gd->c6_eff = reinterpret_cast<double*>(base + offs[5]);
+  gd->alpha_eff = reinterpret_cast<double*>(base + offs[6]);
+  gd->omega = reinterpret_cast<double*>(base + offs[7]);
+  gd->rvdw_eff = reinterpret_cast<double*>(base + offs[8]);
+  gd->scalars = reinterpret_cast<double*>(base + offs[9]);
+  gd->energy = reinterpret_cast<double*>(base + offs[10]);
+  gd->d = reinterpret_cast<double*>(base + offs[11]);
+  gd->e = reinterpret_cast<double*>(base + offs[12]);
+  gd->ev = reinterpret_cast<double*>(base + offs[13]);
+  gd->info = reinterpret_cast<int*>(base + offs[14]);
+  return MBD_OK;
+}
+
+int tridiag_group_ctas(const mbd_ctx* ctx, int n) {
+  const int nt = (n + kTrdTile - 1) / kTrdTile;
+  const int tiles = nt * (nt + 1) / 2;
+  return std::max(1, std::min(ctx->num_sms * ctx->trd_ctas_per_sm, tiles));
+}
+
+// The plain FP64 pipeline for one geometry.
+int run_geometry_plain(mbd_ctx* ctx, GeomDev* gd, int gi) {
+  const GeomPlan& p = gd->plan;
+  cudaStream_t s = ctx->stream;
+  const int N = p.N, n = p.n;
+  cudaEvent_t* ev = ctx->events.data() + (size_t)gi * Stage::kCount;
+  auto mark = [&](int k) { cudaEventRecord(ev[k], s); };
+  mark(0);
+  // 1. per-atom frequency table
+  AtomDev ad{gd->coords, gd->alpha0, gd->c6free, gd->r0, gd->hirsh, gd->alpha_w, gd->sgm, gd->rvdw_iso};
+  launch_atom_freq(ad, N, s);
+  ctx->launches += 1;
+  MBD_CUDA(cudaMemsetAsync(gd->info, 0, sizeof(int) * 32, s));
+  mark(1);
+  // 2. relay matrices (21, FP64)
+  const size_t mstride = (size_t)n * p.ld;
+  RelayBuildArgs rb{N, p.ld, mstride, gd->coords, gd->alpha_w, gd->sgm, gd->rvdw_iso, gd->scs_shifts,
+                    (int)p.scs_shifts.size() / 3, p.beta, p.scs_eval_cut, ctx->relay64.as<double>(), nullptr};
+  launch_relay_build(rb, s);
+  ctx->launches += 1;
+  mark(2);
+  // 3. blocked Cholesky, batched over the 21 frequencies
+  BatchMat bm{ctx->relay64.as<double>(), mstride, p.ld, n, kNFreq};
+  const int nblk = (n + kCholNB - 1) / kCholNB;
+  const size_t lstride = (size_t)nblk * kCholNB * kCholNB;
+  double* Linv = ctx->linv.as<double>();
+  for (int k0 = 0; k0 < n; k0 += kCholNB) {
+    launch_potrf_diag_f64(bm, k0, Linv, lstride, gd->info, s);
+    launch_trsm_panel_f64(bm, k0, Linv, lstride, s);
+    launch_syrk_lower_f64(bm, k0, s);
+    ctx->launches += (k0 + kCholNB < n) ? 3 : 1;
+  }
+  mark(3);
+  // 4. solve X = A^-1 [I;..;I] and reductions
+  const size_t ystride = (size_t)n * 3;
+  double* Wv = ctx->rhs.as<double>();
+  double* Zv = Wv + kNFreq * ystride;
+  double* Xv = Zv + kNFreq * ystride;
+  launch_init_rhs(Wv, ystride, n, kNFreq, s);
+  for (int k0 = 0; k0 < n; k0 += kCholNB) launch_trsv_fwd_step(bm, k0, Linv, lstride, Wv, Zv, ystride, s);
+  for (int k0 = (nblk - 1) * kCholNB; k0 >= 0; k0 -= kCholNB)
+    launch_trsv_bwd_step(bm, k0, Linv, lstride, Zv, Xv, ystride, s);
+  EpilogueArgs ea{N, Xv, ystride, gd->alpha_iw, gd->molpol, gd->alpha0, gd->c6free, gd->r0,
+                  gd->c6_eff, gd->alpha_eff, gd->omega, gd->rvdw_eff, gd->scalars};
+  launch_relay_epilogue(ea, s);
+  launch_relay_post(ea, ctx->weights_dev, s);
+  ctx->launches += 3 + 2 * nblk;
+  mark(4);
+  // 5. CFDM Hamiltonian (lower blocks; the rest of the matrix is never read)
+  CfdmBuildArgs cb{N, p.nsl, p.ldH, gd->coords, gd->omega, gd->alpha_eff, gd->rvdw_eff, gd->cfdm_shifts,
+                   (int)p.cfdm_shifts.size() / 3, gd->diff_shift, gd->diff_is_zero, gd->place_offset,
+                   gd->place_rc, gd->place_cc, (int)p.diff_is_zero.size(), p.beta, p.cfdm_cut,
+                   ctx->hmat.as<double>()};
+  launch_cfdm_build(cb, s);
+  ctx->launches += 1;
+  mark(5);
+  // 6. tridiagonal reduction (one cooperative launch)
+  TridiagJob job{ctx->hmat.as<double>(), p.nH, p.ldH, gd->d, gd->e};
+  MBD_CUDA(cudaMemcpyAsync(ctx->job_dev, &job, sizeof(job), cudaMemcpyHostToDevice, s));
+  const int G = tridiag_group_ctas(ctx, p.nH);
+  const size_t wsb = tridiag_workspace_bytes(p.nH, G);
+  MBD_CUDA(launch_tridiag(ctx->job_dev, 1, 1, G, ctx->tridiag_ws.p, wsb, p.nH, ctx->err_flag, s));
+  ctx->launches += 1;
+  mark(6);
+  // 7. eigenvalues, energy
+  launch_tridiag_eigenvalues(gd->d, gd->e, p.nH, gd->ev, s);
+  launch_energy(gd->ev, p.nH, p.nsl, gd->scalars, gd->energy, s);
+  ctx->launches += 2;
+  mark(7);
+  return cuda_status(cudaGetLastError());
+}
+
+int reserve_shared(mbd_ctx* ctx) {
+  size_t relay = 0, linv = 0, rhs = 0, tws = 0, hm = 0;
+  for (auto& gp : ctx->geoms) {
+    const GeomPlan& p = gp->plan;
+    relay = std::max(relay, sizeof(double) * (size_t)kNFreq * p.n * p.ld);
+    const int nblk = (p.n + kCholNB - 1) / kCholNB;
+    linv = std::max(linv, sizeof(double) * (size_t)kNFreq * nblk * kCholNB * kCholNB);
+    rhs = std::max(rhs, sizeof(double) * 3 * (size_t)kNFreq * p.n * 3);
+    hm = std::max(hm, sizeof(double) * (size_t)p.nH * p.ldH);
+    tws = std::max(tws, tridiag_workspace_bytes(p.nH, tridiag_group_ctas(ctx, p.nH)));
+  }
+  MBD_CUDA(ctx->relay64.reserve(relay));
+  MBD_CUDA(ctx->linv.reserve(linv));
+  MBD_CUDA(ctx->rhs.reserve(rhs));
+  MBD_CUDA(ctx->hmat.reserve(hm));
+  MBD_CUDA(ctx->tridiag_ws.reserve(tws));
+  const size_t nev = ctx->geoms.size() * Stage::kCount;
+  while (ctx->events.size() < nev) {
+    cudaEvent_t e;
+    MBD_CUDA(cudaEventCreate(&e));
+    ctx->events.push_back(e);
+  }
+  return MBD_OK;
+}
+
+}  // namespace
+}  // namespace mbd
+
+using namespace mbd;
+
+extern "C" {
+
+int mbd_rsscs_create(mbd_ctx** out, int device) {
+  if (!out) return MBD_ERR_ARG;
+  *out = nullptr;
+  int count = 0;
+  if (cudaGetDeviceCount(&count) != cudaSuccess || device < 0 || device >= count) return MBD_ERR_DEVICE;
+  cudaDeviceProp prop;
+  if (cudaGetDeviceProperties(&prop, device) != cudaSuccess) return MBD_ERR_DEVICE;
+  if (prop.major != 10) return MBD_ERR_DEVICE;   // sm_100a only
+  if (!prop.cooperativeLaunch) return MBD_ERR_DEVICE;
+  std::unique_ptr<mbd_ctx> ctx(new mbd_ctx());
+  ctx->device = device;
+  MBD_CUDA(cudaSetDevice(device));
+  ctx->num_sms = prop.multiProcessorCount;
+  MBD_CUDA(cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking));
+  MBD_CUDA(init_device_constants());
+  MBD_CUDA(init_chol_attributes());
+  ctx->trd_ctas_per_sm = std::max(1, tridiag_max_ctas_per_sm());
+  MBD_CUDA(ctx->misc.reserve(4096));
+  char* m = ctx->misc.as<char>();
+  ctx->weights_dev = reinterpret_cast<double*>(m);
+  ctx->err_flag = reinterpret_cast<int*>(m + 256);
+  ctx->job_dev = reinterpret_cast<TridiagJob*>(m + 512);
+  MBD_CUDA(cudaMemcpy(ctx->weights_dev, kCasimirWeight, sizeof(double) * kNFreq, cudaMemcpyHostToDevice));
+  MBD_CUDA(cudaMemset(ctx->err_flag, 0, sizeof(int)));
+  *out = ctx.release();
+  return MBD_OK;
+}
+
+void mbd_rsscs_destroy(mbd_ctx* ctx) {
+  if (!ctx) return;
+  cudaSetDevice(ctx->device);
+  cudaStreamSynchronize(ctx->stream);
+  for (auto e : ctx->events) cudaEventDestroy(e);
+  ctx->geoms.clear();
+  if (ctx->stream) cudaStreamDestroy(ctx->stream);
+  delete ctx;
+}
+
+int mbd_rsscs_upload(mbd_ctx* ctx, int n_geom, const mbd_geom* geoms) {
+  if (!ctx || n_geom < 1 || !geoms) return MBD_ERR_ARG;
+  MBD_CUDA(cudaSetDevice(ctx->device));
+  ctx->have_batch = false;
+  ctx->h2d_bytes = 0;
+  while ((int)ctx->geoms.size() < n_geom) ctx->geoms.emplace_back(new GeomDev());
+  ctx->geoms.resize(n_geom);
+  int first = MBD_OK;
+  for (int g = 0; g < n_geom; ++g) {
+    int st = upload_geometry(ctx, geoms[g], ctx->geoms[g].get());
+    ctx->geoms[g]->status_host = st;
+    if (st != MBD_OK && first == MBD_OK) first = st;
+    if (st == MBD_ERR_OUT_OF_MEMORY || st == MBD_ERR_DEVICE) return st;
+  }
+  int st = reserve_shared(ctx);
+  if (st != MBD_OK) return st;
+  ctx->have_batch = true;
+  return first;
+}
+
+int mbd_rsscs_compute(mbd_ctx* ctx, int mode) {
+  if (!ctx || !ctx->have_batch) return MBD_ERR_ARG;
+  if (mode != MBD_MODE_PLAIN_FP64) return MBD_ERR_NOT_BUILT;
+  MBD_CUDA(cudaSetDevice(ctx->device));
+  ctx->last_mode = mode;
+  ctx->launches = 0;
+  MBD_CUDA(cudaMemsetAsync(ctx->err_flag, 0, sizeof(int), ctx->stream));
+  for (size_t g = 0; g < ctx->geoms.size(); ++g) {
+    GeomDev* gd = ctx->geoms[g].get();
+    if (gd->status_host != MBD_OK) continue;
+    int st = run_geometry_plain(ctx, gd, (int)g);
+    if (st != MBD_OK) return st;
+  }
+  return MBD_OK;
+}
+
+int mbd_rsscs_download(mbd_ctx* ctx, mbd_result* out) {
+  if (!ctx || !ctx->have_batch || !out) return MBD_ERR_ARG;
+  MBD_CUDA(cudaSetDevice(ctx->device));
+  MBD_CUDA(cudaStreamSynchronize(ctx->stream));
+  int err = 0;
+  MBD_CUDA(cudaMemcpy(&err, ctx->err_flag, sizeof(int), cudaMemcpyDeviceToHost));
+  // stage timings (summed over geometries)
+  for (int k = 0; k < Stage::kCount; ++k) ctx->last_ms[k] = 0.0;
+  ctx->d2h_bytes = sizeof(int);
+  int first = MBD_OK;
+  for (size_t g = 0; g < ctx->geoms.size(); ++g) {
+    GeomDev* gd = ctx->geoms[g].get();
+    const GeomPlan& p = gd->plan;
+    mbd_result& r = out[g];
+    r.status = gd->status_host;
+    for (int k = 0; k < 3; ++k) r.supercell[k] = p.sl[k];
+    r.refine_iters = 0;
+    for (int k = 0; k < 3; ++k) r.err_est[k] = 0.0;
+    if (gd->status_host != MBD_OK) {
+      r.energy_Ha = std::nan("");
+      r.c6_mol = std::nan("");
+      r.nimag = 0;
+      if (first == MBD_OK) first = r.status;
+      continue;
+    }
+    cudaEvent_t* evs = ctx->events.data() + g * Stage::kCount;
+    for (int k = 1; k < Stage::kCount; ++k) {
+      float ms = 0.f;
+      if (cudaEventElapsedTime(&ms, evs[k - 1], evs[k]) == cudaSuccess) ctx->last_ms[k] += ms;
+    }
+    {
+      float ms = 0.f;
+      if (cudaEventElapsedTime(&ms, evs[0], evs[Stage::kCount - 1]) == cudaSuccess) ctx->last_ms[0] += ms;
+    }
+    const int N = p.N;
+    std::vector<double> aiw(21 * (size_t)N), molpol(21 * 9);
+    double scal[8], en[8];
+    int info[32];
+    MBD_CUDA(cudaMemcpy(aiw.data(), gd->alpha_iw, sizeof(double) * 21 * N, cudaMemcpyDeviceToHost));
+    MBD_CUDA(cudaMemcpy(molpol.data(), gd->molpol, sizeof(double) * 21 * 9, cudaMemcpyDeviceToHost));
+    MBD_CUDA(cudaMemcpy(scal, gd->scalars, sizeof(scal), cudaMemcpyDeviceToHost));
+    MBD_CUDA(cudaMemcpy(en, gd->energy, sizeof(en), cudaMemcpyDeviceToHost));
+    MBD_CUDA(cudaMemcpy(info, gd->info, sizeof(info), cudaMemcpyDeviceToHost));
+    ctx->d2h_bytes += sizeof(double) * (21.0 * N + 21 * 9 + 16) + sizeof(info);
+    int status = MBD_OK;
+    for (int f = 0; f < 21; ++f)
+      if (info[f] != 0) status = MBD_ERR_RELAY_NOT_SPD;
+    if (status == MBD_OK && scal[2] > 0.0) status = MBD_ERR_NONPOSITIVE_ALPHA;
+    if (status == MBD_OK && err != 0) status = err;
+    r.status = status;
+    r.c6_mol = scal[0];
+    if (status == MBD_OK) {
+      r.energy_Ha = en[0];
+      r.nimag = (int)en[2];
+    } else {
+      r.energy_Ha = std::nan("");
+      r.nimag = 0;
+    }
+    if (r.alpha_iw)   // column-major alpha(f, i): element (f, i) at f + 21 i
+      for (int i = 0; i < N; ++i)
+        for (int f = 0; f < 21; ++f) r.alpha_iw[f + 21 * (size_t)i] = aiw[(size_t)f * N + i];
+    if (r.alpha_eff) {
+      MBD_CUDA(cudaMemcpy(r.alpha_eff, gd->alpha_eff, sizeof(double) * N, cudaMemcpyDeviceToHost));
+      ctx->d2h_bytes += sizeof(double) * N;
+    }
+    if (r.c6_eff) {
+      MBD_CUDA(cudaMemcpy(r.c6_eff, gd->c6_eff, sizeof(double) * N, cudaMemcpyDeviceToHost));
+      ctx->d2h_bytes += sizeof(double) * N;
+    }
+    if (r.molpol_eig)
+      for (int f = 0; f < 21; ++f) {
+        double e3[3];
+        sym3_eigenvalues_upper(molpol.data() + 9 * f, e3);
+        for (int k = 0; k < 3; ++k) r.molpol_eig[f + 21 * k] = e3[k];
+      }
+    if (status != MBD_OK && first == MBD_OK) first = status;
+  }
+  return first;
+}
+
+int mbd_rsscs_energy_batch(mbd_ctx* ctx, int n_geom, const mbd_geom* geoms, int mode, mbd_result* out) {
+  if (!ctx || !geoms || !out || n_geom < 1) return MBD_ERR_ARG;
+  int st = mbd_rsscs_upload(ctx, n_geom, geoms);
+  if (st == MBD_ERR_OUT_OF_MEMORY || st == MBD_ERR_DEVICE || st == MBD_ERR_ARG) {
+    for (int g = 0; g < n_geom; ++g) out[g].status = st;
+    return st;
+  }
+  int cs = mbd_rsscs_compute(ctx, mode);
+  if (cs != MBD_OK) {
+    for (int g = 0; g < n_geom; ++g) out[g].status = cs;
+    return cs;
+  }
+  return mbd_rsscs_download(ctx, out);
+}
+
+int mbd_rsscs_energy(mbd_ctx* ctx, const mbd_geom* geom, int mode, mbd_result* out) {
+  if (!out) return MBD_ERR_ARG;
+  int st = mbd_rsscs_energy_batch(ctx, 1, geom, mode, out);
+  out->status = out->status ? out->status : st;
+  return out->status;
+}
+
+int mbd_rsscs_element_z(const char* symbol) { return element_z(symbol); }
+
+int mbd_rsscs_vdw_params(int z, double* alpha0, double* c6, double* r0) {
+  VdwParam v;
+  if (!vdw_param(z, &v)) return MBD_ERR_UNKNOWN_ELEMENT;
+  if (alpha0) *alpha0 = v.alpha0;
+  if (c6) *c6 = v.c6;
+  if (r0) *r0 = v.r0;
+  return MBD_OK;
+}
+
+const char* mbd_rsscs_strerror(int code) {
+  switch (code) {
+    case MBD_OK: return "ok";
+    case MBD_ERR_ARG: return "invalid argument";
+    case MBD_ERR_UNKNOWN_ELEMENT: return "VdW parameters not defined for atom";
+    case MBD_ERR_RELAY_NOT_SPD: return "relay matrix is not positive definite (Cholesky failed)";
+    case MBD_ERR_NONPOSITIVE_ALPHA: return "screened polarizability alpha_eff <= 0; R_vdW_eff undefined";
+    case MBD_ERR_EIGENSOLVER: return "diagonalization of CFDM hamiltonian failed";
+    case MBD_ERR_DEVICE: return "CUDA device error or no sm_100 device";
+    case MBD_ERR_TIMEOUT: return "a bounded device-side wait timed out";
+    case MBD_ERR_OUT_OF_MEMORY: return "out of device memory";
+    case MBD_ERR_REFINEMENT: return "mixed-precision refinement missed the residual gate; FP64 fallback used";
+    case MBD_ERR_NOT_BUILT: return "mode not available in this build";
+    default: return "unknown error";
+  }
+}
+
+int mbd_rsscs_last_stats(mbd_ctx* ctx, double* out, int n) {
+  if (!ctx || !out || n < 3) return MBD_ERR_ARG;
+  out[0] = ctx->launches;
+  out[1] = ctx->h2d_bytes;
+  out[2] = ctx->d2h_bytes;
+  return MBD_OK;
+}
+
+void* mbd_rsscs_stream(mbd_ctx* ctx) { return ctx ? (void*)ctx->stream : nullptr; }
+
+int mbd_rsscs_last_timings(mbd_ctx* ctx, double* ms, int n) {
+  if (!ctx || !ms || n < Stage::kCount) return MBD_ERR_ARG;
+  for (int k = 0; k < Stage::kCount; ++k) ms[k] = ctx->last_ms[k];
+  return MBD_OK;
+}
+
+}  // extern "C"

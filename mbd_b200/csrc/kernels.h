@@ -1,0 +1,130 @@
+// Kernel launch interfaces (device pointers only).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstddef>
+
+namespace mbd {
+
+// ---- per-atom, per-frequency data (get_alpha_and_sgm, UTILS.f90:1157-1184) ----
+struct AtomDev {
+  const double* coords;    // [3N]
+  const double* alpha0;    // [N]
+  const double* c6free;    // [N]
+  const double* r0;        // [N]
+  const double* hirsh;     // [N]
+  double* alpha_w;         // [21][N] free-atom alpha(iw), scaled by Hirshfeld ratio
+  double* sgm;             // [21][N] dipole spread sigma(iw)
+  double* rvdw_iso;        // [N]     h^(1/3) R0
+};
+void launch_atom_freq(const AtomDev& a, int N, cudaStream_t s);
+// Copies the frequency grid to constant memory of the current device.
+cudaError_t init_device_constants();
+
+// ---- relay tensor build (get_screened_alpha UTILS.f90:415-441) ----
+struct RelayBuildArgs {
+  int N, ld;
+  size_t mat_stride;       // elements between consecutive frequency matrices
+  const double* coords;
+  const double* alpha_w;   // [21][N]
+  const double* sgm;       // [21][N]
+  const double* rvdw_iso;  // [N]
+  const double* shifts;    // [3*n_shifts], zero shift first
+  int n_shifts;
+  double beta;
+  double cut;              // min(scs cut-off, damping radius), bohr
+  double* A64;             // 21 matrices, row-major lower (may be null)
+  float* A32;              // 21 matrices, row-major lower (may be null)
+};
+void launch_relay_build(const RelayBuildArgs& a, cudaStream_t s);
+
+// ---- CFDM Hamiltonian build (get_mbd_rSCS UTILS.f90:787-807) ----
+struct CfdmBuildArgs {
+  int N, nsl, ldH;
+  const double* coords;
+  const double* omega;     // [N] screened characteristic frequency
+  const double* alpha_eff; // [N]
+  const double* rvdw_eff;  // [N]
+  const double* shifts;    // [3*n_shifts] supercell image translations, zero first
+  int n_shifts;
+  const double* diff_shift;   // [3*n_diff]
+  const int* diff_is_zero;    // [n_diff]
+  const int* place_offset;    // [n_diff+1]
+  const int* place_rc;
+  const int* place_cc;
+  int n_diff;
+  double beta;
+  double cut;
+  double* H;
+};
+void launch_cfdm_build(const CfdmBuildArgs& a, cudaStream_t s);
+
+// ---- relay factorisation / solve, FP64 (PDPOTRF/PDPOTRS UTILS.f90:469-473) ----
+constexpr int kCholNB = 64;
+struct BatchMat {
+  double* A;               // batch of row-major lower matrices
+  size_t stride;           // elements between matrices
+  int ld, n, batch;
+};
+// Linv: per matrix, ceil(n/64) blocks of 64x64 inverses of the diagonal factor blocks.
+void launch_potrf_diag_f64(const BatchMat& m, int k0, double* Linv, size_t linv_stride, int* info,
+                           cudaStream_t s);
+void launch_trsm_panel_f64(const BatchMat& m, int k0, const double* Linv, size_t linv_stride,
+                           cudaStream_t s);
+void launch_syrk_lower_f64(const BatchMat& m, int k0, cudaStream_t s);
+// Y (n x 3 per matrix, row-major, stride ystride) := stacked identities [I;I;..;I].
+void launch_init_rhs(double* Y, size_t ystride, int n, int batch, cudaStream_t s);
+// Forward step: reads W at block k0, writes Z at block k0, updates W below it.
+void launch_trsv_fwd_step(const BatchMat& m, int k0, const double* Linv, size_t linv_stride, double* W,
+                          double* Z, size_t ystride, cudaStream_t s);
+// Backward step: reads Zw at block k0, writes X at block k0, updates Zw above it.
+void launch_trsv_bwd_step(const BatchMat& m, int k0, const double* Linv, size_t linv_stride, double* Zw,
+                          double* X, size_t ystride, cudaStream_t s);
+cudaError_t init_chol_attributes();
+
+// ---- epilogues (UTILS.f90:479-495, 272-315, 731-741) ----
+struct EpilogueArgs {
+  int N;
+  const double* X;         // [21][3N][3] relay solutions
+  size_t xstride;
+  double* alpha_iw;        // [21][N]
+  double* molpol;          // [21][9] row-major 3x3
+  // post
+  const double* alpha0;
+  const double* c6free;
+  const double* r0;
+  double* c6_eff;          // [N]
+  double* alpha_eff;       // [N]
+  double* omega;           // [N]
+  double* rvdw_eff;        // [N]
+  double* scalars;         // [0] c6_mol, [1] sum 3*omega, [2] #alpha_eff <= 0
+};
+void launch_relay_epilogue(const EpilogueArgs& a, cudaStream_t s);
+void launch_relay_post(const EpilogueArgs& a, const double* weights_dev, cudaStream_t s);
+
+// ---- eigensolver (PDSYEV('N','L') UTILS.f90:835, energy UTILS.f90:839-867) ----
+struct TridiagJob {
+  double* A;               // row-major lower, overwritten
+  int n, ld;
+  double* d;               // [n]
+  double* e;               // [n-1]
+};
+constexpr int kTrdTile = 64;
+constexpr int kTrdNB = 32;
+size_t tridiag_workspace_bytes(int n, int group_ctas);
+// Reduces each job's matrix to tridiagonal form with `groups` groups of
+// `group_ctas` co-resident CTAs (cooperative launch).  Returns a cudaError.
+// nmax: the largest n among the jobs (sizes each group's workspace layout).
+cudaError_t launch_tridiag(const TridiagJob* jobs_dev, int n_jobs, int groups, int group_ctas,
+                           void* workspace, size_t ws_bytes_per_group, int nmax, int* err_flag,
+                           cudaStream_t s);
+int tridiag_max_ctas_per_sm();
+
+// Eigenvalues of (d, e) by bisection; writes ev[n] ascending.
+void launch_tridiag_eigenvalues(const double* d, const double* e, int n, double* ev, cudaStream_t s);
+// energy = 0.5*sum_{ev>=0} sqrt(ev)/nsl - 0.5*sum_nonint; out[0]=E, out[1]=sum sqrt, out[2]=nimag
+void launch_energy(const double* ev, int n, int nsl, const double* scalars, double* out,
+                   cudaStream_t s);
+
+}  // namespace mbd

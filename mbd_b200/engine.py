@@ -1,0 +1,265 @@
+"""ctypes binding of libmbd_b200.so (include/mbd_b200.h).
+
+``Engine`` mirrors the reference's single entry point ``MBD_at_rsSCS``
+(UTILS.f90:153-349): give it a geometry and the settings of setting.in and
+it returns the MBD@rsSCS energy, the screened polarizabilities alpha(iw),
+alpha_eff, C6_eff, the system C6 and NIMAG.  Every call goes through the C
+ABI; there is no Python or CPU fallback -- if the CUDA library is missing or
+no sm_100 GPU is present, construction raises.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from dataclasses import dataclass
+
+import numpy as np
+
+from .io import Geometry, Settings
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libmbd_b200.so")
+
+MBD_OK = 0
+ERRORS = {
+    1: "MBD_ERR_ARG", 2: "MBD_ERR_UNKNOWN_ELEMENT", 3: "MBD_ERR_RELAY_NOT_SPD",
+    4: "MBD_ERR_NONPOSITIVE_ALPHA", 5: "MBD_ERR_EIGENSOLVER", 6: "MBD_ERR_DEVICE",
+    7: "MBD_ERR_TIMEOUT", 8: "MBD_ERR_OUT_OF_MEMORY", 9: "MBD_ERR_REFINEMENT", 10: "MBD_ERR_NOT_BUILT",
+}
+MODES = {"plain": 0, "plain_fp64": 0, "mixed": 1, "mixed_learned": 2, "learned": 2}
+N_FREQ = 21
+BOHR = 0.52917721          # UTILS.f90:85
+
+EXPORTED = [
+    "mbd_rsscs_create", "mbd_rsscs_destroy", "mbd_rsscs_energy", "mbd_rsscs_energy_batch",
+    "mbd_rsscs_upload", "mbd_rsscs_compute", "mbd_rsscs_download", "mbd_rsscs_element_z",
+    "mbd_rsscs_strerror", "mbd_rsscs_vdw_params", "mbd_rsscs_last_timings", "mbd_rsscs_last_stats",
+    "mbd_rsscs_stream",
+]
+
+
+class MbdError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"{ERRORS.get(code, code)}: {msg}")
+        self.code = code
+
+
+class CGeom(ctypes.Structure):
+    _fields_ = [
+        ("n_atoms", ctypes.c_int),
+        ("z", ctypes.POINTER(ctypes.c_int)),
+        ("coords_bohr", ctypes.POINTER(ctypes.c_double)),
+        ("hirshfeld", ctypes.POINTER(ctypes.c_double)),
+        ("n_periodic", ctypes.c_int),
+        ("lattice_bohr", ctypes.POINTER(ctypes.c_double)),
+        ("scs_cut_A", ctypes.c_double),
+        ("cfdm_cut_A", ctypes.c_double),
+        ("sc_cut_A", ctypes.c_double),
+        ("vacuum", ctypes.c_int * 3),
+        ("xc", ctypes.c_int),
+    ]
+
+
+class CResult(ctypes.Structure):
+    _fields_ = [
+        ("energy_Ha", ctypes.c_double),
+        ("c6_mol", ctypes.c_double),
+        ("nimag", ctypes.c_int),
+        ("status", ctypes.c_int),
+        ("supercell", ctypes.c_int * 3),
+        ("refine_iters", ctypes.c_int),
+        ("err_est", ctypes.c_double * 3),
+        ("alpha_eff", ctypes.POINTER(ctypes.c_double)),
+        ("c6_eff", ctypes.POINTER(ctypes.c_double)),
+        ("alpha_iw", ctypes.POINTER(ctypes.c_double)),
+        ("molpol_eig", ctypes.POINTER(ctypes.c_double)),
+    ]
+
+
+_LIB = None
+
+
+def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
+    """Load the CUDA library; raises if it has not been built."""
+    global _LIB
+    if _LIB is not None:
+        return _LIB
+    if not os.path.exists(path):
+        raise OSError(f"{path} not found: build it with `python -m mbd_b200.build`")
+    lib = ctypes.CDLL(path)
+    vp = ctypes.c_void_p
+    lib.mbd_rsscs_create.argtypes = [ctypes.POINTER(vp), ctypes.c_int]
+    lib.mbd_rsscs_create.restype = ctypes.c_int
+    lib.mbd_rsscs_destroy.argtypes = [vp]
+    lib.mbd_rsscs_destroy.restype = None
+    lib.mbd_rsscs_energy.argtypes = [vp, ctypes.POINTER(CGeom), ctypes.c_int, ctypes.POINTER(CResult)]
+    lib.mbd_rsscs_energy.restype = ctypes.c_int
+    lib.mbd_rsscs_energy_batch.argtypes = [vp, ctypes.c_int, ctypes.POINTER(CGeom), ctypes.c_int,
+                                           ctypes.POINTER(CResult)]
+    lib.mbd_rsscs_energy_batch.restype = ctypes.c_int
+    lib.mbd_rsscs_upload.argtypes = [vp, ctypes.c_int, ctypes.POINTER(CGeom)]
+    lib.mbd_rsscs_upload.restype = ctypes.c_int
+    lib.mbd_rsscs_compute.argtypes = [vp, ctypes.c_int]
+    lib.mbd_rsscs_compute.restype = ctypes.c_int
+    lib.mbd_rsscs_download.argtypes = [vp, ctypes.POINTER(CResult)]
+    lib.mbd_rsscs_download.restype = ctypes.c_int
+    lib.mbd_rsscs_element_z.argtypes = [ctypes.c_char_p]
+    lib.mbd_rsscs_element_z.restype = ctypes.c_int
+    lib.mbd_rsscs_strerror.argtypes = [ctypes.c_int]
+    lib.mbd_rsscs_strerror.restype = ctypes.c_char_p
+    lib.mbd_rsscs_vdw_params.argtypes = [ctypes.c_int] + [ctypes.POINTER(ctypes.c_double)] * 3
+    lib.mbd_rsscs_vdw_params.restype = ctypes.c_int
+    lib.mbd_rsscs_last_timings.argtypes = [vp, ctypes.POINTER(ctypes.c_double), ctypes.c_int]
+    lib.mbd_rsscs_last_timings.restype = ctypes.c_int
+    lib.mbd_rsscs_last_stats.argtypes = [vp, ctypes.POINTER(ctypes.c_double), ctypes.c_int]
+    lib.mbd_rsscs_last_stats.restype = ctypes.c_int
+    lib.mbd_rsscs_stream.argtypes = [vp]
+    lib.mbd_rsscs_stream.restype = ctypes.c_void_p
+    _LIB = lib
+    return lib
+
+
+def element_z(symbol: str) -> int:
+    return load_library().mbd_rsscs_element_z(symbol.encode())
+
+
+def strerror(code: int) -> str:
+    return load_library().mbd_rsscs_strerror(code).decode()
+
+
+@dataclass
+class Result:
+    energy: float
+    c6_mol: float
+    nimag: int
+    status: int
+    supercell: tuple
+    refine_iters: int
+    err_est: tuple
+    alpha_eff: np.ndarray
+    c6_eff: np.ndarray
+    alpha_iw: np.ndarray      # (21, N)
+    mol_pol_eig: np.ndarray   # (21, 3)
+
+
+class _Packed:
+    """Host arrays of one geometry kept alive for the duration of a call."""
+
+    def __init__(self, geo: Geometry, st: Settings, z: np.ndarray | None = None):
+        self.z = np.ascontiguousarray(z if z is not None else
+                                      np.array([element_z(s) for s in geo.names], dtype=np.int32))
+        self.coords = np.ascontiguousarray(geo.coords / BOHR, dtype=np.float64)   # MBD_rsSCS.f90:211
+        self.hirsh = np.ascontiguousarray(geo.hirshfeld, dtype=np.float64)
+        # lattice(3,3) column-major, columns = vectors == rows of geo.lattice in C order
+        self.lat = np.ascontiguousarray(geo.lattice / BOHR, dtype=np.float64)      # MBD_rsSCS.f90:212
+        N = len(self.hirsh)
+        g = CGeom()
+        g.n_atoms = N
+        g.z = self.z.ctypes.data_as(ctypes.POINTER(ctypes.c_int))
+        g.coords_bohr = self.coords.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+        g.hirshfeld = self.hirsh.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+        g.n_periodic = int(geo.n_periodic)
+        g.lattice_bohr = self.lat.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+        g.scs_cut_A = float(st.mbd_scs_dip_cutoff)
+        g.cfdm_cut_A = float(st.mbd_cfdm_dip_cutoff)
+        g.sc_cut_A = float(st.mbd_supercell_cutoff)
+        for k in range(3):
+            g.vacuum[k] = int(bool(st.mbd_scs_vacuum_axis[k]))
+        g.xc = int(st.xc)
+        self.geom = g
+        self.out_alpha = np.zeros(N)
+        self.out_c6 = np.zeros(N)
+        self.out_aiw = np.zeros(N_FREQ * N)
+        self.out_eig = np.zeros(N_FREQ * 3)
+
+    def result_struct(self) -> CResult:
+        r = CResult()
+        r.alpha_eff = self.out_alpha.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+        r.c6_eff = self.out_c6.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+        r.alpha_iw = self.out_aiw.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+        r.molpol_eig = self.out_eig.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+        return r
+
+    def to_result(self, r: CResult) -> Result:
+        N = len(self.hirsh)
+        return Result(
+            energy=r.energy_Ha, c6_mol=r.c6_mol, nimag=r.nimag, status=r.status,
+            supercell=tuple(r.supercell), refine_iters=r.refine_iters, err_est=tuple(r.err_est),
+            alpha_eff=self.out_alpha.copy(), c6_eff=self.out_c6.copy(),
+            alpha_iw=self.out_aiw.reshape(N, N_FREQ).T.copy(),
+            mol_pol_eig=self.out_eig.reshape(3, N_FREQ).T.copy())
+
+
+class Engine:
+    """One device context (mbd_rsscs_create)."""
+
+    def __init__(self, device: int = 0):
+        self.lib = load_library()
+        self.ctx = ctypes.c_void_p()
+        code = self.lib.mbd_rsscs_create(ctypes.byref(self.ctx), int(device))
+        if code != MBD_OK:
+            raise MbdError(code, strerror(code))
+        self._packed = []
+
+    def close(self):
+        if self.ctx:
+            self.lib.mbd_rsscs_destroy(self.ctx)
+            self.ctx = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    # -- one geometry (MBD_at_rsSCS) -----------------------------------------
+    def energy(self, geo: Geometry, st: Settings | None = None, mode: str = "plain",
+               check: bool = True) -> Result:
+        return self.energy_batch([geo], [st or Settings()], mode, check)[0]
+
+    # -- many geometries -----------------------------------------------------
+    def energy_batch(self, geos, sts, mode: str = "plain", check: bool = True):
+        packs = [_Packed(g, s) for g, s in zip(geos, sts)]
+        garr = (CGeom * len(packs))(*[p.geom for p in packs])
+        rarr = (CResult * len(packs))(*[p.result_struct() for p in packs])
+        code = self.lib.mbd_rsscs_energy_batch(self.ctx, len(packs), garr, MODES[mode], rarr)
+        res = [p.to_result(rarr[i]) for i, p in enumerate(packs)]
+        if check and code != MBD_OK and all(r.status == code for r in res) and code in (6, 8, 10, 1):
+            raise MbdError(code, strerror(code))
+        return res
+
+    # -- split form for device-resident timing --------------------------------
+    def upload(self, geos, sts) -> int:
+        self._packed = [_Packed(g, s) for g, s in zip(geos, sts)]
+        self._garr = (CGeom * len(self._packed))(*[p.geom for p in self._packed])
+        return self.lib.mbd_rsscs_upload(self.ctx, len(self._packed), self._garr)
+
+    def compute(self, mode: str = "plain") -> int:
+        return self.lib.mbd_rsscs_compute(self.ctx, MODES[mode])
+
+    def download(self):
+        rarr = (CResult * len(self._packed))(*[p.result_struct() for p in self._packed])
+        code = self.lib.mbd_rsscs_download(self.ctx, rarr)
+        return code, [p.to_result(rarr[i]) for i, p in enumerate(self._packed)]
+
+    def stats(self) -> dict:
+        buf = (ctypes.c_double * 3)()
+        self.lib.mbd_rsscs_last_stats(self.ctx, buf, 3)
+        return {"launches": int(buf[0]), "h2d_bytes": int(buf[1]), "d2h_bytes": int(buf[2])}
+
+    def stream_handle(self) -> int:
+        """cudaStream_t of this context (for recording caller-side events)."""
+        return int(self.lib.mbd_rsscs_stream(self.ctx) or 0)
+
+    def timings(self) -> dict:
+        buf = (ctypes.c_double * 8)()
+        self.lib.mbd_rsscs_last_timings(self.ctx, buf, 8)
+        keys = ["total", "setup", "relay_build", "relay_factor", "relay_solve", "cfdm_build",
+                "tridiag", "eig_energy"]
+        return dict(zip(keys, list(buf)))

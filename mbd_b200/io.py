@@ -1,0 +1,148 @@
+"""Input files and the text report of pmbd.x.
+
+* ``parse_geometry`` reads geometry.in as MBD_rsSCS.f90:66-89 does: atom
+  count, a skipped line, ``name x y z hirshfeld`` per atom (Angstrom), then
+  optional ``lattice_vector ax ay az`` records that make the system periodic.
+* ``parse_settings`` reads setting.in as MBD_rsSCS.f90:98-135: for each line
+  the first keyword that occurs as a substring (xc, mbd_supercell_cutoff,
+  mbd_cfdm_dip_cutoff, mbd_scs_dip_cutoff, mbd_scs_vacuum_axis, nprow, npcol)
+  takes the value(s) after the first token.  ``nprow``/``npcol`` are accepted
+  and ignored: there is no process grid.
+* ``format_report`` prints the fields of MBD_at_rsSCS's report
+  (UTILS.f90:223-331).
+"""
+from __future__ import annotations
+
+from dataclasses import dataclass, field
+
+import numpy as np
+
+DEFAULT_SC_CUT = 25.0        # UTILS.f90:81
+DEFAULT_CFDM_CUT = 100.0     # UTILS.f90:82
+DEFAULT_SCS_CUT = 120.0      # UTILS.f90:83
+
+
+class InputError(ValueError):
+    pass
+
+
+@dataclass
+class Settings:
+    xc: int = 1
+    mbd_supercell_cutoff: float = DEFAULT_SC_CUT
+    mbd_cfdm_dip_cutoff: float = DEFAULT_CFDM_CUT
+    mbd_scs_dip_cutoff: float = DEFAULT_SCS_CUT
+    mbd_scs_vacuum_axis: tuple = (False, False, False)
+    nprow: int = 1
+    npcol: int = 1
+    given: set = field(default_factory=set)   # keywords present in the file
+
+
+@dataclass
+class Geometry:
+    names: list
+    coords: np.ndarray                    # (N, 3) Angstrom
+    hirshfeld: np.ndarray                 # (N,)
+    lattice: np.ndarray = field(default_factory=lambda: np.zeros((3, 3)))   # rows = vectors, Angstrom
+    n_periodic: int = 0
+
+
+def _real(tok: str) -> float:
+    return float(tok.strip().lower().replace("d", "e"))
+
+
+def _logical(tok: str) -> bool:
+    t = tok.strip().lower().lstrip(".")
+    if not t or t[0] not in "tf":
+        raise InputError(f"not a Fortran logical: {tok!r}")
+    return t[0] == "t"
+
+
+def _records(text: str):
+    for line in text.splitlines():
+        yield line.replace(",", " ").split()
+
+
+def parse_geometry(text: str) -> Geometry:
+    lines = text.splitlines()
+    try:
+        n = int(lines[0].split()[0])
+    except (IndexError, ValueError) as exc:
+        raise InputError("geometry: first record must hold the atom count") from exc
+    if n < 1:
+        raise InputError("geometry: atom count must be >= 1")
+    names, xyz, hv = [], [], []
+    k = 2
+    for i in range(n):
+        if k >= len(lines):
+            raise InputError(f"geometry: expected {n} atoms, found {i}")
+        tok = lines[k].replace(",", " ").split()
+        k += 1
+        if len(tok) < 5:
+            raise InputError(f"geometry: atom record {i + 1} needs name x y z hirshfeld")
+        names.append(tok[0][:2])                 # CHARACTER*2
+        xyz.append([_real(t) for t in tok[1:4]])
+        hv.append(_real(tok[4]))
+    geo = Geometry(names, np.array(xyz, dtype=np.float64), np.array(hv, dtype=np.float64))
+    if k < len(lines) and "lattice_vector" in lines[k]:
+        geo.n_periodic = 3
+        lat = np.zeros((3, 3))
+        for i in range(3):
+            if k + i >= len(lines):
+                raise InputError("geometry: three lattice_vector records required")
+            tok = lines[k + i].replace(",", " ").split()
+            lat[i] = [_real(t) for t in tok[1:4]]
+        geo.lattice = lat
+    return geo
+
+
+def parse_settings(text: str) -> Settings:
+    s = Settings()
+    for tok, line in zip(_records(text), text.splitlines()):
+        try:
+            if "xc" in line:
+                s.xc = int(tok[1]); s.given.add("xc")
+            elif "mbd_supercell_cutoff" in line:
+                s.mbd_supercell_cutoff = _real(tok[1]); s.given.add("mbd_supercell_cutoff")
+            elif "mbd_cfdm_dip_cutoff" in line:
+                s.mbd_cfdm_dip_cutoff = _real(tok[1]); s.given.add("mbd_cfdm_dip_cutoff")
+            elif "mbd_scs_dip_cutoff" in line:
+                s.mbd_scs_dip_cutoff = _real(tok[1]); s.given.add("mbd_scs_dip_cutoff")
+            elif "mbd_scs_vacuum_axis" in line:
+                s.mbd_scs_vacuum_axis = tuple(_logical(t) for t in tok[1:4]); s.given.add("mbd_scs_vacuum_axis")
+            elif "nprow" in line:
+                s.nprow = int(tok[1]); s.given.add("nprow")
+            elif "npcol" in line:
+                s.npcol = int(tok[1]); s.given.add("npcol")
+        except (IndexError, ValueError) as exc:
+            raise InputError(f"settings: cannot read {line.strip()!r}") from exc
+    return s
+
+
+def format_report(geo: Geometry, res, omega_grid=None) -> str:
+    """Report fields of MBD_at_rsSCS (UTILS.f90:223-331) for a Result."""
+    from .engine import N_FREQ
+    out = []
+    out.append("  | Many-Body Dispersion (MBD@rsSCS) energy ")
+    out.append("  | System dynamic molecular polarizability alpha(iw) (bohr^3)")
+    out.append("  | ---------------------------------------------------------------------------")
+    out.append("  |  omega(Ha)   alpha_iso      alpha_xx       alpha_yy       alpha_zz")
+    for f in range(N_FREQ):
+        ev = res.mol_pol_eig[f]
+        w = omega_grid[f] if omega_grid is not None else float("nan")
+        out.append("  | %10.6f%15.6E%15.6E%15.6E%15.6E" % (w, ev.sum() / 3.0, ev[0], ev[1], ev[2]))
+    out.append("  | ---------------------------------------------------------------------------")
+    out.append("  | System C6 coefficient    :  %20.8f  hartree bohr^6" % res.c6_mol)
+    out.append("  | ---------------------------------------------------------------------------")
+    out.append("  | Partitioned C6 (hartree bohr^6) | alpha (bohr^3)  of atom in system")
+    out.append("  | ---------------------------------------------------------------------------")
+    for i, name in enumerate(geo.names):
+        out.append("  | ATOM %4d  %-2s%12.6f      %12.6f" % (i + 1, name, res.c6_eff[i], res.alpha_eff[i]))
+    out.append("  | ---------------------------------------------------------------------------")
+    sc = res.supercell
+    out.append("  | Creating super cell of dimension%3d X %3d X %3d in MBD calculation" % tuple(sc))
+    out.append("  | containing%6d  atom" % (len(geo.names) * sc[0] * sc[1] * sc[2]))
+    if res.nimag > 0:
+        out.append("***WARNING: found %4d negative eigenvalues in MBD energy calculation." % res.nimag)
+    out.append("  | MBD@rsSCS energy   :%20.9f Ha     %20.9f eV" % (res.energy, res.energy * 27.211))
+    return "\n".join(out)

@@ -1,0 +1,129 @@
+"""GPU parity: the CUDA path (through the C ABI) against the FP64 oracle.
+
+Targets: the reference's shipped examples (tests/golden/*.json, whose oracle
+section is pinned to the reference's printed reports) and seeded synthetic
+inputs of every workload at sizes the oracle finishes in seconds.
+
+Bars (north star): |E - E_oracle| <= 1e-6 Ha, screened C6 within 1e-6
+relative.  The plain FP64 mode is additionally held to 1e-9 Ha / 1e-9
+relative, which only a faithful FP64 implementation meets.
+"""
+import json
+import os
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+GOLDEN = os.path.join(os.path.dirname(__file__), "golden")
+E_TOL = 1e-6
+C6_RTOL = 1e-6
+PLAIN_E_TOL = 1e-9
+PLAIN_RTOL = 1e-9
+
+
+@pytest.fixture(scope="module")
+def engine():
+    from mbd_b200 import Engine
+    eng = Engine(0)
+    yield eng
+    eng.close()
+
+
+def _fixture(name):
+    with open(os.path.join(GOLDEN, name + ".json")) as fh:
+        return json.load(fh)
+
+
+def _check(res, energy, c6_mol, alpha_iw, c6_eff, mode):
+    e_tol = PLAIN_E_TOL if mode == "plain" else E_TOL
+    rtol = PLAIN_RTOL if mode == "plain" else C6_RTOL
+    assert res.status == 0
+    assert abs(res.energy - energy) <= e_tol, (res.energy, energy)
+    assert abs(res.c6_mol - c6_mol) <= rtol * abs(c6_mol)
+    np.testing.assert_allclose(res.c6_eff, c6_eff, rtol=rtol, atol=0)
+    np.testing.assert_allclose(res.alpha_iw, alpha_iw, rtol=10 * rtol, atol=1e-12)
+
+
+@pytest.mark.parametrize("mode", ["plain"])
+@pytest.mark.parametrize("name", ["C6H6", "H2O", "PBBA", "graphene_111"])
+def test_reference_examples(engine, name, mode):
+    from mbd_b200 import parse_geometry, parse_settings
+    fix = _fixture(name)
+    geo = parse_geometry(fix["geometry_in"])
+    st = parse_settings(fix["settings_in"])
+    res = engine.energy(geo, st, mode=mode)
+    o = fix["oracle"]
+    _check(res, o["energy"], o["c6_mol"], np.array(o["alpha_iw"]), np.array(o["c6_eff"]), mode)
+    assert list(res.supercell) == o["supercell"]
+    assert res.nimag == o["nimag"]
+    if "printed" in fix:   # the reference's own printed digits
+        assert abs(res.energy - fix["printed"]["energy"]) <= 0.5e-9 + (E_TOL if mode != "plain" else 1e-12)
+    np.testing.assert_allclose(res.mol_pol_eig, np.array(o["mol_pol_eig"]), rtol=1e-8, atol=1e-10)
+
+
+def test_tiochf_reports_nonpositive_alpha(engine):
+    """TiOCHF screens O atoms to alpha <= 0: the engine reports it instead of
+    feeding NaN to the eigensolver (UTILS.f90:737)."""
+    from mbd_b200 import parse_geometry, parse_settings
+    fix = _fixture("TiOCHF")
+    res = engine.energy(parse_geometry(fix["geometry_in"]), parse_settings(fix["settings_in"]), check=False)
+    assert res.status == 4
+    assert np.isnan(res.energy)
+    np.testing.assert_allclose(res.alpha_iw, np.array(fix["oracle"]["alpha_iw"]), rtol=1e-7, atol=1e-9)
+
+
+def _oracle(geo, st):
+    from oracle import mbd_oracle as mo
+    og = mo.Geometry(list(geo.names), geo.coords.copy(), geo.hirshfeld.copy(), geo.lattice.copy(), geo.n_periodic)
+    os_ = mo.Settings(xc=st.xc, mbd_supercell_cutoff=st.mbd_supercell_cutoff,
+                      mbd_cfdm_dip_cutoff=st.mbd_cfdm_dip_cutoff, mbd_scs_dip_cutoff=st.mbd_scs_dip_cutoff,
+                      mbd_scs_vacuum_axis=tuple(st.mbd_scs_vacuum_axis))
+    return mo.mbd_at_rsscs(og, os_)
+
+
+@pytest.mark.parametrize("mode", ["plain"])
+@pytest.mark.parametrize("case", ["benzene", "cluster60", "cluster300", "graphene_sheet", "box150"])
+def test_synthetic_vs_oracle(engine, case, mode):
+    from mbd_b200 import synthetic as sy
+    geo, st = {
+        "benzene": lambda: sy.benzene(),
+        "cluster60": lambda: sy.cluster(60, seed=3),
+        "cluster300": lambda: sy.cluster(300, seed=4),
+        "graphene_sheet": lambda: sy.graphene_sheet(),
+        "box150": lambda: sy.periodic_box(150, seed=5, scs_cut=30.0, cfdm_cut=30.0, sc_cut=10.0),
+    }[case]()
+    ref = _oracle(geo, st)
+    res = engine.energy(geo, st, mode=mode)
+    _check(res, ref.energy, ref.c6_mol, ref.alpha_iw, ref.c6_eff, mode)
+    assert res.nimag == ref.nimag
+
+
+def test_batch_equals_single(engine):
+    """A ragged batch gives the same numbers as one call per geometry."""
+    from mbd_b200 import synthetic as sy
+    items = [sy.cluster(n, seed=10 + n) for n in (20, 75, 33)]
+    batch = engine.energy_batch([g for g, _ in items], [s for _, s in items])
+    for (g, s), rb in zip(items, batch):
+        rs = engine.energy(g, s)
+        assert rb.status == rs.status == 0
+        assert rb.energy == pytest.approx(rs.energy, abs=1e-12)
+        np.testing.assert_allclose(rb.alpha_iw, rs.alpha_iw, rtol=1e-13)
+
+
+def test_unknown_element_status(engine):
+    from mbd_b200 import Geometry, Settings
+    from mbd_b200.engine import CGeom  # noqa: F401
+    geo = Geometry(["C", "La"], np.array([[0, 0, 0], [0, 0, 2.0]]), np.array([0.8, 0.8]))
+    res = engine.energy(geo, Settings(), check=False)
+    assert res.status == 2
+
+
+def test_repeat_is_deterministic(engine):
+    from mbd_b200 import synthetic as sy
+    geo, st = sy.cluster(120, seed=9)
+    a = engine.energy(geo, st)
+    b = engine.energy(geo, st)
+    assert a.energy == b.energy
+    np.testing.assert_array_equal(a.alpha_iw, b.alpha_iw)
