@@ -159,7 +159,12 @@ def main():
     ap.add_argument("--mode", default="plain")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--sizes", default=None,
+                    help="comma-separated cluster sizes replacing 500,1000,2000 (profiling runs only)")
     args = ap.parse_args()
+    if args.sizes:
+        global SIZES
+        SIZES = tuple(int(x) for x in args.sizes.split(","))
 
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))

@@ -12,8 +12,14 @@
 
 #include "kernels.h"
 #include "mbd_internal.h"
+#include "tc3.h"
 
 namespace mbd {
+
+// Refinement sweeps of the mixed relay solve and the residual gate
+// ||B - A X||_F / ||B||_F that accepts its result.
+constexpr int kRefineIters = 4;
+constexpr double kResidualGate = 1e-10;
 
 // Raw device allocation owned by the context (grow-only).
 struct DevBuf {
@@ -45,7 +51,7 @@ struct GeomDev {
   const int *diff_is_zero, *place_offset, *place_rc, *place_cc;
   // results
   double *alpha_w, *sgm, *rvdw_iso, *alpha_iw, *molpol, *c6_eff, *alpha_eff, *omega, *rvdw_eff;
-  double *scalars, *energy, *d, *e, *ev;
+  double *scalars, *energy, *d, *e, *ev, *rnorm2;
   int* info;
   int status_host = MBD_OK;
 };
@@ -64,6 +70,9 @@ struct mbd_ctx {
   std::vector<std::unique_ptr<mbd::GeomDev>> geoms;
   // shared workspaces, sized for the largest geometry of the batch
   mbd::DevBuf relay64, linv, rhs, tridiag_ws, hmat, misc;
+  // mixed mode: FP32 relay copy, hi/lo panel and diagonal-inverse buffers,
+  // refinement vectors (X, R, Z, D) and residual workspace
+  mbd::DevBuf relay32, p_hi, p_lo, l_hi, l_lo, mixv, res_ws;
   double* weights_dev = nullptr;
   int* err_flag = nullptr;
   mbd::TridiagJob* job_dev = nullptr;
@@ -197,8 +206,9 @@ int upload_geometry(mbd_ctx* ctx, const mbd_geom& g, GeomDev* gd) {
   add(bytes_of<double>(8));        // 10 energy
   add(bytes_of<double>(p.nH));     // 11 d
   add(bytes_of<double>(p.nH));     // 12 e
-  add(bytes_of<double>(p.nH));     // 13 ev
+  add(bytes_of<double>(2 * (size_t)p.nH));   // 13 ev (+ e^2 scratch of the bisection)
   add(bytes_of<int>(32));          // 14 info
+  add(bytes_of<double>(32));       // 15 rnorm2 (squared refinement residual per frequency)
   MBD_CUDA(gd->results.reserve(off));
   base = gd->results.as<char>();
   MBD_CUDA(cudaMemsetAsync(base, 0, off, ctx->stream));
@@ -217,6 +227,7 @@ int upload_geometry(mbd_ctx* ctx, const mbd_geom& g, GeomDev* gd) {
   gd->e = reinterpret_cast<double*>(base + offs[12]);
   gd->ev = reinterpret_cast<double*>(base + offs[13]);
   gd->info = reinterpret_cast<int*>(base + offs[14]);
+  gd->rnorm2 = reinterpret_cast<double*>(base + offs[15]);
   return MBD_OK;
 }
 
@@ -226,13 +237,94 @@ int tridiag_group_ctas(const mbd_ctx* ctx, int n) {
   return std::max(1, std::min(ctx->num_sms * ctx->trd_ctas_per_sm, tiles));
 }
 
-// The plain FP64 pipeline for one geometry.
-int run_geometry_plain(mbd_ctx* ctx, GeomDev* gd, int gi) {
+// Mixed relay solve: FP32 copy factorised with 3xTF32 tcgen05 GEMMs (128-wide
+// panels), FP64 iterative refinement against the FP64 matrices.  Returns the
+// device pointer of the refined solution X (n x 3 per frequency).
+int relay_mixed(mbd_ctx* ctx, GeomDev* gd, size_t mstride, cudaEvent_t* ev) {
+  const GeomPlan& p = gd->plan;
+  cudaStream_t s = ctx->stream;
+  const int n = p.n;
+  const int npad = round_up(n, kMixNB);
+  BatchMat32 m32{ctx->relay32.as<float>(), mstride, p.ld, n, kNFreq};
+  float* phi = ctx->p_hi.as<float>();
+  float* plo = ctx->p_lo.as<float>();
+  float* lhi = ctx->l_hi.as<float>();
+  float* llo = ctx->l_lo.as<float>();
+  const size_t pb = (size_t)npad * kMixNB;   // elements per matrix of the panel / Linv buffers
+  Tc3Maps trsm_maps, syrk_maps;
+  bool ok = make_tc3_map(&trsm_maps.a_hi, phi, npad, kMixNB, kMixNB, pb, kNFreq) &&
+            make_tc3_map(&trsm_maps.a_lo, plo, npad, kMixNB, kMixNB, pb, kNFreq) &&
+            make_tc3_map(&trsm_maps.b_hi, lhi, npad, kMixNB, kMixNB, pb, kNFreq) &&
+            make_tc3_map(&trsm_maps.b_lo, llo, npad, kMixNB, kMixNB, pb, kNFreq);
+  if (!ok) return MBD_ERR_DEVICE;
+  syrk_maps.a_hi = trsm_maps.a_hi;
+  syrk_maps.a_lo = trsm_maps.a_lo;
+  syrk_maps.b_hi = trsm_maps.a_hi;
+  syrk_maps.b_lo = trsm_maps.a_lo;
+  for (int k0 = 0; k0 < n; k0 += kMixNB) {
+    launch_potrf_diag_f32(m32, k0, lhi, llo, pb, gd->info, s);
+    ctx->launches += 1;
+    const int rows = n - k0 - kMixNB;
+    if (rows <= 0) continue;
+    launch_split(m32.A, mstride, p.ld, k0 + kMixNB, k0, rows, kMixNB, phi, plo, pb, kMixNB, kNFreq, s);
+    const int mt = (rows + 127) / 128;
+    Tc3Params tp{};
+    tp.mode = TC3_STORE_SPLIT;
+    tp.batch = kNFreq;
+    tp.a_row0 = k0 + kMixNB;
+    tp.b_row0 = k0;
+    tp.m_rows = rows;
+    tp.n_cols = kMixNB;
+    tp.k = kMixNB;
+    tp.n_tiles_n = 1;
+    tp.C = m32.A;
+    tp.c_bstride = mstride;
+    tp.c_ld = p.ld;
+    tp.c_row0 = k0 + kMixNB;
+    tp.c_col0 = k0;
+    tp.out_hi = phi;
+    tp.out_lo = plo;
+    tp.o_bstride = pb;
+    tp.o_ld = kMixNB;
+    tp.err = ctx->err_flag;
+    launch_tc3_gemm(trsm_maps, tp, mt, s);
+    Tc3Params sp = tp;
+    sp.mode = TC3_SYRK_LOWER;
+    sp.b_row0 = k0 + kMixNB;
+    sp.n_cols = rows;
+    sp.c_col0 = k0 + kMixNB;
+    sp.out_hi = sp.out_lo = nullptr;
+    launch_tc3_gemm(syrk_maps, sp, mt * (mt + 1) / 2, s);
+    ctx->launches += 3;
+  }
+  cudaEventRecord(ev[Stage::kFactor], s);
+  // FP64 iterative refinement: X = 0, R = B; repeat D = (LL^T)^-1 R, X += D, R = B - A X
+  const size_t ystride = (size_t)n * 3;
+  double* X = ctx->mixv.as<double>();
+  double* R = X + kNFreq * ystride;
+  double* Z = R + kNFreq * ystride;
+  double* D = Z + kNFreq * ystride;
+  MBD_CUDA(cudaMemsetAsync(X, 0, sizeof(double) * kNFreq * ystride, s));
+  launch_init_rhs(R, ystride, n, kNFreq, s);
+  ctx->launches += 1;
+  const int nblk = (n + kMixNB - 1) / kMixNB;
+  for (int it = 0; it < kRefineIters; ++it) {
+    launch_solve_f32(m32, lhi, llo, pb, R, Z, D, ystride, s);
+    launch_relay_residual(ctx->relay64.as<double>(), mstride, p.ld, n, kNFreq, X, D, R, ystride,
+                          ctx->res_ws.as<double>(), gd->rnorm2, s);
+    ctx->launches += 2 * nblk + 4;
+  }
+  return MBD_OK;
+}
+
+// The pipeline for one geometry; `mode` selects the relay solve.
+int run_geometry(mbd_ctx* ctx, GeomDev* gd, int gi, int mode) {
   const GeomPlan& p = gd->plan;
   cudaStream_t s = ctx->stream;
   const int N = p.N, n = p.n;
   cudaEvent_t* ev = ctx->events.data() + (size_t)gi * Stage::kCount;
   auto mark = [&](int k) { cudaEventRecord(ev[k], s); };
+  const bool mixed = mode != MBD_MODE_PLAIN_FP64;
   mark(0);
   // 1. per-atom frequency table
   AtomDev ad{gd->coords, gd->alpha0, gd->c6free, gd->r0, gd->hirsh, gd->alpha_w, gd->sgm, gd->rvdw_iso};
@@ -240,39 +332,48 @@ int run_geometry_plain(mbd_ctx* ctx, GeomDev* gd, int gi) {
   ctx->launches += 1;
   MBD_CUDA(cudaMemsetAsync(gd->info, 0, sizeof(int) * 32, s));
   mark(1);
-  // 2. relay matrices (21, FP64)
+  // 2. relay matrices (21, FP64; plus an FP32 copy in mixed mode)
   const size_t mstride = (size_t)n * p.ld;
   RelayBuildArgs rb{N, p.ld, mstride, gd->coords, gd->alpha_w, gd->sgm, gd->rvdw_iso, gd->scs_shifts,
-                    (int)p.scs_shifts.size() / 3, p.beta, p.scs_eval_cut, ctx->relay64.as<double>(), nullptr};
+                    (int)p.scs_shifts.size() / 3, p.beta, p.scs_eval_cut, ctx->relay64.as<double>(),
+                    mixed ? ctx->relay32.as<float>() : nullptr};
   launch_relay_build(rb, s);
   ctx->launches += 1;
   mark(2);
-  // 3. blocked Cholesky, batched over the 21 frequencies
-  BatchMat bm{ctx->relay64.as<double>(), mstride, p.ld, n, kNFreq};
-  const int nblk = (n + kCholNB - 1) / kCholNB;
-  const size_t lstride = (size_t)nblk * kCholNB * kCholNB;
-  double* Linv = ctx->linv.as<double>();
-  for (int k0 = 0; k0 < n; k0 += kCholNB) {
-    launch_potrf_diag_f64(bm, k0, Linv, lstride, gd->info, s);
-    launch_trsm_panel_f64(bm, k0, Linv, lstride, s);
-    launch_syrk_lower_f64(bm, k0, s);
-    ctx->launches += (k0 + kCholNB < n) ? 3 : 1;
-  }
-  mark(3);
-  // 4. solve X = A^-1 [I;..;I] and reductions
   const size_t ystride = (size_t)n * 3;
-  double* Wv = ctx->rhs.as<double>();
-  double* Zv = Wv + kNFreq * ystride;
-  double* Xv = Zv + kNFreq * ystride;
-  launch_init_rhs(Wv, ystride, n, kNFreq, s);
-  for (int k0 = 0; k0 < n; k0 += kCholNB) launch_trsv_fwd_step(bm, k0, Linv, lstride, Wv, Zv, ystride, s);
-  for (int k0 = (nblk - 1) * kCholNB; k0 >= 0; k0 -= kCholNB)
-    launch_trsv_bwd_step(bm, k0, Linv, lstride, Zv, Xv, ystride, s);
+  double* Xv = nullptr;
+  if (mixed) {
+    int st = relay_mixed(ctx, gd, mstride, ev);
+    if (st != MBD_OK) return st;
+    Xv = ctx->mixv.as<double>();
+  } else {
+    // 3. blocked Cholesky, batched over the 21 frequencies
+    BatchMat bm{ctx->relay64.as<double>(), mstride, p.ld, n, kNFreq};
+    const int nblk = (n + kCholNB - 1) / kCholNB;
+    const size_t lstride = (size_t)nblk * kCholNB * kCholNB;
+    double* Linv = ctx->linv.as<double>();
+    for (int k0 = 0; k0 < n; k0 += kCholNB) {
+      launch_potrf_diag_f64(bm, k0, Linv, lstride, gd->info, s);
+      launch_trsm_panel_f64(bm, k0, Linv, lstride, s);
+      launch_syrk_lower_f64(bm, k0, s);
+      ctx->launches += (k0 + kCholNB < n) ? 3 : 1;
+    }
+    mark(3);
+    // 4. solve X = A^-1 [I;..;I]
+    double* Wv = ctx->rhs.as<double>();
+    double* Zv = Wv + kNFreq * ystride;
+    Xv = Zv + kNFreq * ystride;
+    launch_init_rhs(Wv, ystride, n, kNFreq, s);
+    for (int k0 = 0; k0 < n; k0 += kCholNB) launch_trsv_fwd_step(bm, k0, Linv, lstride, Wv, Zv, ystride, s);
+    for (int k0 = (nblk - 1) * kCholNB; k0 >= 0; k0 -= kCholNB)
+      launch_trsv_bwd_step(bm, k0, Linv, lstride, Zv, Xv, ystride, s);
+    ctx->launches += 1 + 2 * nblk;
+  }
   EpilogueArgs ea{N, Xv, ystride, gd->alpha_iw, gd->molpol, gd->alpha0, gd->c6free, gd->r0,
                   gd->c6_eff, gd->alpha_eff, gd->omega, gd->rvdw_eff, gd->scalars};
   launch_relay_epilogue(ea, s);
   launch_relay_post(ea, ctx->weights_dev, s);
-  ctx->launches += 3 + 2 * nblk;
+  ctx->launches += 2;
   mark(4);
   // 5. CFDM Hamiltonian (lower blocks; the rest of the matrix is never read)
   CfdmBuildArgs cb{N, p.nsl, p.ldH, gd->coords, gd->omega, gd->alpha_eff, gd->rvdw_eff, gd->cfdm_shifts,
@@ -323,6 +424,26 @@ int reserve_shared(mbd_ctx* ctx) {
   return MBD_OK;
 }
 
+// Buffers only the mixed modes use (allocated on first use).
+int reserve_mixed(mbd_ctx* ctx) {
+  size_t r32 = 0, pan = 0, vec = 0, res = 0;
+  for (auto& gp : ctx->geoms) {
+    const GeomPlan& p = gp->plan;
+    r32 = std::max(r32, sizeof(float) * (size_t)kNFreq * p.n * p.ld);
+    pan = std::max(pan, sizeof(float) * (size_t)kNFreq * round_up(p.n, kMixNB) * kMixNB);
+    vec = std::max(vec, sizeof(double) * 4 * (size_t)kNFreq * p.n * 3);
+    res = std::max(res, sizeof(double) * relay_residual_ws_doubles(p.n, kNFreq));
+  }
+  MBD_CUDA(ctx->relay32.reserve(r32));
+  MBD_CUDA(ctx->p_hi.reserve(pan));
+  MBD_CUDA(ctx->p_lo.reserve(pan));
+  MBD_CUDA(ctx->l_hi.reserve(pan));
+  MBD_CUDA(ctx->l_lo.reserve(pan));
+  MBD_CUDA(ctx->mixv.reserve(vec));
+  MBD_CUDA(ctx->res_ws.reserve(res));
+  return MBD_OK;
+}
+
 }  // namespace
 }  // namespace mbd
 
@@ -346,6 +467,9 @@ int mbd_rsscs_create(mbd_ctx** out, int device) {
   MBD_CUDA(cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking));
   MBD_CUDA(init_device_constants());
   MBD_CUDA(init_chol_attributes());
+  MBD_CUDA(init_eigval_attributes());
+  MBD_CUDA(init_tc3_attributes());
+  MBD_CUDA(init_mixed_attributes());
   ctx->trd_ctas_per_sm = std::max(1, tridiag_max_ctas_per_sm());
   MBD_CUDA(ctx->misc.reserve(4096));
   char* m = ctx->misc.as<char>();
@@ -390,15 +514,19 @@ int mbd_rsscs_upload(mbd_ctx* ctx, int n_geom, const mbd_geom* geoms) {
 
 int mbd_rsscs_compute(mbd_ctx* ctx, int mode) {
   if (!ctx || !ctx->have_batch) return MBD_ERR_ARG;
-  if (mode != MBD_MODE_PLAIN_FP64) return MBD_ERR_NOT_BUILT;
+  if (mode != MBD_MODE_PLAIN_FP64 && mode != MBD_MODE_MIXED && mode != MBD_MODE_MIXED_LEARNED) return MBD_ERR_ARG;
   MBD_CUDA(cudaSetDevice(ctx->device));
+  if (mode != MBD_MODE_PLAIN_FP64) {
+    int st = reserve_mixed(ctx);
+    if (st != MBD_OK) return st;
+  }
   ctx->last_mode = mode;
   ctx->launches = 0;
   MBD_CUDA(cudaMemsetAsync(ctx->err_flag, 0, sizeof(int), ctx->stream));
   for (size_t g = 0; g < ctx->geoms.size(); ++g) {
     GeomDev* gd = ctx->geoms[g].get();
     if (gd->status_host != MBD_OK) continue;
-    int st = run_geometry_plain(ctx, gd, (int)g);
+    int st = run_geometry(ctx, gd, (int)g, mode);
     if (st != MBD_OK) return st;
   }
   return MBD_OK;
@@ -442,6 +570,22 @@ int mbd_rsscs_download(mbd_ctx* ctx, mbd_result* out) {
     std::vector<double> aiw(21 * (size_t)N), molpol(21 * 9);
     double scal[8], en[8];
     int info[32];
+    if (ctx->last_mode != MBD_MODE_PLAIN_FP64) {
+      // residual gate of the mixed relay solve; a miss re-runs this geometry
+      // with the direct FP64 solve (the plain path) before reading results
+      double rn[32];
+      MBD_CUDA(cudaMemcpy(rn, gd->rnorm2, sizeof(double) * 21, cudaMemcpyDeviceToHost));
+      double worst = 0.0;
+      for (int f = 0; f < 21; ++f) worst = std::max(worst, std::sqrt(rn[f] / (3.0 * N)));
+      r.err_est[0] = r.err_est[1] = r.err_est[2] = worst;
+      r.refine_iters = kRefineIters;
+      if (!(worst <= kResidualGate)) {
+        int st = run_geometry(ctx, gd, (int)g, MBD_MODE_PLAIN_FP64);
+        if (st != MBD_OK) return st;
+        MBD_CUDA(cudaStreamSynchronize(ctx->stream));
+        r.refine_iters = -1;
+      }
+    }
     MBD_CUDA(cudaMemcpy(aiw.data(), gd->alpha_iw, sizeof(double) * 21 * N, cudaMemcpyDeviceToHost));
     MBD_CUDA(cudaMemcpy(molpol.data(), gd->molpol, sizeof(double) * 21 * 9, cudaMemcpyDeviceToHost));
     MBD_CUDA(cudaMemcpy(scal, gd->scalars, sizeof(scal), cudaMemcpyDeviceToHost));

@@ -46,7 +46,7 @@ def _check(res, energy, c6_mol, alpha_iw, c6_eff, mode):
     np.testing.assert_allclose(res.alpha_iw, alpha_iw, rtol=10 * rtol, atol=1e-12)
 
 
-@pytest.mark.parametrize("mode", ["plain"])
+@pytest.mark.parametrize("mode", ["plain", "mixed"])
 @pytest.mark.parametrize("name", ["C6H6", "H2O", "PBBA", "graphene_111"])
 def test_reference_examples(engine, name, mode):
     from mbd_b200 import parse_geometry, parse_settings
@@ -83,7 +83,7 @@ def _oracle(geo, st):
     return mo.mbd_at_rsscs(og, os_)
 
 
-@pytest.mark.parametrize("mode", ["plain"])
+@pytest.mark.parametrize("mode", ["plain", "mixed"])
 @pytest.mark.parametrize("case", ["benzene", "cluster60", "cluster300", "graphene_sheet", "box150"])
 def test_synthetic_vs_oracle(engine, case, mode):
     from mbd_b200 import synthetic as sy
@@ -98,6 +98,9 @@ def test_synthetic_vs_oracle(engine, case, mode):
     res = engine.energy(geo, st, mode=mode)
     _check(res, ref.energy, ref.c6_mol, ref.alpha_iw, ref.c6_eff, mode)
     assert res.nimag == ref.nimag
+    if mode == "mixed":
+        assert res.refine_iters > 0          # the tensor-core result passed the residual gate
+        assert res.err_est[0] <= 1e-10
 
 
 def test_batch_equals_single(engine):
