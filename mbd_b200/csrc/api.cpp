@@ -72,7 +72,8 @@ struct mbd_ctx {
   mbd::DevBuf relay64, linv, rhs, tridiag_ws, hmat, misc;
   // mixed mode: FP32 relay copy, hi/lo panel and diagonal-inverse buffers,
   // refinement vectors (X, R, Z, D) and residual workspace
-  mbd::DevBuf relay32, p_hi, p_lo, l_hi, l_lo, mixv, res_ws;
+  mbd::DevBuf relay32, p_hi, p_lo, l_hi, l_lo, mixv, res_ws, solve_sync;
+  int solve_epoch = 0;
   double* weights_dev = nullptr;
   int* err_flag = nullptr;
   mbd::TridiagJob* job_dev = nullptr;
@@ -252,15 +253,23 @@ int relay_mixed(mbd_ctx* ctx, GeomDev* gd, size_t mstride, cudaEvent_t* ev) {
   float* llo = ctx->l_lo.as<float>();
   const size_t pb = (size_t)npad * kMixNB;   // elements per matrix of the panel / Linv buffers
   Tc3Maps trsm_maps, syrk_maps;
-  bool ok = make_tc3_map(&trsm_maps.a_hi, phi, npad, kMixNB, kMixNB, pb, kNFreq) &&
-            make_tc3_map(&trsm_maps.a_lo, plo, npad, kMixNB, kMixNB, pb, kNFreq) &&
+  // panel operands/outputs cover rows [0, n) (TMA zero-fills beyond), the
+  // diagonal inverses [0, npad), the output matrix is the n x n FP32 relay copy
+  bool ok = make_tc3_map(&trsm_maps.a_hi, phi, n, kMixNB, kMixNB, pb, kNFreq) &&
+            make_tc3_map(&trsm_maps.a_lo, plo, n, kMixNB, kMixNB, pb, kNFreq) &&
             make_tc3_map(&trsm_maps.b_hi, lhi, npad, kMixNB, kMixNB, pb, kNFreq) &&
-            make_tc3_map(&trsm_maps.b_lo, llo, npad, kMixNB, kMixNB, pb, kNFreq);
+            make_tc3_map(&trsm_maps.b_lo, llo, npad, kMixNB, kMixNB, pb, kNFreq) &&
+            make_tc3_map(&trsm_maps.c, m32.A, n, n, p.ld, mstride, kNFreq);
   if (!ok) return MBD_ERR_DEVICE;
+  trsm_maps.c_hi = trsm_maps.a_hi;
+  trsm_maps.c_lo = trsm_maps.a_lo;
   syrk_maps.a_hi = trsm_maps.a_hi;
   syrk_maps.a_lo = trsm_maps.a_lo;
   syrk_maps.b_hi = trsm_maps.a_hi;
   syrk_maps.b_lo = trsm_maps.a_lo;
+  syrk_maps.c = trsm_maps.c;
+  syrk_maps.c_hi = trsm_maps.a_hi;
+  syrk_maps.c_lo = trsm_maps.a_lo;
   for (int k0 = 0; k0 < n; k0 += kMixNB) {
     launch_potrf_diag_f32(m32, k0, lhi, llo, pb, gd->info, s);
     ctx->launches += 1;
@@ -309,7 +318,8 @@ int relay_mixed(mbd_ctx* ctx, GeomDev* gd, size_t mstride, cudaEvent_t* ev) {
   ctx->launches += 1;
   const int nblk = (n + kMixNB - 1) / kMixNB;
   for (int it = 0; it < kRefineIters; ++it) {
-    launch_solve_f32(m32, lhi, llo, pb, R, Z, D, ystride, s);
+    launch_solve_f32(m32, lhi, llo, pb, R, Z, D, ystride, ctx->solve_sync.as<int>(), ++ctx->solve_epoch,
+                     ctx->err_flag, s);
     launch_relay_residual(ctx->relay64.as<double>(), mstride, p.ld, n, kNFreq, X, D, R, ystride,
                           ctx->res_ws.as<double>(), gd->rnorm2, s);
     ctx->launches += 2 * nblk + 4;
@@ -441,6 +451,13 @@ int reserve_mixed(mbd_ctx* ctx) {
   MBD_CUDA(ctx->l_lo.reserve(pan));
   MBD_CUDA(ctx->mixv.reserve(vec));
   MBD_CUDA(ctx->res_ws.reserve(res));
+  size_t sync_ints = 0;
+  for (auto& gp : ctx->geoms) sync_ints = std::max(sync_ints, solve_sync_ints(gp->plan.n, kNFreq));
+  if (ctx->solve_sync.bytes < sizeof(int) * sync_ints) {
+    MBD_CUDA(ctx->solve_sync.reserve(sizeof(int) * sync_ints));
+    MBD_CUDA(cudaMemset(ctx->solve_sync.p, 0, ctx->solve_sync.bytes));
+    ctx->solve_epoch = 0;
+  }
   return MBD_OK;
 }
 

@@ -3,66 +3,69 @@
 // sides and accumulation), and the FP64 residual R = B - A X of the lower-
 // stored FP64 relay matrices used by the iterative refinement
 // (PDPOTRF/PDPOTRS of UTILS.f90:469-473, refined to FP64 accuracy).
+//
+// The triangular solves are sync-free single launches: each CTA takes a
+// ticket (atomicAdd) that fixes its 128-row block in dependency order, then
+// waits on per-block ready flags of the blocks it needs (bounded spins), so
+// a CTA only ever waits for CTAs that already started.
 #include <cuda_runtime.h>
 
 #include <algorithm>
 
 #include "tc3.h"
+#include "../../include/mbd_b200.h"
 
 namespace mbd {
 namespace {
 
 constexpr int NB = kMixNB;   // 128
 constexpr int LDS = NB + 1;
+constexpr long long kSpinCycles = 4000000000LL;
 
 __device__ __forceinline__ float tf32_hi(float x) { return __uint_as_float(__float_as_uint(x) & 0xFFFFE000u); }
 
 // ---------------------------------------------------------------------------
+// 512 threads: thread t works on row t/4 with column phase t%4.
 __global__ void __launch_bounds__(512) potrf_diag_f32_kernel(BatchMat32 m, int k0, float* linv_hi, float* linv_lo,
                                                             size_t l_bstride, int* info) {
   extern __shared__ float fsm[];
   float (*S)[LDS] = reinterpret_cast<float (*)[LDS]>(fsm);
   float (*X)[LDS] = reinterpret_cast<float (*)[LDS]>(fsm + NB * LDS);
-  __shared__ int s_bad;
   const int b = blockIdx.x;
   float* A = m.A + (size_t)b * m.stride;
   const int nbk = min(NB, m.n - k0);
   const int tid = threadIdx.x;
-  if (tid == 0) s_bad = 0;
-  for (int idx = tid; idx < NB * NB; idx += blockDim.x) {
-    const int r = idx / NB, c = idx % NB;
+  const int r = tid / 4, part = tid % 4;
+  for (int c = part; c < NB; c += 4) {
     float v = 0.f;
     if (r < nbk && c < nbk && c <= r) v = A[(size_t)(k0 + r) * m.ld + k0 + c];
-    if (r == c && r >= nbk) v = 1.f;
+    if (r == c && r >= nbk) v = 1.f;                 // identity padding keeps the block SPD
     S[r][c] = v;
     X[r][c] = 0.f;
   }
   __syncthreads();
+  bool bad = false;
   for (int c = 0; c < NB; ++c) {
-    if (tid == 0) {
-      float piv = S[c][c];
-      if (!(piv > 0.f)) {
-        if (!s_bad && c < nbk) {
-          s_bad = 1;
-          atomicCAS(&info[b], 0, k0 + c + 1);
-        }
-        piv = 1.f;
-      }
-      S[c][c] = sqrtf(piv);
+    float piv = S[c][c];
+    if (!(piv > 0.f)) {
+      if (c < nbk) bad = true;
+      piv = 1.f;
     }
+    const float d = sqrtf(piv);
+    const float inv = 1.f / d;
+    if (r > c && part == 0) S[r][c] *= inv;
     __syncthreads();
-    const float inv = 1.f / S[c][c];
-    for (int r = c + 1 + tid; r < NB; r += blockDim.x) S[r][c] *= inv;
-    __syncthreads();
-    const int rem = NB - c - 1;
-    for (int idx = tid; idx < rem * rem; idx += blockDim.x) {
-      const int r = c + 1 + idx / rem, q = c + 1 + idx % rem;
-      if (q <= r) S[r][q] = fmaf(-S[r][c], S[q][c], S[r][q]);
+    if (r > c) {
+      const float lrc = S[r][c];
+      for (int q = c + 1 + part; q <= r; q += 4) S[r][q] = fmaf(-lrc, S[q][c], S[r][q]);
+    } else if (r == c && part == 0) {
+      S[c][c] = d;
     }
     __syncthreads();
   }
+  if (bad && tid == 0) atomicCAS(&info[b], 0, k0 + 1);
   // X = S^-1 row by row; 4 threads per column j split the dot product.
-  const int j = tid / 4, part = tid % 4;
+  const int j = tid / 4;
   for (int i = 0; i < NB; ++i) {
     const float dinv = 1.f / S[i][i];
     float acc = 0.f;
@@ -78,101 +81,177 @@ __global__ void __launch_bounds__(512) potrf_diag_f32_kernel(BatchMat32 m, int k
   }
   float* lh = linv_hi + (size_t)b * l_bstride + (size_t)k0 * NB;
   float* ll = linv_lo + (size_t)b * l_bstride + (size_t)k0 * NB;
-  for (int idx = tid; idx < NB * NB; idx += blockDim.x) {
-    const int r = idx / NB, c = idx % NB;
+  for (int c = part; c < NB; c += 4) {
     const float x = X[r][c];
     const float h = tf32_hi(x);
-    lh[idx] = h;
-    ll[idx] = x - h;
+    lh[r * NB + c] = h;
+    ll[r * NB + c] = x - h;
     if (r < nbk && c < nbk && c <= r) A[(size_t)(k0 + r) * m.ld + k0 + c] = S[r][c];
   }
 }
 
 // ---------------------------------------------------------------------------
-// Forward step at block k0: z_k = Linv_k w_k (into Z); w[rows below] -= L[rows, k] z_k.
-__global__ void __launch_bounds__(256) fwd_f32_kernel(BatchMat32 m, int k0, const float* lh, const float* ll,
-                                                     size_t l_bstride, double* W, double* Z, size_t ystride) {
-  __shared__ double zk[NB][3];
-  __shared__ double wk[NB][3];
-  const int b = blockIdx.y;
-  const float* A = m.A + (size_t)b * m.stride;
-  double* w = W + (size_t)b * ystride;
-  const float* Lh = lh + (size_t)b * l_bstride + (size_t)k0 * NB;
-  const float* Ll = ll + (size_t)b * l_bstride + (size_t)k0 * NB;
-  const int nbk = min(NB, m.n - k0);
-  const int tid = threadIdx.x;
-  for (int idx = tid; idx < NB * 3; idx += blockDim.x) wk[idx / 3][idx % 3] = (idx / 3 < nbk) ? w[(size_t)k0 * 3 + idx] : 0.0;
-  __syncthreads();
-  for (int idx = tid; idx < NB * 3; idx += blockDim.x) {
-    const int r = idx / 3, c = idx % 3;
-    double acc = 0.0;
-    for (int l = 0; l <= r; ++l) acc += ((double)Lh[r * NB + l] + (double)Ll[r * NB + l]) * wk[l][c];
-    zk[r][c] = acc;
+// Sync-free triangular solves, one CTA (256 threads) per (matrix, 128-row block).
+struct SolveArgs {
+  BatchMat32 m;
+  const float* lh;
+  const float* ll;
+  size_t l_bstride;
+  const double* in;      // right-hand side (forward) / forward result (backward)
+  double* out;           // result
+  size_t ystride;
+  int* flags;            // [batch][nblk] epoch of the last block completion
+  int* ticket;
+  int epoch;
+  int nblk;
+  int* err;
+};
+
+__device__ bool wait_flag(const int* f, int epoch, int* err) {
+  const long long t0 = clock64();
+  while (*(volatile const int*)f != epoch) {
+    if (*(volatile int*)err != 0 || clock64() - t0 > kSpinCycles) {
+      atomicCAS(err, 0, MBD_ERR_TIMEOUT);
+      return false;
+    }
+    __nanosleep(64);
   }
-  __syncthreads();
-  if (blockIdx.x == 0)
-    for (int idx = tid; idx < nbk * 3; idx += blockDim.x) Z[(size_t)b * ystride + (size_t)k0 * 3 + idx] = zk[idx / 3][idx % 3];
-  const int warp = tid / 32, lane = tid % 32;
-  const int rbase = k0 + nbk + blockIdx.x * 64;
-  for (int rr = warp; rr < 64; rr += 8) {
-    const int r = rbase + rr;
-    if (r >= m.n) break;
-    double s0 = 0, s1 = 0, s2 = 0;
-    for (int l = lane; l < nbk; l += 32) {
-      const double a = A[(size_t)r * m.ld + k0 + l];
-      s0 += a * zk[l][0];
-      s1 += a * zk[l][1];
-      s2 += a * zk[l][2];
-    }
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-      s0 += __shfl_xor_sync(0xffffffffu, s0, o);
-      s1 += __shfl_xor_sync(0xffffffffu, s1, o);
-      s2 += __shfl_xor_sync(0xffffffffu, s2, o);
-    }
-    if (lane == 0) {
-      w[(size_t)r * 3 + 0] -= s0;
-      w[(size_t)r * 3 + 1] -= s1;
-      w[(size_t)r * 3 + 2] -= s2;
-    }
-  }
+  __threadfence();
+  return true;
 }
 
-// Backward step at block k0: x_k = Linv_k^T z_k (into D); z[rows above] -= L[k, rows]^T x_k.
-__global__ void __launch_bounds__(256) bwd_f32_kernel(BatchMat32 m, int k0, const float* lh, const float* ll,
-                                                     size_t l_bstride, double* Zw, double* D, size_t ystride) {
-  __shared__ double xk[NB][3];
+// Forward: z_blk = Linv_blk (w_blk - sum_{k<blk} L_{blk,k} z_k).
+// Warp w owns rows 16w..16w+15 of the block; lane l owns columns 4l..4l+3 of
+// each 128-wide tile and keeps per-row partial sums until the end.
+__global__ void __launch_bounds__(256) fwd_syncfree_kernel(SolveArgs a) {
+  __shared__ int s_t;
   __shared__ double zk[NB][3];
-  const int b = blockIdx.y;
-  const float* A = m.A + (size_t)b * m.stride;
-  double* z = Zw + (size_t)b * ystride;
-  const float* Lh = lh + (size_t)b * l_bstride + (size_t)k0 * NB;
-  const float* Ll = ll + (size_t)b * l_bstride + (size_t)k0 * NB;
-  const int nbk = min(NB, m.n - k0);
-  const int tid = threadIdx.x;
-  for (int idx = tid; idx < NB * 3; idx += blockDim.x) zk[idx / 3][idx % 3] = (idx / 3 < nbk) ? z[(size_t)k0 * 3 + idx] : 0.0;
+  __shared__ double acc_s[NB][3];
+  __shared__ int s_ok;
+  if (threadIdx.x == 0) s_t = atomicAdd(a.ticket, 1);
   __syncthreads();
-  for (int idx = tid; idx < NB * 3; idx += blockDim.x) {
-    const int r = idx / 3, c = idx % 3;
-    double acc = 0.0;
-    for (int l = r; l < NB; ++l) acc += ((double)Lh[l * NB + r] + (double)Ll[l * NB + r]) * zk[l][c];
-    xk[r][c] = acc;
+  const int batch = a.m.batch;
+  const int t = s_t;
+  const int blk = t / batch, b = t % batch;
+  const int n = a.m.n;
+  const int r0 = blk * NB;
+  const int nbk = min(NB, n - r0);
+  const float* A = a.m.A + (size_t)b * a.m.stride;
+  const int warp = threadIdx.x / 32, lane = threadIdx.x % 32;
+  double part[16][3];
+#pragma unroll
+  for (int u = 0; u < 16; ++u) part[u][0] = part[u][1] = part[u][2] = 0.0;
+  for (int k = 0; k < blk; ++k) {
+    if (threadIdx.x == 0) s_ok = wait_flag(a.flags + b * a.nblk + k, a.epoch, a.err);
+    __syncthreads();
+    if (!s_ok) return;
+    for (int idx = threadIdx.x; idx < NB * 3; idx += blockDim.x)
+      zk[idx / 3][idx % 3] = __ldcg(a.out + (size_t)b * a.ystride + (size_t)k * NB * 3 + idx);
+    __syncthreads();
+    const int c0 = k * NB + 4 * lane;
+    const double z00 = zk[4 * lane][0], z01 = zk[4 * lane][1], z02 = zk[4 * lane][2];
+    const double z10 = zk[4 * lane + 1][0], z11 = zk[4 * lane + 1][1], z12 = zk[4 * lane + 1][2];
+    const double z20 = zk[4 * lane + 2][0], z21 = zk[4 * lane + 2][1], z22 = zk[4 * lane + 2][2];
+    const double z30 = zk[4 * lane + 3][0], z31 = zk[4 * lane + 3][1], z32 = zk[4 * lane + 3][2];
+#pragma unroll
+    for (int u = 0; u < 16; ++u) {
+      const int row = r0 + warp * 16 + u;
+      if (row < n) {
+        const float4 l4 = *reinterpret_cast<const float4*>(A + (size_t)row * a.m.ld + c0);
+        part[u][0] += l4.x * z00 + l4.y * z10 + l4.z * z20 + l4.w * z30;
+        part[u][1] += l4.x * z01 + l4.y * z11 + l4.z * z21 + l4.w * z31;
+        part[u][2] += l4.x * z02 + l4.y * z12 + l4.z * z22 + l4.w * z32;
+      }
+    }
+  }
+  // rhs - sum, gathered per row
+#pragma unroll
+  for (int u = 0; u < 16; ++u) {
+#pragma unroll
+    for (int q = 0; q < 3; ++q) {
+      double v = part[u][q];
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+      part[u][q] = v;
+    }
+    const int rr = warp * 16 + u;
+    if (lane < 3) {
+      const double rhs = (rr < nbk) ? a.in[(size_t)b * a.ystride + (size_t)(r0 + rr) * 3 + lane] : 0.0;
+      acc_s[rr][lane] = rhs - (lane == 0 ? part[u][0] : lane == 1 ? part[u][1] : part[u][2]);
+    }
   }
   __syncthreads();
-  if (blockIdx.x == 0)
-    for (int idx = tid; idx < nbk * 3; idx += blockDim.x) D[(size_t)b * ystride + (size_t)k0 * 3 + idx] = xk[idx / 3][idx % 3];
-  const int jc = blockIdx.x * blockDim.x + tid;
-  if (jc >= k0) return;
-  double s0 = 0, s1 = 0, s2 = 0;
-  for (int i = 0; i < nbk; ++i) {
-    const double a = A[(size_t)(k0 + i) * m.ld + jc];
-    s0 += a * xk[i][0];
-    s1 += a * xk[i][1];
-    s2 += a * xk[i][2];
+  // z_blk = Linv_blk acc (lower triangular)
+  const float* Lh = a.lh + (size_t)b * a.l_bstride + (size_t)r0 * NB;
+  const float* Ll = a.ll + (size_t)b * a.l_bstride + (size_t)r0 * NB;
+  for (int idx = threadIdx.x; idx < NB * 3; idx += blockDim.x) {
+    const int rr = idx / 3, q = idx % 3;
+    double s = 0.0;
+    for (int l = 0; l <= rr; ++l) s += ((double)Lh[rr * NB + l] + (double)Ll[rr * NB + l]) * acc_s[l][q];
+    if (rr < nbk) a.out[(size_t)b * a.ystride + (size_t)(r0 + rr) * 3 + q] = s;
   }
-  z[(size_t)jc * 3 + 0] -= s0;
-  z[(size_t)jc * 3 + 1] -= s1;
-  z[(size_t)jc * 3 + 2] -= s2;
+  __threadfence();
+  __syncthreads();
+  if (threadIdx.x == 0) atomicExch(a.flags + b * a.nblk + blk, a.epoch);
+}
+
+// Backward: x_blk = Linv_blk^T (z_blk - sum_{k>blk} L_{k,blk}^T x_k).
+// Thread t owns column c = t/2 of the block (half-row split by t%2).
+__global__ void __launch_bounds__(256) bwd_syncfree_kernel(SolveArgs a) {
+  __shared__ int s_t;
+  __shared__ double xk[NB][3];
+  __shared__ double acc_s[NB][3];
+  __shared__ int s_ok;
+  if (threadIdx.x == 0) s_t = atomicAdd(a.ticket, 1);
+  __syncthreads();
+  const int batch = a.m.batch;
+  const int t = s_t;
+  const int blk = a.nblk - 1 - t / batch, b = t % batch;
+  const int n = a.m.n;
+  const int c0 = blk * NB;
+  const int nbk = min(NB, n - c0);
+  const float* A = a.m.A + (size_t)b * a.m.stride;
+  const int c = threadIdx.x % NB, half = threadIdx.x / NB;
+  double p0 = 0.0, p1 = 0.0, p2 = 0.0;
+  for (int k = a.nblk - 1; k > blk; --k) {
+    if (threadIdx.x == 0) s_ok = wait_flag(a.flags + b * a.nblk + k, a.epoch, a.err);
+    __syncthreads();
+    if (!s_ok) return;
+    for (int idx = threadIdx.x; idx < NB * 3; idx += blockDim.x)
+      xk[idx / 3][idx % 3] = __ldcg(a.out + (size_t)b * a.ystride + (size_t)k * NB * 3 + idx);
+    __syncthreads();
+    const int kr = min(NB, n - k * NB);
+    for (int rr = half; rr < kr; rr += 2) {
+      const double l = A[(size_t)(k * NB + rr) * a.m.ld + c0 + c];
+      p0 += l * xk[rr][0];
+      p1 += l * xk[rr][1];
+      p2 += l * xk[rr][2];
+    }
+    __syncthreads();
+  }
+  // combine the two row halves through shared memory
+  __shared__ double hsum[2][NB][3];
+  hsum[half][c][0] = p0;
+  hsum[half][c][1] = p1;
+  hsum[half][c][2] = p2;
+  __syncthreads();
+  for (int idx = threadIdx.x; idx < NB * 3; idx += blockDim.x) {
+    const int cc = idx / 3, q = idx % 3;
+    const double zin = (cc < nbk) ? a.in[(size_t)b * a.ystride + (size_t)(c0 + cc) * 3 + q] : 0.0;
+    acc_s[cc][q] = zin - hsum[0][cc][q] - hsum[1][cc][q];
+  }
+  __syncthreads();
+  const float* Lh = a.lh + (size_t)b * a.l_bstride + (size_t)c0 * NB;
+  const float* Ll = a.ll + (size_t)b * a.l_bstride + (size_t)c0 * NB;
+  for (int idx = threadIdx.x; idx < NB * 3; idx += blockDim.x) {
+    const int rr = idx / 3, q = idx % 3;
+    double s = 0.0;
+    for (int l = rr; l < NB; ++l) s += ((double)Lh[l * NB + rr] + (double)Ll[l * NB + rr]) * acc_s[l][q];
+    if (rr < nbk) a.out[(size_t)b * a.ystride + (size_t)(c0 + rr) * 3 + q] = s;
+  }
+  __threadfence();
+  __syncthreads();
+  if (threadIdx.x == 0) atomicExch(a.flags + b * a.nblk + blk, a.epoch);
 }
 
 // ---------------------------------------------------------------------------
@@ -280,19 +359,18 @@ void launch_potrf_diag_f32(const BatchMat32& m, int k0, float* linv_hi, float* l
   potrf_diag_f32_kernel<<<m.batch, 512, kPotrf32Smem, s>>>(m, k0, linv_hi, linv_lo, l_bstride, info);
 }
 
+size_t solve_sync_ints(int n, int batch) { return (size_t)batch * ((n + NB - 1) / NB) + 8; }
+
 void launch_solve_f32(const BatchMat32& m, const float* linv_hi, const float* linv_lo, size_t l_bstride, double* R,
-                      double* Z, double* D, size_t ystride, cudaStream_t s) {
+                      double* Z, double* D, size_t ystride, int* sync, int epoch, int* err, cudaStream_t s) {
   const int nblk = (m.n + NB - 1) / NB;
-  for (int k0 = 0; k0 < m.n; k0 += NB) {
-    const int nbk = std::min(NB, m.n - k0);
-    const int rows = m.n - k0 - nbk;
-    const int ctas = std::max(1, (rows + 63) / 64);
-    fwd_f32_kernel<<<dim3(ctas, m.batch), 256, 0, s>>>(m, k0, linv_hi, linv_lo, l_bstride, R, Z, ystride);
-  }
-  for (int k0 = (nblk - 1) * NB; k0 >= 0; k0 -= NB) {
-    const int ctas = std::max(1, (k0 + 255) / 256);
-    bwd_f32_kernel<<<dim3(ctas, m.batch), 256, 0, s>>>(m, k0, linv_hi, linv_lo, l_bstride, Z, D, ystride);
-  }
+  int* ticket = sync;                 // [0] forward ticket, [1] backward ticket
+  int* flags = sync + 8;              // [batch][nblk]
+  cudaMemsetAsync(ticket, 0, 2 * sizeof(int), s);
+  SolveArgs fa{m, linv_hi, linv_lo, l_bstride, R, Z, ystride, flags, ticket, 2 * epoch + 1, nblk, err};
+  fwd_syncfree_kernel<<<nblk * m.batch, 256, 0, s>>>(fa);
+  SolveArgs ba{m, linv_hi, linv_lo, l_bstride, Z, D, ystride, flags, ticket + 1, 2 * epoch + 2, nblk, err};
+  bwd_syncfree_kernel<<<nblk * m.batch, 256, 0, s>>>(ba);
 }
 
 size_t relay_residual_ws_doubles(int n, int batch) {

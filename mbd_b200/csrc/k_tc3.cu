@@ -11,12 +11,13 @@
 //
 // One CTA computes one 128x128 tile of C (batch index = blockIdx.y):
 //   warp 0, one lane : TMA producer (cp.async.bulk.tensor, 128B swizzle)
-//                      into a 4-stage shared-memory ring (A,B 16 KB each);
+//                      into a 3-stage shared-memory ring (A,B 16 KB each);
 //   warp 1, one lane : issues tcgen05.mma.kind::tf32 (128x128x8) into a
 //                      128-column TMEM accumulator, releases each stage with
 //                      tcgen05.commit -> mbarrier;
 //   all 4 warps      : epilogue, tcgen05.ld 32x32b (warp w owns TMEM lanes /
-//                      rows 32w..32w+31) and the global update of C.
+//                      rows 32w..32w+31) into a swizzled staging tile, then a
+//                      TMA reduce-add (C -= acc) or TMA stores (C = acc, hi, lo).
 // Every mbarrier wait is bounded: on time-out the kernel records
 // MBD_ERR_TIMEOUT, skips the remaining work and still frees its TMEM.
 #include <cuda.h>
@@ -32,7 +33,7 @@ namespace mbd {
 namespace {
 
 constexpr int BM = 128, BN = 128, BK = 32;   // BK fp32 = 128 bytes = one swizzle atom row
-constexpr int STAGES = 4;
+constexpr int STAGES = 3;                    // 97 KB: two CTAs per SM overlap epilogue and main loop
 constexpr int TILE_BYTES = BM * BK * 4;      // 16 KB
 constexpr int STAGE_BYTES = 2 * TILE_BYTES;
 constexpr int TMEM_COLS = 128;
@@ -76,6 +77,18 @@ __device__ __forceinline__ void tma_load_3d(uint32_t dst, const CUtensorMap* map
       "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%3, %4, %5}], [%2];"
       ::"r"(dst), "l"(reinterpret_cast<uint64_t>(map)), "r"(bar), "r"(c0), "r"(c1), "r"(c2)
       : "memory");
+}
+
+__device__ __forceinline__ void tma_store_3d(const CUtensorMap* map, uint32_t src, int c0, int c1, int c2) {
+  asm volatile("cp.async.bulk.tensor.3d.global.shared::cta.bulk_group [%0, {%2, %3, %4}], [%1];"
+               ::"l"(reinterpret_cast<uint64_t>(map)), "r"(src), "r"(c0), "r"(c1), "r"(c2)
+               : "memory");
+}
+
+__device__ __forceinline__ void tma_reduce_add_3d(const CUtensorMap* map, uint32_t src, int c0, int c1, int c2) {
+  asm volatile("cp.reduce.async.bulk.tensor.3d.global.shared::cta.add.bulk_group [%0, {%2, %3, %4}], [%1];"
+               ::"l"(reinterpret_cast<uint64_t>(map)), "r"(src), "r"(c0), "r"(c1), "r"(c2)
+               : "memory");
 }
 
 // Shared-memory matrix descriptor: K-major, 128-byte swizzle, 8-row groups
@@ -136,7 +149,7 @@ __device__ __forceinline__ void tri_index(int t, int* ti, int* tj) {
   *tj = t - i * (i + 1) / 2;
 }
 
-__global__ void __launch_bounds__(128, 1) tc3_gemm_kernel(const __grid_constant__ Tc3Maps maps, Tc3Params p) {
+__global__ void __launch_bounds__(128, 2) tc3_gemm_kernel(const __grid_constant__ Tc3Maps maps, Tc3Params p) {
   extern __shared__ __align__(1024) uint8_t smem_raw[];
   // 1024-byte alignment for the swizzled tiles
   uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
@@ -222,40 +235,66 @@ __global__ void __launch_bounds__(128, 1) tc3_gemm_kernel(const __grid_constant_
   }
   __syncwarp();
   // ---------------- epilogue ----------------
+  // TMEM -> registers -> 128-byte-swizzled staging tile in the (now idle)
+  // pipeline shared memory -> one TMA bulk operation per 128x32 chunk:
+  // reduce-add of -acc (SYRK) or plain stores of acc and its hi/lo split.
+  // The tensor bounds clip rows/columns outside the matrix.
   const bool ok = mbar_wait(smem_u32(&done_bar), 0, p.err);
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
   if (ok) {
-    const int row = tm * BM + warp * 32 + lane;     // row within the C region
-    const bool row_ok = row < p.m_rows;
-    float* crow = p.C + (size_t)b * p.c_bstride + (size_t)(p.c_row0 + row) * p.c_ld + p.c_col0;
+    const int rl = warp * 32 + lane;                // tile row == TMEM lane
+    const int row = tm * BM + rl;                   // row within the C region
+    const bool diag_tile = (p.mode == TC3_SYRK_LOWER) && (tm == tn);
+    uint8_t* stg0 = smem;                           // 16 KB each
+    uint8_t* stg1 = smem + TILE_BYTES;
+    uint8_t* stg2 = smem + 2 * TILE_BYTES;
 #pragma unroll 1
     for (int cc = 0; cc < BN / 32; ++cc) {
       uint32_t r[32];
       tmem_ld32(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(cc * 32), r);
-      if (!row_ok) continue;
       const int col0 = tn * BN + cc * 32;
-      if (p.mode == TC3_SYRK_LOWER) {
 #pragma unroll
-        for (int q = 0; q < 32; ++q) {
-          const int col = col0 + q;
-          if (col < p.n_cols && col <= row) crow[col] -= __uint_as_float(r[q]);
-        }
-      } else {
-        float* hi = p.out_hi + (size_t)b * p.o_bstride + (size_t)(p.c_row0 + row) * p.o_ld;
-        float* lo = p.out_lo + (size_t)b * p.o_bstride + (size_t)(p.c_row0 + row) * p.o_ld;
+      for (int j = 0; j < 8; ++j) {
+        float4 v, h, l;
+        float* pv = reinterpret_cast<float*>(&v);
+        float* ph = reinterpret_cast<float*>(&h);
+        float* pl = reinterpret_cast<float*>(&l);
 #pragma unroll
-        for (int q = 0; q < 32; ++q) {
-          const int col = col0 + q;
-          if (col < p.n_cols) {
-            const float x = __uint_as_float(r[q]);
-            const float h = tf32_hi(x);
-            crow[col] = x;
-            hi[col] = h;
-            lo[col] = x - h;
+        for (int u = 0; u < 4; ++u) {
+          const int col = col0 + 4 * j + u;
+          const float x = __uint_as_float(r[4 * j + u]);
+          if (p.mode == TC3_SYRK_LOWER) {
+            pv[u] = (diag_tile && col > row) ? 0.f : -x;
+          } else {
+            pv[u] = x;
+            ph[u] = tf32_hi(x);
+            pl[u] = x - ph[u];
           }
         }
+        const uint32_t off = (uint32_t)rl * 128u + ((uint32_t)(j ^ (rl & 7)) << 4);
+        *reinterpret_cast<float4*>(stg0 + off) = v;
+        if (p.mode != TC3_SYRK_LOWER) {
+          *reinterpret_cast<float4*>(stg1 + off) = h;
+          *reinterpret_cast<float4*>(stg2 + off) = l;
+        }
       }
+      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+      asm volatile("bar.sync 1, 128;" ::: "memory");
+      if (threadIdx.x == 0) {
+        const int gx = p.c_col0 + col0, gy = p.c_row0 + tm * BM;
+        if (p.mode == TC3_SYRK_LOWER) {
+          tma_reduce_add_3d(&maps.c, smem_u32(stg0), gx, gy, b);
+        } else {
+          tma_store_3d(&maps.c, smem_u32(stg0), gx, gy, b);
+          tma_store_3d(&maps.c_hi, smem_u32(stg1), col0, gy, b);
+          tma_store_3d(&maps.c_lo, smem_u32(stg2), col0, gy, b);
+        }
+        asm volatile("cp.async.bulk.commit_group;" ::: "memory");
+        asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory");
+      }
+      asm volatile("bar.sync 1, 128;" ::: "memory");
     }
+    if (threadIdx.x == 0) asm volatile("cp.async.bulk.wait_group 0;" ::: "memory");
   }
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
   __syncthreads();

@@ -3,13 +3,15 @@
 // 32 columns as LAPACK's DSYTRD/DLATRD.
 //
 // The whole reduction is ONE cooperative launch.  The CTAs of a group meet at
-// bounded global-memory barriers, two per column:
+// bounded global-memory barriers, two per column, and every phase issues all
+// of its global loads before it first needs one, so a column costs about two
+// dependent memory round trips plus two barriers:
 //   A  reflector of column c from the previous phase's norm partials;
-//      y = A22 v over the trailing lower triangle, one 64x64 tile per warp
-//      (8 rows of 16-byte loads in flight, no CTA-wide syncs); the partial
-//      sums land in Pb[I][J][0..63] so a row's total is a coalesced read;
-//      v^T A22 v and the panel dots W^T v, V^T v on the side.
-//   B  one thread per row: w = tau (y - V (W^T v) - W (V^T v)) + alpha2 v with
+//      y = A22 v over the trailing lower triangle: 64x64 tiles, four warps per
+//      tile (16 rows each, all 16 rows of 16-byte loads in flight), four tiles
+//      per CTA per round; partial sums land in Pb[I][J][0..63] so a row's total
+//      is a coalesced read; v^T A22 v and the panel dots W^T v, V^T v aside.
+//   B  8 threads per row: w = tau (y - V (W^T v) - W (V^T v)) + alpha2 v with
 //      alpha2 = -tau^2/2 (v^T A22 v - 2 (W^T v).(V^T v)), all from phase-A
 //      sums; store w and v; update column c+1 with the panel (at a panel end:
 //      A22 -= V W^T + W V^T); norm of the new column for the next reflector.
@@ -26,6 +28,7 @@ constexpr int T = kTrdTile;   // 64
 constexpr int P = kTrdNB;     // 32 panel width
 constexpr int THREADS = 512;
 constexpr int NWARP = THREADS / 32;
+constexpr int SLOTS = 4;      // tiles per CTA per round (4 warps each)
 constexpr long long kSpinCycles = 4000000000LL;   // ~2 s at 2 GHz, then give up
 
 struct GroupWS {
@@ -35,8 +38,8 @@ struct GroupWS {
   double* col0;    // [nmax] contiguous copy of the current column (double-buffered)
   double* col1;
   double* Pb;      // [nt][nt][T] y partials of tile (I,J) for row block I
-  double* dotp;    // [2P][G]
-  double* scal;    // [4][G]: [0] norm partial, [1] v^T A v partial
+  double* dotp;    // [2P+1][G] panel dots and v^T A v
+  double* scal;    // [G] norm partials
   int nmax;
 };
 
@@ -53,11 +56,11 @@ __host__ __device__ inline size_t ws_layout(int nmax, int G, GroupWS* w, char* b
   size_t o_bar = take(256);
   size_t o_W = take(sizeof(double) * (size_t)nmax * P);
   size_t o_V = take(sizeof(double) * (size_t)nmax * P);
-  size_t o_c0 = take(sizeof(double) * (size_t)nmax);
-  size_t o_c1 = take(sizeof(double) * (size_t)nmax);
+  size_t o_c0 = take(sizeof(double) * (size_t)(nmax + T));
+  size_t o_c1 = take(sizeof(double) * (size_t)(nmax + T));
   size_t o_Pb = take(sizeof(double) * (size_t)nt * nt * T);
-  size_t o_dp = take(sizeof(double) * (size_t)G * 2 * P);
-  size_t o_sc = take(sizeof(double) * (size_t)G * 4);
+  size_t o_dp = take(sizeof(double) * (size_t)G * (2 * P + 1));
+  size_t o_sc = take(sizeof(double) * (size_t)G);
   if (w) {
     w->bar = reinterpret_cast<unsigned*>(base + o_bar);
     w->W = reinterpret_cast<double*>(base + o_W);
@@ -80,39 +83,34 @@ __device__ __forceinline__ double warp_sum(double v) {
   return v;
 }
 
-// Sum of G consecutive doubles by one warp.
-__device__ __forceinline__ double warp_sum_g(const double* p, int G) {
-  double s = 0.0;
-  for (int q = threadIdx.x % 32; q < G; q += 32) s += ldg_cg(p + q);
-  return warp_sum(s);
-}
-
-// Bounded barrier among the G CTAs of one group.  Returns false (and sets
-// *err) when the wait runs out or another CTA already failed.
+// Bounded barrier among the G CTAs of one group (acquire-release atomics,
+// no separate fences).  Returns false (and sets *err) when the wait runs out
+// or another CTA already failed.
 __device__ bool group_sync(unsigned* bar, int G, unsigned& gen, int* err) {
   __shared__ int s_ok;
   __syncthreads();
+  if (G == 1) return true;
   if (threadIdx.x == 0) {
     int ok = 1;
     const unsigned target = gen + 1;
-    __threadfence();
-    const unsigned arrived = atomicAdd(&bar[0], 1u);
+    unsigned arrived;
+    asm volatile("atom.add.acq_rel.gpu.u32 %0, [%1], 1;" : "=r"(arrived) : "l"(bar) : "memory");
     if (arrived == (unsigned)G - 1) {
-      atomicExch(&bar[0], 0u);
-      __threadfence();
-      atomicExch(&bar[1], target);
+      asm volatile("st.relaxed.gpu.u32 [%0], 0;" ::"l"(bar) : "memory");
+      asm volatile("st.release.gpu.u32 [%0], %1;" ::"l"(bar + 1), "r"(target) : "memory");
     } else {
       const long long t0 = clock64();
-      while (*(volatile unsigned*)&bar[1] != target) {
+      while (true) {
+        unsigned cur;
+        asm volatile("ld.acquire.gpu.u32 %0, [%1];" : "=r"(cur) : "l"(bar + 1) : "memory");
+        if (cur == target) break;
         if (*(volatile int*)err != 0 || clock64() - t0 > kSpinCycles) {
           ok = 0;
           atomicCAS(err, 0, MBD_ERR_TIMEOUT);
           break;
         }
-        __nanosleep(20);
       }
     }
-    __threadfence();
     gen = target;
     s_ok = ok && (*(volatile int*)err == 0);
   }
@@ -132,23 +130,19 @@ struct Refl {
   double tau, scale, beta;
 };
 
-// Householder vector of column c: v(c1) = 1, v(r > c1) = col[r] * scale, 0 otherwise.
-struct VecV {
-  const double* col;
-  double scale;
-  int c1, n;
-  __device__ __forceinline__ double operator()(int r) const {
-    if (r == c1) return 1.0;
-    if (r > c1 && r < n) return ldg_cg(col + r) * scale;
-    return 0.0;
-  }
-};
+// v(r) of column c's reflector from the stored column value x = col[r].
+__device__ __forceinline__ double vfun(int r, double x, int c1, int n, double scale) {
+  if (r == c1) return 1.0;
+  if (r > c1 && r < n) return x * scale;
+  return 0.0;
+}
 
 struct Smem {
+  double red[SLOTS][4][T];   // column partials per warp quarter
+  double rows[SLOTS][T];     // row sums
   double t1[P], t2[P], wc[P + 1], vc[P + 1];
   double small[NWARP];
-  double vav_all;
-  double s_alpha2;
+  double vav_all, alpha2, wc1, yc1;
   Refl rf;
 };
 
@@ -163,80 +157,6 @@ __device__ double block_sum(double v, Smem& sm) {
   for (int q = 0; q < NWARP; ++q) s += sm.small[q];
   __syncthreads();
   return s;
-}
-
-// Phase A, SYMV part: every warp of the group takes 64x64 lower tiles of the
-// trailing matrix in turn.  Returns this warp's share of v^T A v.
-__device__ double symv_tiles_warp(const double* A, int ld, int n, int c1, const VecV& v, double* Pb,
-                                  int nt, int gw, int WG) {
-  const int lane = threadIdx.x % 32;
-  const int I0 = c1 / T;
-  const int mt = nt - I0;
-  const int ntile = mt * (mt + 1) / 2;
-  double vav = 0.0;
-  for (int t = gw; t < ntile; t += WG) {
-    int ti, tj;
-    tri_index(t, &ti, &tj);
-    const int I = I0 + ti, J = I0 + tj;
-    const bool diag = (I == J);
-    const int s0 = J * T + 2 * lane;
-    const double vj0 = v(s0), vj1 = v(s0 + 1);
-    const double vi_lo = v(I * T + lane), vi_hi = v(I * T + 32 + lane);
-    double row_lo = 0.0, row_hi = 0.0, cx = 0.0, cy = 0.0;
-#pragma unroll 1
-    for (int rb = 0; rb < T; rb += 16) {
-      double2 a[16];
-#pragma unroll
-      for (int u = 0; u < 16; ++u) {
-        const int row = I * T + rb + u;
-        a[u] = make_double2(0.0, 0.0);
-        if (row < n && s0 < n) {
-          const double2 q = __ldcg(reinterpret_cast<const double2*>(A + (size_t)row * ld + s0));
-          a[u].x = q.x;
-          a[u].y = (s0 + 1 < n) ? q.y : 0.0;
-        }
-      }
-#pragma unroll
-      for (int u = 0; u < 16; ++u) {
-        const int r = rb + u;
-        double ax = a[u].x, ay = a[u].y;
-        double bx = ax, by = ay;               // column-part values
-        if (diag) {                            // lower triangle of the diagonal tile only
-          const int sx = 2 * lane, sy = 2 * lane + 1;
-          if (sx > r) ax = 0.0;
-          if (sy > r) ay = 0.0;
-          if (sx >= r) bx = 0.0;
-          if (sy >= r) by = 0.0;
-        }
-        const double rp = warp_sum(ax * vj0 + ay * vj1);
-        if (lane == (r & 31)) {
-          if (r < 32) row_lo = rp; else row_hi = rp;
-        }
-        const double vir = __shfl_sync(0xffffffffu, r < 32 ? vi_lo : vi_hi, r & 31);
-        cx += bx * vir;
-        cy += by * vir;
-      }
-    }
-    double* pr = Pb + ((size_t)I * nt + J) * T;
-    if (!diag) {
-      pr[lane] = row_lo;
-      pr[32 + lane] = row_hi;
-      double* pc = Pb + ((size_t)J * nt + I) * T;
-      *reinterpret_cast<double2*>(pc + 2 * lane) = make_double2(cx, cy);
-      vav += vi_lo * row_lo + vi_hi * row_hi + vj0 * cx + vj1 * cy;
-    } else {
-      // column sum of row k lives in lane k/2, component k%2
-      const double ox = __shfl_sync(0xffffffffu, cx, lane / 2), oy = __shfl_sync(0xffffffffu, cy, lane / 2);
-      const double ox2 = __shfl_sync(0xffffffffu, cx, 16 + lane / 2);
-      const double oy2 = __shfl_sync(0xffffffffu, cy, 16 + lane / 2);
-      const double comb_lo = row_lo + ((lane & 1) ? oy : ox);
-      const double comb_hi = row_hi + ((lane & 1) ? oy2 : ox2);
-      pr[lane] = comb_lo;
-      pr[32 + lane] = comb_hi;
-      vav += vi_lo * comb_lo + vi_hi * comb_hi;
-    }
-  }
-  return warp_sum(vav);
 }
 
 // A22 -= V W^T + W V^T over rows/cols >= q0 (end of a panel); one 64x64 tile per CTA step.
@@ -285,6 +205,7 @@ __device__ void syr2k_tiles(double* A, int ld, int n, int q0, const GroupWS& w, 
       }
     }
   }
+  __syncthreads();
 }
 
 // Rows of [lo, n) owned by CTA g of G (contiguous chunks).
@@ -295,13 +216,82 @@ __device__ __forceinline__ void chunk_rows(int lo, int n, int g, int G, int* rs,
   *re = min(n, lo + (g + 1) * ch);
 }
 
+// Loaded data of one warp's 16-row strip of a tile.
+struct Strip {
+  double2 a[16];
+  double xj0, xj1, xr, xc;   // column values behind v at cols s0, s0+1, row (lane<16), col k (tid<256)
+  int I, J;
+  bool live;
+};
+
+__device__ __forceinline__ void load_strip(Strip& st, const double* A, int ld, int n, const double* col, int t,
+                                           int ntile, int I0, int quarter, int lane, int tid) {
+  st.live = t < ntile;
+  st.I = st.J = I0;
+  if (st.live) {
+    int ti, tj;
+    tri_index(t, &ti, &tj);
+    st.I = I0 + ti;
+    st.J = I0 + tj;
+  }
+  const int s0 = st.J * T + 2 * lane;
+#pragma unroll
+  for (int u = 0; u < 16; ++u) {
+    const int row = st.I * T + 16 * quarter + u;
+    st.a[u] = make_double2(0.0, 0.0);
+    if (st.live && row < n && s0 < n) {
+      const double2 q = __ldcg(reinterpret_cast<const double2*>(A + (size_t)row * ld + s0));
+      st.a[u].x = q.x;
+      st.a[u].y = (s0 + 1 < n) ? q.y : 0.0;
+    }
+  }
+  st.xj0 = (st.live && s0 < n) ? ldg_cg(col + s0) : 0.0;
+  st.xj1 = (st.live && s0 + 1 < n) ? ldg_cg(col + s0 + 1) : 0.0;
+  const int rr = st.I * T + 16 * quarter + (lane & 15);
+  st.xr = (st.live && rr < n) ? ldg_cg(col + rr) : 0.0;
+  (void)tid;
+}
+
+// Process one loaded strip: row sums (kept in sm.rows), column partials (sm.red);
+// returns this lane's share of v^T A v from the rows.
+__device__ __forceinline__ double strip_compute(const Strip& st, int slot, int quarter, int lane, int c1, int n,
+                                                double scale, Smem& sm) {
+  const bool diag = st.I == st.J;
+  const int s0 = st.J * T + 2 * lane;
+  const double vj0 = vfun(s0, st.xj0, c1, n, scale), vj1 = vfun(s0 + 1, st.xj1, c1, n, scale);
+  const double vr = vfun(st.I * T + 16 * quarter + (lane & 15), st.xr, c1, n, scale);
+  double rs = 0.0, cx = 0.0, cy = 0.0;
+#pragma unroll
+  for (int u = 0; u < 16; ++u) {
+    const int r = 16 * quarter + u;   // row within the tile
+    double ax = st.a[u].x, ay = st.a[u].y;
+    double bx = ax, by = ay;
+    if (diag) {
+      const int sx = 2 * lane, sy = 2 * lane + 1;
+      if (sx > r) ax = 0.0;
+      if (sy > r) ay = 0.0;
+      if (sx >= r) bx = 0.0;
+      if (sy >= r) by = 0.0;
+    }
+    const double rp = warp_sum(ax * vj0 + ay * vj1);
+    if (lane == u) rs = rp;
+    const double vu = __shfl_sync(0xffffffffu, vr, u);
+    cx += bx * vu;
+    cy += by * vu;
+  }
+  sm.red[slot][quarter][2 * lane] = st.live ? cx : 0.0;
+  sm.red[slot][quarter][2 * lane + 1] = st.live ? cy : 0.0;
+  if (lane < 16) sm.rows[slot][16 * quarter + lane] = st.live ? rs : 0.0;
+  return (st.live && lane < 16) ? vr * rs : 0.0;
+}
+
 __device__ bool tridiag_one(const TridiagJob& job, const GroupWS& w, int g, int G, unsigned& gen,
                             int* err, Smem& sm, double* dyn) {
   double* A = job.A;
   const int n = job.n, ld = job.ld;
   const int nt = (n + T - 1) / T;
   const int tid = threadIdx.x, lane = tid % 32, warp = tid / 32;
-  const int gw = g * NWARP + warp, WG = G * NWARP;
+  const int slot = warp / 4, quarter = warp % 4;
   const size_t nm = (size_t)w.nmax;
   if (n == 1) {
     if (g == 0 && tid == 0) job.d[0] = ldg_cg(A);
@@ -320,7 +310,7 @@ __device__ bool tridiag_one(const TridiagJob& job, const GroupWS& w, int g, int 
       if (r >= 2) s += x * x;
     }
     s = block_sum(s, sm);
-    if (tid == 0) w.scal[0 * G + g] = s;
+    if (tid == 0) w.scal[g] = s;
     if (g == 0 && tid == 0) job.d[0] = ldg_cg(A);
   }
   if (!group_sync(w.bar, G, gen, err)) return false;
@@ -329,124 +319,196 @@ __device__ bool tridiag_one(const TridiagJob& job, const GroupWS& w, int g, int 
     const int p = c - c % P, j = c - p;
     const int c1 = c + 1;
     const int I0 = c1 / T;
-    // ---------------- phase A: reflector, SYMV, v^T A v, panel dots ----------------
-    if (warp == 0) {
-      const double xn2 = warp_sum_g(w.scal + 0 * G, G);
-      if (lane == 0) {
-        const double alpha = ldg_cg(col_cur + c1);
-        Refl r;
-        if (xn2 == 0.0) {
-          r.tau = 0.0;
-          r.scale = 0.0;
-          r.beta = alpha;
-        } else {
-          const double beta = -copysign(sqrt(alpha * alpha + xn2), alpha);
-          r.tau = (beta - alpha) / beta;
-          r.scale = 1.0 / (alpha - beta);
-          r.beta = beta;
-        }
-        sm.rf = r;
-        if (g == 0) job.e[c] = r.beta;
-      }
-    }
-    __syncthreads();
-    const Refl rf = sm.rf;
-    const VecV v{col_cur, rf.scale, c1, n};
+    const int mt = nt - I0;
+    const int ntile = mt * (mt + 1) / 2;
     int rs, re;
     chunk_rows(c1, n, g, G, &rs, &re);
-    double vav = 0.0;
-    if (rf.tau != 0.0) {
-      vav = symv_tiles_warp(A, ld, n, c1, v, w.Pb, nt, gw, WG);
-      // W^T v (items 0..j-1) and V^T v (items P..P+j-1) over own rows, one warp per item
-      for (int it = warp; it < 2 * j; it += NWARP) {
-        const int k = it % j;
-        const double* M = (it < j ? w.W : w.V) + k * nm;
-        double s = 0.0;
-        for (int r = rs + lane; r < re; r += 32) s += ldg_cg(M + r) * v(r);
-        s = warp_sum(s);
-        if (lane == 0) w.dotp[(size_t)(it < j ? k : P + k) * G + g] = s;
-      }
+    // ================= phase A =================
+    // loads first: norm partials + alpha (warp 0), the first round of tiles,
+    // and the panel-dot operands of this CTA's rows
+    double nrm_part = 0.0, alpha = 0.0;
+    if (warp == 0) {
+      for (int q = lane; q < G; q += 32) nrm_part += ldg_cg(w.scal + q);
+      alpha = ldg_cg(col_cur + c1);
     }
-    if (lane == 0) sm.small[warp] = vav;
-    __syncthreads();
-    if (tid == 0) {
-      double s = 0.0;
-      for (int q = 0; q < NWARP; ++q) s += sm.small[q];
-      w.scal[1 * G + g] = s;
-    }
-    if (!group_sync(w.bar, G, gen, err)) return false;
-
-    // ---------------- phase B: w, column update, next norm ----------------
-    if (rf.tau != 0.0) {
-      for (int it = warp; it <= 2 * j; it += NWARP) {
-        if (it == 2 * j) {
-          const double s = warp_sum_g(w.scal + 1 * G, G);
-          if (lane == 0) sm.vav_all = s;
-        } else {
-          const int k = it % j;
-          const double s = warp_sum_g(w.dotp + (size_t)(it < j ? k : P + k) * G, G);
-          if (lane == 0) {
-            if (it < j) sm.t1[k] = s; else sm.t2[k] = s;
+    Strip st;
+    load_strip(st, A, ld, n, col_cur, SLOTS * g + slot, ntile, I0, quarter, lane, tid);
+    // panel dots: item it = warp (and warp+16, ...) over rows r = rs + lane (+32 ...)
+    double dx[2] = {0.0, 0.0}, dm[2][4] = {{0, 0, 0, 0}, {0, 0, 0, 0}};
+    {
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        const int r = rs + lane + 32 * h;
+        if (r < re) {
+          dx[h] = ldg_cg(col_cur + r);
+#pragma unroll
+          for (int q = 0; q < 4; ++q) {
+            const int it = warp + NWARP * q;
+            if (it < 2 * j) {
+              const int k = it % j;
+              dm[h][q] = ldg_cg((it < j ? w.W : w.V) + k * nm + r);
+            }
           }
         }
       }
     }
+    if (warp == 0) {
+      const double xn2 = warp_sum(nrm_part);
+      if (lane == 0) {
+        Refl rfl;
+        if (xn2 == 0.0) {
+          rfl.tau = 0.0;
+          rfl.scale = 0.0;
+          rfl.beta = alpha;
+        } else {
+          const double beta = -copysign(sqrt(alpha * alpha + xn2), alpha);
+          rfl.tau = (beta - alpha) / beta;
+          rfl.scale = 1.0 / (alpha - beta);
+          rfl.beta = beta;
+        }
+        sm.rf = rfl;
+        if (g == 0) job.e[c] = rfl.beta;
+      }
+    }
+    __syncthreads();
+    const Refl rf = sm.rf;
+    double vav = 0.0;
+    if (rf.tau != 0.0) {
+      // dots over this CTA's rows (more than 64 rows: remaining rows loaded here)
+      double acc[4] = {0, 0, 0, 0};
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        const int r = rs + lane + 32 * h;
+        const double vr = (r < re) ? vfun(r, dx[h], c1, n, rf.scale) : 0.0;
+#pragma unroll
+        for (int q = 0; q < 4; ++q) acc[q] += dm[h][q] * vr;
+      }
+      for (int r = rs + lane + 64; r < re; r += 32) {
+        const double vr = vfun(r, ldg_cg(col_cur + r), c1, n, rf.scale);
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+          const int it = warp + NWARP * q;
+          if (it < 2 * j) acc[q] += ldg_cg((it < j ? w.W : w.V) + (it % j) * nm + r) * vr;
+        }
+      }
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        const int it = warp + NWARP * q;
+        const double s = warp_sum(acc[q]);
+        if (it < 2 * j && lane == 0) w.dotp[(size_t)(it < j ? it : P + it - j) * G + g] = s;
+      }
+      // SYMV rounds: SLOTS tiles per CTA per round
+      for (int round = 0;; ++round) {
+        vav += strip_compute(st, slot, quarter, lane, c1, n, rf.scale, sm);
+        __syncthreads();
+        if (tid < SLOTS * T) {
+          const int sl = tid / T, k = tid % T;
+          const int t = round * SLOTS * G + SLOTS * g + sl;
+          if (t < ntile) {
+            int ti, tj;
+            tri_index(t, &ti, &tj);
+            const int I = I0 + ti, J = I0 + tj;
+            const double cs = sm.red[sl][0][k] + sm.red[sl][1][k] + sm.red[sl][2][k] + sm.red[sl][3][k];
+            const int sk = J * T + k;
+            const double vk = (sk < n) ? vfun(sk, ldg_cg(col_cur + sk), c1, n, rf.scale) : 0.0;
+            if (I != J) {
+              w.Pb[((size_t)I * nt + J) * T + k] = sm.rows[sl][k];
+              w.Pb[((size_t)J * nt + I) * T + k] = cs;
+            } else {
+              w.Pb[((size_t)I * nt + I) * T + k] = sm.rows[sl][k] + cs;
+            }
+            vav += vk * cs;
+          }
+        }
+        const int next = (round + 1) * SLOTS * G + SLOTS * g;
+        if (next >= ntile) break;   // uniform across the CTA
+        load_strip(st, A, ld, n, col_cur, next + slot, ntile, I0, quarter, lane, tid);
+        __syncthreads();
+      }
+    }
+    vav = block_sum(vav, sm);
+    if (tid == 0) w.dotp[(size_t)(2 * P) * G + g] = vav;
+    if (!group_sync(w.bar, G, gen, err)) return false;
+
+    // ================= phase B =================
+    const bool panel_end = (j + 1 == P);
+    constexpr int RPT = 8;
+    const int part = tid % RPT;
+    const int r = rs + tid / RPT;          // chunk <= 64 rows handled in one pass below
+    // loads: per-row y partials, panel rows, A[r][c1], x(r)
+    double y = 0.0, vk[4] = {0, 0, 0, 0}, wk[4] = {0, 0, 0, 0}, arc = 0.0, xr = 0.0;
+    const bool live = r < re;
+    if (live) {
+      if (rf.tau != 0.0) {
+        const double* pb = w.Pb + (size_t)(r / T) * nt * T + (r % T);
+        for (int J = I0 + part; J < nt; J += RPT) y += ldg_cg(pb + (size_t)J * T);
+      }
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        const int k = part + RPT * q;
+        if (k < j) {
+          vk[q] = ldg_cg(w.V + k * nm + r);
+          wk[q] = ldg_cg(w.W + k * nm + r);
+        }
+      }
+      if (!panel_end && part == 0) arc = ldg_cg(A + (size_t)r * ld + c1);
+      xr = ldg_cg(col_cur + r);
+    }
+    // cross-CTA sums: items 0..2j-1 (t1, t2) and 2P (v^T A v); row c1 for w(c1)
+    if (rf.tau != 0.0) {
+      for (int it = warp; it <= 2 * j; it += NWARP) {
+        const int src = (it == 2 * j) ? 2 * P : (it < j ? it : P + it - j);
+        double s = 0.0;
+        for (int q = lane; q < G; q += 32) s += ldg_cg(w.dotp + (size_t)src * G + q);
+        s = warp_sum(s);
+        if (lane == 0) {
+          if (it == 2 * j) sm.vav_all = s;
+          else if (it < j) sm.t1[it] = s;
+          else sm.t2[it - j] = s;
+        }
+      }
+    }
+    if (warp == NWARP - 1 && !panel_end) {
+      double yc = 0.0;
+      if (rf.tau != 0.0)
+        for (int J = I0 + lane; J < nt; J += 32) yc += ldg_cg(w.Pb + ((size_t)(c1 / T) * nt + J) * T + (c1 % T));
+      yc = warp_sum(yc);
+      if (lane < j) {
+        sm.wc[lane] = ldg_cg(w.W + lane * nm + c1);
+        sm.vc[lane] = ldg_cg(w.V + lane * nm + c1);
+      }
+      if (lane == 0) sm.yc1 = yc;
+    }
     __syncthreads();
     if (tid == 0) {
-      double alpha2 = 0.0;
+      double alpha2 = 0.0, wc1 = 0.0;
       if (rf.tau != 0.0) {
         double s12 = 0.0;
         for (int k = 0; k < j; ++k) s12 += sm.t1[k] * sm.t2[k];
         alpha2 = -0.5 * rf.tau * (rf.tau * (sm.vav_all - 2.0 * s12));
+        if (!panel_end) {
+          double corr = 0.0;
+          for (int k = 0; k < j; ++k) corr += sm.vc[k] * sm.t1[k] + sm.wc[k] * sm.t2[k];
+          wc1 = rf.tau * (sm.yc1 - corr) + alpha2;      // v(c1) = 1
+        }
       }
-      sm.s_alpha2 = alpha2;
+      sm.alpha2 = alpha2;
+      if (!panel_end) {
+        sm.wc[j] = wc1;
+        sm.vc[j] = 1.0;
+      }
     }
     __syncthreads();
-    const double alpha2 = sm.s_alpha2;
-    const bool panel_end = (j + 1 == P);
-    if (!panel_end) {
-      // w(c1), and W[c1][k], V[c1][k] for the update of column c1
-      if (warp == 0) {
-        double wc1 = 0.0;
-        if (rf.tau != 0.0) {
-          const int X = c1 / T;
-          double y = 0.0;
-          for (int J = I0 + lane; J < nt; J += 32) y += ldg_cg(w.Pb + ((size_t)X * nt + J) * T + (c1 % T));
-          if (lane < j) y -= ldg_cg(w.V + lane * nm + c1) * sm.t1[lane] + ldg_cg(w.W + lane * nm + c1) * sm.t2[lane];
-          y = warp_sum(y);
-          wc1 = rf.tau * y + alpha2;          // v(c1) = 1
-        }
-        if (lane < j) {
-          sm.wc[lane] = ldg_cg(w.W + lane * nm + c1);
-          sm.vc[lane] = ldg_cg(w.V + lane * nm + c1);
-        }
-        if (lane == 0) {
-          sm.wc[j] = wc1;
-          sm.vc[j] = 1.0;
-        }
-      }
-      __syncthreads();
-    }
+    const double alpha2 = sm.alpha2;
     double nrm = 0.0;
-    // 8 threads per row: part p sums J = I0+p, I0+p+8, ... and k = p, p+8, ...
-    // so every load of a row is independent of the others.
-    constexpr int RPT = 8;
-    const int part = tid % RPT;
-    for (int rbase = rs; rbase < re; rbase += THREADS / RPT) {
-      const int r = rbase + tid / RPT;
-      const bool live = r < re;
-      const double vr = live ? v(r) : 0.0;
-      double y = 0.0, corr = 0.0, upd = 0.0;
-      if (live) {
-        if (rf.tau != 0.0) {
-          const double* pb = w.Pb + (size_t)(r / T) * nt * T + (r % T);
-#pragma unroll 4
-          for (int J = I0 + part; J < nt; J += RPT) y += ldg_cg(pb + (size_t)J * T);
-        }
-        for (int k = part; k < j; k += RPT) {
-          const double vk = ldg_cg(w.V + k * nm + r), wk = ldg_cg(w.W + k * nm + r);
-          corr += vk * sm.t1[k] + wk * sm.t2[k];
-          upd += vk * sm.wc[k] + wk * sm.vc[k];
+    {
+      double corr = 0.0, upd = 0.0;
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        const int k = part + RPT * q;
+        if (k < j) {
+          corr += vk[q] * sm.t1[k] + wk[q] * sm.t2[k];
+          if (!panel_end) upd += vk[q] * sm.wc[k] + wk[q] * sm.vc[k];
         }
       }
 #pragma unroll
@@ -455,34 +517,68 @@ __device__ bool tridiag_one(const TridiagJob& job, const GroupWS& w, int g, int 
         corr += __shfl_xor_sync(0xffffffffu, corr, o);
         upd += __shfl_xor_sync(0xffffffffu, upd, o);
       }
-      if (!live || part != 0) continue;
-      const double wr = (rf.tau != 0.0) ? rf.tau * (y - corr) + alpha2 * vr : 0.0;
-      w.W[j * nm + r] = wr;
-      w.V[j * nm + r] = vr;
-      if (!panel_end) {
-        // A[r][c1] -= sum_{k<=j} V[r][k] W[c1][k] + W[r][k] V[c1][k]
-        const double s = upd + vr * sm.wc[j] + wr * sm.vc[j];
-        double* pa = A + (size_t)r * ld + c1;
-        const double x = ldg_cg(pa) - s;
-        *pa = x;
-        col_nxt[r] = x;
-        if (r == c1) job.d[c1] = x;
-        if (r >= c1 + 2) nrm += x * x;
+      if (live && part == 0) {
+        const double vr = vfun(r, xr, c1, n, rf.scale);
+        const double wr = (rf.tau != 0.0) ? rf.tau * (y - corr) + alpha2 * vr : 0.0;
+        w.W[j * nm + r] = wr;
+        w.V[j * nm + r] = vr;
+        if (!panel_end) {
+          const double x = arc - (upd + vr * sm.wc[j] + wr * sm.vc[j]);
+          A[(size_t)r * ld + c1] = x;
+          col_nxt[r] = x;
+          if (r == c1) job.d[c1] = x;
+          if (r >= c1 + 2) nrm += x * x;
+        }
+      }
+    }
+    // chunks of more than 64 rows (very large n): the same steps, loads in place
+    for (int r2 = rs + THREADS / RPT + tid / RPT; r2 - tid / RPT < re; r2 += THREADS / RPT) {
+      const bool lv = r2 < re;
+      double y2 = 0.0, corr = 0.0, upd = 0.0;
+      if (lv) {
+        if (rf.tau != 0.0) {
+          const double* pb = w.Pb + (size_t)(r2 / T) * nt * T + (r2 % T);
+          for (int J = I0 + part; J < nt; J += RPT) y2 += ldg_cg(pb + (size_t)J * T);
+        }
+        for (int k = part; k < j; k += RPT) {
+          const double a1 = ldg_cg(w.V + k * nm + r2), a2 = ldg_cg(w.W + k * nm + r2);
+          corr += a1 * sm.t1[k] + a2 * sm.t2[k];
+          if (!panel_end) upd += a1 * sm.wc[k] + a2 * sm.vc[k];
+        }
+      }
+#pragma unroll
+      for (int o = 1; o < RPT; o <<= 1) {
+        y2 += __shfl_xor_sync(0xffffffffu, y2, o);
+        corr += __shfl_xor_sync(0xffffffffu, corr, o);
+        upd += __shfl_xor_sync(0xffffffffu, upd, o);
+      }
+      if (lv && part == 0) {
+        const double vr = vfun(r2, ldg_cg(col_cur + r2), c1, n, rf.scale);
+        const double wr = (rf.tau != 0.0) ? rf.tau * (y2 - corr) + alpha2 * vr : 0.0;
+        w.W[j * nm + r2] = wr;
+        w.V[j * nm + r2] = vr;
+        if (!panel_end) {
+          const double x = ldg_cg(A + (size_t)r2 * ld + c1) - (upd + vr * sm.wc[j] + wr * sm.vc[j]);
+          A[(size_t)r2 * ld + c1] = x;
+          col_nxt[r2] = x;
+          if (r2 == c1) job.d[c1] = x;
+          if (r2 >= c1 + 2) nrm += x * x;
+        }
       }
     }
     if (panel_end) {
       if (!group_sync(w.bar, G, gen, err)) return false;
       syr2k_tiles(A, ld, n, c1, w, g, G, dyn);
       if (!group_sync(w.bar, G, gen, err)) return false;
-      for (int r = rs + tid; r < re; r += THREADS) {
-        const double x = ldg_cg(A + (size_t)r * ld + c1);
-        col_nxt[r] = x;
-        if (r == c1) job.d[c1] = x;
-        if (r >= c1 + 2) nrm += x * x;
+      for (int r2 = rs + tid; r2 < re; r2 += THREADS) {
+        const double x = ldg_cg(A + (size_t)r2 * ld + c1);
+        col_nxt[r2] = x;
+        if (r2 == c1) job.d[c1] = x;
+        if (r2 >= c1 + 2) nrm += x * x;
       }
     }
     nrm = block_sum(nrm, sm);
-    if (tid == 0) w.scal[0 * G + g] = nrm;
+    if (tid == 0) w.scal[g] = nrm;
     if (!group_sync(w.bar, G, gen, err)) return false;
     double* tmp = col_cur;
     col_cur = col_nxt;

@@ -15,6 +15,8 @@ enum { TC3_SYRK_LOWER = 0, TC3_STORE_SPLIT = 1 };
 // FP32 remainder (lo); all 3-D [batch][rows][K] FP32, 32x128 box, 128B swizzle.
 struct Tc3Maps {
   CUtensorMap a_hi, a_lo, b_hi, b_lo;
+  CUtensorMap c;              // output matrix (TMA reduce-add / store target)
+  CUtensorMap c_hi, c_lo;     // TC3_STORE_SPLIT: hi/lo copies of the output
 };
 
 struct Tc3Params {
@@ -52,10 +54,14 @@ struct BatchMat32 {
 // hi/lo split of L_kk^-1 at rows [k0, k0+128) of Linv_hi / Linv_lo ([b][n_pad][128]).
 void launch_potrf_diag_f32(const BatchMat32& m, int k0, float* linv_hi, float* linv_lo, size_t l_bstride,
                            int* info, cudaStream_t s);
-// Solve L L^T D = R with the FP32 factor (FP64 right-hand sides and accumulation).
-// W, Z are n x 3 FP64 work arrays per matrix; D receives the solution.
+// Solve L L^T D = R with the FP32 factor (FP64 right-hand sides and
+// accumulation) in two sync-free launches.  Z: n x 3 work array per matrix.
+// sync: solve_sync_ints(n, batch) ints, zeroed once at allocation; epoch must
+// grow by one per call on the same sync array.
+size_t solve_sync_ints(int n, int batch);
 void launch_solve_f32(const BatchMat32& m, const float* linv_hi, const float* linv_lo, size_t l_bstride,
-                      double* R, double* Z, double* D, size_t ystride, cudaStream_t s);
+                      double* R, double* Z, double* D, size_t ystride, int* sync, int epoch, int* err,
+                      cudaStream_t s);
 // R = B - A64 X for the lower-stored FP64 relay matrices (B = stacked identities),
 // and X += D first when D != null.  partial: workspace of relay_residual_ws_doubles().
 cudaError_t init_mixed_attributes();
