@@ -235,7 +235,7 @@ int upload_geometry(mbd_ctx* ctx, const mbd_geom& g, GeomDev* gd) {
 int tridiag_group_ctas(const mbd_ctx* ctx, int n) {
   const int nt = (n + kTrdTile - 1) / kTrdTile;
   const int tiles = nt * (nt + 1) / 2;
-  return std::max(1, std::min(ctx->num_sms * ctx->trd_ctas_per_sm, tiles));
+  return std::max(1, std::min(std::min(ctx->num_sms * ctx->trd_ctas_per_sm, tiles), kTridiagMaxGroup));
 }
 
 // Mixed relay solve: FP32 copy factorised with 3xTF32 tcgen05 GEMMs (128-wide

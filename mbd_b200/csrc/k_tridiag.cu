@@ -18,6 +18,8 @@
 // Cross-CTA sums are laid out [item][cta] and reduced by whole warps.
 #include <cuda_runtime.h>
 
+#include <cstdint>
+
 #include "kernels.h"
 #include "../../include/mbd_b200.h"
 
@@ -28,8 +30,10 @@ constexpr int T = kTrdTile;   // 64
 constexpr int P = kTrdNB;     // 32 panel width
 constexpr int THREADS = 512;
 constexpr int NWARP = THREADS / 32;
-constexpr int SLOTS = 4;      // tiles per CTA per round (4 warps each)
+constexpr int SLOTS = 2;      // tiles per CTA per round (8 warps x 8 rows each)
+constexpr int TILE_DBL = SLOTS * T * T;   // doubles of one staging buffer (64 KB)
 constexpr long long kSpinCycles = 4000000000LL;   // ~2 s at 2 GHz, then give up
+constexpr int kMaxG = kTridiagMaxGroup;   // largest group (CTAs) the cross-CTA reductions unroll for
 
 struct GroupWS {
   unsigned* bar;   // [0] arrivals, [1] generation
@@ -138,8 +142,9 @@ __device__ __forceinline__ double vfun(int r, double x, int c1, int n, double sc
 }
 
 struct Smem {
-  double red[SLOTS][4][T];   // column partials per warp quarter
+  double red[SLOTS][8][T];   // column partials per warp octet
   double rows[SLOTS][T];     // row sums
+  double item[64];           // cross-CTA sums: W^T v, V^T v, v^T A v
   double t1[P], t2[P], wc[P + 1], vc[P + 1];
   double small[NWARP];
   double vav_all, alpha2, wc1, yc1;
@@ -216,55 +221,77 @@ __device__ __forceinline__ void chunk_rows(int lo, int n, int g, int G, int* rs,
   *re = min(n, lo + (g + 1) * ch);
 }
 
-// Loaded data of one warp's 16-row strip of a tile.
+// One warp's 8-row strip of a 64x64 tile, staged in shared memory by
+// cp.async (16 bytes per lane per row, zero-filled outside the matrix), plus
+// the column values behind v that the compute step needs.
 struct Strip {
-  double2 a[16];
-  double xj0, xj1, xr, xc;   // column values behind v at cols s0, s0+1, row (lane<16), col k (tid<256)
+  double xj0, xj1, xr, xk;   // v's column values at cols s0, s0+1, row (lane<8), combine column (tid<128)
   int I, J;
   bool live;
 };
 
-__device__ __forceinline__ void load_strip(Strip& st, const double* A, int ld, int n, const double* col, int t,
-                                           int ntile, int I0, int quarter, int lane, int tid) {
-  st.live = t < ntile;
-  st.I = st.J = I0;
-  if (st.live) {
-    int ti, tj;
-    tri_index(t, &ti, &tj);
-    st.I = I0 + ti;
-    st.J = I0 + tj;
-  }
-  const int s0 = st.J * T + 2 * lane;
-#pragma unroll
-  for (int u = 0; u < 16; ++u) {
-    const int row = st.I * T + 16 * quarter + u;
-    st.a[u] = make_double2(0.0, 0.0);
-    if (st.live && row < n && s0 < n) {
-      const double2 q = __ldcg(reinterpret_cast<const double2*>(A + (size_t)row * ld + s0));
-      st.a[u].x = q.x;
-      st.a[u].y = (s0 + 1 < n) ? q.y : 0.0;
-    }
-  }
-  st.xj0 = (st.live && s0 < n) ? ldg_cg(col + s0) : 0.0;
-  st.xj1 = (st.live && s0 + 1 < n) ? ldg_cg(col + s0 + 1) : 0.0;
-  const int rr = st.I * T + 16 * quarter + (lane & 15);
-  st.xr = (st.live && rr < n) ? ldg_cg(col + rr) : 0.0;
-  (void)tid;
+__device__ __forceinline__ void cp_async16(double* dst, const double* src, int bytes) {
+  const uint32_t d = static_cast<uint32_t>(__cvta_generic_to_shared(dst));
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(d), "l"(src), "r"(bytes) : "memory");
 }
 
-// Process one loaded strip: row sums (kept in sm.rows), column partials (sm.red);
-// returns this lane's share of v^T A v from the rows.
-__device__ __forceinline__ double strip_compute(const Strip& st, int slot, int quarter, int lane, int c1, int n,
-                                                double scale, Smem& sm) {
+__device__ __forceinline__ void tile_of(int t, int ntile, int I0, int* I, int* J, bool* live) {
+  *live = t < ntile;
+  *I = *J = I0;
+  if (*live) {
+    int ti, tj;
+    tri_index(t, &ti, &tj);
+    *I = I0 + ti;
+    *J = I0 + tj;
+  }
+}
+
+// Issue the copies of round `round` into `buf` and load the column values.
+__device__ __forceinline__ void issue_round(Strip& st, const double* A, int ld, int n, const double* col, int round,
+                                            int g, int G, int ntile, int I0, double* buf, int warp, int lane,
+                                            int tid) {
+  const int sl = warp / 8, oct = warp % 8;
+  const int t = round * SLOTS * G + SLOTS * g + sl;
+  tile_of(t, ntile, I0, &st.I, &st.J, &st.live);
+  const int s0 = st.J * T + 2 * lane;
+  const int bytes = (!st.live || s0 >= n) ? 0 : (s0 + 1 < n ? 16 : 8);
+#pragma unroll
+  for (int u = 0; u < 8; ++u) {
+    const int rt = 8 * oct + u;               // row within the tile
+    const int row = st.I * T + rt;
+    const bool ok = bytes > 0 && row < n;
+    cp_async16(buf + ((size_t)sl * T + rt) * T + 2 * lane, ok ? A + (size_t)row * ld + s0 : A, ok ? bytes : 0);
+  }
+  asm volatile("cp.async.commit_group;" ::: "memory");
+  st.xj0 = (bytes > 0) ? ldg_cg(col + s0) : 0.0;
+  st.xj1 = (bytes == 16) ? ldg_cg(col + s0 + 1) : 0.0;
+  const int rr = st.I * T + 8 * oct + (lane & 7);
+  st.xr = (st.live && rr < n) ? ldg_cg(col + rr) : 0.0;
+  st.xk = 0.0;
+  if (tid < SLOTS * T) {
+    int I, J;
+    bool lv;
+    tile_of(round * SLOTS * G + SLOTS * g + tid / T, ntile, I0, &I, &J, &lv);
+    const int sk = J * T + tid % T;
+    st.xk = (lv && sk < n) ? ldg_cg(col + sk) : 0.0;
+  }
+}
+
+// Row sums (into sm.rows) and column partials (into sm.red) of this warp's
+// staged strip; returns this lane's share of v^T A v from the rows.
+__device__ __forceinline__ double strip_compute(const Strip& st, const double* buf, int warp, int lane, int c1,
+                                                int n, double scale, Smem& sm) {
+  const int sl = warp / 8, oct = warp % 8;
   const bool diag = st.I == st.J;
   const int s0 = st.J * T + 2 * lane;
   const double vj0 = vfun(s0, st.xj0, c1, n, scale), vj1 = vfun(s0 + 1, st.xj1, c1, n, scale);
-  const double vr = vfun(st.I * T + 16 * quarter + (lane & 15), st.xr, c1, n, scale);
+  const double vr = vfun(st.I * T + 8 * oct + (lane & 7), st.xr, c1, n, scale);
   double rs = 0.0, cx = 0.0, cy = 0.0;
 #pragma unroll
-  for (int u = 0; u < 16; ++u) {
-    const int r = 16 * quarter + u;   // row within the tile
-    double ax = st.a[u].x, ay = st.a[u].y;
+  for (int u = 0; u < 8; ++u) {
+    const int r = 8 * oct + u;   // row within the tile
+    const double2 a = *reinterpret_cast<const double2*>(buf + ((size_t)sl * T + r) * T + 2 * lane);
+    double ax = a.x, ay = a.y;
     double bx = ax, by = ay;
     if (diag) {
       const int sx = 2 * lane, sy = 2 * lane + 1;
@@ -279,10 +306,10 @@ __device__ __forceinline__ double strip_compute(const Strip& st, int slot, int q
     cx += bx * vu;
     cy += by * vu;
   }
-  sm.red[slot][quarter][2 * lane] = st.live ? cx : 0.0;
-  sm.red[slot][quarter][2 * lane + 1] = st.live ? cy : 0.0;
-  if (lane < 16) sm.rows[slot][16 * quarter + lane] = st.live ? rs : 0.0;
-  return (st.live && lane < 16) ? vr * rs : 0.0;
+  sm.red[sl][oct][2 * lane] = st.live ? cx : 0.0;
+  sm.red[sl][oct][2 * lane + 1] = st.live ? cy : 0.0;
+  if (lane < 8) sm.rows[sl][8 * oct + lane] = st.live ? rs : 0.0;
+  return (st.live && lane < 8) ? vr * rs : 0.0;
 }
 
 __device__ bool tridiag_one(const TridiagJob& job, const GroupWS& w, int g, int G, unsigned& gen,
@@ -291,7 +318,6 @@ __device__ bool tridiag_one(const TridiagJob& job, const GroupWS& w, int g, int 
   const int n = job.n, ld = job.ld;
   const int nt = (n + T - 1) / T;
   const int tid = threadIdx.x, lane = tid % 32, warp = tid / 32;
-  const int slot = warp / 4, quarter = warp % 4;
   const size_t nm = (size_t)w.nmax;
   if (n == 1) {
     if (g == 0 && tid == 0) job.d[0] = ldg_cg(A);
@@ -328,11 +354,15 @@ __device__ bool tridiag_one(const TridiagJob& job, const GroupWS& w, int g, int 
     // and the panel-dot operands of this CTA's rows
     double nrm_part = 0.0, alpha = 0.0;
     if (warp == 0) {
-      for (int q = lane; q < G; q += 32) nrm_part += ldg_cg(w.scal + q);
+      double v[kMaxG / 32];
+#pragma unroll
+      for (int u = 0; u < kMaxG / 32; ++u) v[u] = (lane + 32 * u < G) ? ldg_cg(w.scal + lane + 32 * u) : 0.0;
       alpha = ldg_cg(col_cur + c1);
+#pragma unroll
+      for (int u = 0; u < kMaxG / 32; ++u) nrm_part += v[u];
     }
     Strip st;
-    load_strip(st, A, ld, n, col_cur, SLOTS * g + slot, ntile, I0, quarter, lane, tid);
+    issue_round(st, A, ld, n, col_cur, 0, g, G, ntile, I0, dyn, warp, lane, tid);
     // panel dots: item it = warp (and warp+16, ...) over rows r = rs + lane (+32 ...)
     double dx[2] = {0.0, 0.0}, dm[2][4] = {{0, 0, 0, 0}, {0, 0, 0, 0}};
     {
@@ -397,20 +427,32 @@ __device__ bool tridiag_one(const TridiagJob& job, const GroupWS& w, int g, int 
         const double s = warp_sum(acc[q]);
         if (it < 2 * j && lane == 0) w.dotp[(size_t)(it < j ? it : P + it - j) * G + g] = s;
       }
-      // SYMV rounds: SLOTS tiles per CTA per round
+      // SYMV rounds: SLOTS tiles per CTA per round, the next round's copies
+      // in flight while the current one is reduced
       for (int round = 0;; ++round) {
-        vav += strip_compute(st, slot, quarter, lane, c1, n, rf.scale, sm);
+        const bool has_next = (round + 1) * SLOTS * G + SLOTS * g < ntile;   // uniform across the CTA
+        Strip nx;
+        if (has_next) {
+          issue_round(nx, A, ld, n, col_cur, round + 1, g, G, ntile, I0, dyn + ((round + 1) & 1) * TILE_DBL, warp,
+                      lane, tid);
+          asm volatile("cp.async.wait_group 1;" ::: "memory");
+        } else {
+          asm volatile("cp.async.wait_group 0;" ::: "memory");
+        }
+        __syncwarp();
+        vav += strip_compute(st, dyn + (round & 1) * TILE_DBL, warp, lane, c1, n, rf.scale, sm);
         __syncthreads();
         if (tid < SLOTS * T) {
           const int sl = tid / T, k = tid % T;
-          const int t = round * SLOTS * G + SLOTS * g + sl;
-          if (t < ntile) {
-            int ti, tj;
-            tri_index(t, &ti, &tj);
-            const int I = I0 + ti, J = I0 + tj;
-            const double cs = sm.red[sl][0][k] + sm.red[sl][1][k] + sm.red[sl][2][k] + sm.red[sl][3][k];
+          int I, J;
+          bool lv;
+          tile_of(round * SLOTS * G + SLOTS * g + sl, ntile, I0, &I, &J, &lv);
+          if (lv) {
+            double cs = 0.0;
+#pragma unroll
+            for (int o = 0; o < 8; ++o) cs += sm.red[sl][o][k];
             const int sk = J * T + k;
-            const double vk = (sk < n) ? vfun(sk, ldg_cg(col_cur + sk), c1, n, rf.scale) : 0.0;
+            const double vk = (sk < n) ? vfun(sk, st.xk, c1, n, rf.scale) : 0.0;
             if (I != J) {
               w.Pb[((size_t)I * nt + J) * T + k] = sm.rows[sl][k];
               w.Pb[((size_t)J * nt + I) * T + k] = cs;
@@ -420,12 +462,12 @@ __device__ bool tridiag_one(const TridiagJob& job, const GroupWS& w, int g, int 
             vav += vk * cs;
           }
         }
-        const int next = (round + 1) * SLOTS * G + SLOTS * g;
-        if (next >= ntile) break;   // uniform across the CTA
-        load_strip(st, A, ld, n, col_cur, next + slot, ntile, I0, quarter, lane, tid);
         __syncthreads();
+        if (!has_next) break;
+        st = nx;
       }
     }
+    asm volatile("cp.async.wait_group 0;" ::: "memory");
     vav = block_sum(vav, sm);
     if (tid == 0) w.dotp[(size_t)(2 * P) * G + g] = vav;
     if (!group_sync(w.bar, G, gen, err)) return false;
@@ -441,7 +483,15 @@ __device__ bool tridiag_one(const TridiagJob& job, const GroupWS& w, int g, int 
     if (live) {
       if (rf.tau != 0.0) {
         const double* pb = w.Pb + (size_t)(r / T) * nt * T + (r % T);
-        for (int J = I0 + part; J < nt; J += RPT) y += ldg_cg(pb + (size_t)J * T);
+        double v[12];   // independent loads for up to 96 tile columns; the rest in a loop
+#pragma unroll
+        for (int u = 0; u < 12; ++u) {
+          const int J = I0 + part + RPT * u;
+          v[u] = (J < nt) ? ldg_cg(pb + (size_t)J * T) : 0.0;
+        }
+        for (int J = I0 + part + RPT * 12; J < nt; J += RPT) y += ldg_cg(pb + (size_t)J * T);
+#pragma unroll
+        for (int u = 0; u < 12; ++u) y += v[u];
       }
 #pragma unroll
       for (int q = 0; q < 4; ++q) {
@@ -455,17 +505,29 @@ __device__ bool tridiag_one(const TridiagJob& job, const GroupWS& w, int g, int 
       xr = ldg_cg(col_cur + r);
     }
     // cross-CTA sums: items 0..2j-1 (t1, t2) and 2P (v^T A v); row c1 for w(c1)
+    // (8 threads per item, every load independent: one round trip)
     if (rf.tau != 0.0) {
-      for (int it = warp; it <= 2 * j; it += NWARP) {
+      const int it = tid / 8, ip = tid % 8;
+      double s = 0.0;
+      if (it <= 2 * j) {
         const int src = (it == 2 * j) ? 2 * P : (it < j ? it : P + it - j);
-        double s = 0.0;
-        for (int q = lane; q < G; q += 32) s += ldg_cg(w.dotp + (size_t)src * G + q);
-        s = warp_sum(s);
-        if (lane == 0) {
-          if (it == 2 * j) sm.vav_all = s;
-          else if (it < j) sm.t1[it] = s;
-          else sm.t2[it - j] = s;
+        const double* dp = w.dotp + (size_t)src * G;
+        double v[kMaxG / 8];
+#pragma unroll
+        for (int u = 0; u < kMaxG / 8; ++u) {
+          const int q = ip + 8 * u;
+          v[u] = (q < G) ? ldg_cg(dp + q) : 0.0;
         }
+#pragma unroll
+        for (int u = 0; u < kMaxG / 8; ++u) s += v[u];
+      }
+      s += __shfl_xor_sync(0xffffffffu, s, 1);
+      s += __shfl_xor_sync(0xffffffffu, s, 2);
+      s += __shfl_xor_sync(0xffffffffu, s, 4);
+      if (ip == 0 && it <= 2 * j) {
+        if (it == 2 * j) sm.vav_all = s;
+        else if (it < j) sm.t1[it] = s;
+        else sm.t2[it - j] = s;
       }
     }
     if (warp == NWARP - 1 && !panel_end) {
@@ -480,22 +542,23 @@ __device__ bool tridiag_one(const TridiagJob& job, const GroupWS& w, int g, int 
       if (lane == 0) sm.yc1 = yc;
     }
     __syncthreads();
-    if (tid == 0) {
+    if (warp == 0) {
       double alpha2 = 0.0, wc1 = 0.0;
       if (rf.tau != 0.0) {
-        double s12 = 0.0;
-        for (int k = 0; k < j; ++k) s12 += sm.t1[k] * sm.t2[k];
+        const double s12 = warp_sum(lane < j ? sm.t1[lane] * sm.t2[lane] : 0.0);
         alpha2 = -0.5 * rf.tau * (rf.tau * (sm.vav_all - 2.0 * s12));
         if (!panel_end) {
-          double corr = 0.0;
-          for (int k = 0; k < j; ++k) corr += sm.vc[k] * sm.t1[k] + sm.wc[k] * sm.t2[k];
+          const double corr =
+              warp_sum(lane < j ? sm.vc[lane] * sm.t1[lane] + sm.wc[lane] * sm.t2[lane] : 0.0);
           wc1 = rf.tau * (sm.yc1 - corr) + alpha2;      // v(c1) = 1
         }
       }
-      sm.alpha2 = alpha2;
-      if (!panel_end) {
-        sm.wc[j] = wc1;
-        sm.vc[j] = 1.0;
+      if (lane == 0) {
+        sm.alpha2 = alpha2;
+        if (!panel_end) {
+          sm.wc[j] = wc1;
+          sm.vc[j] = 1.0;
+        }
       }
     }
     __syncthreads();
@@ -607,7 +670,9 @@ __global__ void __launch_bounds__(THREADS, 1) tridiag_kernel(const TridiagJob* j
 
 size_t tridiag_workspace_bytes(int n, int group_ctas) { return ws_layout(n, group_ctas, nullptr, nullptr); }
 
-constexpr size_t kTridiagDynSmem = 4 * T * (P + 1) * sizeof(double);
+// two SYMV staging buffers (128 KB); the panel-end SYR2K reuses the same space
+constexpr size_t kTridiagDynSmem = 2 * TILE_DBL * sizeof(double);
+static_assert(kTridiagDynSmem >= 4 * T * (P + 1) * sizeof(double), "SYR2K tiles must fit the staging space");
 
 int tridiag_max_ctas_per_sm() {
   int nb = 0;

@@ -112,6 +112,7 @@ struct TridiagJob {
 };
 constexpr int kTrdTile = 64;
 constexpr int kTrdNB = 32;
+constexpr int kTridiagMaxGroup = 160;   // CTAs per group the kernel's reductions are sized for
 size_t tridiag_workspace_bytes(int n, int group_ctas);
 // Reduces each job's matrix to tridiagonal form with `groups` groups of
 // `group_ctas` co-resident CTAs (cooperative launch).  Returns a cudaError.
