@@ -115,6 +115,16 @@ int mbd_rsscs_upload(mbd_ctx* ctx, int n_geom, const mbd_geom* geoms);
 int mbd_rsscs_compute(mbd_ctx* ctx, int mode);
 int mbd_rsscs_download(mbd_ctx* ctx, mbd_result* out);
 
+/* All eigenvalues of a real symmetric n x n matrix in FP64, ascending: the
+ * CFDM eigenvalue step on its own (PDSYEV('N','L') at UTILS.f90:835), for
+ * callers that build their own Hamiltonian.  H is HOST memory holding the
+ * lower triangle in C row-major order, H(i,j) for j <= i at H[i*ld + j]
+ * (for a Fortran column-major array that is its upper triangle, UPLO='U');
+ * the rest of H is not read.  w (host) receives n eigenvalues.  Device
+ * buffers come from (and stay with) the context. */
+int mbd_rsscs_eigvalsh(mbd_ctx* ctx, const double* H, int n, int ld, double* w);
+
+
 /* Fortran-friendly helpers. */
 int mbd_rsscs_element_z(const char* symbol);   /* "C" -> 6; 0 if no vdW parameters (UTILS.f90:1336-1701) */
 const char* mbd_rsscs_strerror(int code);

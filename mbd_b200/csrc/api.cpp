@@ -73,6 +73,8 @@ struct mbd_ctx {
   // mixed mode: FP32 relay copy, hi/lo panel and diagonal-inverse buffers,
   // refinement vectors (X, R, Z, D) and residual workspace
   mbd::DevBuf relay32, p_hi, p_lo, l_hi, l_lo, mixv, res_ws, solve_sync;
+  // standalone eigenvalue call: matrix, (d, e, eigenvalues, scratch), workspace
+  mbd::DevBuf eig_a, eig_vec, eig_ws;
   int solve_epoch = 0;
   double* weights_dev = nullptr;
   int* err_flag = nullptr;
@@ -665,6 +667,34 @@ int mbd_rsscs_energy(mbd_ctx* ctx, const mbd_geom* geom, int mode, mbd_result* o
   int st = mbd_rsscs_energy_batch(ctx, 1, geom, mode, out);
   out->status = out->status ? out->status : st;
   return out->status;
+}
+
+int mbd_rsscs_eigvalsh(mbd_ctx* ctx, const double* H, int n, int ld, double* w) {
+  if (!ctx || !H || !w || n < 1 || ld < n) return MBD_ERR_ARG;
+  MBD_CUDA(cudaSetDevice(ctx->device));
+  cudaStream_t s = ctx->stream;
+  const int ldp = round_up(n, 32);
+  const int G = tridiag_group_ctas(ctx, n);
+  const size_t wsb = tridiag_workspace_bytes(n, G);
+  MBD_CUDA(ctx->eig_a.reserve(sizeof(double) * (size_t)n * ldp));
+  MBD_CUDA(ctx->eig_vec.reserve(sizeof(double) * 4 * (size_t)n));   // d, e, ev (2n)
+  MBD_CUDA(ctx->eig_ws.reserve(wsb));
+  double* A = ctx->eig_a.as<double>();
+  double* d = ctx->eig_vec.as<double>();
+  double* e = d + n;
+  double* ev = e + n;
+  MBD_CUDA(cudaMemcpy2DAsync(A, sizeof(double) * ldp, H, sizeof(double) * ld, sizeof(double) * n, n,
+                             cudaMemcpyHostToDevice, s));
+  TridiagJob job{A, n, ldp, d, e};
+  MBD_CUDA(cudaMemcpyAsync(ctx->job_dev, &job, sizeof(job), cudaMemcpyHostToDevice, s));
+  MBD_CUDA(cudaMemsetAsync(ctx->err_flag, 0, sizeof(int), s));
+  MBD_CUDA(launch_tridiag(ctx->job_dev, 1, 1, G, ctx->eig_ws.p, wsb, n, ctx->err_flag, s));
+  launch_tridiag_eigenvalues(d, e, n, ev, s);
+  MBD_CUDA(cudaMemcpyAsync(w, ev, sizeof(double) * n, cudaMemcpyDeviceToHost, s));
+  MBD_CUDA(cudaStreamSynchronize(s));
+  int err = 0;
+  MBD_CUDA(cudaMemcpy(&err, ctx->err_flag, sizeof(int), cudaMemcpyDeviceToHost));
+  return err ? err : MBD_OK;
 }
 
 int mbd_rsscs_element_z(const char* symbol) { return element_z(symbol); }

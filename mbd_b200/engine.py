@@ -34,7 +34,7 @@ EXPORTED = [
     "mbd_rsscs_create", "mbd_rsscs_destroy", "mbd_rsscs_energy", "mbd_rsscs_energy_batch",
     "mbd_rsscs_upload", "mbd_rsscs_compute", "mbd_rsscs_download", "mbd_rsscs_element_z",
     "mbd_rsscs_strerror", "mbd_rsscs_vdw_params", "mbd_rsscs_last_timings", "mbd_rsscs_last_stats",
-    "mbd_rsscs_stream",
+    "mbd_rsscs_stream", "mbd_rsscs_eigvalsh",
 ]
 
 
@@ -115,6 +115,9 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
     lib.mbd_rsscs_last_stats.restype = ctypes.c_int
     lib.mbd_rsscs_stream.argtypes = [vp]
     lib.mbd_rsscs_stream.restype = ctypes.c_void_p
+    lib.mbd_rsscs_eigvalsh.argtypes = [vp, ctypes.POINTER(ctypes.c_double), ctypes.c_int, ctypes.c_int,
+                                       ctypes.POINTER(ctypes.c_double)]
+    lib.mbd_rsscs_eigvalsh.restype = ctypes.c_int
     _LIB = lib
     return lib
 
@@ -247,6 +250,18 @@ class Engine:
         rarr = (CResult * len(self._packed))(*[p.result_struct() for p in self._packed])
         code = self.lib.mbd_rsscs_download(self.ctx, rarr)
         return code, [p.to_result(rarr[i]) for i, p in enumerate(self._packed)]
+
+    def eigvalsh(self, H: np.ndarray) -> np.ndarray:
+        """Eigenvalues (ascending) of a symmetric matrix; only its lower
+        triangle is read (mbd_rsscs_eigvalsh)."""
+        H = np.ascontiguousarray(H, dtype=np.float64)
+        n = H.shape[0]
+        w = np.zeros(n)
+        code = self.lib.mbd_rsscs_eigvalsh(self.ctx, H.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), n,
+                                           H.shape[1], w.ctypes.data_as(ctypes.POINTER(ctypes.c_double)))
+        if code != MBD_OK:
+            raise MbdError(code, strerror(code))
+        return w
 
     def stats(self) -> dict:
         buf = (ctypes.c_double * 3)()
