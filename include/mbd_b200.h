@@ -35,7 +35,8 @@ enum {
     MBD_ERR_OUT_OF_MEMORY = 8,
     MBD_ERR_REFINEMENT = 9,       /* mixed mode: refinement did not reach the residual gate
                                      (informational: the direct FP64 fallback then ran) */
-    MBD_ERR_NOT_BUILT = 10        /* requested mode is not available in this build */
+    MBD_ERR_NOT_BUILT = 10,       /* requested mode is not available in this build */
+    MBD_ERR_TOO_LARGE = 11        /* mbd_rsscs_eigvalsh_noalloc: n > MBD_NOALLOC_MAX_N */
 };
 
 /* ---- compute modes ------------------------------------------------------- */
@@ -124,6 +125,25 @@ int mbd_rsscs_download(mbd_ctx* ctx, mbd_result* out);
  * buffers come from (and stay with) the context. */
 int mbd_rsscs_eigvalsh(mbd_ctx* ctx, const double* H, int n, int ld, double* w);
 
+/* mbd_rsscs_eigvalsh for callers that must not allocate device memory.
+ * (No counterpart in the reference: pmbd.x lets ScaLAPACK allocate its work
+ * arrays.)  Meant for hosts that own the GPU's memory through their own pool
+ * or arena, or run this step where cudaMalloc's implicit synchronisation and
+ * latency are not acceptable.  It calls no cudaMalloc/cudaFree and needs no
+ * context: all scratch lives in one fixed 4 MiB device array inside the
+ * library, which every GPU that loads the library keeps until exit.
+ *   H      DEVICE pointer, 16-byte aligned, lower triangle in C row-major
+ *          order (H(i,j), j <= i, at H[i*ld + j]); ld even, ld >= n.
+ *          OVERWRITTEN by the reduction.
+ *   w      DEVICE pointer, n doubles: eigenvalues in ascending order.
+ *   stream cudaStream_t (NULL = legacy default stream); the call returns
+ *          after the work on it has finished.
+ * n must not exceed MBD_NOALLOC_MAX_N (else MBD_ERR_TOO_LARGE).  The first
+ * call on a device looks up the scratch address with cudaGetSymbolAddress;
+ * make that first call before any stream capture.  Calls share the scratch:
+ * calls that overlap on the GPU (other streams or threads, same device) race. */
+#define MBD_NOALLOC_MAX_N 2048
+int mbd_rsscs_eigvalsh_noalloc(double* H, int n, int ld, double* w, void* stream);
 
 /* Fortran-friendly helpers. */
 int mbd_rsscs_element_z(const char* symbol);   /* "C" -> 6; 0 if no vdW parameters (UTILS.f90:1336-1701) */

@@ -721,6 +721,7 @@ const char* mbd_rsscs_strerror(int code) {
     case MBD_ERR_OUT_OF_MEMORY: return "out of device memory";
     case MBD_ERR_REFINEMENT: return "mixed-precision refinement missed the residual gate; FP64 fallback used";
     case MBD_ERR_NOT_BUILT: return "mode not available in this build";
+    case MBD_ERR_TOO_LARGE: return "matrix larger than the fixed scratch of the allocation-free entry point";
     default: return "unknown error";
   }
 }

@@ -187,6 +187,18 @@ void launch_tridiag_eigenvalues(const double* d, const double* e, int n, double*
   bisect_kernel<<<blocks, 256, staged ? need : 0, s>>>(d, e, e2, n, staged, ev);
 }
 
+// Same as launch_tridiag_eigenvalues with the e^2 scratch given separately
+// (n doubles), so ev needs only n doubles.
+void launch_tridiag_eigenvalues_scratch(const double* d, const double* e, int n, double* ev, double* e2,
+                                        cudaStream_t s) {
+  const size_t need = sizeof(double) * 2 * (size_t)n;
+  const int staged = need <= kBisectMaxSmem;
+  if (!staged && n > 1) square_kernel<<<(n + 255) / 256, 256, 0, s>>>(e, e2, n - 1);
+  const long long threads = (long long)n * kLanesPerEig;
+  const int blocks = (int)((threads + 255) / 256);
+  bisect_kernel<<<blocks, 256, staged ? need : 0, s>>>(d, e, e2, n, staged, ev);
+}
+
 void launch_energy(const double* ev, int n, int nsl, const double* scalars, double* out, cudaStream_t s) {
   energy_kernel<<<1, 1024, 0, s>>>(ev, n, nsl, scalars, out);
 }

@@ -125,6 +125,8 @@ int tridiag_max_ctas_per_sm();
 // Eigenvalues of (d, e) by multisection; writes ev[0..n) ascending and uses
 // ev[n..2n) as scratch (ev must hold 2n doubles).
 void launch_tridiag_eigenvalues(const double* d, const double* e, int n, double* ev, cudaStream_t s);
+void launch_tridiag_eigenvalues_scratch(const double* d, const double* e, int n, double* ev, double* e2,
+                                        cudaStream_t s);
 cudaError_t init_eigval_attributes();
 // energy = 0.5*sum_{ev>=0} sqrt(ev)/nsl - 0.5*sum_nonint; out[0]=E, out[1]=sum sqrt, out[2]=nimag
 void launch_energy(const double* ev, int n, int nsl, const double* scalars, double* out,
