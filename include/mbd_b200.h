@@ -156,7 +156,10 @@ int mbd_rsscs_vdw_params(int z, double* alpha0, double* c6, double* r0);
 /* Device time in milliseconds of the last mbd_rsscs_compute, per stage:
  * [0] total, [1] atom/frequency setup, [2] relay tensor build, [3] relay
  * factorisation, [4] relay solve/refinement + epilogue, [5] CFDM build,
- * [6] tridiagonal reduction, [7] eigenvalues + energy.  n must be >= 8. */
+ * [6] tridiagonal reduction, [7] eigenvalues + energy.  Stages [1]-[5] run
+ * per geometry, several geometries at once on separate streams, and are
+ * summed over the geometries (their sum can exceed [0]); [6] and [7] are
+ * single batch-wide launches.  n must be >= 8. */
 int mbd_rsscs_last_timings(mbd_ctx* ctx, double* ms, int n);
 
 /* Counters of the last upload/compute/download: [0] kernel launches issued

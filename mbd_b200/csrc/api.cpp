@@ -2,12 +2,21 @@
 // download, and the orchestration of the kernels for one batch of
 // geometries.  Replaces MBD_at_rsSCS (UTILS.f90:153-349) and the BLACS /
 // MPI plumbing around it (UTILS.f90:97-149, 499-529) with one GPU.
+//
+// A batch runs in two parts.  The relay and CFDM stages of each geometry
+// (UTILS.f90:239-315 and 745-807) run on one of up to kMaxSlots relay slots,
+// each a CUDA stream with its own workspace, so the stages of different
+// geometries overlap on the GPU.  Every geometry keeps its own CFDM
+// Hamiltonian.  Then one cooperative launch reduces all Hamiltonians to
+// tridiagonal form with CTA groups planned on the host (plan_tridiag), and
+// one launch each computes all eigenvalues and all energies.
 #include <cuda_runtime.h>
 
 #include <algorithm>
 #include <cmath>
 #include <cstring>
 #include <memory>
+#include <numeric>
 #include <vector>
 
 #include "kernels.h"
@@ -20,6 +29,10 @@ namespace mbd {
 // ||B - A X||_F / ||B||_F that accepts its result.
 constexpr int kRefineIters = 4;
 constexpr double kResidualGate = 1e-10;
+// Relay slots (streams with private relay workspaces) of one context.
+constexpr int kMaxSlots = 8;
+// Share of free device memory the relay slots of one batch may plan for.
+constexpr double kSlotMemoryShare = 0.7;
 
 // Raw device allocation owned by the context (grow-only).
 struct DevBuf {
@@ -46,6 +59,7 @@ struct GeomDev {
   GeomPlan plan;
   DevBuf inputs;     // coords, alpha0, c6free, r0, hirsh, shifts, diff data
   DevBuf results;    // alpha_w, sgm, rvdw_iso, alpha_iw, molpol, c6_eff, alpha_eff, omega, rvdw_eff, scalars, energy, info, d, e, ev
+  DevBuf hmat;       // CFDM Hamiltonian (nH x ldH, lower blocks), reduced in place
   // offsets into inputs (doubles unless noted)
   const double *coords, *alpha0, *c6free, *r0, *hirsh, *scs_shifts, *cfdm_shifts, *diff_shift;
   const int *diff_is_zero, *place_offset, *place_rc, *place_cc;
@@ -54,11 +68,32 @@ struct GeomDev {
   double *scalars, *energy, *d, *e, *ev, *rnorm2;
   int* info;
   int status_host = MBD_OK;
+  int slot = 0;      // relay slot running this geometry's relay and CFDM stages
+};
+
+// One relay slot: a stream and the relay workspaces of the geometries it runs
+// (sized for the largest of them).
+struct RelaySlot {
+  cudaStream_t stream = nullptr;
+  cudaEvent_t done = nullptr;
+  DevBuf relay64, linv, rhs;                                  // plain FP64 path
+  DevBuf relay32, p_hi, p_lo, l_hi, l_lo, mixv, res_ws, solve_sync;   // mixed path
+  int solve_epoch = 0;
+  ~RelaySlot() {
+    if (done) cudaEventDestroy(done);
+    if (stream) cudaStreamDestroy(stream);
+  }
+  size_t held() const {
+    return relay64.bytes + linv.bytes + rhs.bytes + relay32.bytes + p_hi.bytes + p_lo.bytes + l_hi.bytes +
+           l_lo.bytes + mixv.bytes + res_ws.bytes + solve_sync.bytes;
+  }
 };
 
 struct Stage {
   enum { kTotal = 0, kSetup, kBuild, kFactor, kSolve, kCfdm, kTridiag, kEig, kCount };
 };
+// Events per geometry: start, then the ends of setup, build, factor, solve, CFDM.
+constexpr int kGeomEvents = 6;
 
 }  // namespace mbd
 
@@ -66,20 +101,26 @@ struct mbd_ctx {
   int device = 0;
   int num_sms = 0;
   int trd_ctas_per_sm = 1;
-  cudaStream_t stream = nullptr;
+  cudaStream_t stream = nullptr;             // batch stream: tridiagonal reduction, eigenvalues, energies
   std::vector<std::unique_ptr<mbd::GeomDev>> geoms;
-  // shared workspaces, sized for the largest geometry of the batch
-  mbd::DevBuf relay64, linv, rhs, tridiag_ws, hmat, misc;
-  // mixed mode: FP32 relay copy, hi/lo panel and diagonal-inverse buffers,
-  // refinement vectors (X, R, Z, D) and residual workspace
-  mbd::DevBuf relay32, p_hi, p_lo, l_hi, l_lo, mixv, res_ws, solve_sync;
+  std::vector<std::unique_ptr<mbd::RelaySlot>> slots;
+  int n_slots = 0;                           // slots in use for the current batch
+  mbd::DevBuf tridiag_ws, tables, misc, fb_ws;
   // standalone eigenvalue call: matrix, (d, e, eigenvalues, scratch), workspace
   mbd::DevBuf eig_a, eig_vec, eig_ws;
-  int solve_epoch = 0;
+  // batch plan (device tables in `tables`)
+  mbd::TridiagJob* trd_jobs = nullptr;
+  mbd::TridiagGroup* trd_groups = nullptr;
+  mbd::EigJob* eig_jobs = nullptr;
+  int n_trd_groups = 0, trd_total_ctas = 0, n_eig_jobs = 0, n_eig_batch = 0, eig_batch_max_n = 0;
+  double trd_est_ms = 0.0;
+  std::vector<int> order;                    // geometries that run, descending relay size
+  std::vector<int> eig_single;               // geometries whose eigenvalues need their own launch
   double* weights_dev = nullptr;
   int* err_flag = nullptr;
   mbd::TridiagJob* job_dev = nullptr;
-  std::vector<cudaEvent_t> events;
+  std::vector<cudaEvent_t> events;           // kGeomEvents per geometry
+  cudaEvent_t bev[4] = {nullptr, nullptr, nullptr, nullptr};   // start, relay done, tridiag done, end
   double last_ms[mbd::Stage::kCount] = {0};
   double launches = 0, h2d_bytes = 0, d2h_bytes = 0;
   int last_mode = 0;
@@ -240,19 +281,84 @@ int tridiag_group_ctas(const mbd_ctx* ctx, int n) {
   return std::max(1, std::min(std::min(ctx->num_sms * ctx->trd_ctas_per_sm, tiles), kTridiagMaxGroup));
 }
 
+// ---- plan of the grouped tridiagonal reduction ----------------------------
+// Time model of reducing one n x n matrix with a group of G CTAs, in
+// microseconds per column: a fixed part (reflector, cross-CTA sums, and two
+// group barriers when G > 1) plus the SYMV over the trailing triangle, whose
+// average size per column is n^2/6 elements, shared by min(G, tiles) CTAs.
+// Coefficients fitted to B200 runs of the kernel at n = 1500, 3000, 6000.
+double trd_col_us(int n, int G) {
+  const int nt = (n + kTrdTile - 1) / kTrdTile;
+  const int ge = std::max(1, std::min(G, nt * (nt + 1) / 2));
+  return (G == 1 ? 7.0 : 12.0) + 9.1e-5 * (double)n * (double)n / ge;
+}
+double trd_us(int n, int G) { return n < 2 ? 1.0 : (double)n * trd_col_us(n, G); }
+
+struct TrdPlan {
+  std::vector<std::vector<int>> bins;   // job indices per group, descending n
+  std::vector<int> G;
+  double makespan_us = 0.0;
+};
+
+// Partitions `ctas` co-resident CTAs into groups and the jobs (matrix sizes)
+// among them to minimise the modelled makespan: for B = min(jobs, ctas),
+// B/2, ..., 1 groups, longest-first assignment of the jobs at one CTA per
+// group, then the spare CTAs go one at a time to the slowest group while that
+// shortens it.  The best B wins.
+TrdPlan plan_tridiag(const std::vector<int>& sizes, int ctas) {
+  TrdPlan best;
+  const int J = (int)sizes.size();
+  if (J == 0 || ctas < 1) return best;
+  std::vector<int> idx(J);
+  std::iota(idx.begin(), idx.end(), 0);
+  std::stable_sort(idx.begin(), idx.end(), [&](int a, int b) { return sizes[a] > sizes[b]; });
+  best.makespan_us = 1e300;
+  for (int B = std::min(J, ctas); B >= 1; B = (B == 1) ? 0 : std::max(1, B / 2)) {
+    TrdPlan p;
+    p.bins.assign(B, {});
+    p.G.assign(B, 1);
+    std::vector<double> load(B, 0.0);
+    for (int j : idx) {
+      const int b = (int)(std::min_element(load.begin(), load.end()) - load.begin());
+      p.bins[b].push_back(j);
+      load[b] += trd_us(sizes[j], 1);
+    }
+    auto bin_time = [&](int b, int g) {
+      double t = 0.0;
+      for (int j : p.bins[b]) t += trd_us(sizes[j], g);
+      return t;
+    };
+    int spare = ctas - B;
+    while (spare > 0) {
+      const int b = (int)(std::max_element(load.begin(), load.end()) - load.begin());
+      if (p.G[b] >= kTridiagMaxGroup) break;
+      const double t2 = bin_time(b, p.G[b] + 1);
+      if (!(t2 < load[b])) break;
+      p.G[b] += 1;
+      load[b] = t2;
+      --spare;
+    }
+    p.makespan_us = *std::max_element(load.begin(), load.end());
+    if (p.makespan_us < best.makespan_us) best = p;
+  }
+  return best;
+}
+
+// ---- relay stages of one geometry (on its slot's stream) ------------------
+
 // Mixed relay solve: FP32 copy factorised with 3xTF32 tcgen05 GEMMs (128-wide
-// panels), FP64 iterative refinement against the FP64 matrices.  Returns the
-// device pointer of the refined solution X (n x 3 per frequency).
-int relay_mixed(mbd_ctx* ctx, GeomDev* gd, size_t mstride, cudaEvent_t* ev) {
+// panels), FP64 iterative refinement against the FP64 matrices.  Leaves the
+// refined solution X (n x 3 per frequency) at the start of slot.mixv.
+int relay_mixed(mbd_ctx* ctx, GeomDev* gd, RelaySlot& sl, size_t mstride, cudaEvent_t ev_factor) {
   const GeomPlan& p = gd->plan;
-  cudaStream_t s = ctx->stream;
+  cudaStream_t s = sl.stream;
   const int n = p.n;
   const int npad = round_up(n, kMixNB);
-  BatchMat32 m32{ctx->relay32.as<float>(), mstride, p.ld, n, kNFreq};
-  float* phi = ctx->p_hi.as<float>();
-  float* plo = ctx->p_lo.as<float>();
-  float* lhi = ctx->l_hi.as<float>();
-  float* llo = ctx->l_lo.as<float>();
+  BatchMat32 m32{sl.relay32.as<float>(), mstride, p.ld, n, kNFreq};
+  float* phi = sl.p_hi.as<float>();
+  float* plo = sl.p_lo.as<float>();
+  float* lhi = sl.l_hi.as<float>();
+  float* llo = sl.l_lo.as<float>();
   const size_t pb = (size_t)npad * kMixNB;   // elements per matrix of the panel / Linv buffers
   Tc3Maps trsm_maps, syrk_maps;
   // panel operands/outputs cover rows [0, n) (TMA zero-fills beyond), the
@@ -308,10 +414,10 @@ int relay_mixed(mbd_ctx* ctx, GeomDev* gd, size_t mstride, cudaEvent_t* ev) {
     launch_tc3_gemm(syrk_maps, sp, mt * (mt + 1) / 2, s);
     ctx->launches += 3;
   }
-  cudaEventRecord(ev[Stage::kFactor], s);
+  cudaEventRecord(ev_factor, s);
   // FP64 iterative refinement: X = 0, R = B; repeat D = (LL^T)^-1 R, X += D, R = B - A X
   const size_t ystride = (size_t)n * 3;
-  double* X = ctx->mixv.as<double>();
+  double* X = sl.mixv.as<double>();
   double* R = X + kNFreq * ystride;
   double* Z = R + kNFreq * ystride;
   double* D = Z + kNFreq * ystride;
@@ -320,21 +426,24 @@ int relay_mixed(mbd_ctx* ctx, GeomDev* gd, size_t mstride, cudaEvent_t* ev) {
   ctx->launches += 1;
   const int nblk = (n + kMixNB - 1) / kMixNB;
   for (int it = 0; it < kRefineIters; ++it) {
-    launch_solve_f32(m32, lhi, llo, pb, R, Z, D, ystride, ctx->solve_sync.as<int>(), ++ctx->solve_epoch,
+    launch_solve_f32(m32, lhi, llo, pb, R, Z, D, ystride, sl.solve_sync.as<int>(), ++sl.solve_epoch,
                      ctx->err_flag, s);
-    launch_relay_residual(ctx->relay64.as<double>(), mstride, p.ld, n, kNFreq, X, D, R, ystride,
-                          ctx->res_ws.as<double>(), gd->rnorm2, s);
+    launch_relay_residual(sl.relay64.as<double>(), mstride, p.ld, n, kNFreq, X, D, R, ystride,
+                          sl.res_ws.as<double>(), gd->rnorm2, s);
     ctx->launches += 2 * nblk + 4;
   }
   return MBD_OK;
 }
 
-// The pipeline for one geometry; `mode` selects the relay solve.
-int run_geometry(mbd_ctx* ctx, GeomDev* gd, int gi, int mode) {
+// Relay and CFDM stages of geometry gi on its slot's stream: per-atom
+// frequency table, relay tensors, relay factorisation and solve (plain or
+// mixed), screened polarizabilities and C6, CFDM Hamiltonian into gd->hmat.
+int run_front(mbd_ctx* ctx, GeomDev* gd, int gi, int mode) {
   const GeomPlan& p = gd->plan;
-  cudaStream_t s = ctx->stream;
+  RelaySlot& sl = *ctx->slots[gd->slot];
+  cudaStream_t s = sl.stream;
   const int N = p.N, n = p.n;
-  cudaEvent_t* ev = ctx->events.data() + (size_t)gi * Stage::kCount;
+  cudaEvent_t* ev = ctx->events.data() + (size_t)gi * kGeomEvents;
   auto mark = [&](int k) { cudaEventRecord(ev[k], s); };
   const bool mixed = mode != MBD_MODE_PLAIN_FP64;
   mark(0);
@@ -347,23 +456,23 @@ int run_geometry(mbd_ctx* ctx, GeomDev* gd, int gi, int mode) {
   // 2. relay matrices (21, FP64; plus an FP32 copy in mixed mode)
   const size_t mstride = (size_t)n * p.ld;
   RelayBuildArgs rb{N, p.ld, mstride, gd->coords, gd->alpha_w, gd->sgm, gd->rvdw_iso, gd->scs_shifts,
-                    (int)p.scs_shifts.size() / 3, p.beta, p.scs_eval_cut, ctx->relay64.as<double>(),
-                    mixed ? ctx->relay32.as<float>() : nullptr};
+                    (int)p.scs_shifts.size() / 3, p.beta, p.scs_eval_cut, sl.relay64.as<double>(),
+                    mixed ? sl.relay32.as<float>() : nullptr};
   launch_relay_build(rb, s);
   ctx->launches += 1;
   mark(2);
   const size_t ystride = (size_t)n * 3;
   double* Xv = nullptr;
   if (mixed) {
-    int st = relay_mixed(ctx, gd, mstride, ev);
+    int st = relay_mixed(ctx, gd, sl, mstride, ev[3]);
     if (st != MBD_OK) return st;
-    Xv = ctx->mixv.as<double>();
+    Xv = sl.mixv.as<double>();
   } else {
     // 3. blocked Cholesky, batched over the 21 frequencies
-    BatchMat bm{ctx->relay64.as<double>(), mstride, p.ld, n, kNFreq};
+    BatchMat bm{sl.relay64.as<double>(), mstride, p.ld, n, kNFreq};
     const int nblk = (n + kCholNB - 1) / kCholNB;
     const size_t lstride = (size_t)nblk * kCholNB * kCholNB;
-    double* Linv = ctx->linv.as<double>();
+    double* Linv = sl.linv.as<double>();
     for (int k0 = 0; k0 < n; k0 += kCholNB) {
       launch_potrf_diag_f64(bm, k0, Linv, lstride, gd->info, s);
       launch_trsm_panel_f64(bm, k0, Linv, lstride, s);
@@ -372,7 +481,7 @@ int run_geometry(mbd_ctx* ctx, GeomDev* gd, int gi, int mode) {
     }
     mark(3);
     // 4. solve X = A^-1 [I;..;I]
-    double* Wv = ctx->rhs.as<double>();
+    double* Wv = sl.rhs.as<double>();
     double* Zv = Wv + kNFreq * ystride;
     Xv = Zv + kNFreq * ystride;
     launch_init_rhs(Wv, ystride, n, kNFreq, s);
@@ -391,74 +500,215 @@ int run_geometry(mbd_ctx* ctx, GeomDev* gd, int gi, int mode) {
   CfdmBuildArgs cb{N, p.nsl, p.ldH, gd->coords, gd->omega, gd->alpha_eff, gd->rvdw_eff, gd->cfdm_shifts,
                    (int)p.cfdm_shifts.size() / 3, gd->diff_shift, gd->diff_is_zero, gd->place_offset,
                    gd->place_rc, gd->place_cc, (int)p.diff_is_zero.size(), p.beta, p.cfdm_cut,
-                   ctx->hmat.as<double>()};
+                   gd->hmat.as<double>()};
   launch_cfdm_build(cb, s);
   ctx->launches += 1;
   mark(5);
-  // 6. tridiagonal reduction (one cooperative launch)
-  TridiagJob job{ctx->hmat.as<double>(), p.nH, p.ldH, gd->d, gd->e};
-  MBD_CUDA(cudaMemcpyAsync(ctx->job_dev, &job, sizeof(job), cudaMemcpyHostToDevice, s));
-  const int G = tridiag_group_ctas(ctx, p.nH);
-  const size_t wsb = tridiag_workspace_bytes(p.nH, G);
-  MBD_CUDA(launch_tridiag(ctx->job_dev, 1, 1, G, ctx->tridiag_ws.p, wsb, p.nH, ctx->err_flag, s));
-  ctx->launches += 1;
-  mark(6);
-  // 7. eigenvalues, energy
-  launch_tridiag_eigenvalues(gd->d, gd->e, p.nH, gd->ev, s);
-  launch_energy(gd->ev, p.nH, p.nsl, gd->scalars, gd->energy, s);
-  ctx->launches += 2;
-  mark(7);
   return cuda_status(cudaGetLastError());
 }
 
-int reserve_shared(mbd_ctx* ctx) {
-  size_t relay = 0, linv = 0, rhs = 0, tws = 0, hm = 0;
-  for (auto& gp : ctx->geoms) {
-    const GeomPlan& p = gp->plan;
-    relay = std::max(relay, sizeof(double) * (size_t)kNFreq * p.n * p.ld);
-    const int nblk = (p.n + kCholNB - 1) / kCholNB;
-    linv = std::max(linv, sizeof(double) * (size_t)kNFreq * nblk * kCholNB * kCholNB);
-    rhs = std::max(rhs, sizeof(double) * 3 * (size_t)kNFreq * p.n * 3);
-    hm = std::max(hm, sizeof(double) * (size_t)p.nH * p.ldH);
-    tws = std::max(tws, tridiag_workspace_bytes(p.nH, tridiag_group_ctas(ctx, p.nH)));
+// Eigen stages of one geometry on stream s with its own tridiagonal launch
+// (the residual-gate fallback of download).
+int run_tail_single(mbd_ctx* ctx, GeomDev* gd, cudaStream_t s) {
+  const GeomPlan& p = gd->plan;
+  TridiagJob job{gd->hmat.as<double>(), p.nH, p.ldH, gd->d, gd->e};
+  MBD_CUDA(cudaMemcpyAsync(ctx->job_dev, &job, sizeof(job), cudaMemcpyHostToDevice, s));
+  const int G = tridiag_group_ctas(ctx, p.nH);
+  const size_t wsb = tridiag_workspace_bytes(p.nH, G);
+  MBD_CUDA(ctx->fb_ws.reserve(wsb));
+  MBD_CUDA(launch_tridiag(ctx->job_dev, 1, 1, G, ctx->fb_ws.p, wsb, p.nH, ctx->err_flag, s));
+  launch_tridiag_eigenvalues(gd->d, gd->e, p.nH, gd->ev, s);
+  launch_energy(gd->ev, p.nH, p.nsl, gd->scalars, gd->energy, s);
+  ctx->launches += 3;
+  return cuda_status(cudaGetLastError());
+}
+
+// ---- workspaces and the batch plan ----------------------------------------
+
+size_t plain_bytes(const GeomPlan& p, size_t* relay, size_t* linv, size_t* rhs) {
+  const int nblk = (p.n + kCholNB - 1) / kCholNB;
+  *relay = sizeof(double) * (size_t)kNFreq * p.n * p.ld;
+  *linv = sizeof(double) * (size_t)kNFreq * nblk * kCholNB * kCholNB;
+  *rhs = sizeof(double) * 3 * (size_t)kNFreq * p.n * 3;
+  return *relay + *linv + *rhs;
+}
+
+size_t mixed_bytes(const GeomPlan& p, size_t* r32, size_t* pan, size_t* vec, size_t* res, size_t* sync) {
+  *r32 = sizeof(float) * (size_t)kNFreq * p.n * p.ld;
+  *pan = sizeof(float) * (size_t)kNFreq * round_up(p.n, kMixNB) * kMixNB;
+  *vec = sizeof(double) * 4 * (size_t)kNFreq * p.n * 3;
+  *res = sizeof(double) * relay_residual_ws_doubles(p.n, kNFreq);
+  *sync = sizeof(int) * solve_sync_ints(p.n, kNFreq);
+  return *r32 + 4 * *pan + *vec + *res + *sync;
+}
+
+// Assigns the geometries to relay slots (longest first onto the least loaded
+// slot, load = (3N)^3), with as many slots as fit in the device memory share.
+int plan_slots(mbd_ctx* ctx) {
+  const int ng = (int)ctx->order.size();
+  size_t free_b = 0, total_b = 0;
+  MBD_CUDA(cudaMemGetInfo(&free_b, &total_b));
+  size_t held = 0;
+  for (auto& s : ctx->slots) held += s->held();
+  const double budget = kSlotMemoryShare * (double)(free_b + held);
+  int S = std::max(1, std::min(kMaxSlots, ng));
+  std::vector<int> slot_of(ctx->geoms.size(), 0);
+  for (; S >= 1; --S) {
+    std::vector<double> load(S, 0.0);
+    std::vector<size_t> need(S, 0);
+    for (int g : ctx->order) {
+      const GeomPlan& p = ctx->geoms[g]->plan;
+      const int s = (int)(std::min_element(load.begin(), load.end()) - load.begin());
+      slot_of[g] = s;
+      load[s] += std::pow((double)p.n, 3.0);
+      size_t a, b, c, d, e, f, h;
+      need[s] = std::max(need[s], plain_bytes(p, &a, &b, &c) + mixed_bytes(p, &d, &e, &f, &h, &a));
+    }
+    double total = 0.0;
+    for (size_t x : need) total += (double)x;
+    if (total <= budget || S == 1) break;
   }
-  MBD_CUDA(ctx->relay64.reserve(relay));
-  MBD_CUDA(ctx->linv.reserve(linv));
-  MBD_CUDA(ctx->rhs.reserve(rhs));
-  MBD_CUDA(ctx->hmat.reserve(hm));
-  MBD_CUDA(ctx->tridiag_ws.reserve(tws));
-  const size_t nev = ctx->geoms.size() * Stage::kCount;
+  for (int g : ctx->order) ctx->geoms[g]->slot = slot_of[g];
+  while ((int)ctx->slots.size() < S) {
+    std::unique_ptr<RelaySlot> sl(new RelaySlot());
+    MBD_CUDA(cudaStreamCreateWithFlags(&sl->stream, cudaStreamNonBlocking));
+    MBD_CUDA(cudaEventCreateWithFlags(&sl->done, cudaEventDisableTiming));
+    ctx->slots.push_back(std::move(sl));
+  }
+  ctx->n_slots = S;
+  return MBD_OK;
+}
+
+// Plain-path slot buffers, per-geometry Hamiltonians, the tridiagonal plan and
+// the device job tables of the uploaded batch.
+int prepare_batch(mbd_ctx* ctx) {
+  ctx->order.clear();
+  for (size_t g = 0; g < ctx->geoms.size(); ++g)
+    if (ctx->geoms[g]->status_host == MBD_OK) ctx->order.push_back((int)g);
+  std::stable_sort(ctx->order.begin(), ctx->order.end(),
+                   [&](int a, int b) { return ctx->geoms[a]->plan.n > ctx->geoms[b]->plan.n; });
+  for (int g : ctx->order) {
+    const GeomPlan& p = ctx->geoms[g]->plan;
+    MBD_CUDA(ctx->geoms[g]->hmat.reserve(sizeof(double) * (size_t)p.nH * p.ldH));
+  }
+  const size_t nev = ctx->geoms.size() * kGeomEvents;
   while (ctx->events.size() < nev) {
     cudaEvent_t e;
     MBD_CUDA(cudaEventCreate(&e));
     ctx->events.push_back(e);
   }
+  if (ctx->order.empty()) {
+    ctx->n_slots = 0;
+    ctx->n_trd_groups = ctx->trd_total_ctas = ctx->n_eig_jobs = ctx->n_eig_batch = 0;
+    return MBD_OK;
+  }
+  int st = plan_slots(ctx);
+  if (st != MBD_OK) return st;
+  for (int s = 0; s < ctx->n_slots; ++s) {
+    size_t relay = 0, linv = 0, rhs = 0;
+    for (int g : ctx->order) {
+      if (ctx->geoms[g]->slot != s) continue;
+      size_t a, b, c;
+      plain_bytes(ctx->geoms[g]->plan, &a, &b, &c);
+      relay = std::max(relay, a);
+      linv = std::max(linv, b);
+      rhs = std::max(rhs, c);
+    }
+    RelaySlot& sl = *ctx->slots[s];
+    MBD_CUDA(sl.relay64.reserve(relay));
+    MBD_CUDA(sl.linv.reserve(linv));
+    MBD_CUDA(sl.rhs.reserve(rhs));
+  }
+  // tridiagonal plan
+  std::vector<int> sizes;
+  for (int g : ctx->order) sizes.push_back(ctx->geoms[g]->plan.nH);
+  const TrdPlan tp = plan_tridiag(sizes, ctx->num_sms * ctx->trd_ctas_per_sm);
+  std::vector<TridiagJob> jobs;
+  std::vector<TridiagGroup> groups;
+  size_t ws_off = 0;
+  int cta = 0;
+  for (size_t b = 0; b < tp.bins.size(); ++b) {
+    TridiagGroup gr{};
+    gr.first_cta = cta;
+    gr.G = tp.G[b];
+    gr.job_begin = (int)jobs.size();
+    gr.nmax = 1;
+    for (int j : tp.bins[b]) {
+      GeomDev* gd = ctx->geoms[ctx->order[j]].get();
+      const GeomPlan& p = gd->plan;
+      jobs.push_back(TridiagJob{gd->hmat.as<double>(), p.nH, p.ldH, gd->d, gd->e});
+      gr.nmax = std::max(gr.nmax, p.nH);
+    }
+    gr.job_end = (int)jobs.size();
+    gr.ws_offset = ws_off;
+    ws_off += (tridiag_workspace_bytes(gr.nmax, gr.G) + 255) & ~size_t(255);
+    cta += gr.G;
+    groups.push_back(gr);
+  }
+  ctx->n_trd_groups = (int)groups.size();
+  ctx->trd_total_ctas = cta;
+  ctx->trd_est_ms = tp.makespan_us / 1000.0;
+  MBD_CUDA(ctx->tridiag_ws.reserve(ws_off));
+  // eigenvalue jobs: the batched launch first, then matrices too large for it
+  std::vector<EigJob> eig;
+  ctx->eig_single.clear();
+  ctx->eig_batch_max_n = 0;
+  for (int pass = 0; pass < 2; ++pass)
+    for (int g : ctx->order) {
+      GeomDev* gd = ctx->geoms[g].get();
+      const GeomPlan& p = gd->plan;
+      const bool fits = p.nH <= kEigBatchMaxN;
+      if (fits != (pass == 0)) continue;
+      eig.push_back(EigJob{gd->d, gd->e, gd->ev, gd->scalars, gd->energy, p.nH, p.nsl});
+      if (fits) ctx->eig_batch_max_n = std::max(ctx->eig_batch_max_n, p.nH);
+      else ctx->eig_single.push_back(g);
+    }
+  ctx->n_eig_jobs = (int)eig.size();
+  ctx->n_eig_batch = ctx->n_eig_jobs - (int)ctx->eig_single.size();
+  const size_t b_jobs = bytes_of<TridiagJob>(jobs.size());
+  const size_t b_groups = bytes_of<TridiagGroup>(groups.size());
+  const size_t b_eig = bytes_of<EigJob>(eig.size());
+  MBD_CUDA(ctx->tables.reserve(b_jobs + b_groups + b_eig));
+  char* base = ctx->tables.as<char>();
+  ctx->trd_jobs = reinterpret_cast<TridiagJob*>(base);
+  ctx->trd_groups = reinterpret_cast<TridiagGroup*>(base + b_jobs);
+  ctx->eig_jobs = reinterpret_cast<EigJob*>(base + b_jobs + b_groups);
+  std::vector<char> host(b_jobs + b_groups + b_eig, 0);
+  std::memcpy(host.data(), jobs.data(), sizeof(TridiagJob) * jobs.size());
+  std::memcpy(host.data() + b_jobs, groups.data(), sizeof(TridiagGroup) * groups.size());
+  std::memcpy(host.data() + b_jobs + b_groups, eig.data(), sizeof(EigJob) * eig.size());
+  MBD_CUDA(cudaMemcpy(base, host.data(), host.size(), cudaMemcpyHostToDevice));
+  ctx->h2d_bytes += (double)host.size();
   return MBD_OK;
 }
 
 // Buffers only the mixed modes use (allocated on first use).
 int reserve_mixed(mbd_ctx* ctx) {
-  size_t r32 = 0, pan = 0, vec = 0, res = 0;
-  for (auto& gp : ctx->geoms) {
-    const GeomPlan& p = gp->plan;
-    r32 = std::max(r32, sizeof(float) * (size_t)kNFreq * p.n * p.ld);
-    pan = std::max(pan, sizeof(float) * (size_t)kNFreq * round_up(p.n, kMixNB) * kMixNB);
-    vec = std::max(vec, sizeof(double) * 4 * (size_t)kNFreq * p.n * 3);
-    res = std::max(res, sizeof(double) * relay_residual_ws_doubles(p.n, kNFreq));
-  }
-  MBD_CUDA(ctx->relay32.reserve(r32));
-  MBD_CUDA(ctx->p_hi.reserve(pan));
-  MBD_CUDA(ctx->p_lo.reserve(pan));
-  MBD_CUDA(ctx->l_hi.reserve(pan));
-  MBD_CUDA(ctx->l_lo.reserve(pan));
-  MBD_CUDA(ctx->mixv.reserve(vec));
-  MBD_CUDA(ctx->res_ws.reserve(res));
-  size_t sync_ints = 0;
-  for (auto& gp : ctx->geoms) sync_ints = std::max(sync_ints, solve_sync_ints(gp->plan.n, kNFreq));
-  if (ctx->solve_sync.bytes < sizeof(int) * sync_ints) {
-    MBD_CUDA(ctx->solve_sync.reserve(sizeof(int) * sync_ints));
-    MBD_CUDA(cudaMemset(ctx->solve_sync.p, 0, ctx->solve_sync.bytes));
-    ctx->solve_epoch = 0;
+  for (int s = 0; s < ctx->n_slots; ++s) {
+    size_t r32 = 0, pan = 0, vec = 0, res = 0, sync = 0;
+    for (int g : ctx->order) {
+      if (ctx->geoms[g]->slot != s) continue;
+      size_t a, b, c, d, e;
+      mixed_bytes(ctx->geoms[g]->plan, &a, &b, &c, &d, &e);
+      r32 = std::max(r32, a);
+      pan = std::max(pan, b);
+      vec = std::max(vec, c);
+      res = std::max(res, d);
+      sync = std::max(sync, e);
+    }
+    RelaySlot& sl = *ctx->slots[s];
+    MBD_CUDA(sl.relay32.reserve(r32));
+    MBD_CUDA(sl.p_hi.reserve(pan));
+    MBD_CUDA(sl.p_lo.reserve(pan));
+    MBD_CUDA(sl.l_hi.reserve(pan));
+    MBD_CUDA(sl.l_lo.reserve(pan));
+    MBD_CUDA(sl.mixv.reserve(vec));
+    MBD_CUDA(sl.res_ws.reserve(res));
+    if (sl.solve_sync.bytes < sync) {
+      MBD_CUDA(sl.solve_sync.reserve(sync));
+      MBD_CUDA(cudaMemset(sl.solve_sync.p, 0, sl.solve_sync.bytes));
+      sl.solve_epoch = 0;
+    }
   }
   return MBD_OK;
 }
@@ -484,6 +734,7 @@ int mbd_rsscs_create(mbd_ctx** out, int device) {
   MBD_CUDA(cudaSetDevice(device));
   ctx->num_sms = prop.multiProcessorCount;
   MBD_CUDA(cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking));
+  for (auto& e : ctx->bev) MBD_CUDA(cudaEventCreate(&e));
   MBD_CUDA(init_device_constants());
   MBD_CUDA(init_chol_attributes());
   MBD_CUDA(init_eigval_attributes());
@@ -504,9 +755,12 @@ int mbd_rsscs_create(mbd_ctx** out, int device) {
 void mbd_rsscs_destroy(mbd_ctx* ctx) {
   if (!ctx) return;
   cudaSetDevice(ctx->device);
-  cudaStreamSynchronize(ctx->stream);
+  cudaDeviceSynchronize();
   for (auto e : ctx->events) cudaEventDestroy(e);
+  for (auto e : ctx->bev)
+    if (e) cudaEventDestroy(e);
   ctx->geoms.clear();
+  ctx->slots.clear();
   if (ctx->stream) cudaStreamDestroy(ctx->stream);
   delete ctx;
 }
@@ -514,6 +768,8 @@ void mbd_rsscs_destroy(mbd_ctx* ctx) {
 int mbd_rsscs_upload(mbd_ctx* ctx, int n_geom, const mbd_geom* geoms) {
   if (!ctx || n_geom < 1 || !geoms) return MBD_ERR_ARG;
   MBD_CUDA(cudaSetDevice(ctx->device));
+  // buffers of the previous batch may still be in use by its kernels
+  MBD_CUDA(cudaDeviceSynchronize());
   ctx->have_batch = false;
   ctx->h2d_bytes = 0;
   while ((int)ctx->geoms.size() < n_geom) ctx->geoms.emplace_back(new GeomDev());
@@ -525,7 +781,7 @@ int mbd_rsscs_upload(mbd_ctx* ctx, int n_geom, const mbd_geom* geoms) {
     if (st != MBD_OK && first == MBD_OK) first = st;
     if (st == MBD_ERR_OUT_OF_MEMORY || st == MBD_ERR_DEVICE) return st;
   }
-  int st = reserve_shared(ctx);
+  int st = prepare_batch(ctx);
   if (st != MBD_OK) return st;
   ctx->have_batch = true;
   return first;
@@ -534,6 +790,7 @@ int mbd_rsscs_upload(mbd_ctx* ctx, int n_geom, const mbd_geom* geoms) {
 int mbd_rsscs_compute(mbd_ctx* ctx, int mode) {
   if (!ctx || !ctx->have_batch) return MBD_ERR_ARG;
   if (mode != MBD_MODE_PLAIN_FP64 && mode != MBD_MODE_MIXED && mode != MBD_MODE_MIXED_LEARNED) return MBD_ERR_ARG;
+  if (mode == MBD_MODE_MIXED_LEARNED) return MBD_ERR_NOT_BUILT;
   MBD_CUDA(cudaSetDevice(ctx->device));
   if (mode != MBD_MODE_PLAIN_FP64) {
     int st = reserve_mixed(ctx);
@@ -541,14 +798,41 @@ int mbd_rsscs_compute(mbd_ctx* ctx, int mode) {
   }
   ctx->last_mode = mode;
   ctx->launches = 0;
-  MBD_CUDA(cudaMemsetAsync(ctx->err_flag, 0, sizeof(int), ctx->stream));
-  for (size_t g = 0; g < ctx->geoms.size(); ++g) {
-    GeomDev* gd = ctx->geoms[g].get();
-    if (gd->status_host != MBD_OK) continue;
-    int st = run_geometry(ctx, gd, (int)g, mode);
+  cudaStream_t s = ctx->stream;
+  MBD_CUDA(cudaMemsetAsync(ctx->err_flag, 0, sizeof(int), s));
+  MBD_CUDA(cudaEventRecord(ctx->bev[0], s));
+  if (ctx->order.empty()) {
+    for (int k = 1; k < 4; ++k) MBD_CUDA(cudaEventRecord(ctx->bev[k], s));
+    return MBD_OK;
+  }
+  // relay and CFDM stages, geometries spread over the slots' streams
+  for (int k = 0; k < ctx->n_slots; ++k) MBD_CUDA(cudaStreamWaitEvent(ctx->slots[k]->stream, ctx->bev[0], 0));
+  for (int g : ctx->order) {
+    int st = run_front(ctx, ctx->geoms[g].get(), g, mode);
     if (st != MBD_OK) return st;
   }
-  return MBD_OK;
+  for (int k = 0; k < ctx->n_slots; ++k) {
+    MBD_CUDA(cudaEventRecord(ctx->slots[k]->done, ctx->slots[k]->stream));
+    MBD_CUDA(cudaStreamWaitEvent(s, ctx->slots[k]->done, 0));
+  }
+  MBD_CUDA(cudaEventRecord(ctx->bev[1], s));
+  // every Hamiltonian to tridiagonal form in one cooperative launch
+  MBD_CUDA(launch_tridiag_groups(ctx->trd_jobs, ctx->trd_groups, ctx->n_trd_groups, ctx->trd_total_ctas,
+                                 ctx->tridiag_ws.p, ctx->err_flag, s));
+  ctx->launches += 2;
+  MBD_CUDA(cudaEventRecord(ctx->bev[2], s));
+  // eigenvalues and energies
+  launch_eigen_batch(ctx->eig_jobs, ctx->n_eig_batch, ctx->eig_batch_max_n, s);
+  ctx->launches += ctx->n_eig_batch > 0 ? 1 : 0;
+  for (int g : ctx->eig_single) {
+    GeomDev* gd = ctx->geoms[g].get();
+    launch_tridiag_eigenvalues(gd->d, gd->e, gd->plan.nH, gd->ev, s);
+    ctx->launches += 2;
+  }
+  launch_energy_batch(ctx->eig_jobs, ctx->n_eig_jobs, s);
+  ctx->launches += 1;
+  MBD_CUDA(cudaEventRecord(ctx->bev[3], s));
+  return cuda_status(cudaGetLastError());
 }
 
 int mbd_rsscs_download(mbd_ctx* ctx, mbd_result* out) {
@@ -557,8 +841,20 @@ int mbd_rsscs_download(mbd_ctx* ctx, mbd_result* out) {
   MBD_CUDA(cudaStreamSynchronize(ctx->stream));
   int err = 0;
   MBD_CUDA(cudaMemcpy(&err, ctx->err_flag, sizeof(int), cudaMemcpyDeviceToHost));
-  // stage timings (summed over geometries)
+  // stage timings: relay/CFDM stages summed over geometries (they overlap on
+  // the slots' streams), the batch-wide stages and the total from batch events
   for (int k = 0; k < Stage::kCount; ++k) ctx->last_ms[k] = 0.0;
+  auto elapsed = [](cudaEvent_t a, cudaEvent_t b) {
+    float ms = 0.f;
+    return cudaEventElapsedTime(&ms, a, b) == cudaSuccess ? (double)ms : 0.0;
+  };
+  ctx->last_ms[Stage::kTotal] = elapsed(ctx->bev[0], ctx->bev[3]);
+  ctx->last_ms[Stage::kTridiag] = elapsed(ctx->bev[1], ctx->bev[2]);
+  ctx->last_ms[Stage::kEig] = elapsed(ctx->bev[2], ctx->bev[3]);
+  for (int g : ctx->order) {
+    cudaEvent_t* evs = ctx->events.data() + (size_t)g * kGeomEvents;
+    for (int k = 1; k < kGeomEvents; ++k) ctx->last_ms[k] += elapsed(evs[k - 1], evs[k]);
+  }
   ctx->d2h_bytes = sizeof(int);
   int first = MBD_OK;
   for (size_t g = 0; g < ctx->geoms.size(); ++g) {
@@ -576,15 +872,6 @@ int mbd_rsscs_download(mbd_ctx* ctx, mbd_result* out) {
       if (first == MBD_OK) first = r.status;
       continue;
     }
-    cudaEvent_t* evs = ctx->events.data() + g * Stage::kCount;
-    for (int k = 1; k < Stage::kCount; ++k) {
-      float ms = 0.f;
-      if (cudaEventElapsedTime(&ms, evs[k - 1], evs[k]) == cudaSuccess) ctx->last_ms[k] += ms;
-    }
-    {
-      float ms = 0.f;
-      if (cudaEventElapsedTime(&ms, evs[0], evs[Stage::kCount - 1]) == cudaSuccess) ctx->last_ms[0] += ms;
-    }
     const int N = p.N;
     std::vector<double> aiw(21 * (size_t)N), molpol(21 * 9);
     double scal[8], en[8];
@@ -599,9 +886,10 @@ int mbd_rsscs_download(mbd_ctx* ctx, mbd_result* out) {
       r.err_est[0] = r.err_est[1] = r.err_est[2] = worst;
       r.refine_iters = kRefineIters;
       if (!(worst <= kResidualGate)) {
-        int st = run_geometry(ctx, gd, (int)g, MBD_MODE_PLAIN_FP64);
+        int st = run_front(ctx, gd, (int)g, MBD_MODE_PLAIN_FP64);
+        if (st == MBD_OK) st = run_tail_single(ctx, gd, ctx->slots[gd->slot]->stream);
         if (st != MBD_OK) return st;
-        MBD_CUDA(cudaStreamSynchronize(ctx->stream));
+        MBD_CUDA(cudaStreamSynchronize(ctx->slots[gd->slot]->stream));
         r.refine_iters = -1;
       }
     }

@@ -46,9 +46,8 @@ constexpr int kLanesPerEig = 8;
 
 // blockDim 256: 32 eigenvalues per CTA, 8 lanes each.  sh = [d | e^2] when
 // staged (n small enough for shared memory), else global memory is read.
-__global__ void __launch_bounds__(256) bisect_kernel(const double* d, const double* e, const double* e2g, int n,
-                                                     int staged, double* ev) {
-  extern __shared__ double sh[];
+__device__ __forceinline__ void bisect_block(const double* d, const double* e, const double* e2g, int n, int staged,
+                                             double* ev, int block, double* sh) {
   const double* dd = d;
   const double* ee = e2g;
   if (staged) {
@@ -83,7 +82,7 @@ __global__ void __launch_bounds__(256) bisect_kernel(const double* d, const doub
   const double tn = fmax(fabs(lo), fabs(hi));
   lo -= 4.0 * 2.2e-16 * tn + 1e-300;
   hi += 4.0 * 2.2e-16 * tn + 1e-300;
-  const int gid = blockIdx.x * blockDim.x + threadIdx.x;
+  const int gid = block * blockDim.x + threadIdx.x;
   const int k = gid / kLanesPerEig;
   const int q = gid % kLanesPerEig;
   const int lane = threadIdx.x % 32;
@@ -117,14 +116,27 @@ __global__ void __launch_bounds__(256) bisect_kernel(const double* d, const doub
   if (q == 0) ev[k] = 0.5 * (lo + hi);
 }
 
+__global__ void __launch_bounds__(256) bisect_kernel(const double* d, const double* e, const double* e2g, int n,
+                                                     int staged, double* ev) {
+  extern __shared__ double sh[];
+  bisect_block(d, e, e2g, n, staged, ev, blockIdx.x, sh);
+}
+
+// blockIdx.y = job; blocks past a job's eigenvalues leave before any barrier.
+__global__ void __launch_bounds__(256) bisect_batch_kernel(const EigJob* jobs) {
+  extern __shared__ double sh[];
+  const EigJob jb = jobs[blockIdx.y];
+  if ((long long)blockIdx.x * blockDim.x >= (long long)jb.n * kLanesPerEig) return;
+  bisect_block(jb.d, jb.e, nullptr, jb.n, 1, jb.ev, blockIdx.x, sh);
+}
+
 __device__ __forceinline__ void two_sum(double a, double b, double& s, double& err) {
   s = a + b;
   const double bb = s - a;
   err = (a - (s - bb)) + (b - bb);
 }
 
-__global__ void __launch_bounds__(1024) energy_kernel(const double* ev, int n, int nsl, const double* scalars,
-                                                      double* out) {
+__device__ __forceinline__ void energy_block(const double* ev, int n, int nsl, const double* scalars, double* out) {
   __shared__ double ss[1024], sc[1024];
   __shared__ int sn[1024];
   double s = 0.0, comp = 0.0;
@@ -163,6 +175,16 @@ __global__ void __launch_bounds__(1024) energy_kernel(const double* ev, int n, i
   }
 }
 
+__global__ void __launch_bounds__(1024) energy_kernel(const double* ev, int n, int nsl, const double* scalars,
+                                                      double* out) {
+  energy_block(ev, n, nsl, scalars, out);
+}
+
+__global__ void __launch_bounds__(1024) energy_batch_kernel(const EigJob* jobs) {
+  const EigJob jb = jobs[blockIdx.x];
+  energy_block(jb.ev, jb.n, jb.nsl, jb.scalars, jb.out);
+}
+
 __global__ void square_kernel(const double* e, double* e2, int m) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i < m) e2[i] = e[i] * e[i];
@@ -172,8 +194,12 @@ __global__ void square_kernel(const double* e, double* e2, int m) {
 
 constexpr size_t kBisectMaxSmem = 200 * 1024;
 
+static_assert(2 * sizeof(double) * kEigBatchMaxN <= kBisectMaxSmem, "batched bisection stages d and e^2");
+
 cudaError_t init_eigval_attributes() {
-  return cudaFuncSetAttribute(bisect_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kBisectMaxSmem);
+  cudaError_t e = cudaFuncSetAttribute(bisect_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kBisectMaxSmem);
+  if (e != cudaSuccess) return e;
+  return cudaFuncSetAttribute(bisect_batch_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kBisectMaxSmem);
 }
 
 // ev must hold 2n doubles: [0, n) eigenvalues, [n, 2n) scratch for e^2.
@@ -201,6 +227,18 @@ void launch_tridiag_eigenvalues_scratch(const double* d, const double* e, int n,
 
 void launch_energy(const double* ev, int n, int nsl, const double* scalars, double* out, cudaStream_t s) {
   energy_kernel<<<1, 1024, 0, s>>>(ev, n, nsl, scalars, out);
+}
+
+void launch_eigen_batch(const EigJob* jobs_dev, int n_jobs, int max_n, cudaStream_t s) {
+  if (n_jobs < 1 || max_n < 1) return;
+  const long long threads = (long long)max_n * kLanesPerEig;
+  const dim3 grid((unsigned)((threads + 255) / 256), (unsigned)n_jobs);
+  bisect_batch_kernel<<<grid, 256, sizeof(double) * 2 * (size_t)max_n, s>>>(jobs_dev);
+}
+
+void launch_energy_batch(const EigJob* jobs_dev, int n_jobs, cudaStream_t s) {
+  if (n_jobs < 1) return;
+  energy_batch_kernel<<<n_jobs, 1024, 0, s>>>(jobs_dev);
 }
 
 }  // namespace mbd

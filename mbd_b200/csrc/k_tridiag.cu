@@ -650,19 +650,58 @@ __device__ bool tridiag_one(const TridiagJob& job, const GroupWS& w, int g, int 
   return true;
 }
 
-__global__ void __launch_bounds__(THREADS, 1) tridiag_kernel(const TridiagJob* jobs, int n_jobs, int G,
-                                                             char* ws, size_t ws_bytes, int nmax,
+// groups == nullptr: gridDim.x / G_uniform equal groups of G_uniform CTAs,
+// group k reducing jobs k, k + groups, ... with workspace ws + k * ws_bytes.
+// Otherwise groups[0..n_groups) (ascending first_cta) partition the grid:
+// the CTAs [first_cta, first_cta + G) reduce jobs [job_begin, job_end) one
+// after another with workspace ws + ws_offset.
+__global__ void __launch_bounds__(THREADS, 1) tridiag_kernel(const TridiagJob* jobs, int n_jobs,
+                                                             const TridiagGroup* groups, int n_groups,
+                                                             int G_uniform, char* ws, size_t ws_bytes, int nmax,
                                                              int* err) {
   extern __shared__ double dyn[];
   __shared__ Smem sm;
-  const int group = blockIdx.x / G, g = blockIdx.x % G;
-  const int ngroups = gridDim.x / G;
-  GroupWS w;
-  ws_layout(nmax, G, &w, ws + (size_t)group * ws_bytes);
+  __shared__ int s_grp;
   unsigned gen = 0;
-  for (int jb = group; jb < n_jobs; jb += ngroups) {
+  GroupWS w;
+  if (groups == nullptr) {
+    const int G = G_uniform;
+    const int group = blockIdx.x / G, g = blockIdx.x % G;
+    const int ngroups = gridDim.x / G;
+    ws_layout(nmax, G, &w, ws + (size_t)group * ws_bytes);
+    for (int jb = group; jb < n_jobs; jb += ngroups) {
+      const TridiagJob job = jobs[jb];
+      if (!tridiag_one(job, w, g, G, gen, err, sm, dyn)) return;
+    }
+    return;
+  }
+  if (threadIdx.x == 0) {
+    int lo = 0, hi = n_groups - 1;   // last group with first_cta <= blockIdx.x
+    while (lo < hi) {
+      const int mid = (lo + hi + 1) / 2;
+      if (groups[mid].first_cta <= (int)blockIdx.x) lo = mid;
+      else hi = mid - 1;
+    }
+    s_grp = lo;
+  }
+  __syncthreads();
+  const TridiagGroup gr = groups[s_grp];
+  const int g = (int)blockIdx.x - gr.first_cta;
+  if (g < 0 || g >= gr.G) return;   // CTAs beyond the table (none when the launch matches it)
+  ws_layout(gr.nmax, gr.G, &w, ws + gr.ws_offset);
+  for (int jb = gr.job_begin; jb < gr.job_end; ++jb) {
     const TridiagJob job = jobs[jb];
-    if (!tridiag_one(job, w, g, G, gen, err, sm, dyn)) return;
+    if (!tridiag_one(job, w, g, gr.G, gen, err, sm, dyn)) return;
+  }
+}
+
+// Zeroes the barrier words of every group before a table launch.
+__global__ void reset_group_bars(const TridiagGroup* groups, int n_groups, char* ws) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n_groups) {
+    unsigned* bar = reinterpret_cast<unsigned*>(ws + groups[i].ws_offset);
+    bar[0] = 0u;
+    bar[1] = 0u;
   }
 }
 
@@ -690,10 +729,25 @@ cudaError_t launch_tridiag(const TridiagJob* jobs_dev, int n_jobs, int groups, i
   }
   int G = group_ctas;
   char* ws = static_cast<char*>(workspace);
-  void* args[] = {(void*)&jobs_dev, (void*)&n_jobs, (void*)&G, (void*)&ws, (void*)&ws_bytes_per_group,
-                  (void*)&nmax, (void*)&err_flag};
+  const TridiagGroup* no_table = nullptr;
+  int zero = 0;
+  void* args[] = {(void*)&jobs_dev, (void*)&n_jobs, (void*)&no_table, (void*)&zero, (void*)&G, (void*)&ws,
+                  (void*)&ws_bytes_per_group, (void*)&nmax, (void*)&err_flag};
   return cudaLaunchCooperativeKernel((const void*)tridiag_kernel, dim3(groups * group_ctas), dim3(THREADS),
                                      args, kTridiagDynSmem, s);
+}
+
+cudaError_t launch_tridiag_groups(const TridiagJob* jobs_dev, const TridiagGroup* groups_dev, int n_groups,
+                                  int total_ctas, void* workspace, int* err_flag, cudaStream_t s) {
+  if (n_groups < 1 || total_ctas < 1) return cudaSuccess;
+  char* ws = static_cast<char*>(workspace);
+  reset_group_bars<<<(n_groups + 255) / 256, 256, 0, s>>>(groups_dev, n_groups, ws);
+  int n_jobs = 0, G = 0, nmax = 0;
+  size_t wsb = 0;
+  void* args[] = {(void*)&jobs_dev, (void*)&n_jobs, (void*)&groups_dev, (void*)&n_groups, (void*)&G, (void*)&ws,
+                  (void*)&wsb, (void*)&nmax, (void*)&err_flag};
+  return cudaLaunchCooperativeKernel((const void*)tridiag_kernel, dim3(total_ctas), dim3(THREADS), args,
+                                     kTridiagDynSmem, s);
 }
 
 }  // namespace mbd

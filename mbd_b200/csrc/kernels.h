@@ -120,6 +120,20 @@ size_t tridiag_workspace_bytes(int n, int group_ctas);
 cudaError_t launch_tridiag(const TridiagJob* jobs_dev, int n_jobs, int groups, int group_ctas,
                            void* workspace, size_t ws_bytes_per_group, int nmax, int* err_flag,
                            cudaStream_t s);
+// One CTA group of a table launch: CTAs [first_cta, first_cta + G) reduce
+// jobs [job_begin, job_end) in order; workspace at ws_offset, laid out for
+// nmax (tridiag_workspace_bytes(nmax, G) bytes).
+struct TridiagGroup {
+  int first_cta, G;
+  int job_begin, job_end;
+  int nmax, pad;
+  size_t ws_offset;
+};
+// Groups of different sizes in one cooperative launch of total_ctas CTAs
+// (groups ascending in first_cta, covering [0, total_ctas)); zeroes their
+// barrier words first.  Returns a cudaError.
+cudaError_t launch_tridiag_groups(const TridiagJob* jobs_dev, const TridiagGroup* groups_dev, int n_groups,
+                                  int total_ctas, void* workspace, int* err_flag, cudaStream_t s);
 int tridiag_max_ctas_per_sm();
 
 // Eigenvalues of (d, e) by multisection; writes ev[0..n) ascending and uses
@@ -131,5 +145,18 @@ cudaError_t init_eigval_attributes();
 // energy = 0.5*sum_{ev>=0} sqrt(ev)/nsl - 0.5*sum_nonint; out[0]=E, out[1]=sum sqrt, out[2]=nimag
 void launch_energy(const double* ev, int n, int nsl, const double* scalars, double* out,
                    cudaStream_t s);
+// Many tridiagonal eigenproblems and energies in one launch each.
+struct EigJob {
+  const double* d;
+  const double* e;
+  double* ev;              // [n]
+  const double* scalars;   // relay scalars ([1] = sum of 3 omega)
+  double* out;             // energy outputs as launch_energy
+  int n, nsl;
+};
+constexpr int kEigBatchMaxN = 12800;    // d and e^2 staged in shared memory
+// jobs with n <= kEigBatchMaxN only; max_n the largest n among them.
+void launch_eigen_batch(const EigJob* jobs_dev, int n_jobs, int max_n, cudaStream_t s);
+void launch_energy_batch(const EigJob* jobs_dev, int n_jobs, cudaStream_t s);
 
 }  // namespace mbd

@@ -1,0 +1,101 @@
+"""GPU parity of batched runs: many geometries of uneven size in one call.
+
+A batch runs the relay stages of its geometries concurrently on several
+streams and reduces all CFDM Hamiltonians in one grouped launch, so these
+tests cover the group planning (one matrix per CTA group, several matrices
+per group when geometries outnumber CTAs, groups of different widths) and the
+batched eigenvalue / energy launches against the FP64 oracle.
+"""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+E_TOL = 1e-6
+C6_RTOL = 1e-6
+PLAIN_E_TOL = 1e-9
+PLAIN_RTOL = 1e-9
+
+
+@pytest.fixture(scope="module")
+def engine():
+    from mbd_b200 import Engine
+    eng = Engine(0)
+    yield eng
+    eng.close()
+
+
+def _oracle(geo, st):
+    from oracle import mbd_oracle as mo
+    og = mo.Geometry(list(geo.names), geo.coords.copy(), geo.hirshfeld.copy(), geo.lattice.copy(), geo.n_periodic)
+    os_ = mo.Settings(xc=st.xc, mbd_supercell_cutoff=st.mbd_supercell_cutoff,
+                      mbd_cfdm_dip_cutoff=st.mbd_cfdm_dip_cutoff, mbd_scs_dip_cutoff=st.mbd_scs_dip_cutoff,
+                      mbd_scs_vacuum_axis=tuple(st.mbd_scs_vacuum_axis))
+    return mo.mbd_at_rsscs(og, os_)
+
+
+def _assert_close(res, ref, mode):
+    e_tol = PLAIN_E_TOL if mode == "plain" else E_TOL
+    rtol = PLAIN_RTOL if mode == "plain" else C6_RTOL
+    assert res.status == 0
+    assert abs(res.energy - ref.energy) <= e_tol, (res.energy, ref.energy)
+    assert abs(res.c6_mol - ref.c6_mol) <= rtol * abs(ref.c6_mol)
+    np.testing.assert_allclose(res.c6_eff, ref.c6_eff, rtol=rtol, atol=0)
+    assert res.nimag == ref.nimag
+
+
+@pytest.mark.parametrize("mode", ["plain", "mixed"])
+def test_more_geometries_than_ctas(engine, mode):
+    """200 small clusters: more matrices than co-resident CTAs, so CTA groups
+    reduce several Hamiltonians one after another."""
+    from mbd_b200 import synthetic as sy
+    items = sy.cluster_batch(200, nmin=4, nmax=40, seed=7)
+    res = engine.energy_batch([g for g, _ in items], [s for _, s in items], mode)
+    for (g, s), r in zip(items, res):
+        _assert_close(r, _oracle(g, s), mode)
+
+
+@pytest.mark.parametrize("mode", ["plain", "mixed"])
+def test_uneven_batch_vs_oracle(engine, mode):
+    """Sizes spread over two orders of magnitude plus a periodic sheet: CTA
+    groups of different widths in the same launch."""
+    from mbd_b200 import synthetic as sy
+    items = [sy.cluster(n, seed=20 + n) for n in (12, 350, 40, 180, 7, 90)]
+    items.append(sy.graphene_sheet(reps=4))
+    res = engine.energy_batch([g for g, _ in items], [s for _, s in items], mode)
+    for (g, s), r in zip(items, res):
+        _assert_close(r, _oracle(g, s), mode)
+
+
+def test_batch_with_failing_member(engine):
+    """A geometry with an element outside the table fails alone; the rest of
+    the batch is unaffected."""
+    from mbd_b200 import Geometry, Settings
+    from mbd_b200 import synthetic as sy
+    good = [sy.cluster(n, seed=n) for n in (30, 15)]
+    bad = Geometry(["C", "La"], np.array([[0, 0, 0], [0, 0, 2.0]]), np.array([0.8, 0.8]))
+    geos = [good[0][0], bad, good[1][0]]
+    res = engine.energy_batch(geos, [good[0][1], Settings(), good[1][1]], "mixed", check=False)
+    assert res[1].status == 2
+    for k, (g, s) in zip((0, 2), good):
+        _assert_close(res[k], _oracle(g, s), "mixed")
+
+
+def test_batched_workload_mixed_vs_plain(engine):
+    """The 256-cluster batched workload (N ~ U{20..600}): every mixed energy
+    within 1e-6 Ha of the plain FP64 one, a sample against the oracle."""
+    from mbd_b200 import synthetic as sy
+    items = sy.cluster_batch(256)
+    geos, sets = [g for g, _ in items], [s for _, s in items]
+    mixed = engine.energy_batch(geos, sets, "mixed")
+    plain = engine.energy_batch(geos, sets, "plain")
+    for rm, rp in zip(mixed, plain):
+        assert rm.status == 0 and rp.status == 0
+        assert abs(rm.energy - rp.energy) <= E_TOL
+        assert abs(rm.c6_mol - rp.c6_mol) <= C6_RTOL * abs(rp.c6_mol)
+        assert rm.refine_iters > 0
+    sizes = [len(g.names) for g in geos]
+    for k in (int(np.argmin(sizes)), int(np.argsort(sizes)[len(sizes) // 2])):
+        ref = _oracle(*items[k])
+        _assert_close(plain[k], ref, "plain")
+        _assert_close(mixed[k], ref, "mixed")
