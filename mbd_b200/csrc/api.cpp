@@ -14,6 +14,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 #include <memory>
 #include <numeric>
@@ -121,6 +122,13 @@ struct mbd_ctx {
   mbd::TridiagJob* job_dev = nullptr;
   std::vector<cudaEvent_t> events;           // kGeomEvents per geometry
   cudaEvent_t bev[4] = {nullptr, nullptr, nullptr, nullptr};   // start, relay done, tridiag done, end
+  cudaEvent_t fork_ev = nullptr;             // releases the slot streams at the start of a compute
+  // one captured graph of mbd_rsscs_compute per mode, valid until the next
+  // upload or workspace reallocation
+  cudaGraphExec_t graph[3] = {nullptr, nullptr, nullptr};
+  double graph_launches[3] = {0, 0, 0};
+  bool use_graphs = true;
+  bool capturing = false;
   double last_ms[mbd::Stage::kCount] = {0};
   double launches = 0, h2d_bytes = 0, d2h_bytes = 0;
   int last_mode = 0;
@@ -178,6 +186,20 @@ void sym3_eigenvalues_upper(const double* M, double out[3]) {
   out[1] = a[1][1];
   out[2] = a[2][2];
   std::sort(out, out + 3);
+}
+
+// Records a timing event; inside a stream capture it becomes an event-record
+// node of the graph, so the event is recorded again on every replay.
+void record_timing(const mbd_ctx* ctx, cudaEvent_t ev, cudaStream_t s) {
+  cudaEventRecordWithFlags(ev, s, ctx->capturing ? cudaEventRecordExternal : cudaEventRecordDefault);
+}
+
+void drop_graphs(mbd_ctx* ctx) {
+  for (auto& g : ctx->graph)
+    if (g) {
+      cudaGraphExecDestroy(g);
+      g = nullptr;
+    }
 }
 
 int upload_geometry(mbd_ctx* ctx, const mbd_geom& g, GeomDev* gd) {
@@ -414,7 +436,7 @@ int relay_mixed(mbd_ctx* ctx, GeomDev* gd, RelaySlot& sl, size_t mstride, cudaEv
     launch_tc3_gemm(syrk_maps, sp, mt * (mt + 1) / 2, s);
     ctx->launches += 3;
   }
-  cudaEventRecord(ev_factor, s);
+  record_timing(ctx, ev_factor, s);
   // FP64 iterative refinement: X = 0, R = B; repeat D = (LL^T)^-1 R, X += D, R = B - A X
   const size_t ystride = (size_t)n * 3;
   double* X = sl.mixv.as<double>();
@@ -444,7 +466,7 @@ int run_front(mbd_ctx* ctx, GeomDev* gd, int gi, int mode) {
   cudaStream_t s = sl.stream;
   const int N = p.N, n = p.n;
   cudaEvent_t* ev = ctx->events.data() + (size_t)gi * kGeomEvents;
-  auto mark = [&](int k) { cudaEventRecord(ev[k], s); };
+  auto mark = [&](int k) { record_timing(ctx, ev[k], s); };
   const bool mixed = mode != MBD_MODE_PLAIN_FP64;
   mark(0);
   // 1. per-atom frequency table
@@ -582,6 +604,7 @@ int plan_slots(mbd_ctx* ctx) {
 // Plain-path slot buffers, per-geometry Hamiltonians, the tridiagonal plan and
 // the device job tables of the uploaded batch.
 int prepare_batch(mbd_ctx* ctx) {
+  drop_graphs(ctx);
   ctx->order.clear();
   for (size_t g = 0; g < ctx->geoms.size(); ++g)
     if (ctx->geoms[g]->status_host == MBD_OK) ctx->order.push_back((int)g);
@@ -697,20 +720,100 @@ int reserve_mixed(mbd_ctx* ctx) {
       sync = std::max(sync, e);
     }
     RelaySlot& sl = *ctx->slots[s];
-    MBD_CUDA(sl.relay32.reserve(r32));
-    MBD_CUDA(sl.p_hi.reserve(pan));
-    MBD_CUDA(sl.p_lo.reserve(pan));
-    MBD_CUDA(sl.l_hi.reserve(pan));
-    MBD_CUDA(sl.l_lo.reserve(pan));
-    MBD_CUDA(sl.mixv.reserve(vec));
-    MBD_CUDA(sl.res_ws.reserve(res));
-    if (sl.solve_sync.bytes < sync) {
-      MBD_CUDA(sl.solve_sync.reserve(sync));
-      MBD_CUDA(cudaMemset(sl.solve_sync.p, 0, sl.solve_sync.bytes));
+    bool moved = false;
+    auto grow = [&](DevBuf& b, size_t bytes) {
+      const bool re = bytes > b.bytes;
+      moved = moved || re;
+      return b.reserve(bytes);
+    };
+    MBD_CUDA(grow(sl.relay32, r32));
+    MBD_CUDA(grow(sl.p_hi, pan));
+    MBD_CUDA(grow(sl.p_lo, pan));
+    MBD_CUDA(grow(sl.l_hi, pan));
+    MBD_CUDA(grow(sl.l_lo, pan));
+    MBD_CUDA(grow(sl.mixv, vec));
+    MBD_CUDA(grow(sl.res_ws, res));
+    MBD_CUDA(grow(sl.solve_sync, sync));
+    if (moved) drop_graphs(ctx);
+  }
+  return MBD_OK;
+}
+
+// Enqueues the whole batch (relay stages on the slots' streams, then the
+// batch-wide eigen stages on the context stream).  Stream-capture safe: no
+// allocation, no host-side copies, and the mixed solve's progress flags are
+// cleared and its epochs restarted on every run.
+int enqueue_batch(mbd_ctx* ctx, int mode) {
+  cudaStream_t s = ctx->stream;
+  ctx->launches = 0;
+  MBD_CUDA(cudaMemsetAsync(ctx->err_flag, 0, sizeof(int), s));
+  record_timing(ctx, ctx->bev[0], s);
+  if (ctx->order.empty()) {
+    for (int k = 1; k < 4; ++k) record_timing(ctx, ctx->bev[k], s);
+    return cuda_status(cudaGetLastError());
+  }
+  // relay and CFDM stages, geometries spread over the slots' streams
+  MBD_CUDA(cudaEventRecord(ctx->fork_ev, s));
+  for (int k = 0; k < ctx->n_slots; ++k) {
+    RelaySlot& sl = *ctx->slots[k];
+    MBD_CUDA(cudaStreamWaitEvent(sl.stream, ctx->fork_ev, 0));
+    if (mode != MBD_MODE_PLAIN_FP64) {
+      MBD_CUDA(cudaMemsetAsync(sl.solve_sync.p, 0, sl.solve_sync.bytes, sl.stream));
       sl.solve_epoch = 0;
     }
   }
-  return MBD_OK;
+  for (int g : ctx->order) {
+    int st = run_front(ctx, ctx->geoms[g].get(), g, mode);
+    if (st != MBD_OK) return st;
+  }
+  for (int k = 0; k < ctx->n_slots; ++k) {
+    MBD_CUDA(cudaEventRecord(ctx->slots[k]->done, ctx->slots[k]->stream));
+    MBD_CUDA(cudaStreamWaitEvent(s, ctx->slots[k]->done, 0));
+  }
+  record_timing(ctx, ctx->bev[1], s);
+  // every Hamiltonian to tridiagonal form in one cooperative launch
+  MBD_CUDA(launch_tridiag_groups(ctx->trd_jobs, ctx->trd_groups, ctx->n_trd_groups, ctx->trd_total_ctas,
+                                 ctx->tridiag_ws.p, ctx->err_flag, s));
+  ctx->launches += 2;
+  record_timing(ctx, ctx->bev[2], s);
+  // eigenvalues and energies
+  launch_eigen_batch(ctx->eig_jobs, ctx->n_eig_batch, ctx->eig_batch_max_n, s);
+  ctx->launches += ctx->n_eig_batch > 0 ? 1 : 0;
+  for (int g : ctx->eig_single) {
+    GeomDev* gd = ctx->geoms[g].get();
+    launch_tridiag_eigenvalues(gd->d, gd->e, gd->plan.nH, gd->ev, s);
+    ctx->launches += 2;
+  }
+  launch_energy_batch(ctx->eig_jobs, ctx->n_eig_jobs, s);
+  ctx->launches += 1;
+  record_timing(ctx, ctx->bev[3], s);
+  return cuda_status(cudaGetLastError());
+}
+
+// Captures enqueue_batch into a graph for `mode`; false when capture is not
+// possible (the caller then enqueues directly).
+bool capture_batch(mbd_ctx* ctx, int mode) {
+  cudaGraph_t graph = nullptr;
+  if (cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  ctx->capturing = true;
+  const int st = enqueue_batch(ctx, mode);
+  ctx->capturing = false;
+  const cudaError_t ec = cudaStreamEndCapture(ctx->stream, &graph);
+  cudaGraphExec_t exec = nullptr;
+  const bool ok = st == MBD_OK && ec == cudaSuccess && graph &&
+                  cudaGraphInstantiate(&exec, graph, 0) == cudaSuccess;
+  if (graph) cudaGraphDestroy(graph);
+  if (!ok) {
+    if (exec) cudaGraphExecDestroy(exec);
+    cudaGetLastError();
+    return false;
+  }
+  ctx->graph[mode] = exec;
+  ctx->graph_launches[mode] = ctx->launches;
+  return true;
 }
 
 }  // namespace
@@ -735,6 +838,11 @@ int mbd_rsscs_create(mbd_ctx** out, int device) {
   ctx->num_sms = prop.multiProcessorCount;
   MBD_CUDA(cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking));
   for (auto& e : ctx->bev) MBD_CUDA(cudaEventCreate(&e));
+  MBD_CUDA(cudaEventCreateWithFlags(&ctx->fork_ev, cudaEventDisableTiming));
+  {
+    const char* ng = std::getenv("MBD_B200_NO_GRAPHS");
+    ctx->use_graphs = !(ng && ng[0] && ng[0] != '0');
+  }
   MBD_CUDA(init_device_constants());
   MBD_CUDA(init_chol_attributes());
   MBD_CUDA(init_eigval_attributes());
@@ -757,8 +865,10 @@ void mbd_rsscs_destroy(mbd_ctx* ctx) {
   cudaSetDevice(ctx->device);
   cudaDeviceSynchronize();
   for (auto e : ctx->events) cudaEventDestroy(e);
+  drop_graphs(ctx);
   for (auto e : ctx->bev)
     if (e) cudaEventDestroy(e);
+  if (ctx->fork_ev) cudaEventDestroy(ctx->fork_ev);
   ctx->geoms.clear();
   ctx->slots.clear();
   if (ctx->stream) cudaStreamDestroy(ctx->stream);
@@ -797,42 +907,13 @@ int mbd_rsscs_compute(mbd_ctx* ctx, int mode) {
     if (st != MBD_OK) return st;
   }
   ctx->last_mode = mode;
-  ctx->launches = 0;
-  cudaStream_t s = ctx->stream;
-  MBD_CUDA(cudaMemsetAsync(ctx->err_flag, 0, sizeof(int), s));
-  MBD_CUDA(cudaEventRecord(ctx->bev[0], s));
-  if (ctx->order.empty()) {
-    for (int k = 1; k < 4; ++k) MBD_CUDA(cudaEventRecord(ctx->bev[k], s));
-    return MBD_OK;
+  // replay the captured graph of this batch and mode (capture it first)
+  if (ctx->use_graphs && !ctx->graph[mode] && !capture_batch(ctx, mode)) ctx->use_graphs = false;
+  if (ctx->use_graphs && ctx->graph[mode]) {
+    ctx->launches = ctx->graph_launches[mode];
+    return cuda_status(cudaGraphLaunch(ctx->graph[mode], ctx->stream));
   }
-  // relay and CFDM stages, geometries spread over the slots' streams
-  for (int k = 0; k < ctx->n_slots; ++k) MBD_CUDA(cudaStreamWaitEvent(ctx->slots[k]->stream, ctx->bev[0], 0));
-  for (int g : ctx->order) {
-    int st = run_front(ctx, ctx->geoms[g].get(), g, mode);
-    if (st != MBD_OK) return st;
-  }
-  for (int k = 0; k < ctx->n_slots; ++k) {
-    MBD_CUDA(cudaEventRecord(ctx->slots[k]->done, ctx->slots[k]->stream));
-    MBD_CUDA(cudaStreamWaitEvent(s, ctx->slots[k]->done, 0));
-  }
-  MBD_CUDA(cudaEventRecord(ctx->bev[1], s));
-  // every Hamiltonian to tridiagonal form in one cooperative launch
-  MBD_CUDA(launch_tridiag_groups(ctx->trd_jobs, ctx->trd_groups, ctx->n_trd_groups, ctx->trd_total_ctas,
-                                 ctx->tridiag_ws.p, ctx->err_flag, s));
-  ctx->launches += 2;
-  MBD_CUDA(cudaEventRecord(ctx->bev[2], s));
-  // eigenvalues and energies
-  launch_eigen_batch(ctx->eig_jobs, ctx->n_eig_batch, ctx->eig_batch_max_n, s);
-  ctx->launches += ctx->n_eig_batch > 0 ? 1 : 0;
-  for (int g : ctx->eig_single) {
-    GeomDev* gd = ctx->geoms[g].get();
-    launch_tridiag_eigenvalues(gd->d, gd->e, gd->plan.nH, gd->ev, s);
-    ctx->launches += 2;
-  }
-  launch_energy_batch(ctx->eig_jobs, ctx->n_eig_jobs, s);
-  ctx->launches += 1;
-  MBD_CUDA(cudaEventRecord(ctx->bev[3], s));
-  return cuda_status(cudaGetLastError());
+  return enqueue_batch(ctx, mode);
 }
 
 int mbd_rsscs_download(mbd_ctx* ctx, mbd_result* out) {

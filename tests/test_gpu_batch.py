@@ -99,3 +99,27 @@ def test_batched_workload_mixed_vs_plain(engine):
         ref = _oracle(*items[k])
         _assert_close(plain[k], ref, "plain")
         _assert_close(mixed[k], ref, "mixed")
+
+
+@pytest.mark.parametrize("mode", ["plain", "mixed"])
+def test_graph_replay_matches_direct_launches(engine, mode, monkeypatch):
+    """compute() captures the batch into a CUDA graph on its first call and
+    replays it afterwards; replays equal a context that launches directly."""
+    from mbd_b200 import Engine
+    from mbd_b200 import synthetic as sy
+    items = [sy.cluster(n, seed=40 + n) for n in (25, 140, 60)]
+    geos, sets = [g for g, _ in items], [s for _, s in items]
+    assert engine.upload(geos, sets) == 0
+    runs = []
+    for _ in range(3):   # capture, replay, replay
+        assert engine.compute(mode) == 0
+        code, res = engine.download()
+        assert code == 0
+        runs.append(res)
+    monkeypatch.setenv("MBD_B200_NO_GRAPHS", "1")
+    with Engine(0) as direct:
+        ref = direct.energy_batch(geos, sets, mode)
+    for res in runs:
+        for a, b in zip(res, ref):
+            assert a.energy == b.energy
+            np.testing.assert_array_equal(a.alpha_iw, b.alpha_iw)
