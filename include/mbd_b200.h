@@ -36,7 +36,8 @@ enum {
     MBD_ERR_REFINEMENT = 9,       /* mixed mode: refinement did not reach the residual gate
                                      (informational: the direct FP64 fallback then ran) */
     MBD_ERR_NOT_BUILT = 10,       /* requested mode is not available in this build */
-    MBD_ERR_TOO_LARGE = 11        /* mbd_rsscs_eigvalsh_noalloc: n > MBD_NOALLOC_MAX_N */
+    MBD_ERR_TOO_LARGE = 11,       /* mbd_rsscs_eigvalsh_noalloc: n > MBD_NOALLOC_MAX_N */
+    MBD_ERR_NO_NETWORK = 12       /* MIXED_LEARNED without a trained or loaded network */
 };
 
 /* ---- compute modes ------------------------------------------------------- */
@@ -44,8 +45,10 @@ enum {
     MBD_MODE_PLAIN_FP64 = 0,      /* FP64 tensor build, FP64 Cholesky, FP64 eigensolve */
     MBD_MODE_MIXED = 1,           /* FP32 relay copy factorised on tcgen05 tensor cores
                                      (3xTF32), FP64 iterative refinement to 1e-10 */
-    MBD_MODE_MIXED_LEARNED = 2    /* MIXED + learned block preconditioner / warm start
-                                     for a block-CG relay solve, direct-solve fallback */
+    MBD_MODE_MIXED_LEARNED = 2    /* relay solved by block-CG (block-Jacobi preconditioned,
+                                     FP64) started from a message-passing network's
+                                     prediction of every atom's screened-polarizability
+                                     block; direct FP64 fallback on a residual miss */
 };
 
 #define MBD_N_FREQ 21             /* omega = 0 plus 20 Gauss-Legendre points, UTILS.f90:1188-1211 */
@@ -170,6 +173,44 @@ int mbd_rsscs_last_stats(mbd_ctx* ctx, double* out, int n);
 /* The CUDA stream (cudaStream_t) every kernel of this context runs on, so a
  * caller can record its own events around mbd_rsscs_compute. */
 void* mbd_rsscs_stream(mbd_ctx* ctx);
+
+/* ---- learned warm start of MBD_MODE_MIXED_LEARNED -----------------------
+ * (No counterpart in the reference, which solves the relay system directly
+ * at UTILS.f90:469-473.)  A message-passing network (3 layers, 64 hidden,
+ * FP32; atoms within 5 A are neighbours) predicts each atom's 3x3 block
+ * X_i = sum_j (A^-1)_ij of the relay solution for every frequency; block
+ * conjugate gradients start from it.  The context owns the network. */
+
+/* Number of FP32 network parameters (the layout of *_params). */
+int mbd_rsscs_learned_param_count(void);
+
+/* Trains the network on the GPU: uploads the geometries (REPLACING the
+ * context's uploaded batch), solves their relay systems with the plain FP64
+ * direct solve, and runs `epochs` passes of Adam (learning rate lr, one
+ * geometry per step, order shuffled with `seed`) on the mean squared error of
+ * the predicted blocks X_i / alpha_i.  epoch_loss (may be NULL) receives the
+ * mean loss of each epoch. */
+int mbd_rsscs_learned_train(mbd_ctx* ctx, int n_geom, const mbd_geom* geoms, int epochs, double lr,
+                            int seed, double* epoch_loss);
+
+/* Copy the parameters out of / into the context (n = param_count). */
+int mbd_rsscs_learned_get_params(mbd_ctx* ctx, float* params, int n);
+int mbd_rsscs_learned_set_params(mbd_ctx* ctx, const float* params, int n);
+
+/* on = 0: MIXED_LEARNED starts block-CG from zero (the method without the
+ * network); on = 1 (default): from the network's prediction. */
+int mbd_rsscs_learned_use_network(mbd_ctx* ctx, int on);
+
+/* The network's kernels on caller-given inputs, for checking them against a
+ * CPU restatement: n_atoms atoms, n_freq frequency copies, CSR neighbour lists
+ * off[n_atoms + 1] / nbr[off[n_atoms]] with displacement vectors dvec (bohr,
+ * 3 per edge, r_nbr - r_atom), node inputs x[n_freq * n_atoms][8].  Writes the
+ * predicted blocks S_pred[n_freq * n_atoms][9]; with S_true and grad given,
+ * also the loss (mean over nodes of ||S - S_true||_F^2) and its gradient
+ * with respect to params.  Host pointers; the context's network is not used. */
+int mbd_rsscs_learned_eval(mbd_ctx* ctx, const float* params, int n_atoms, int n_freq, const int* off,
+                           const int* nbr, const float* dvec, const float* x, const float* S_true,
+                           float* S_pred, float* grad, double* loss);
 
 #ifdef __cplusplus
 }

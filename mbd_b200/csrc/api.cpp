@@ -24,136 +24,11 @@
 #include "mbd_internal.h"
 #include "tc3.h"
 
-namespace mbd {
+#include "context.h"
 
-// Refinement sweeps of the mixed relay solve and the residual gate
-// ||B - A X||_F / ||B||_F that accepts its result.
-constexpr int kRefineIters = 4;
-constexpr double kResidualGate = 1e-10;
-// Relay slots (streams with private relay workspaces) of one context.
-constexpr int kMaxSlots = 8;
-// Share of free device memory the relay slots of one batch may plan for.
-constexpr double kSlotMemoryShare = 0.7;
-
-// Raw device allocation owned by the context (grow-only).
-struct DevBuf {
-  void* p = nullptr;
-  size_t bytes = 0;
-  ~DevBuf() {
-    if (p) cudaFree(p);
-  }
-  cudaError_t reserve(size_t b) {
-    if (b <= bytes) return cudaSuccess;
-    if (p) cudaFree(p);
-    p = nullptr;
-    bytes = 0;
-    cudaError_t e = cudaMalloc(&p, b);
-    if (e == cudaSuccess) bytes = b;
-    return e;
-  }
-  template <class T>
-  T* as() const { return static_cast<T*>(p); }
-};
-
-// Per-geometry device state that must survive until download.
-struct GeomDev {
-  GeomPlan plan;
-  DevBuf inputs;     // coords, alpha0, c6free, r0, hirsh, shifts, diff data
-  DevBuf results;    // alpha_w, sgm, rvdw_iso, alpha_iw, molpol, c6_eff, alpha_eff, omega, rvdw_eff, scalars, energy, info, d, e, ev
-  DevBuf hmat;       // CFDM Hamiltonian (nH x ldH, lower blocks), reduced in place
-  // offsets into inputs (doubles unless noted)
-  const double *coords, *alpha0, *c6free, *r0, *hirsh, *scs_shifts, *cfdm_shifts, *diff_shift;
-  const int *diff_is_zero, *place_offset, *place_rc, *place_cc;
-  // results
-  double *alpha_w, *sgm, *rvdw_iso, *alpha_iw, *molpol, *c6_eff, *alpha_eff, *omega, *rvdw_eff;
-  double *scalars, *energy, *d, *e, *ev, *rnorm2;
-  int* info;
-  int status_host = MBD_OK;
-  int slot = 0;      // relay slot running this geometry's relay and CFDM stages
-};
-
-// One relay slot: a stream and the relay workspaces of the geometries it runs
-// (sized for the largest of them).
-struct RelaySlot {
-  cudaStream_t stream = nullptr;
-  cudaEvent_t done = nullptr;
-  DevBuf relay64, linv, rhs;                                  // plain FP64 path
-  DevBuf relay32, p_hi, p_lo, l_hi, l_lo, mixv, res_ws, solve_sync;   // mixed path
-  int solve_epoch = 0;
-  ~RelaySlot() {
-    if (done) cudaEventDestroy(done);
-    if (stream) cudaStreamDestroy(stream);
-  }
-  size_t held() const {
-    return relay64.bytes + linv.bytes + rhs.bytes + relay32.bytes + p_hi.bytes + p_lo.bytes + l_hi.bytes +
-           l_lo.bytes + mixv.bytes + res_ws.bytes + solve_sync.bytes;
-  }
-};
-
-struct Stage {
-  enum { kTotal = 0, kSetup, kBuild, kFactor, kSolve, kCfdm, kTridiag, kEig, kCount };
-};
-// Events per geometry: start, then the ends of setup, build, factor, solve, CFDM.
-constexpr int kGeomEvents = 6;
-
-}  // namespace mbd
-
-struct mbd_ctx {
-  int device = 0;
-  int num_sms = 0;
-  int trd_ctas_per_sm = 1;
-  cudaStream_t stream = nullptr;             // batch stream: tridiagonal reduction, eigenvalues, energies
-  std::vector<std::unique_ptr<mbd::GeomDev>> geoms;
-  std::vector<std::unique_ptr<mbd::RelaySlot>> slots;
-  int n_slots = 0;                           // slots in use for the current batch
-  mbd::DevBuf tridiag_ws, tables, misc, fb_ws;
-  // standalone eigenvalue call: matrix, (d, e, eigenvalues, scratch), workspace
-  mbd::DevBuf eig_a, eig_vec, eig_ws;
-  // batch plan (device tables in `tables`)
-  mbd::TridiagJob* trd_jobs = nullptr;
-  mbd::TridiagGroup* trd_groups = nullptr;
-  mbd::EigJob* eig_jobs = nullptr;
-  int n_trd_groups = 0, trd_total_ctas = 0, n_eig_jobs = 0, n_eig_batch = 0, eig_batch_max_n = 0;
-  double trd_est_ms = 0.0;
-  std::vector<int> order;                    // geometries that run, descending relay size
-  std::vector<int> eig_single;               // geometries whose eigenvalues need their own launch
-  double* weights_dev = nullptr;
-  int* err_flag = nullptr;
-  mbd::TridiagJob* job_dev = nullptr;
-  std::vector<cudaEvent_t> events;           // kGeomEvents per geometry
-  cudaEvent_t bev[4] = {nullptr, nullptr, nullptr, nullptr};   // start, relay done, tridiag done, end
-  cudaEvent_t fork_ev = nullptr;             // releases the slot streams at the start of a compute
-  // one captured graph of mbd_rsscs_compute per mode, valid until the next
-  // upload or workspace reallocation
-  cudaGraphExec_t graph[3] = {nullptr, nullptr, nullptr};
-  double graph_launches[3] = {0, 0, 0};
-  bool use_graphs = true;
-  bool capturing = false;
-  double last_ms[mbd::Stage::kCount] = {0};
-  double launches = 0, h2d_bytes = 0, d2h_bytes = 0;
-  int last_mode = 0;
-  bool have_batch = false;
-};
 
 namespace mbd {
 namespace {
-
-int cuda_status(cudaError_t e) {
-  if (e == cudaSuccess) return MBD_OK;
-  if (e == cudaErrorMemoryAllocation) return MBD_ERR_OUT_OF_MEMORY;
-  return MBD_ERR_DEVICE;
-}
-
-#define MBD_CUDA(x)                          \
-  do {                                       \
-    cudaError_t _e = (x);                    \
-    if (_e != cudaSuccess) return cuda_status(_e); \
-  } while (0)
-
-template <class T>
-size_t bytes_of(size_t n) {
-  return ((n * sizeof(T)) + 255) & ~size_t(255);
-}
 
 // Symmetric 3x3 eigenvalues from the upper triangle (DSYEV('V','U'), UTILS.f90:273),
 // cyclic Jacobi in FP64, ascending.
@@ -186,20 +61,6 @@ void sym3_eigenvalues_upper(const double* M, double out[3]) {
   out[1] = a[1][1];
   out[2] = a[2][2];
   std::sort(out, out + 3);
-}
-
-// Records a timing event; inside a stream capture it becomes an event-record
-// node of the graph, so the event is recorded again on every replay.
-void record_timing(const mbd_ctx* ctx, cudaEvent_t ev, cudaStream_t s) {
-  cudaEventRecordWithFlags(ev, s, ctx->capturing ? cudaEventRecordExternal : cudaEventRecordDefault);
-}
-
-void drop_graphs(mbd_ctx* ctx) {
-  for (auto& g : ctx->graph)
-    if (g) {
-      cudaGraphExecDestroy(g);
-      g = nullptr;
-    }
 }
 
 int upload_geometry(mbd_ctx* ctx, const mbd_geom& g, GeomDev* gd) {
@@ -275,6 +136,7 @@ int upload_geometry(mbd_ctx* ctx, const mbd_geom& g, GeomDev* gd) {
   add(bytes_of<double>(2 * (size_t)p.nH));   // 13 ev (+ e^2 scratch of the bisection)
   add(bytes_of<int>(32));          // 14 info
   add(bytes_of<double>(32));       // 15 rnorm2 (squared refinement residual per frequency)
+  add(bytes_of<double>(kNFreq * kCgState));   // 16 block-CG state
   MBD_CUDA(gd->results.reserve(off));
   base = gd->results.as<char>();
   MBD_CUDA(cudaMemsetAsync(base, 0, off, ctx->stream));
@@ -294,6 +156,8 @@ int upload_geometry(mbd_ctx* ctx, const mbd_geom& g, GeomDev* gd) {
   gd->ev = reinterpret_cast<double*>(base + offs[13]);
   gd->info = reinterpret_cast<int*>(base + offs[14]);
   gd->rnorm2 = reinterpret_cast<double*>(base + offs[15]);
+  gd->cgstate = reinterpret_cast<double*>(base + offs[16]);
+  gd->n_edges = -1;   // the learned-mode graph of the new geometry is built on first use
   return MBD_OK;
 }
 
@@ -457,6 +321,16 @@ int relay_mixed(mbd_ctx* ctx, GeomDev* gd, RelaySlot& sl, size_t mstride, cudaEv
   return MBD_OK;
 }
 
+}  // namespace
+
+void drop_graphs(mbd_ctx* ctx) {
+  for (auto& g : ctx->graph)
+    if (g) {
+      cudaGraphExecDestroy(g);
+      g = nullptr;
+    }
+}
+
 // Relay and CFDM stages of geometry gi on its slot's stream: per-atom
 // frequency table, relay tensors, relay factorisation and solve (plain or
 // mixed), screened polarizabilities and C6, CFDM Hamiltonian into gd->hmat.
@@ -467,7 +341,8 @@ int run_front(mbd_ctx* ctx, GeomDev* gd, int gi, int mode) {
   const int N = p.N, n = p.n;
   cudaEvent_t* ev = ctx->events.data() + (size_t)gi * kGeomEvents;
   auto mark = [&](int k) { record_timing(ctx, ev[k], s); };
-  const bool mixed = mode != MBD_MODE_PLAIN_FP64;
+  const bool mixed = mode == MBD_MODE_MIXED;
+  const bool learned = mode == MBD_MODE_MIXED_LEARNED;
   mark(0);
   // 1. per-atom frequency table
   AtomDev ad{gd->coords, gd->alpha0, gd->c6free, gd->r0, gd->hirsh, gd->alpha_w, gd->sgm, gd->rvdw_iso};
@@ -489,6 +364,10 @@ int run_front(mbd_ctx* ctx, GeomDev* gd, int gi, int mode) {
     int st = relay_mixed(ctx, gd, sl, mstride, ev[3]);
     if (st != MBD_OK) return st;
     Xv = sl.mixv.as<double>();
+  } else if (learned) {
+    // network warm start (stage 3), block-CG (stage 4)
+    int st = relay_learned(ctx, gd, sl, mstride, ev[3], &Xv);
+    if (st != MBD_OK) return st;
   } else {
     // 3. blocked Cholesky, batched over the 21 frequencies
     BatchMat bm{sl.relay64.as<double>(), mstride, p.ld, n, kNFreq};
@@ -528,6 +407,8 @@ int run_front(mbd_ctx* ctx, GeomDev* gd, int gi, int mode) {
   mark(5);
   return cuda_status(cudaGetLastError());
 }
+
+namespace {
 
 // Eigen stages of one geometry on stream s with its own tridiagonal launch
 // (the residual-gate fallback of download).
@@ -700,7 +581,7 @@ int prepare_batch(mbd_ctx* ctx) {
   std::memcpy(host.data(), jobs.data(), sizeof(TridiagJob) * jobs.size());
   std::memcpy(host.data() + b_jobs, groups.data(), sizeof(TridiagGroup) * groups.size());
   std::memcpy(host.data() + b_jobs + b_groups, eig.data(), sizeof(EigJob) * eig.size());
-  MBD_CUDA(cudaMemcpy(base, host.data(), host.size(), cudaMemcpyHostToDevice));
+  MBD_CUDA(h2d_ordered(ctx, base, host.data(), host.size()));
   ctx->h2d_bytes += (double)host.size();
   return MBD_OK;
 }
@@ -757,7 +638,7 @@ int enqueue_batch(mbd_ctx* ctx, int mode) {
   for (int k = 0; k < ctx->n_slots; ++k) {
     RelaySlot& sl = *ctx->slots[k];
     MBD_CUDA(cudaStreamWaitEvent(sl.stream, ctx->fork_ev, 0));
-    if (mode != MBD_MODE_PLAIN_FP64) {
+    if (mode == MBD_MODE_MIXED) {
       MBD_CUDA(cudaMemsetAsync(sl.solve_sync.p, 0, sl.solve_sync.bytes, sl.stream));
       sl.solve_epoch = 0;
     }
@@ -854,8 +735,11 @@ int mbd_rsscs_create(mbd_ctx** out, int device) {
   ctx->weights_dev = reinterpret_cast<double*>(m);
   ctx->err_flag = reinterpret_cast<int*>(m + 256);
   ctx->job_dev = reinterpret_cast<TridiagJob*>(m + 512);
-  MBD_CUDA(cudaMemcpy(ctx->weights_dev, kCasimirWeight, sizeof(double) * kNFreq, cudaMemcpyHostToDevice));
-  MBD_CUDA(cudaMemset(ctx->err_flag, 0, sizeof(int)));
+  ctx->omega_dev = reinterpret_cast<double*>(m + 1024);
+  ctx->loss_dev = reinterpret_cast<double*>(m + 1280);
+  MBD_CUDA(h2d_ordered(ctx.get(), ctx->omega_dev, kCasimirOmega, sizeof(double) * kNFreq));
+  MBD_CUDA(h2d_ordered(ctx.get(), ctx->weights_dev, kCasimirWeight, sizeof(double) * kNFreq));
+  MBD_CUDA(zero_ordered(ctx.get(), ctx->err_flag, sizeof(int)));
   *out = ctx.release();
   return MBD_OK;
 }
@@ -900,10 +784,13 @@ int mbd_rsscs_upload(mbd_ctx* ctx, int n_geom, const mbd_geom* geoms) {
 int mbd_rsscs_compute(mbd_ctx* ctx, int mode) {
   if (!ctx || !ctx->have_batch) return MBD_ERR_ARG;
   if (mode != MBD_MODE_PLAIN_FP64 && mode != MBD_MODE_MIXED && mode != MBD_MODE_MIXED_LEARNED) return MBD_ERR_ARG;
-  if (mode == MBD_MODE_MIXED_LEARNED) return MBD_ERR_NOT_BUILT;
+  if (mode == MBD_MODE_MIXED_LEARNED && ctx->use_net && !ctx->have_net) return MBD_ERR_NO_NETWORK;
   MBD_CUDA(cudaSetDevice(ctx->device));
-  if (mode != MBD_MODE_PLAIN_FP64) {
+  if (mode == MBD_MODE_MIXED) {
     int st = reserve_mixed(ctx);
+    if (st != MBD_OK) return st;
+  } else if (mode == MBD_MODE_MIXED_LEARNED) {
+    int st = reserve_learned(ctx);
     if (st != MBD_OK) return st;
   }
   ctx->last_mode = mode;
@@ -966,6 +853,13 @@ int mbd_rsscs_download(mbd_ctx* ctx, mbd_result* out) {
       for (int f = 0; f < 21; ++f) worst = std::max(worst, std::sqrt(rn[f] / (3.0 * N)));
       r.err_est[0] = r.err_est[1] = r.err_est[2] = worst;
       r.refine_iters = kRefineIters;
+      if (ctx->last_mode == MBD_MODE_MIXED_LEARNED) {
+        std::vector<double> cs((size_t)kNFreq * kCgState);
+        MBD_CUDA(cudaMemcpy(cs.data(), gd->cgstate, sizeof(double) * cs.size(), cudaMemcpyDeviceToHost));
+        double most = 0.0;
+        for (int f = 0; f < kNFreq; ++f) most = std::max(most, cs[(size_t)f * kCgState + 1]);
+        r.refine_iters = (int)most;
+      }
       if (!(worst <= kResidualGate)) {
         int st = run_front(ctx, gd, (int)g, MBD_MODE_PLAIN_FP64);
         if (st == MBD_OK) st = run_tail_single(ctx, gd, ctx->slots[gd->slot]->stream);
@@ -1091,6 +985,7 @@ const char* mbd_rsscs_strerror(int code) {
     case MBD_ERR_REFINEMENT: return "mixed-precision refinement missed the residual gate; FP64 fallback used";
     case MBD_ERR_NOT_BUILT: return "mode not available in this build";
     case MBD_ERR_TOO_LARGE: return "matrix larger than the fixed scratch of the allocation-free entry point";
+    case MBD_ERR_NO_NETWORK: return "MIXED_LEARNED needs a trained or loaded network (or the network switched off)";
     default: return "unknown error";
   }
 }

@@ -1,0 +1,183 @@
+// Context and per-geometry device state shared by the C ABI (api.cpp) and
+// the learned relay path (learn.cpp).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <memory>
+#include <vector>
+
+#include "gnn.h"
+#include "kernels.h"
+#include "mbd_internal.h"
+
+namespace mbd {
+
+// Refinement sweeps of the mixed relay solve and the residual gate
+// ||B - A X||_F / ||B||_F that accepts its result.
+constexpr int kRefineIters = 4;
+constexpr double kResidualGate = 1e-10;
+// Relay slots (streams with private relay workspaces) of one context.
+constexpr int kMaxSlots = 8;
+// Share of free device memory the relay slots of one batch may plan for.
+constexpr double kSlotMemoryShare = 0.7;
+
+// Raw device allocation owned by the context (grow-only).
+struct DevBuf {
+  void* p = nullptr;
+  size_t bytes = 0;
+  ~DevBuf() {
+    if (p) cudaFree(p);
+  }
+  cudaError_t reserve(size_t b) {
+    if (b <= bytes) return cudaSuccess;
+    if (p) cudaFree(p);
+    p = nullptr;
+    bytes = 0;
+    cudaError_t e = cudaMalloc(&p, b);
+    if (e == cudaSuccess) bytes = b;
+    return e;
+  }
+  template <class T>
+  T* as() const { return static_cast<T*>(p); }
+};
+
+// Per-geometry device state that must survive until download.
+struct GeomDev {
+  GeomPlan plan;
+  DevBuf inputs;     // coords, alpha0, c6free, r0, hirsh, shifts, diff data
+  DevBuf results;    // alpha_w, sgm, rvdw_iso, alpha_iw, molpol, c6_eff, alpha_eff, omega, rvdw_eff, scalars, energy, info, d, e, ev
+  DevBuf hmat;       // CFDM Hamiltonian (nH x ldH, lower blocks), reduced in place
+  // offsets into inputs (doubles unless noted)
+  const double *coords, *alpha0, *c6free, *r0, *hirsh, *scs_shifts, *cfdm_shifts, *diff_shift;
+  const int *diff_is_zero, *place_offset, *place_rc, *place_cc;
+  // results
+  double *alpha_w, *sgm, *rvdw_iso, *alpha_iw, *molpol, *c6_eff, *alpha_eff, *omega, *rvdw_eff;
+  double *scalars, *energy, *d, *e, *ev, *rnorm2;
+  double* cgstate;   // [21][kCgState] block-CG recurrence state (MIXED_LEARNED)
+  int* info;
+  int status_host = MBD_OK;
+  int slot = 0;      // relay slot running this geometry's relay and CFDM stages
+  // learned warm start: neighbour graph (built on first use), training data
+  DevBuf graph;      // off, nbr, src, species (int); dvec, efeat, eproj (float)
+  int n_edges = -1;  // -1 until the graph is built
+  GnnGraph gnn{};    // device views into `graph` (x set per use)
+  DevBuf train;      // x [21N][8] and S_true [21N][9] of a training batch
+};
+
+// One relay slot: a stream and the relay workspaces of the geometries it runs
+// (sized for the largest of them).
+struct RelaySlot {
+  cudaStream_t stream = nullptr;
+  cudaEvent_t done = nullptr;
+  DevBuf relay64, linv, rhs;                                  // plain FP64 path
+  DevBuf relay32, p_hi, p_lo, l_hi, l_lo, mixv, res_ws, solve_sync;   // mixed path
+  DevBuf cg, gnn;                                             // learned path: CG vectors, network work
+  int solve_epoch = 0;
+  ~RelaySlot() {
+    if (done) cudaEventDestroy(done);
+    if (stream) cudaStreamDestroy(stream);
+  }
+  size_t held() const {
+    return relay64.bytes + linv.bytes + rhs.bytes + relay32.bytes + p_hi.bytes + p_lo.bytes + l_hi.bytes +
+           l_lo.bytes + mixv.bytes + res_ws.bytes + solve_sync.bytes + cg.bytes + gnn.bytes;
+  }
+};
+
+struct Stage {
+  enum { kTotal = 0, kSetup, kBuild, kFactor, kSolve, kCfdm, kTridiag, kEig, kCount };
+};
+// Events per geometry: start, then the ends of setup, build, factor, solve, CFDM.
+constexpr int kGeomEvents = 6;
+
+}  // namespace mbd
+
+struct mbd_ctx {
+  int device = 0;
+  int num_sms = 0;
+  int trd_ctas_per_sm = 1;
+  cudaStream_t stream = nullptr;             // batch stream: tridiagonal reduction, eigenvalues, energies
+  std::vector<std::unique_ptr<mbd::GeomDev>> geoms;
+  std::vector<std::unique_ptr<mbd::RelaySlot>> slots;
+  int n_slots = 0;                           // slots in use for the current batch
+  mbd::DevBuf tridiag_ws, tables, misc, fb_ws;
+  // standalone eigenvalue call: matrix, (d, e, eigenvalues, scratch), workspace
+  mbd::DevBuf eig_a, eig_vec, eig_ws;
+  // batch plan (device tables in `tables`)
+  mbd::TridiagJob* trd_jobs = nullptr;
+  mbd::TridiagGroup* trd_groups = nullptr;
+  mbd::EigJob* eig_jobs = nullptr;
+  int n_trd_groups = 0, trd_total_ctas = 0, n_eig_jobs = 0, n_eig_batch = 0, eig_batch_max_n = 0;
+  double trd_est_ms = 0.0;
+  std::vector<int> order;                    // geometries that run, descending relay size
+  std::vector<int> eig_single;               // geometries whose eigenvalues need their own launch
+  double* weights_dev = nullptr;
+  double* omega_dev = nullptr;               // the 21 imaginary frequencies
+  // learned warm start: network parameters, Adam state, training work
+  mbd::DevBuf gnn_params, gnn_grad, gnn_m1, gnn_m2, gnn_train_work, gnn_eval;
+  bool have_net = false;
+  bool use_net = true;
+  double* loss_dev = nullptr;
+  int* err_flag = nullptr;
+  mbd::TridiagJob* job_dev = nullptr;
+  std::vector<cudaEvent_t> events;           // kGeomEvents per geometry
+  cudaEvent_t bev[4] = {nullptr, nullptr, nullptr, nullptr};   // start, relay done, tridiag done, end
+  cudaEvent_t fork_ev = nullptr;             // releases the slot streams at the start of a compute
+  // one captured graph of mbd_rsscs_compute per mode, valid until the next
+  // upload or workspace reallocation
+  cudaGraphExec_t graph[3] = {nullptr, nullptr, nullptr};
+  double graph_launches[3] = {0, 0, 0};
+  bool use_graphs = true;
+  bool capturing = false;
+  double last_ms[mbd::Stage::kCount] = {0};
+  double launches = 0, h2d_bytes = 0, d2h_bytes = 0;
+  int last_mode = 0;
+  bool have_batch = false;
+};
+
+namespace mbd {
+
+inline int cuda_status(cudaError_t e) {
+  if (e == cudaSuccess) return MBD_OK;
+  if (e == cudaErrorMemoryAllocation) return MBD_ERR_OUT_OF_MEMORY;
+  return MBD_ERR_DEVICE;
+}
+
+#define MBD_CUDA(x)                                \
+  do {                                             \
+    cudaError_t _e = (x);                          \
+    if (_e != cudaSuccess) return ::mbd::cuda_status(_e); \
+  } while (0)
+
+template <class T>
+size_t bytes_of(size_t n) {
+  return ((n * sizeof(T)) + 255) & ~size_t(255);
+}
+
+// Records a timing event; inside a stream capture it becomes an event-record
+// node of the graph, so the event is recorded again on every replay.
+inline void record_timing(const mbd_ctx* ctx, cudaEvent_t ev, cudaStream_t s) {
+  cudaEventRecordWithFlags(ev, s, ctx->capturing ? cudaEventRecordExternal : cudaEventRecordDefault);
+}
+
+// Host-to-device copy ordered with the context's streams: a plain
+// cudaMemcpy / cudaMemset runs on the legacy default stream, which the
+// context's non-blocking streams do not wait for, and may return before a
+// copy from pageable memory has landed.
+inline cudaError_t h2d_ordered(const mbd_ctx* ctx, void* dst, const void* src, size_t bytes) {
+  cudaError_t e = cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, ctx->stream);
+  return e != cudaSuccess ? e : cudaStreamSynchronize(ctx->stream);
+}
+inline cudaError_t zero_ordered(const mbd_ctx* ctx, void* dst, size_t bytes) {
+  cudaError_t e = cudaMemsetAsync(dst, 0, bytes, ctx->stream);
+  return e != cudaSuccess ? e : cudaStreamSynchronize(ctx->stream);
+}
+
+// api.cpp
+void drop_graphs(mbd_ctx* ctx);
+int run_front(mbd_ctx* ctx, GeomDev* gd, int gi, int mode);
+// learn.cpp
+int reserve_learned(mbd_ctx* ctx);
+int relay_learned(mbd_ctx* ctx, GeomDev* gd, RelaySlot& sl, size_t mstride, cudaEvent_t ev_net, double** X_out);
+
+}  // namespace mbd

@@ -145,6 +145,29 @@ cudaError_t init_eigval_attributes();
 // energy = 0.5*sum_{ev>=0} sqrt(ev)/nsl - 0.5*sum_nonint; out[0]=E, out[1]=sum sqrt, out[2]=nimag
 void launch_energy(const double* ev, int n, int nsl, const double* scalars, double* out,
                    cudaStream_t s);
+// ---- block-CG relay solve of the MIXED_LEARNED mode (UTILS.f90:469-473) ----
+constexpr int kCgState = 24;   // per-frequency recurrence state (doubles)
+struct CgArgs {
+  const double* A;         // 21 relay matrices, row-major lower FP64
+  size_t a_stride;
+  int ld, n, N, nt;        // n = 3N, nt = ceil(n / 64)
+  int batch;               // frequencies
+  double *X, *R, *Z, *P, *Q;   // [batch][n][3]; X holds the start on entry
+  size_t ystride;          // n * 3
+  double* Dinv;            // [batch][N][9] block-Jacobi inverses
+  double* partial;         // cg_partial_doubles
+  double* red;             // cg_red_doubles (row-block partials)
+  double* red2;            // cg_red_doubles (atom-block partials)
+  double* state;           // [batch][kCgState]: [0] stop flag, [1] iterations
+  double tol2;             // stop when ||R||_F^2 <= tol2
+};
+size_t cg_partial_doubles(int n, int batch);
+size_t cg_red_doubles(int n, int batch);
+// Jacobi blocks, R = B - A X, Z, P and Z^T R for every frequency.
+void launch_cg_setup(const CgArgs& a, cudaStream_t s);
+// One iteration (iteration index it = 0, 1, ...); a converged frequency skips it.
+void launch_cg_iteration(const CgArgs& a, int it, cudaStream_t s);
+
 // Many tridiagonal eigenproblems and energies in one launch each.
 struct EigJob {
   const double* d;

@@ -1,0 +1,501 @@
+// MIXED_LEARNED relay solve and the training of its network.
+//
+// The relay system A(iw) X = [I3; ...; I3] of every frequency (the solve of
+// get_screened_alpha, UTILS.f90:469-473) is solved by block conjugate
+// gradients (k_cg.cu) started from a network's prediction of each atom's 3x3
+// screened-polarizability block X_i (k_gnn.cu).  The network is trained here,
+// on the GPU, on relay solutions that the plain direct solve produces for a
+// training set of geometries.  A frequency whose final residual misses the
+// gate is re-solved directly at download (the plain path), as in MIXED.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdint>
+#include <cstring>
+#include <vector>
+
+#include "context.h"
+#include "tc3.h"
+
+namespace mbd {
+namespace {
+
+constexpr int kCgMaxIters = 80;
+constexpr double kCgTol = 3e-11;   // relative residual the iteration stops at (gate: 1e-10)
+
+// Neighbour lists within the network's cut-off, including periodic images
+// along non-vacuum axes (an atom may meet another atom, or itself, through
+// several images).  Lists are symmetric: edge (i, j + t) implies (j, i - t).
+void build_graph(const GeomPlan& p, std::vector<int>& off, std::vector<int>& nbr, std::vector<int>& src,
+                 std::vector<float>& dvec) {
+  const int N = p.N;
+  const double rc = kGnnCutoffBohr;
+  int rng[3] = {0, 0, 0};
+  if (p.n_periodic != 0) {
+    // images up to the cut-off plus a cell: widths from |a_k| lower-bound nothing,
+    // so use the perpendicular width V / |a_i x a_j|
+    const double* a = p.lat;
+    auto cross = [](const double* u, const double* v, double* w) {
+      w[0] = u[1] * v[2] - u[2] * v[1];
+      w[1] = u[2] * v[0] - u[0] * v[2];
+      w[2] = u[0] * v[1] - u[1] * v[0];
+    };
+    double c12[3], c20[3], c01[3];
+    cross(a + 3, a + 6, c12);
+    cross(a + 6, a + 0, c20);
+    cross(a + 0, a + 3, c01);
+    const double vol = std::fabs(a[0] * c12[0] + a[1] * c12[1] + a[2] * c12[2]);
+    const double* cs[3] = {c12, c20, c01};
+    for (int k = 0; k < 3; ++k) {
+      if (p.vac[k]) continue;
+      const double area = std::sqrt(cs[k][0] * cs[k][0] + cs[k][1] * cs[k][1] + cs[k][2] * cs[k][2]);
+      const double width = vol > 0.0 ? vol / area : 0.0;
+      rng[k] = width > 0.0 ? (int)std::ceil(rc / width) + 1 : 0;
+    }
+  }
+  double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
+  for (int i = 0; i < N; ++i)
+    for (int c = 0; c < 3; ++c) {
+      lo[c] = std::min(lo[c], p.coords[3 * i + c]);
+      hi[c] = std::max(hi[c], p.coords[3 * i + c]);
+    }
+  // image points near the box: (atom, position)
+  struct Pt {
+    int atom;
+    double x[3];
+  };
+  std::vector<Pt> pts;
+  for (int n0 = -rng[0]; n0 <= rng[0]; ++n0)
+    for (int n1 = -rng[1]; n1 <= rng[1]; ++n1)
+      for (int n2 = -rng[2]; n2 <= rng[2]; ++n2) {
+        double t[3];
+        for (int c = 0; c < 3; ++c) t[c] = n0 * p.lat[c] + n1 * p.lat[3 + c] + n2 * p.lat[6 + c];
+        for (int j = 0; j < N; ++j) {
+          Pt q{j, {p.coords[3 * j] + t[0], p.coords[3 * j + 1] + t[1], p.coords[3 * j + 2] + t[2]}};
+          bool keep = true;
+          for (int c = 0; c < 3; ++c) keep = keep && q.x[c] >= lo[c] - rc && q.x[c] <= hi[c] + rc;
+          if (keep) pts.push_back(q);
+        }
+      }
+  // uniform bins of edge rc over the padded box
+  int nb[3];
+  for (int c = 0; c < 3; ++c) nb[c] = std::max(1, (int)std::ceil((hi[c] - lo[c] + 2 * rc) / rc));
+  auto bin_of = [&](const double* x, int* b) {
+    for (int c = 0; c < 3; ++c) b[c] = std::min(nb[c] - 1, std::max(0, (int)((x[c] - (lo[c] - rc)) / rc)));
+  };
+  const size_t nbins = (size_t)nb[0] * nb[1] * nb[2];
+  std::vector<int> head(nbins + 1, 0);
+  std::vector<int> order(pts.size());
+  std::vector<size_t> pb(pts.size());
+  for (size_t k = 0; k < pts.size(); ++k) {
+    int b[3];
+    bin_of(pts[k].x, b);
+    pb[k] = ((size_t)b[0] * nb[1] + b[1]) * nb[2] + b[2];
+    head[pb[k] + 1]++;
+  }
+  for (size_t k = 0; k < nbins; ++k) head[k + 1] += head[k];
+  {
+    std::vector<int> fill(head.begin(), head.end() - 1);
+    for (size_t k = 0; k < pts.size(); ++k) order[fill[pb[k]]++] = (int)k;
+  }
+  off.assign(N + 1, 0);
+  nbr.clear();
+  src.clear();
+  dvec.clear();
+  const double rc2 = rc * rc;
+  for (int i = 0; i < N; ++i) {
+    const double* xi = &p.coords[3 * i];
+    int b[3];
+    bin_of(xi, b);
+    for (int d0 = -1; d0 <= 1; ++d0)
+      for (int d1 = -1; d1 <= 1; ++d1)
+        for (int d2 = -1; d2 <= 1; ++d2) {
+          const int c0 = b[0] + d0, c1 = b[1] + d1, c2 = b[2] + d2;
+          if (c0 < 0 || c1 < 0 || c2 < 0 || c0 >= nb[0] || c1 >= nb[1] || c2 >= nb[2]) continue;
+          const size_t bin = ((size_t)c0 * nb[1] + c1) * nb[2] + c2;
+          for (int k = head[bin]; k < head[bin + 1]; ++k) {
+            const Pt& q = pts[order[k]];
+            const double dx = q.x[0] - xi[0], dy = q.x[1] - xi[1], dz = q.x[2] - xi[2];
+            const double r2 = dx * dx + dy * dy + dz * dz;
+            if (r2 >= rc2 || r2 < 1e-12) continue;   // the atom itself (zero shift) has r = 0
+            nbr.push_back(q.atom);
+            src.push_back(i);
+            dvec.push_back((float)dx);
+            dvec.push_back((float)dy);
+            dvec.push_back((float)dz);
+          }
+        }
+    off[i + 1] = (int)nbr.size();
+  }
+}
+
+// Device copy of a graph: [off | nbr | src | species] ints, [dvec | efeat | eproj] floats.
+int upload_graph(mbd_ctx* ctx, GeomDev* gd, cudaStream_t s) {
+  const GeomPlan& p = gd->plan;
+  std::vector<int> off, nbr, src;
+  std::vector<float> dvec;
+  build_graph(p, off, nbr, src, dvec);
+  const int N = p.N, E = (int)nbr.size();
+  const size_t b_off = bytes_of<int>(N + 1), b_e = bytes_of<int>(std::max(E, 1)), b_sp = bytes_of<int>(N);
+  const size_t b_dv = bytes_of<float>(3 * (size_t)std::max(E, 1)), b_ef = bytes_of<float>(kGnnRbf * (size_t)std::max(E, 1));
+  const size_t b_ep = bytes_of<float>(6 * (size_t)std::max(E, 1));
+  const size_t total = b_off + 2 * b_e + b_sp + b_dv + b_ef + b_ep;
+  MBD_CUDA(gd->graph.reserve(total));
+  char* base = gd->graph.as<char>();
+  std::vector<char> host(b_off + 2 * b_e + b_sp + b_dv, 0);
+  std::memcpy(host.data(), off.data(), sizeof(int) * off.size());
+  std::memcpy(host.data() + b_off, nbr.data(), sizeof(int) * nbr.size());
+  std::memcpy(host.data() + b_off + b_e, src.data(), sizeof(int) * src.size());
+  std::memcpy(host.data() + b_off + 2 * b_e, p.species.data(), sizeof(int) * N);
+  std::memcpy(host.data() + b_off + 2 * b_e + b_sp, dvec.data(), sizeof(float) * dvec.size());
+  MBD_CUDA(h2d_ordered(ctx, base, host.data(), host.size()));
+  ctx->h2d_bytes += (double)host.size();
+  GnnGraph& g = gd->gnn;
+  g.N = N;
+  g.F = kNFreq;
+  g.E = E;
+  g.off = reinterpret_cast<const int*>(base);
+  g.nbr = reinterpret_cast<const int*>(base + b_off);
+  g.src = reinterpret_cast<const int*>(base + b_off + b_e);
+  const int* species = reinterpret_cast<const int*>(base + b_off + 2 * b_e);
+  const float* dv = reinterpret_cast<const float*>(base + b_off + 2 * b_e + b_sp);
+  float* ef = reinterpret_cast<float*>(base + b_off + 2 * b_e + b_sp + b_dv);
+  float* ep = reinterpret_cast<float*>(base + b_off + 2 * b_e + b_sp + b_dv + b_ef);
+  g.efeat = ef;
+  g.eproj = ep;
+  g.x = nullptr;
+  gd->n_edges = E;
+  (void)species;
+  gnn_edges(dv, E, ef, ep, s);
+  ctx->launches += E > 0 ? 1 : 0;
+  return cuda_status(cudaGetLastError());
+}
+
+const int* graph_species(const GeomDev* gd) {
+  const int N = gd->plan.N;
+  const int E = std::max(gd->n_edges, 1);
+  return reinterpret_cast<const int*>(gd->graph.as<char>() + bytes_of<int>(N + 1) + 2 * bytes_of<int>(E));
+}
+
+size_t cg_doubles(const GeomPlan& p) {
+  const size_t ys = (size_t)p.n * 3;
+  return 5 * kNFreq * ys + (size_t)kNFreq * p.N * 9 + cg_partial_doubles(p.n, kNFreq) +
+         2 * cg_red_doubles(p.n, kNFreq) + 64;
+}
+
+// Deterministic parameter initialisation (splitmix64 + Box-Muller): weights
+// N(0, 1/fan_in), readout vectors zero, wg N(0, 0.01), biases zero.
+void init_params(std::vector<float>& P, uint64_t seed) {
+  P.assign(kGnnParams, 0.0f);
+  uint64_t st = seed * 0x9E3779B97F4A7C15ull + 1;
+  auto next = [&]() {
+    uint64_t z = (st += 0x9E3779B97F4A7C15ull);
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+    z ^= z >> 31;
+    return ((z >> 11) + 0.5) * (1.0 / 9007199254740992.0);
+  };
+  auto normal = [&]() { return std::sqrt(-2.0 * std::log(next())) * std::cos(2.0 * kPi * next()); };
+  auto fill = [&](int off, int rows, int cols, double sd) {
+    for (int k = 0; k < rows * cols; ++k) P[off + k] = (float)(normal() * sd);
+  };
+  fill(kGnnOffW0, kGnnHidden, kGnnIn, std::sqrt(1.0 / kGnnIn));
+  for (int l = 0; l < kGnnLayers; ++l) {
+    fill(kGnnOffWf(l), kGnnHidden, kGnnRbf, std::sqrt(1.0 / kGnnRbf));
+    fill(kGnnOffWu(l), kGnnHidden, kGnnHidden, std::sqrt(1.0 / kGnnHidden));
+  }
+  fill(kGnnOffWg, 1, kGnnRbf, 0.1);
+}
+
+int reserve_params(mbd_ctx* ctx) {
+  const size_t b = sizeof(float) * kGnnParams;
+  if (ctx->gnn_params.bytes < b) {
+    MBD_CUDA(ctx->gnn_params.reserve(b));
+    MBD_CUDA(ctx->gnn_grad.reserve(b));
+    MBD_CUDA(ctx->gnn_m1.reserve(b));
+    MBD_CUDA(ctx->gnn_m2.reserve(b));
+  }
+  return MBD_OK;
+}
+
+}  // namespace
+
+// Per-slot CG and network buffers and every geometry's graph.
+int reserve_learned(mbd_ctx* ctx) {
+  for (int g : ctx->order) {
+    GeomDev* gd = ctx->geoms[g].get();
+    if (gd->n_edges < 0) {
+      int st = upload_graph(ctx, gd, ctx->stream);
+      if (st != MBD_OK) return st;
+    }
+  }
+  bool moved = false;
+  for (int s = 0; s < ctx->n_slots; ++s) {
+    size_t cg = 0, gw = 0, res = 0;
+    for (int g : ctx->order) {
+      GeomDev* gd = ctx->geoms[g].get();
+      if (gd->slot != s) continue;
+      const GeomPlan& p = gd->plan;
+      cg = std::max(cg, sizeof(double) * cg_doubles(p));
+      gw = std::max(gw, sizeof(float) * (gnn_work_floats(p.N, kNFreq, gd->n_edges, false) +
+                                         (size_t)kNFreq * p.N * kGnnIn + 64));
+      res = std::max(res, sizeof(double) * relay_residual_ws_doubles(p.n, kNFreq));
+    }
+    RelaySlot& sl = *ctx->slots[s];
+    moved = moved || cg > sl.cg.bytes || gw > sl.gnn.bytes || res > sl.res_ws.bytes;
+    MBD_CUDA(sl.cg.reserve(cg));
+    MBD_CUDA(sl.gnn.reserve(gw));
+    MBD_CUDA(sl.res_ws.reserve(res));
+  }
+  if (moved) drop_graphs(ctx);
+  return MBD_OK;
+}
+
+// Learned relay solve of one geometry on its slot's stream; *X_out = the
+// solution (n x 3 per frequency) in the slot's CG buffer.
+int relay_learned(mbd_ctx* ctx, GeomDev* gd, RelaySlot& sl, size_t mstride, cudaEvent_t ev_net, double** X_out) {
+  const GeomPlan& p = gd->plan;
+  cudaStream_t s = sl.stream;
+  const int n = p.n, N = p.N;
+  const size_t ys = (size_t)n * 3;
+  double* base = sl.cg.as<double>();
+  CgArgs a{};
+  a.A = sl.relay64.as<double>();
+  a.a_stride = mstride;
+  a.ld = p.ld;
+  a.n = n;
+  a.N = N;
+  a.nt = (n + 63) / 64;
+  a.batch = kNFreq;
+  a.X = base;
+  a.R = a.X + kNFreq * ys;
+  a.Z = a.R + kNFreq * ys;
+  a.P = a.Z + kNFreq * ys;
+  a.Q = a.P + kNFreq * ys;
+  a.ystride = ys;
+  a.Dinv = a.Q + kNFreq * ys;
+  a.partial = a.Dinv + (size_t)kNFreq * N * 9;
+  a.red = a.partial + cg_partial_doubles(n, kNFreq);
+  a.red2 = a.red + cg_red_doubles(n, kNFreq);
+  a.state = gd->cgstate;
+  a.tol2 = kCgTol * kCgTol * 3.0 * N;
+  // start: the network's prediction, or zero
+  if (ctx->use_net) {
+    float* w = sl.gnn.as<float>();
+    float* x = w;
+    float* work = w + (((size_t)kNFreq * N * kGnnIn + 63) & ~size_t(63));
+    gnn_features(graph_species(gd), gd->hirsh, gd->alpha_w, ctx->omega_dev, N, kNFreq, x, s);
+    GnnGraph g = gd->gnn;
+    g.x = x;
+    const GnnWork wk = gnn_work_layout(work, N, kNFreq, gd->n_edges, false);
+    ctx->launches += 1 + gnn_forward(ctx->gnn_params.as<float>(), g, wk, s);
+    gnn_warmstart(wk.S, gd->alpha_w, N, kNFreq, a.X, ys, s);
+    ctx->launches += 1;
+  } else {
+    MBD_CUDA(cudaMemsetAsync(a.X, 0, sizeof(double) * kNFreq * ys, s));
+  }
+  record_timing(ctx, ev_net, s);
+  launch_cg_setup(a, s);
+  ctx->launches += 5;
+  for (int it = 0; it < kCgMaxIters; ++it) launch_cg_iteration(a, it, s);
+  ctx->launches += 4 * kCgMaxIters;
+  // the gate's residual, recomputed from X: R = B - A X
+  launch_relay_residual(sl.relay64.as<double>(), mstride, p.ld, n, kNFreq, a.X, nullptr, a.R, ys,
+                        sl.res_ws.as<double>(), gd->rnorm2, s);
+  ctx->launches += 3;
+  *X_out = a.X;
+  return cuda_status(cudaGetLastError());
+}
+
+}  // namespace mbd
+
+using namespace mbd;
+
+extern "C" {
+
+int mbd_rsscs_learned_param_count(void) { return kGnnParams; }
+
+int mbd_rsscs_learned_set_params(mbd_ctx* ctx, const float* params, int n) {
+  if (!ctx || !params || n != kGnnParams) return MBD_ERR_ARG;
+  MBD_CUDA(cudaSetDevice(ctx->device));
+  int st = reserve_params(ctx);
+  if (st != MBD_OK) return st;
+  MBD_CUDA(h2d_ordered(ctx, ctx->gnn_params.p, params, sizeof(float) * kGnnParams));
+  drop_graphs(ctx);
+  ctx->have_net = true;
+  return MBD_OK;
+}
+
+int mbd_rsscs_learned_get_params(mbd_ctx* ctx, float* params, int n) {
+  if (!ctx || !params || n != kGnnParams) return MBD_ERR_ARG;
+  if (!ctx->have_net) return MBD_ERR_NO_NETWORK;
+  MBD_CUDA(cudaSetDevice(ctx->device));
+  MBD_CUDA(cudaMemcpy(params, ctx->gnn_params.p, sizeof(float) * kGnnParams, cudaMemcpyDeviceToHost));
+  return MBD_OK;
+}
+
+int mbd_rsscs_learned_use_network(mbd_ctx* ctx, int on) {
+  if (!ctx) return MBD_ERR_ARG;
+  if (ctx->use_net != (on != 0)) drop_graphs(ctx);
+  ctx->use_net = on != 0;
+  return MBD_OK;
+}
+
+int mbd_rsscs_learned_train(mbd_ctx* ctx, int n_geom, const mbd_geom* geoms, int epochs, double lr, int seed,
+                            double* epoch_loss) {
+  if (!ctx || !geoms || n_geom < 1 || epochs < 1 || !(lr > 0.0)) return MBD_ERR_ARG;
+  int st = mbd_rsscs_upload(ctx, n_geom, geoms);
+  if (st == MBD_ERR_OUT_OF_MEMORY || st == MBD_ERR_DEVICE || st == MBD_ERR_ARG) return st;
+  if (ctx->order.empty()) return st != MBD_OK ? st : MBD_ERR_ARG;
+  st = reserve_learned(ctx);
+  if (st != MBD_OK) return st;
+  st = reserve_params(ctx);
+  if (st != MBD_OK) return st;
+  // training targets: direct FP64 relay solutions of every geometry
+  size_t work = 0;
+  for (int g : ctx->order) {
+    GeomDev* gd = ctx->geoms[g].get();
+    const GeomPlan& p = gd->plan;
+    MBD_CUDA(gd->train.reserve(sizeof(float) * (size_t)kNFreq * p.N * (kGnnIn + 9) + 256));
+    work = std::max(work, gnn_work_floats(p.N, kNFreq, gd->n_edges, true));
+  }
+  MBD_CUDA(ctx->gnn_train_work.reserve(sizeof(float) * work));
+  MBD_CUDA(cudaStreamSynchronize(ctx->stream));
+  ctx->launches = 0;
+  for (int g : ctx->order) {
+    GeomDev* gd = ctx->geoms[g].get();
+    const GeomPlan& p = gd->plan;
+    RelaySlot& sl = *ctx->slots[gd->slot];
+    st = run_front(ctx, gd, g, MBD_MODE_PLAIN_FP64);
+    if (st != MBD_OK) return st;
+    const size_t ys = (size_t)p.n * 3;
+    const double* X = sl.rhs.as<double>() + 2 * kNFreq * ys;
+    float* x = gd->train.as<float>();
+    float* St = x + (size_t)kNFreq * p.N * kGnnIn;
+    gnn_features(graph_species(gd), gd->hirsh, gd->alpha_w, ctx->omega_dev, p.N, kNFreq, x, sl.stream);
+    gnn_targets(X, ys, gd->alpha_w, p.N, kNFreq, St, sl.stream);
+  }
+  MBD_CUDA(cudaDeviceSynchronize());
+  {
+    int info_bad = 0;
+    for (int g : ctx->order) {
+      int info[32];
+      MBD_CUDA(cudaMemcpy(info, ctx->geoms[g]->info, sizeof(info), cudaMemcpyDeviceToHost));
+      for (int f = 0; f < kNFreq; ++f) info_bad |= info[f] != 0;
+    }
+    if (info_bad) return MBD_ERR_RELAY_NOT_SPD;
+  }
+  // Adam over the geometries (one geometry = one step), shuffled every epoch
+  std::vector<float> P0;
+  init_params(P0, (uint64_t)seed);
+  cudaStream_t s = ctx->stream;
+  float* P = ctx->gnn_params.as<float>();
+  float* G = ctx->gnn_grad.as<float>();
+  MBD_CUDA(h2d_ordered(ctx, P, P0.data(), sizeof(float) * kGnnParams));
+  MBD_CUDA(zero_ordered(ctx, G, sizeof(float) * kGnnParams));
+  MBD_CUDA(zero_ordered(ctx, ctx->gnn_m1.p, sizeof(float) * kGnnParams));
+  MBD_CUDA(zero_ordered(ctx, ctx->gnn_m2.p, sizeof(float) * kGnnParams));
+  std::vector<int> order = ctx->order;
+  uint64_t rs = (uint64_t)seed * 6364136223846793005ull + 1442695040888963407ull;
+  int step = 0;
+  for (int ep = 0; ep < epochs; ++ep) {
+    for (int k = (int)order.size() - 1; k > 0; --k) {
+      rs = rs * 6364136223846793005ull + 1442695040888963407ull;
+      std::swap(order[k], order[(int)((rs >> 33) % (uint64_t)(k + 1))]);
+    }
+    MBD_CUDA(cudaMemsetAsync(ctx->loss_dev, 0, sizeof(double), s));
+    for (int g : order) {
+      GeomDev* gd = ctx->geoms[g].get();
+      const GeomPlan& p = gd->plan;
+      GnnGraph gg = gd->gnn;
+      gg.x = gd->train.as<float>();
+      GnnWork w = gnn_work_layout(ctx->gnn_train_work.as<float>(), p.N, kNFreq, gd->n_edges, true);
+      w.S_true = gd->train.as<float>() + (size_t)kNFreq * p.N * kGnnIn;
+      gnn_forward(P, gg, w, s);
+      gnn_loss_backward(P, gg, w, G, ctx->loss_dev, s);
+      gnn_adam(P, G, ctx->gnn_m1.as<float>(), ctx->gnn_m2.as<float>(), ++step, (float)lr, s);
+    }
+    double loss = 0.0;
+    MBD_CUDA(cudaMemcpyAsync(&loss, ctx->loss_dev, sizeof(double), cudaMemcpyDeviceToHost, s));
+    MBD_CUDA(cudaStreamSynchronize(s));
+    if (epoch_loss) epoch_loss[ep] = loss / (double)order.size();
+    if (!std::isfinite(loss)) {
+      ctx->have_net = false;
+      return MBD_ERR_NO_NETWORK;   // training diverged: no usable network
+    }
+  }
+  ctx->have_net = true;
+  drop_graphs(ctx);
+  return MBD_OK;
+}
+
+// Forward pass, loss and gradient of the network on caller-given inputs
+// (host arrays; a check of the kernels against a CPU restatement).  Leaves
+// the context's own network untouched.
+int mbd_rsscs_learned_eval(mbd_ctx* ctx, const float* params, int n_atoms, int n_freq, const int* off,
+                           const int* nbr, const float* dvec, const float* x, const float* S_true, float* S_pred,
+                           float* grad, double* loss) {
+  if (!ctx || !params || n_atoms < 1 || n_freq < 1 || !off || !x || !S_pred) return MBD_ERR_ARG;
+  MBD_CUDA(cudaSetDevice(ctx->device));
+  const int N = n_atoms, F = n_freq, E = off[N];
+  if (E < 0 || (E > 0 && (!nbr || !dvec))) return MBD_ERR_ARG;
+  std::vector<int> src(std::max(E, 1), 0);
+  for (int i = 0; i < N; ++i)
+    for (int e = off[i]; e < off[i + 1]; ++e) {
+      if (e < 0 || e >= E || nbr[e] < 0 || nbr[e] >= N) return MBD_ERR_ARG;
+      src[e] = i;
+    }
+  const size_t M = (size_t)N * F;
+  const int Ep = std::max(E, 1);
+  const size_t fl = kGnnParams + kGnnParams + M * kGnnIn + 9 * M + (size_t)Ep * (3 + kGnnRbf + 6) +
+                    gnn_work_floats(N, F, E, true) + 1024;
+  const size_t il = (size_t)(N + 1) + 2 * (size_t)Ep + 64;
+  MBD_CUDA(ctx->gnn_eval.reserve(sizeof(float) * fl + sizeof(int) * il + 4096));
+  float* f = ctx->gnn_eval.as<float>();
+  auto takef = [&](size_t k) {
+    float* q = f;
+    f += (k + 63) & ~size_t(63);
+    return q;
+  };
+  float* P = takef(kGnnParams);
+  float* G = takef(kGnnParams);
+  float* xd = takef(M * kGnnIn);
+  float* St = takef(9 * M);
+  float* dv = takef(3 * (size_t)Ep);
+  float* ef = takef(kGnnRbf * (size_t)Ep);
+  float* epj = takef(6 * (size_t)Ep);
+  float* work = takef(gnn_work_floats(N, F, E, true));
+  int* ib = reinterpret_cast<int*>(f);
+  int* d_off = ib;
+  int* d_nbr = ib + ((N + 1 + 63) & ~63);
+  int* d_src = d_nbr + ((Ep + 63) & ~63);
+  double* d_loss = ctx->loss_dev;
+  cudaStream_t s = ctx->stream;
+  MBD_CUDA(cudaMemcpyAsync(P, params, sizeof(float) * kGnnParams, cudaMemcpyHostToDevice, s));
+  MBD_CUDA(cudaMemsetAsync(G, 0, sizeof(float) * kGnnParams, s));
+  MBD_CUDA(cudaMemcpyAsync(xd, x, sizeof(float) * M * kGnnIn, cudaMemcpyHostToDevice, s));
+  MBD_CUDA(cudaMemcpyAsync(d_off, off, sizeof(int) * (N + 1), cudaMemcpyHostToDevice, s));
+  if (E > 0) {
+    MBD_CUDA(cudaMemcpyAsync(d_nbr, nbr, sizeof(int) * E, cudaMemcpyHostToDevice, s));
+    MBD_CUDA(cudaMemcpyAsync(d_src, src.data(), sizeof(int) * E, cudaMemcpyHostToDevice, s));
+    MBD_CUDA(cudaMemcpyAsync(dv, dvec, sizeof(float) * 3 * E, cudaMemcpyHostToDevice, s));
+  }
+  gnn_edges(dv, E, ef, epj, s);
+  GnnGraph g{N, F, E, d_off, d_nbr, d_src, ef, epj, xd};
+  GnnWork w = gnn_work_layout(work, N, F, E, true);
+  w.S_true = St;
+  gnn_forward(P, g, w, s);
+  if (S_true && grad) {
+    MBD_CUDA(cudaMemcpyAsync(St, S_true, sizeof(float) * 9 * M, cudaMemcpyHostToDevice, s));
+    MBD_CUDA(cudaMemsetAsync(d_loss, 0, sizeof(double), s));
+    gnn_loss_backward(P, g, w, G, d_loss, s);
+    MBD_CUDA(cudaMemcpyAsync(grad, G, sizeof(float) * kGnnParams, cudaMemcpyDeviceToHost, s));
+    if (loss) MBD_CUDA(cudaMemcpyAsync(loss, d_loss, sizeof(double), cudaMemcpyDeviceToHost, s));
+  }
+  MBD_CUDA(cudaMemcpyAsync(S_pred, w.S, sizeof(float) * 9 * M, cudaMemcpyDeviceToHost, s));
+  MBD_CUDA(cudaStreamSynchronize(s));
+  return cuda_status(cudaGetLastError());
+}
+
+}  // extern "C"

@@ -60,6 +60,8 @@ struct GeomPlan {
   std::vector<int> diff_is_zero;        // 1 for the zero difference
   std::vector<int> place_offset;        // CSR offsets into place_rc/place_cc, per difference
   std::vector<int> place_rc, place_cc;  // cell indices (k*SLj*SLi + j*SLi + i)
+  int vac[3] = {0, 0, 0};     // vacuum axes (no images along them)
+  std::vector<int> species;   // learned warm start: 0 H, 1 C, 2 N, 3 O, 4 other
   // per-atom free-atom data
   std::vector<double> alpha0, c6free, r0, hirsh;
   std::vector<double> coords;           // 3N, xyz per atom (bohr)

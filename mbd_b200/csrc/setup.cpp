@@ -161,9 +161,12 @@ int build_plan(const mbd_geom& g, GeomPlan* p) {
   p->r0.resize(N);
   p->hirsh.assign(g.hirshfeld, g.hirshfeld + N);
   p->coords.assign(g.coords_bohr, g.coords_bohr + 3 * N);
+  for (int k = 0; k < 3; ++k) p->vac[k] = (g.n_periodic != 0 && g.vacuum[k]) ? 1 : 0;
+  p->species.resize(N);
   for (int i = 0; i < N; ++i) {
     VdwParam v;
     if (!vdw_param(g.z[i], &v)) return MBD_ERR_UNKNOWN_ELEMENT;
+    p->species[i] = g.z[i] == 1 ? 0 : g.z[i] == 6 ? 1 : g.z[i] == 7 ? 2 : g.z[i] == 8 ? 3 : 4;
     p->alpha0[i] = v.alpha0;
     p->c6free[i] = v.c6;
     p->r0[i] = v.r0;

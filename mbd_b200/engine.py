@@ -25,6 +25,7 @@ ERRORS = {
     1: "MBD_ERR_ARG", 2: "MBD_ERR_UNKNOWN_ELEMENT", 3: "MBD_ERR_RELAY_NOT_SPD",
     4: "MBD_ERR_NONPOSITIVE_ALPHA", 5: "MBD_ERR_EIGENSOLVER", 6: "MBD_ERR_DEVICE",
     7: "MBD_ERR_TIMEOUT", 8: "MBD_ERR_OUT_OF_MEMORY", 9: "MBD_ERR_REFINEMENT", 10: "MBD_ERR_NOT_BUILT",
+    11: "MBD_ERR_TOO_LARGE", 12: "MBD_ERR_NO_NETWORK",
 }
 MODES = {"plain": 0, "plain_fp64": 0, "mixed": 1, "mixed_learned": 2, "learned": 2}
 N_FREQ = 21
@@ -34,7 +35,9 @@ EXPORTED = [
     "mbd_rsscs_create", "mbd_rsscs_destroy", "mbd_rsscs_energy", "mbd_rsscs_energy_batch",
     "mbd_rsscs_upload", "mbd_rsscs_compute", "mbd_rsscs_download", "mbd_rsscs_element_z",
     "mbd_rsscs_strerror", "mbd_rsscs_vdw_params", "mbd_rsscs_last_timings", "mbd_rsscs_last_stats",
-    "mbd_rsscs_stream", "mbd_rsscs_eigvalsh",
+    "mbd_rsscs_stream", "mbd_rsscs_eigvalsh", "mbd_rsscs_eigvalsh_noalloc",
+    "mbd_rsscs_learned_param_count", "mbd_rsscs_learned_train", "mbd_rsscs_learned_get_params",
+    "mbd_rsscs_learned_set_params", "mbd_rsscs_learned_use_network", "mbd_rsscs_learned_eval",
 ]
 
 
@@ -118,6 +121,22 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
     lib.mbd_rsscs_eigvalsh.argtypes = [vp, ctypes.POINTER(ctypes.c_double), ctypes.c_int, ctypes.c_int,
                                        ctypes.POINTER(ctypes.c_double)]
     lib.mbd_rsscs_eigvalsh.restype = ctypes.c_int
+    fp = ctypes.POINTER(ctypes.c_float)
+    ip = ctypes.POINTER(ctypes.c_int)
+    dp = ctypes.POINTER(ctypes.c_double)
+    lib.mbd_rsscs_learned_param_count.argtypes = []
+    lib.mbd_rsscs_learned_param_count.restype = ctypes.c_int
+    lib.mbd_rsscs_learned_train.argtypes = [vp, ctypes.c_int, ctypes.POINTER(CGeom), ctypes.c_int, ctypes.c_double,
+                                            ctypes.c_int, dp]
+    lib.mbd_rsscs_learned_train.restype = ctypes.c_int
+    lib.mbd_rsscs_learned_get_params.argtypes = [vp, fp, ctypes.c_int]
+    lib.mbd_rsscs_learned_get_params.restype = ctypes.c_int
+    lib.mbd_rsscs_learned_set_params.argtypes = [vp, fp, ctypes.c_int]
+    lib.mbd_rsscs_learned_set_params.restype = ctypes.c_int
+    lib.mbd_rsscs_learned_use_network.argtypes = [vp, ctypes.c_int]
+    lib.mbd_rsscs_learned_use_network.restype = ctypes.c_int
+    lib.mbd_rsscs_learned_eval.argtypes = [vp, fp, ctypes.c_int, ctypes.c_int, ip, ip, fp, fp, fp, fp, fp, dp]
+    lib.mbd_rsscs_learned_eval.restype = ctypes.c_int
     _LIB = lib
     return lib
 
@@ -233,7 +252,7 @@ class Engine:
         rarr = (CResult * len(packs))(*[p.result_struct() for p in packs])
         code = self.lib.mbd_rsscs_energy_batch(self.ctx, len(packs), garr, MODES[mode], rarr)
         res = [p.to_result(rarr[i]) for i, p in enumerate(packs)]
-        if check and code != MBD_OK and all(r.status == code for r in res) and code in (6, 8, 10, 1):
+        if check and code != MBD_OK and all(r.status == code for r in res) and code in (6, 8, 10, 1, 12):
             raise MbdError(code, strerror(code))
         return res
 
@@ -262,6 +281,68 @@ class Engine:
         if code != MBD_OK:
             raise MbdError(code, strerror(code))
         return w
+
+    # -- learned warm start (MBD_MODE_MIXED_LEARNED) --------------------------
+    def learned_train(self, geos, sts, epochs: int = 20, lr: float = 2e-3, seed: int = 0) -> np.ndarray:
+        """Trains the context's network on direct relay solutions of the
+        given geometries (replaces the uploaded batch); returns the mean
+        loss of every epoch."""
+        packs = [_Packed(g, s) for g, s in zip(geos, sts)]
+        garr = (CGeom * len(packs))(*[p.geom for p in packs])
+        loss = np.zeros(epochs)
+        code = self.lib.mbd_rsscs_learned_train(self.ctx, len(packs), garr, int(epochs), float(lr), int(seed),
+                                                loss.ctypes.data_as(ctypes.POINTER(ctypes.c_double)))
+        self._packed = []
+        if code != MBD_OK:
+            raise MbdError(code, strerror(code))
+        return loss
+
+    def learned_params(self) -> np.ndarray:
+        n = self.lib.mbd_rsscs_learned_param_count()
+        out = np.zeros(n, dtype=np.float32)
+        code = self.lib.mbd_rsscs_learned_get_params(self.ctx, out.ctypes.data_as(ctypes.POINTER(ctypes.c_float)), n)
+        if code != MBD_OK:
+            raise MbdError(code, strerror(code))
+        return out
+
+    def set_learned_params(self, params) -> None:
+        p = np.ascontiguousarray(params, dtype=np.float32)
+        code = self.lib.mbd_rsscs_learned_set_params(self.ctx, p.ctypes.data_as(ctypes.POINTER(ctypes.c_float)),
+                                                     p.size)
+        if code != MBD_OK:
+            raise MbdError(code, strerror(code))
+
+    def use_network(self, on: bool) -> None:
+        self.lib.mbd_rsscs_learned_use_network(self.ctx, 1 if on else 0)
+
+    def learned_eval(self, params, n_atoms, n_freq, off, nbr, dvec, x, S_true=None):
+        """The network's kernels on explicit inputs: returns (S_pred (M,3,3),
+        grad or None, loss or None)."""
+        f32 = lambda a: np.ascontiguousarray(a, dtype=np.float32)
+        i32 = lambda a: np.ascontiguousarray(a, dtype=np.int32)
+        P, dv, xx = f32(params), f32(dvec), f32(x)
+        o, nb = i32(off), i32(nbr)
+        M = n_atoms * n_freq
+        S = np.zeros((M, 9), dtype=np.float32)
+        fp = ctypes.POINTER(ctypes.c_float)
+        ip = ctypes.POINTER(ctypes.c_int)
+        grad = loss = None
+        st_ptr = g_ptr = None
+        l_ptr = None
+        if S_true is not None:
+            St = f32(np.asarray(S_true).reshape(M, 9))
+            grad = np.zeros(P.size, dtype=np.float32)
+            lbuf = np.zeros(1)
+            st_ptr, g_ptr = St.ctypes.data_as(fp), grad.ctypes.data_as(fp)
+            l_ptr = lbuf.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+        code = self.lib.mbd_rsscs_learned_eval(self.ctx, P.ctypes.data_as(fp), int(n_atoms), int(n_freq),
+                                               o.ctypes.data_as(ip), nb.ctypes.data_as(ip), dv.ctypes.data_as(fp),
+                                               xx.ctypes.data_as(fp), st_ptr, S.ctypes.data_as(fp), g_ptr, l_ptr)
+        if code != MBD_OK:
+            raise MbdError(code, strerror(code))
+        if S_true is not None:
+            loss = float(lbuf[0])
+        return S.reshape(M, 3, 3), grad, loss
 
     def stats(self) -> dict:
         buf = (ctypes.c_double * 3)()

@@ -56,7 +56,8 @@ def pack(d):
 
 
 def init_params(seed=0):
-    """Deterministic initialisation (the engine draws the same numbers)."""
+    """Deterministic initialisation of the same shape as the engine's (whose
+    own generator draws different numbers from the same distributions)."""
     rng = np.random.default_rng(seed)
     d = {}
     for name, shp in LAYOUT:
@@ -80,26 +81,47 @@ def rbf(r):
     return np.exp(-0.5 * ((r[:, None] - mu[None, :]) / width) ** 2) * fc[:, None]
 
 
-def neighbours(coords_bohr, lattice_bohr=None):
-    """CSR neighbour lists within the cut-off, i != j (minimum image for a
-    periodic cell whose perpendicular widths exceed twice the cut-off).
-    lattice_bohr rows are the cell vectors.  Returns off, nbr, d (d = r_j - r_i)."""
+def neighbours(coords_bohr, lattice_bohr=None, vacuum=(False, False, False)):
+    """CSR neighbour lists within the cut-off: every image r_j + t (t a lattice
+    translation along non-vacuum axes) within the cut-off of atom i, except
+    atom i itself at t = 0.  An atom can meet another atom, or itself, through
+    several images when the cell is narrower than twice the cut-off.
+    lattice_bohr rows are the cell vectors.  Returns off, nbr, d
+    (d = r_j + t - r_i), edges of atom i in ascending (t, j) order."""
     n = len(coords_bohr)
-    diff = coords_bohr[None, :, :] - coords_bohr[:, None, :]
+    shifts = [np.zeros(3)]
     if lattice_bohr is not None:
-        inv = np.linalg.inv(lattice_bohr)
-        frac = diff @ inv
-        frac -= np.round(frac)
-        diff = frac @ lattice_bohr
-    r = np.linalg.norm(diff, axis=-1)
-    mask = (r < CUTOFF_BOHR) & ~np.eye(n, dtype=bool)
+        a = np.asarray(lattice_bohr, dtype=float)
+        vol = abs(np.linalg.det(a))
+        rng = []
+        for k in range(3):
+            if vacuum[k]:
+                rng.append(0)
+                continue
+            area = np.linalg.norm(np.cross(a[(k + 1) % 3], a[(k + 2) % 3]))
+            rng.append(int(np.ceil(CUTOFF_BOHR / (vol / area))) + 1)
+        shifts = [i * a[0] + j * a[1] + k * a[2]
+                  for i in range(-rng[0], rng[0] + 1) for j in range(-rng[1], rng[1] + 1)
+                  for k in range(-rng[2], rng[2] + 1)]
+    nbr, dv, cnt = [], [], np.zeros(n, dtype=np.int64)
+    per_atom = [[] for _ in range(n)]
+    for t in shifts:
+        diff = coords_bohr[None, :, :] + t[None, None, :] - coords_bohr[:, None, :]
+        r = np.linalg.norm(diff, axis=-1)
+        mask = (r < CUTOFF_BOHR) & (r > 1e-6)
+        for i in range(n):
+            js = np.nonzero(mask[i])[0]
+            if len(js):
+                per_atom[i].append((js, diff[i, js]))
     off = np.zeros(n + 1, dtype=np.int64)
-    nbr, dv = [], []
     for i in range(n):
-        js = np.nonzero(mask[i])[0]
-        nbr.append(js)
-        dv.append(diff[i, js])
-        off[i + 1] = off[i] + len(js)
+        for js, d in per_atom[i]:
+            nbr.append(js)
+            dv.append(d)
+            cnt[i] += len(js)
+        off[i + 1] = off[i] + cnt[i]
+    if not nbr:
+        return off, np.zeros(0, dtype=np.int64), np.zeros((0, 3))
     return off, np.concatenate(nbr).astype(np.int64), np.concatenate(dv).reshape(-1, 3)
 
 
