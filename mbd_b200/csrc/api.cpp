@@ -334,7 +334,7 @@ void drop_graphs(mbd_ctx* ctx) {
 // Relay and CFDM stages of geometry gi on its slot's stream: per-atom
 // frequency table, relay tensors, relay factorisation and solve (plain or
 // mixed), screened polarizabilities and C6, CFDM Hamiltonian into gd->hmat.
-int run_front(mbd_ctx* ctx, GeomDev* gd, int gi, int mode) {
+int run_front(mbd_ctx* ctx, GeomDev* gd, int gi, int mode, bool relay_only) {
   const GeomPlan& p = gd->plan;
   RelaySlot& sl = *ctx->slots[gd->slot];
   cudaStream_t s = sl.stream;
@@ -397,6 +397,10 @@ int run_front(mbd_ctx* ctx, GeomDev* gd, int gi, int mode) {
   launch_relay_post(ea, ctx->weights_dev, s);
   ctx->launches += 2;
   mark(4);
+  if (relay_only) {
+    mark(5);
+    return cuda_status(cudaGetLastError());
+  }
   // 5. CFDM Hamiltonian (lower blocks; the rest of the matrix is never read)
   CfdmBuildArgs cb{N, p.nsl, p.ldH, gd->coords, gd->omega, gd->alpha_eff, gd->rvdw_eff, gd->cfdm_shifts,
                    (int)p.cfdm_shifts.size() / 3, gd->diff_shift, gd->diff_is_zero, gd->place_offset,
@@ -484,7 +488,7 @@ int plan_slots(mbd_ctx* ctx) {
 
 // Plain-path slot buffers, per-geometry Hamiltonians, the tridiagonal plan and
 // the device job tables of the uploaded batch.
-int prepare_batch(mbd_ctx* ctx) {
+int prepare_batch(mbd_ctx* ctx, bool eigen) {
   drop_graphs(ctx);
   ctx->order.clear();
   for (size_t g = 0; g < ctx->geoms.size(); ++g)
@@ -493,7 +497,7 @@ int prepare_batch(mbd_ctx* ctx) {
                    [&](int a, int b) { return ctx->geoms[a]->plan.n > ctx->geoms[b]->plan.n; });
   for (int g : ctx->order) {
     const GeomPlan& p = ctx->geoms[g]->plan;
-    MBD_CUDA(ctx->geoms[g]->hmat.reserve(sizeof(double) * (size_t)p.nH * p.ldH));
+    if (eigen) MBD_CUDA(ctx->geoms[g]->hmat.reserve(sizeof(double) * (size_t)p.nH * p.ldH));
   }
   const size_t nev = ctx->geoms.size() * kGeomEvents;
   while (ctx->events.size() < nev) {
@@ -522,6 +526,10 @@ int prepare_batch(mbd_ctx* ctx) {
     MBD_CUDA(sl.relay64.reserve(relay));
     MBD_CUDA(sl.linv.reserve(linv));
     MBD_CUDA(sl.rhs.reserve(rhs));
+  }
+  if (!eigen) {
+    ctx->n_trd_groups = ctx->trd_total_ctas = ctx->n_eig_jobs = ctx->n_eig_batch = 0;
+    return MBD_OK;
   }
   // tridiagonal plan
   std::vector<int> sizes;
@@ -761,6 +769,16 @@ void mbd_rsscs_destroy(mbd_ctx* ctx) {
 
 int mbd_rsscs_upload(mbd_ctx* ctx, int n_geom, const mbd_geom* geoms) {
   if (!ctx || n_geom < 1 || !geoms) return MBD_ERR_ARG;
+  return upload_batch(ctx, n_geom, geoms, true);
+}
+
+}  // extern "C"
+
+namespace mbd {
+
+// Uploads a batch; eigen = false prepares only the relay stages (training
+// batches: no CFDM Hamiltonians, no eigen plan, not computable).
+int upload_batch(mbd_ctx* ctx, int n_geom, const mbd_geom* geoms, bool eigen) {
   MBD_CUDA(cudaSetDevice(ctx->device));
   // buffers of the previous batch may still be in use by its kernels
   MBD_CUDA(cudaDeviceSynchronize());
@@ -775,11 +793,15 @@ int mbd_rsscs_upload(mbd_ctx* ctx, int n_geom, const mbd_geom* geoms) {
     if (st != MBD_OK && first == MBD_OK) first = st;
     if (st == MBD_ERR_OUT_OF_MEMORY || st == MBD_ERR_DEVICE) return st;
   }
-  int st = prepare_batch(ctx);
+  int st = prepare_batch(ctx, eigen);
   if (st != MBD_OK) return st;
-  ctx->have_batch = true;
+  ctx->have_batch = eigen;
   return first;
 }
+
+}  // namespace mbd
+
+extern "C" {
 
 int mbd_rsscs_compute(mbd_ctx* ctx, int mode) {
   if (!ctx || !ctx->have_batch) return MBD_ERR_ARG;

@@ -175,7 +175,8 @@ inline cudaError_t zero_ordered(const mbd_ctx* ctx, void* dst, size_t bytes) {
 
 // api.cpp
 void drop_graphs(mbd_ctx* ctx);
-int run_front(mbd_ctx* ctx, GeomDev* gd, int gi, int mode);
+int run_front(mbd_ctx* ctx, GeomDev* gd, int gi, int mode, bool relay_only = false);
+int upload_batch(mbd_ctx* ctx, int n_geom, const mbd_geom* geoms, bool eigen);
 // learn.cpp
 int reserve_learned(mbd_ctx* ctx);
 int relay_learned(mbd_ctx* ctx, GeomDev* gd, RelaySlot& sl, size_t mstride, cudaEvent_t ev_net, double** X_out);

@@ -21,7 +21,7 @@
 namespace mbd {
 namespace {
 
-constexpr int kCgMaxIters = 80;
+constexpr int kCgMaxIters = 64;
 constexpr double kCgTol = 3e-11;   // relative residual the iteration stops at (gate: 1e-10)
 
 // Neighbour lists within the network's cut-off, including periodic images
@@ -345,7 +345,8 @@ int mbd_rsscs_learned_use_network(mbd_ctx* ctx, int on) {
 int mbd_rsscs_learned_train(mbd_ctx* ctx, int n_geom, const mbd_geom* geoms, int epochs, double lr, int seed,
                             double* epoch_loss) {
   if (!ctx || !geoms || n_geom < 1 || epochs < 1 || !(lr > 0.0)) return MBD_ERR_ARG;
-  int st = mbd_rsscs_upload(ctx, n_geom, geoms);
+  MBD_CUDA(cudaSetDevice(ctx->device));
+  int st = upload_batch(ctx, n_geom, geoms, false);
   if (st == MBD_ERR_OUT_OF_MEMORY || st == MBD_ERR_DEVICE || st == MBD_ERR_ARG) return st;
   if (ctx->order.empty()) return st != MBD_OK ? st : MBD_ERR_ARG;
   st = reserve_learned(ctx);
@@ -367,7 +368,7 @@ int mbd_rsscs_learned_train(mbd_ctx* ctx, int n_geom, const mbd_geom* geoms, int
     GeomDev* gd = ctx->geoms[g].get();
     const GeomPlan& p = gd->plan;
     RelaySlot& sl = *ctx->slots[gd->slot];
-    st = run_front(ctx, gd, g, MBD_MODE_PLAIN_FP64);
+    st = run_front(ctx, gd, g, MBD_MODE_PLAIN_FP64, true);
     if (st != MBD_OK) return st;
     const size_t ys = (size_t)p.n * 3;
     const double* X = sl.rhs.as<double>() + 2 * kNFreq * ys;

@@ -107,7 +107,7 @@ def test_cg_without_network_matches_plain(engine):
         assert abs(a.energy - b.energy) <= E_TOL
         assert abs(a.c6_mol - b.c6_mol) <= C6_RTOL * abs(b.c6_mol)
         np.testing.assert_allclose(a.alpha_iw, b.alpha_iw, rtol=1e-8)
-        assert 0 < a.refine_iters < 80
+        assert 0 < a.refine_iters < 64
         assert a.err_est[0] <= 1e-10
 
 
