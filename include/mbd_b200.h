@@ -161,13 +161,17 @@ int mbd_rsscs_vdw_params(int z, double* alpha0, double* c6, double* r0);
  * factorisation, [4] relay solve/refinement + epilogue, [5] CFDM build,
  * [6] tridiagonal reduction, [7] eigenvalues + energy.  Stages [1]-[5] run
  * per geometry, several geometries at once on separate streams, and are
- * summed over the geometries (their sum can exceed [0]); [6] and [7] are
- * single batch-wide launches.  n must be >= 8. */
+ * summed over the geometries (their sum can exceed [0]).  [6] is the sum over
+ * geometries of the dense -> band reduction (also per geometry, on the same
+ * streams) plus the batch-wide band -> tridiagonal launch; [7] is batch-wide.
+ * n must be >= 8. */
 int mbd_rsscs_last_timings(mbd_ctx* ctx, double* ms, int n);
 
 /* Counters of the last upload/compute/download: [0] kernel launches issued
  * by mbd_rsscs_compute, [1] host->device bytes copied by mbd_rsscs_upload,
- * [2] device->host bytes copied by mbd_rsscs_download.  n must be >= 3. */
+ * [2] device->host bytes copied by mbd_rsscs_download, [3] (n >= 4) 1 when
+ * the last compute replayed the batch's captured CUDA graph, 0 when it
+ * launched the kernels one by one.  n must be >= 3. */
 int mbd_rsscs_last_stats(mbd_ctx* ctx, double* out, int n);
 
 /* The CUDA stream (cudaStream_t) every kernel of this context runs on, so a

@@ -331,6 +331,26 @@ void drop_graphs(mbd_ctx* ctx) {
     }
 }
 
+int band_to_tridiag_single(mbd_ctx* ctx, double* Br, int n, double* d, double* e, DevBuf& scratch, cudaStream_t s) {
+  std::vector<SweepItem> items;
+  for (int i = 0; i + 3 <= n; ++i) items.push_back(SweepItem{0, i, i - 1, 0});
+  const BandJob job{Br, n, d, e};
+  const size_t b_job = bytes_of<BandJob>(1), b_it = bytes_of<SweepItem>(std::max<size_t>(items.size(), 1));
+  const size_t b_pr = bytes_of<int>(std::max<size_t>(items.size(), 1));
+  MBD_CUDA(scratch.reserve(b_job + b_it + b_pr));
+  char* base = scratch.as<char>();
+  std::vector<char> host(b_job + b_it, 0);
+  std::memcpy(host.data(), &job, sizeof(job));
+  std::memcpy(host.data() + b_job, items.data(), sizeof(SweepItem) * items.size());
+  MBD_CUDA(cudaMemcpyAsync(base, host.data(), host.size(), cudaMemcpyHostToDevice, s));
+  MBD_CUDA(cudaStreamSynchronize(s));   // the pageable source must outlive the copy
+  MBD_CUDA(launch_sb2st(reinterpret_cast<BandJob*>(base), 1, reinterpret_cast<SweepItem*>(base + b_job),
+                        (int)items.size(), reinterpret_cast<int*>(base + b_job + b_it), ctx->err_flag,
+                        ctx->num_sms, n, s));
+  ctx->launches += 3;
+  return MBD_OK;
+}
+
 // Relay and CFDM stages of geometry gi on its slot's stream: per-atom
 // frequency table, relay tensors, relay factorisation and solve (plain or
 // mixed), screened polarizabilities and C6, CFDM Hamiltonian into gd->hmat.
@@ -399,6 +419,7 @@ int run_front(mbd_ctx* ctx, GeomDev* gd, int gi, int mode, bool relay_only) {
   mark(4);
   if (relay_only) {
     mark(5);
+    mark(6);
     return cuda_status(cudaGetLastError());
   }
   // 5. CFDM Hamiltonian (lower blocks; the rest of the matrix is never read)
@@ -409,24 +430,38 @@ int run_front(mbd_ctx* ctx, GeomDev* gd, int gi, int mode, bool relay_only) {
   launch_cfdm_build(cb, s);
   ctx->launches += 1;
   mark(5);
+  // 6. dense -> band (stage 1 of the two-stage tridiagonalisation)
+  if (two_stage(ctx, p.nH)) {
+    MBD_CUDA(launch_sy2sb(gd->hmat.as<double>(), p.ldH, p.nH, sl.trd_ws.as<double>(), gd->band.as<double>(),
+                          ctx->num_sms, s));
+    ctx->launches += sy2sb_launches(p.nH);
+  }
+  mark(6);
   return cuda_status(cudaGetLastError());
 }
 
 namespace {
 
-// Eigen stages of one geometry on stream s with its own tridiagonal launch
-// (the residual-gate fallback of download).
+// Eigen stages of one geometry on stream s with its own launches (the
+// residual-gate fallback of download; run_front has reduced a two-stage
+// geometry's Hamiltonian to its band already).
 int run_tail_single(mbd_ctx* ctx, GeomDev* gd, cudaStream_t s) {
   const GeomPlan& p = gd->plan;
-  TridiagJob job{gd->hmat.as<double>(), p.nH, p.ldH, gd->d, gd->e};
-  MBD_CUDA(cudaMemcpyAsync(ctx->job_dev, &job, sizeof(job), cudaMemcpyHostToDevice, s));
-  const int G = tridiag_group_ctas(ctx, p.nH);
-  const size_t wsb = tridiag_workspace_bytes(p.nH, G);
-  MBD_CUDA(ctx->fb_ws.reserve(wsb));
-  MBD_CUDA(launch_tridiag(ctx->job_dev, 1, 1, G, ctx->fb_ws.p, wsb, p.nH, ctx->err_flag, s));
+  if (two_stage(ctx, p.nH)) {
+    int st = band_to_tridiag_single(ctx, gd->band.as<double>(), p.nH, gd->d, gd->e, ctx->fb_ws, s);
+    if (st != MBD_OK) return st;
+  } else {
+    TridiagJob job{gd->hmat.as<double>(), p.nH, p.ldH, gd->d, gd->e};
+    MBD_CUDA(cudaMemcpyAsync(ctx->job_dev, &job, sizeof(job), cudaMemcpyHostToDevice, s));
+    const int G = tridiag_group_ctas(ctx, p.nH);
+    const size_t wsb = tridiag_workspace_bytes(p.nH, G);
+    MBD_CUDA(ctx->fb_ws.reserve(wsb));
+    MBD_CUDA(launch_tridiag(ctx->job_dev, 1, 1, G, ctx->fb_ws.p, wsb, p.nH, ctx->err_flag, s));
+    ctx->launches += 1;
+  }
   launch_tridiag_eigenvalues(gd->d, gd->e, p.nH, gd->ev, s);
   launch_energy(gd->ev, p.nH, p.nsl, gd->scalars, gd->energy, s);
-  ctx->launches += 3;
+  ctx->launches += 2;
   return cuda_status(cudaGetLastError());
 }
 
@@ -497,7 +532,9 @@ int prepare_batch(mbd_ctx* ctx, bool eigen) {
                    [&](int a, int b) { return ctx->geoms[a]->plan.n > ctx->geoms[b]->plan.n; });
   for (int g : ctx->order) {
     const GeomPlan& p = ctx->geoms[g]->plan;
-    if (eigen) MBD_CUDA(ctx->geoms[g]->hmat.reserve(sizeof(double) * (size_t)p.nH * p.ldH));
+    if (!eigen) continue;
+    MBD_CUDA(ctx->geoms[g]->hmat.reserve(sizeof(double) * (size_t)p.nH * p.ldH));
+    if (two_stage(ctx, p.nH)) MBD_CUDA(ctx->geoms[g]->band.reserve(sizeof(double) * (size_t)p.nH * kBandLd));
   }
   const size_t nev = ctx->geoms.size() * kGeomEvents;
   while (ctx->events.size() < nev) {
@@ -526,14 +563,25 @@ int prepare_batch(mbd_ctx* ctx, bool eigen) {
     MBD_CUDA(sl.relay64.reserve(relay));
     MBD_CUDA(sl.linv.reserve(linv));
     MBD_CUDA(sl.rhs.reserve(rhs));
+    if (eigen) {
+      size_t tw = 0;
+      for (int g : ctx->order)
+        if (ctx->geoms[g]->slot == s && two_stage(ctx, ctx->geoms[g]->plan.nH))
+          tw = std::max(tw, sizeof(double) * sy2sb_workspace_doubles(ctx->geoms[g]->plan.nH));
+      MBD_CUDA(sl.trd_ws.reserve(tw));
+    }
   }
   if (!eigen) {
     ctx->n_trd_groups = ctx->trd_total_ctas = ctx->n_eig_jobs = ctx->n_eig_batch = 0;
     return MBD_OK;
   }
-  // tridiagonal plan
-  std::vector<int> sizes;
-  for (int g : ctx->order) sizes.push_back(ctx->geoms[g]->plan.nH);
+  // one-stage tridiagonal plan for the matrices too large for the two-stage path
+  std::vector<int> sizes, one_stage;
+  for (int g : ctx->order)
+    if (!two_stage(ctx, ctx->geoms[g]->plan.nH)) {
+      sizes.push_back(ctx->geoms[g]->plan.nH);
+      one_stage.push_back(g);
+    }
   const TrdPlan tp = plan_tridiag(sizes, ctx->num_sms * ctx->trd_ctas_per_sm);
   std::vector<TridiagJob> jobs;
   std::vector<TridiagGroup> groups;
@@ -546,7 +594,7 @@ int prepare_batch(mbd_ctx* ctx, bool eigen) {
     gr.job_begin = (int)jobs.size();
     gr.nmax = 1;
     for (int j : tp.bins[b]) {
-      GeomDev* gd = ctx->geoms[ctx->order[j]].get();
+      GeomDev* gd = ctx->geoms[one_stage[j]].get();
       const GeomPlan& p = gd->plan;
       jobs.push_back(TridiagJob{gd->hmat.as<double>(), p.nH, p.ldH, gd->d, gd->e});
       gr.nmax = std::max(gr.nmax, p.nH);
@@ -577,18 +625,47 @@ int prepare_batch(mbd_ctx* ctx, bool eigen) {
     }
   ctx->n_eig_jobs = (int)eig.size();
   ctx->n_eig_batch = ctx->n_eig_jobs - (int)ctx->eig_single.size();
+  // band -> tridiagonal: one job per two-stage matrix, (job, sweep) items
+  // ordered by sweep then job, each pointing at its job's previous sweep
+  std::vector<BandJob> bjobs;
+  ctx->band_max_n = 0;
+  for (int g : ctx->order) {
+    GeomDev* gd = ctx->geoms[g].get();
+    if (!two_stage(ctx, gd->plan.nH)) continue;
+    bjobs.push_back(BandJob{gd->band.as<double>(), gd->plan.nH, gd->d, gd->e});
+    ctx->band_max_n = std::max(ctx->band_max_n, gd->plan.nH);
+  }
+  std::vector<SweepItem> items;
+  {
+    std::vector<int> last(bjobs.size(), -1);
+    for (int i = 0; i + 3 <= ctx->band_max_n; ++i)
+      for (size_t j = 0; j < bjobs.size(); ++j) {
+        if (i + 3 > bjobs[j].n) continue;
+        items.push_back(SweepItem{(int)j, i, last[j], 0});
+        last[j] = (int)items.size() - 1;
+      }
+  }
+  ctx->n_band_jobs = (int)bjobs.size();
+  ctx->n_sweep_items = (int)items.size();
+  MBD_CUDA(ctx->sweep_progress.reserve(sizeof(int) * std::max<size_t>(items.size(), 1)));
   const size_t b_jobs = bytes_of<TridiagJob>(jobs.size());
   const size_t b_groups = bytes_of<TridiagGroup>(groups.size());
   const size_t b_eig = bytes_of<EigJob>(eig.size());
-  MBD_CUDA(ctx->tables.reserve(b_jobs + b_groups + b_eig));
+  const size_t b_bj = bytes_of<BandJob>(bjobs.size());
+  const size_t b_it = bytes_of<SweepItem>(items.size());
+  MBD_CUDA(ctx->tables.reserve(b_jobs + b_groups + b_eig + b_bj + b_it));
   char* base = ctx->tables.as<char>();
   ctx->trd_jobs = reinterpret_cast<TridiagJob*>(base);
   ctx->trd_groups = reinterpret_cast<TridiagGroup*>(base + b_jobs);
   ctx->eig_jobs = reinterpret_cast<EigJob*>(base + b_jobs + b_groups);
-  std::vector<char> host(b_jobs + b_groups + b_eig, 0);
+  ctx->band_jobs = reinterpret_cast<BandJob*>(base + b_jobs + b_groups + b_eig);
+  ctx->sweep_items = reinterpret_cast<SweepItem*>(base + b_jobs + b_groups + b_eig + b_bj);
+  std::vector<char> host(b_jobs + b_groups + b_eig + b_bj + b_it, 0);
   std::memcpy(host.data(), jobs.data(), sizeof(TridiagJob) * jobs.size());
   std::memcpy(host.data() + b_jobs, groups.data(), sizeof(TridiagGroup) * groups.size());
   std::memcpy(host.data() + b_jobs + b_groups, eig.data(), sizeof(EigJob) * eig.size());
+  std::memcpy(host.data() + b_jobs + b_groups + b_eig, bjobs.data(), sizeof(BandJob) * bjobs.size());
+  std::memcpy(host.data() + b_jobs + b_groups + b_eig + b_bj, items.data(), sizeof(SweepItem) * items.size());
   MBD_CUDA(h2d_ordered(ctx, base, host.data(), host.size()));
   ctx->h2d_bytes += (double)host.size();
   return MBD_OK;
@@ -660,10 +737,18 @@ int enqueue_batch(mbd_ctx* ctx, int mode) {
     MBD_CUDA(cudaStreamWaitEvent(s, ctx->slots[k]->done, 0));
   }
   record_timing(ctx, ctx->bev[1], s);
-  // every Hamiltonian to tridiagonal form in one cooperative launch
-  MBD_CUDA(launch_tridiag_groups(ctx->trd_jobs, ctx->trd_groups, ctx->n_trd_groups, ctx->trd_total_ctas,
-                                 ctx->tridiag_ws.p, ctx->err_flag, s));
-  ctx->launches += 2;
+  // bands -> tridiagonal in one persistent launch; matrices too large for the
+  // two-stage path in one grouped one-stage launch
+  if (ctx->n_trd_groups > 0) {
+    MBD_CUDA(launch_tridiag_groups(ctx->trd_jobs, ctx->trd_groups, ctx->n_trd_groups, ctx->trd_total_ctas,
+                                   ctx->tridiag_ws.p, ctx->err_flag, s));
+    ctx->launches += 2;
+  }
+  if (ctx->n_band_jobs > 0) {
+    MBD_CUDA(launch_sb2st(ctx->band_jobs, ctx->n_band_jobs, ctx->sweep_items, ctx->n_sweep_items,
+                          ctx->sweep_progress.as<int>(), ctx->err_flag, ctx->num_sms, ctx->band_max_n, s));
+    ctx->launches += 3;
+  }
   record_timing(ctx, ctx->bev[2], s);
   // eigenvalues and energies
   launch_eigen_batch(ctx->eig_jobs, ctx->n_eig_batch, ctx->eig_batch_max_n, s);
@@ -737,6 +822,15 @@ int mbd_rsscs_create(mbd_ctx** out, int device) {
   MBD_CUDA(init_eigval_attributes());
   MBD_CUDA(init_tc3_attributes());
   MBD_CUDA(init_mixed_attributes());
+  MBD_CUDA(init_sy2sb_attributes());
+  {
+    // the two-stage tridiagonalisation serves the batch pipeline only when
+    // MBD_B200_TWO_STAGE=1 (the standalone eigenvalue call always uses it)
+    const char* ts = std::getenv("MBD_B200_TWO_STAGE");
+    ctx->two_stage_max_n = sy2sb_max_n();
+    ctx->two_stage_batch = ts && ts[0] == '1';
+  }
+  MBD_CUDA(init_sb2st_attributes());
   ctx->trd_ctas_per_sm = std::max(1, tridiag_max_ctas_per_sm());
   MBD_CUDA(ctx->misc.reserve(4096));
   char* m = ctx->misc.as<char>();
@@ -820,8 +914,10 @@ int mbd_rsscs_compute(mbd_ctx* ctx, int mode) {
   if (ctx->use_graphs && !ctx->graph[mode] && !capture_batch(ctx, mode)) ctx->use_graphs = false;
   if (ctx->use_graphs && ctx->graph[mode]) {
     ctx->launches = ctx->graph_launches[mode];
+    ctx->graph_replayed = true;
     return cuda_status(cudaGraphLaunch(ctx->graph[mode], ctx->stream));
   }
+  ctx->graph_replayed = false;
   return enqueue_batch(ctx, mode);
 }
 
@@ -843,7 +939,7 @@ int mbd_rsscs_download(mbd_ctx* ctx, mbd_result* out) {
   ctx->last_ms[Stage::kEig] = elapsed(ctx->bev[2], ctx->bev[3]);
   for (int g : ctx->order) {
     cudaEvent_t* evs = ctx->events.data() + (size_t)g * kGeomEvents;
-    for (int k = 1; k < kGeomEvents; ++k) ctx->last_ms[k] += elapsed(evs[k - 1], evs[k]);
+    for (int k = 1; k < kGeomEvents; ++k) ctx->last_ms[k] += elapsed(evs[k - 1], evs[k]);   // [6]: dense -> band
   }
   ctx->d2h_bytes = sizeof(int);
   int first = MBD_OK;
@@ -959,21 +1055,31 @@ int mbd_rsscs_eigvalsh(mbd_ctx* ctx, const double* H, int n, int ld, double* w) 
   MBD_CUDA(cudaSetDevice(ctx->device));
   cudaStream_t s = ctx->stream;
   const int ldp = round_up(n, 32);
-  const int G = tridiag_group_ctas(ctx, n);
-  const size_t wsb = tridiag_workspace_bytes(n, G);
   MBD_CUDA(ctx->eig_a.reserve(sizeof(double) * (size_t)n * ldp));
   MBD_CUDA(ctx->eig_vec.reserve(sizeof(double) * 4 * (size_t)n));   // d, e, ev (2n)
-  MBD_CUDA(ctx->eig_ws.reserve(wsb));
   double* A = ctx->eig_a.as<double>();
   double* d = ctx->eig_vec.as<double>();
   double* e = d + n;
   double* ev = e + n;
   MBD_CUDA(cudaMemcpy2DAsync(A, sizeof(double) * ldp, H, sizeof(double) * ld, sizeof(double) * n, n,
                              cudaMemcpyHostToDevice, s));
-  TridiagJob job{A, n, ldp, d, e};
-  MBD_CUDA(cudaMemcpyAsync(ctx->job_dev, &job, sizeof(job), cudaMemcpyHostToDevice, s));
   MBD_CUDA(cudaMemsetAsync(ctx->err_flag, 0, sizeof(int), s));
-  MBD_CUDA(launch_tridiag(ctx->job_dev, 1, 1, G, ctx->eig_ws.p, wsb, n, ctx->err_flag, s));
+  if (n <= ctx->two_stage_max_n) {
+    const size_t wsd = sy2sb_workspace_doubles(n);
+    MBD_CUDA(ctx->eig_ws.reserve(sizeof(double) * (wsd + (size_t)n * kBandLd)));
+    double* ws = ctx->eig_ws.as<double>();
+    double* band = ws + wsd;
+    MBD_CUDA(launch_sy2sb(A, ldp, n, ws, band, ctx->num_sms, s));
+    int st = band_to_tridiag_single(ctx, band, n, d, e, ctx->fb_ws, s);
+    if (st != MBD_OK) return st;
+  } else {
+    const int G = tridiag_group_ctas(ctx, n);
+    const size_t wsb = tridiag_workspace_bytes(n, G);
+    MBD_CUDA(ctx->eig_ws.reserve(wsb));
+    TridiagJob job{A, n, ldp, d, e};
+    MBD_CUDA(cudaMemcpyAsync(ctx->job_dev, &job, sizeof(job), cudaMemcpyHostToDevice, s));
+    MBD_CUDA(launch_tridiag(ctx->job_dev, 1, 1, G, ctx->eig_ws.p, wsb, n, ctx->err_flag, s));
+  }
   launch_tridiag_eigenvalues(d, e, n, ev, s);
   MBD_CUDA(cudaMemcpyAsync(w, ev, sizeof(double) * n, cudaMemcpyDeviceToHost, s));
   MBD_CUDA(cudaStreamSynchronize(s));
@@ -1017,6 +1123,7 @@ int mbd_rsscs_last_stats(mbd_ctx* ctx, double* out, int n) {
   out[0] = ctx->launches;
   out[1] = ctx->h2d_bytes;
   out[2] = ctx->d2h_bytes;
+  if (n >= 4) out[3] = ctx->graph_replayed ? 1.0 : 0.0;
   return MBD_OK;
 }
 

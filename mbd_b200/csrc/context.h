@@ -48,6 +48,7 @@ struct GeomDev {
   DevBuf inputs;     // coords, alpha0, c6free, r0, hirsh, shifts, diff data
   DevBuf results;    // alpha_w, sgm, rvdw_iso, alpha_iw, molpol, c6_eff, alpha_eff, omega, rvdw_eff, scalars, energy, info, d, e, ev
   DevBuf hmat;       // CFDM Hamiltonian (nH x ldH, lower blocks), reduced in place
+  DevBuf band;       // two-stage reduction: the band, nH x kBandLd
   // offsets into inputs (doubles unless noted)
   const double *coords, *alpha0, *c6free, *r0, *hirsh, *scs_shifts, *cfdm_shifts, *diff_shift;
   const int *diff_is_zero, *place_offset, *place_rc, *place_cc;
@@ -73,6 +74,7 @@ struct RelaySlot {
   DevBuf relay64, linv, rhs;                                  // plain FP64 path
   DevBuf relay32, p_hi, p_lo, l_hi, l_lo, mixv, res_ws, solve_sync;   // mixed path
   DevBuf cg, gnn;                                             // learned path: CG vectors, network work
+  DevBuf trd_ws;                                              // dense -> band workspace
   int solve_epoch = 0;
   ~RelaySlot() {
     if (done) cudaEventDestroy(done);
@@ -80,15 +82,18 @@ struct RelaySlot {
   }
   size_t held() const {
     return relay64.bytes + linv.bytes + rhs.bytes + relay32.bytes + p_hi.bytes + p_lo.bytes + l_hi.bytes +
-           l_lo.bytes + mixv.bytes + res_ws.bytes + solve_sync.bytes + cg.bytes + gnn.bytes;
+           l_lo.bytes + mixv.bytes + res_ws.bytes + solve_sync.bytes + cg.bytes + gnn.bytes + trd_ws.bytes;
   }
 };
 
 struct Stage {
   enum { kTotal = 0, kSetup, kBuild, kFactor, kSolve, kCfdm, kTridiag, kEig, kCount };
 };
-// Events per geometry: start, then the ends of setup, build, factor, solve, CFDM.
-constexpr int kGeomEvents = 6;
+// Events per geometry: start, then the ends of setup, build, factor, solve,
+// CFDM build and dense -> band reduction.
+constexpr int kGeomEvents = 7;
+
+
 
 }  // namespace mbd
 
@@ -107,6 +112,10 @@ struct mbd_ctx {
   mbd::TridiagJob* trd_jobs = nullptr;
   mbd::TridiagGroup* trd_groups = nullptr;
   mbd::EigJob* eig_jobs = nullptr;
+  mbd::BandJob* band_jobs = nullptr;
+  mbd::SweepItem* sweep_items = nullptr;
+  mbd::DevBuf sweep_progress;
+  int n_band_jobs = 0, n_sweep_items = 0, band_max_n = 0;
   int n_trd_groups = 0, trd_total_ctas = 0, n_eig_jobs = 0, n_eig_batch = 0, eig_batch_max_n = 0;
   double trd_est_ms = 0.0;
   std::vector<int> order;                    // geometries that run, descending relay size
@@ -128,6 +137,9 @@ struct mbd_ctx {
   cudaGraphExec_t graph[3] = {nullptr, nullptr, nullptr};
   double graph_launches[3] = {0, 0, 0};
   bool use_graphs = true;
+  bool graph_replayed = false;               // the last compute ran as a graph replay
+  int two_stage_max_n = 0;                   // largest matrix the two-stage reduction takes on this device
+  bool two_stage_batch = false;              // batches use the two-stage reduction
   bool capturing = false;
   double last_ms[mbd::Stage::kCount] = {0};
   double launches = 0, h2d_bytes = 0, d2h_bytes = 0;
@@ -179,6 +191,12 @@ int run_front(mbd_ctx* ctx, GeomDev* gd, int gi, int mode, bool relay_only = fal
 int upload_batch(mbd_ctx* ctx, int n_geom, const mbd_geom* geoms, bool eigen);
 // learn.cpp
 int reserve_learned(mbd_ctx* ctx);
+// Band -> tridiagonal (d, e) of one band with its own tables in `scratch`
+// (grown as needed), on stream s.
+int band_to_tridiag_single(mbd_ctx* ctx, double* Br, int n, double* d, double* e, DevBuf& scratch, cudaStream_t s);
 int relay_learned(mbd_ctx* ctx, GeomDev* gd, RelaySlot& sl, size_t mstride, cudaEvent_t ev_net, double** X_out);
+
+// Matrices reduced by the two-stage path (larger ones by the one-stage kernel).
+inline bool two_stage(const mbd_ctx* ctx, int n) { return ctx->two_stage_batch && n <= ctx->two_stage_max_n; }
 
 }  // namespace mbd

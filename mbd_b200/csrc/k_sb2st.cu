@@ -1,0 +1,230 @@
+// Stage 2 of the two-stage tridiagonalisation: symmetric band (half-bandwidth
+// kBand) -> tridiagonal by bulge chasing with Householder reflectors of
+// length kBand, FP64, for every band of a batch in ONE persistent
+// cooperative launch.
+//
+// Band storage per matrix: Br[r][d] = A(r, r - d), d = 0 .. 2 kBand; the
+// diagonals beyond kBand hold the bulges between sweeps.  Sweep i annihilates
+// column i below the subdiagonal; its task k (rows r_k = i + 1 + k kBand):
+//   k = 0: reflector H from column i (A(r_0 .. r_0 + kBand, i)).
+//   D_k <- H D_k H            (diagonal block, rows/cols [r_k, r_k + kBand))
+//   O   <- O H                (O = A[r_k + kBand .. + kBand, r_k .. + kBand))
+//   H'  from O[:, 0];  O <- H' O;  carry H' to task k + 1.
+// Task (i, k) touches columns [r_k, r_k + kBand) and must follow task
+// (i-1, k+1), the last task of the previous sweep that touches one of them:
+// each sweep's warp publishes its completed task count, the next sweep's
+// warp waits (bounded) until it reaches k + 2.
+//
+// Work items are (matrix, sweep) pairs ordered by sweep, then matrix; warp w
+// takes items w, w + W, ...  Every wait points to an item of lower index, so
+// the lowest unfinished item always progresses (all CTAs are co-resident).
+// One warp owns a task: lane l holds row l of D and of O in registers.
+#include <cuda_runtime.h>
+
+#include "kernels.h"
+#include "../../include/mbd_b200.h"
+
+namespace mbd {
+namespace {
+
+constexpr int B = kBand;
+constexpr int LD = kBandLd;
+constexpr int WARPS = 4;
+constexpr long long kSpinCycles = 4000000000LL;   // ~2 s, then the wait gives up
+
+struct WarpSmem {
+  double v[B];        // current reflector
+  double w[B];
+  double v2[B];       // next reflector
+  double s[B];
+  double Ot[B][B + 1];
+};
+
+__device__ __forceinline__ double warp_sum(double x) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
+  return x;
+}
+
+__device__ __forceinline__ int ld_acquire(const int* p) {
+  int v;
+  asm volatile("ld.acquire.gpu.b32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+
+__device__ __forceinline__ void st_release(int* p, int v) {
+  asm volatile("st.release.gpu.b32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+
+// Lane 0 spins (bounded) until *p >= target; then every lane acquires.
+__device__ bool wait_progress(const int* p, int target, int* err) {
+  int ok = 1;
+  if ((threadIdx.x & 31) == 0) {
+    const long long t0 = clock64();
+    while (ld_acquire(p) < target) {
+      if (*(volatile int*)err != 0 || clock64() - t0 > kSpinCycles) {
+        atomicCAS(err, 0, MBD_ERR_TIMEOUT);
+        ok = 0;
+        break;
+      }
+      __nanosleep(32);
+    }
+  }
+  ok = __shfl_sync(0xffffffffu, ok, 0);
+  if (ok) (void)ld_acquire(p);
+  __syncwarp();
+  return ok != 0;
+}
+
+// Householder reflector of x (lane l holds x[l], length len): H x = beta e_1.
+// Returns tau; v[l] (lane l) with v[0] = 1; beta through *beta.
+__device__ __forceinline__ double make_reflector(double x, int len, double* v, double* beta) {
+  const int l = threadIdx.x & 31;
+  const double xn2 = warp_sum((l >= 1 && l < len) ? x * x : 0.0);
+  const double alpha = __shfl_sync(0xffffffffu, x, 0);
+  double tau = 0.0, b = alpha, scale = 0.0;
+  if (len >= 2 && xn2 > 0.0) {
+    b = -copysign(sqrt(alpha * alpha + xn2), alpha);
+    tau = (b - alpha) / b;
+    scale = 1.0 / (alpha - b);
+  }
+  *v = (l == 0) ? 1.0 : ((l < len && tau != 0.0) ? x * scale : 0.0);
+  *beta = b;
+  return tau;
+}
+
+__global__ void __launch_bounds__(WARPS * 32) sb2st_kernel(const BandJob* jobs, const SweepItem* items,
+                                                           int n_items, int* progress, int* err) {
+  __shared__ WarpSmem wsm[WARPS];
+  const int warp = threadIdx.x / 32, l = threadIdx.x & 31;
+  WarpSmem& S = wsm[warp];
+  const int W = gridDim.x * WARPS;
+  for (int t = blockIdx.x * WARPS + warp; t < n_items; t += W) {
+    const SweepItem it = items[t];
+    const BandJob jb = jobs[it.job];
+    const int n = jb.n, i = it.sweep;
+    double* Br = jb.Br;
+    const int K = (n - i - 1 + B - 1) / B;           // tasks of sweep i
+    const int Kp = (n - i + B - 1) / B;              // tasks of sweep i - 1
+    double tau = 0.0, vl = 0.0;
+    for (int k = 0; k < K; ++k) {
+      if (it.pred >= 0 && !wait_progress(progress + it.pred, min(k + 2, Kp), err)) return;
+      const int r = i + 1 + k * B;
+      const int L = min(B, n - r);
+      const int rn = r + B;
+      const int Ln = max(0, min(B, n - rn));
+      if (k == 0) {
+        // reflector from column i: x[l] = A(i + 1 + l, i) = Br[i + 1 + l][1 + l]
+        const double x = (l < L) ? __ldcg(Br + (size_t)(r + l) * LD + 1 + l) : 0.0;
+        double beta;
+        tau = make_reflector(x, L, &vl, &beta);
+        if (l < L) Br[(size_t)(r + l) * LD + 1 + l] = (l == 0) ? beta : (tau != 0.0 ? 0.0 : x);
+      }
+      S.v[l] = vl;
+      // D row l (symmetric, from the lower band) and O row l
+      double dr[B], orow[B];
+#pragma unroll
+      for (int j = 0; j < B; ++j) {
+        double x = 0.0;
+        if (l < L && j < L) x = (j <= l) ? __ldcg(Br + (size_t)(r + l) * LD + (l - j))
+                                         : __ldcg(Br + (size_t)(r + j) * LD + (j - l));
+        dr[j] = x;
+        orow[j] = (l < Ln && j < L) ? __ldcg(Br + (size_t)(rn + l) * LD + (B + l - j)) : 0.0;
+      }
+      __syncwarp();
+      if (tau != 0.0) {
+        // D <- H D H:  w = tau D v - (tau^2 / 2)(v^T D v) v;  D -= v w^T + w v^T
+        double dv = 0.0;
+#pragma unroll
+        for (int j = 0; j < B; ++j) dv += dr[j] * S.v[j];
+        const double vdv = warp_sum(vl * dv);
+        const double wl = tau * dv - 0.5 * tau * tau * vdv * vl;
+        S.w[l] = wl;
+        __syncwarp();
+#pragma unroll
+        for (int j = 0; j < B; ++j) dr[j] -= vl * S.w[j] + wl * S.v[j];
+        // O <- O H = O - tau (O v) v^T
+        double ov = 0.0;
+#pragma unroll
+        for (int j = 0; j < B; ++j) ov += orow[j] * S.v[j];
+#pragma unroll
+        for (int j = 0; j < B; ++j) orow[j] -= tau * ov * S.v[j];
+      }
+      // next reflector from O[:, 0]; O <- H' O
+      double v2 = 0.0, tau2 = 0.0, beta2 = 0.0;
+      if (Ln > 0) {
+        tau2 = make_reflector(orow[0], Ln, &v2, &beta2);
+        if (tau2 != 0.0) {
+          S.v2[l] = v2;
+#pragma unroll
+          for (int j = 0; j < B; ++j) S.Ot[l][j] = orow[j];
+          __syncwarp();
+          double sj = 0.0;
+#pragma unroll
+          for (int q = 0; q < B; ++q) sj += S.v2[q] * S.Ot[q][l];   // lane l: column l of v2^T O
+          S.s[l] = sj;
+          __syncwarp();
+#pragma unroll
+          for (int j = 0; j < B; ++j) orow[j] -= tau2 * v2 * S.s[j];
+          orow[0] = (l == 0) ? beta2 : 0.0;
+        }
+      }
+      // store D (lower part) and O
+      if (l < L) {
+#pragma unroll
+        for (int j = 0; j < B; ++j)
+          if (j <= l) Br[(size_t)(r + l) * LD + (l - j)] = dr[j];
+      }
+      if (l < Ln) {
+#pragma unroll
+        for (int j = 0; j < B; ++j)
+          if (j < L) Br[(size_t)(rn + l) * LD + (B + l - j)] = orow[j];
+      }
+      __threadfence();
+      __syncwarp();
+      if (l == 0) st_release(progress + t, k + 1);
+      tau = tau2;
+      vl = v2;
+      __syncwarp();
+    }
+  }
+}
+
+// d[r] = A(r, r), e[r] = A(r + 1, r) after the last sweep
+__global__ void extract_kernel(const BandJob* jobs) {
+  const BandJob jb = jobs[blockIdx.y];
+  const int r = blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= jb.n) return;
+  jb.d[r] = jb.Br[(size_t)r * LD];
+  if (r + 1 < jb.n) jb.e[r] = jb.Br[(size_t)(r + 1) * LD + 1];
+}
+
+}  // namespace
+
+cudaError_t init_sb2st_attributes() { return cudaSuccess; }
+
+int sb2st_max_ctas(int num_sms) {
+  int nb = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, sb2st_kernel, WARPS * 32, 0) != cudaSuccess || nb < 1)
+    nb = 1;
+  return nb * num_sms;
+}
+
+cudaError_t launch_sb2st(const BandJob* jobs, int n_jobs, const SweepItem* items, int n_items, int* progress,
+                         int* err, int num_sms, int max_n, cudaStream_t s) {
+  if (n_jobs < 1) return cudaSuccess;
+  if (n_items > 0) {
+    cudaError_t e = cudaMemsetAsync(progress, 0, sizeof(int) * (size_t)n_items, s);
+    if (e != cudaSuccess) return e;
+    int grid = sb2st_max_ctas(num_sms);
+    const int need = (n_items + WARPS - 1) / WARPS;
+    if (grid > need) grid = need;
+    void* args[] = {(void*)&jobs, (void*)&items, (void*)&n_items, (void*)&progress, (void*)&err};
+    e = cudaLaunchCooperativeKernel((const void*)sb2st_kernel, dim3(grid), dim3(WARPS * 32), args, 0, s);
+    if (e != cudaSuccess) return e;
+  }
+  extract_kernel<<<dim3((max_n + 255) / 256, n_jobs), 256, 0, s>>>(jobs);
+  return cudaGetLastError();
+}
+
+}  // namespace mbd

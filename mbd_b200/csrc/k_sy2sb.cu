@@ -1,0 +1,527 @@
+// Stage 1 of the two-stage tridiagonalisation of the CFDM Hamiltonian (the
+// reduction half of PDSYEV('N','L') at UTILS.f90:835): symmetric dense ->
+// band of half-bandwidth kBand, FP64, lower triangle, row-major.
+//
+// For each panel of kBand columns c0 = k*kBand (rows below the band r >= c0 +
+// kBand, m of them):
+//   qr_panel   Householder QR of the m x kBand panel in ONE thread-block
+//              cluster: the panel's rows are spread over the CTAs' shared
+//              memory, cross-CTA sums go through distributed shared memory
+//              and two hardware cluster barriers per column.  Writes R in
+//              place (the band), V explicitly (unit lower trapezoidal) and
+//              the compact-WY factor T (Q = I - V T V^T, dlarft forward).
+//   symm       Y = A22 V (A22 the trailing m x m lower-stored block), row
+//              blocks of 64 split over S column chunks (fixed-order partials)
+//   yred       Y <- sum of the partials; Y <- Y T; block partials of V^T Y
+//   mform      M = T^T (V^T Y)
+//   zform      Z = Y - 1/2 V M
+//   syr2k      A22 -= V Z^T + Z V^T (lower 64 x 64 tiles)
+// so that A22 <- Q^T A22 Q.  Every reduction is summed in a fixed order: the
+// result does not depend on scheduling.
+#include <cooperative_groups.h>
+#include <cuda_runtime.h>
+
+#include "kernels.h"
+
+namespace cg = cooperative_groups;
+
+namespace mbd {
+namespace {
+
+constexpr int B = kBand;            // 32
+constexpr int QR_THREADS = 256;
+constexpr int QR_LD = B + 1;        // shared-memory row stride of the panel (doubles)
+constexpr int TL = 64;              // tile edge of symm / syr2k
+
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+
+// CTA-wide sum (QR_THREADS threads); red holds QR_THREADS/32 doubles.
+__device__ double cta_sum(double v, double* red) {
+  v = warp_sum(v);
+  const int w = threadIdx.x / 32, l = threadIdx.x % 32;
+  __syncthreads();
+  if (l == 0) red[w] = v;
+  __syncthreads();
+  double s = 0.0;
+#pragma unroll
+  for (int q = 0; q < QR_THREADS / 32; ++q) s += red[q];
+  return s;
+}
+
+// Shared layout of qr_panel: P[rows][QR_LD] | pub[2 + B] (values this CTA
+// publishes to the cluster) | gram[B*B] | misc
+__global__ void __launch_bounds__(QR_THREADS) qr_panel_kernel(PanelArgs a) {
+  extern __shared__ double sm[];
+  cg::cluster_group cl = cg::this_cluster();
+  const int rank = (int)cl.block_rank();
+  const int C = (int)cl.num_blocks();
+  const int m = a.m;
+  const int R = a.rows_per_cta;
+  const int lo = rank * R, hi = min(m, lo + R);
+  const int nr = max(0, hi - lo);
+  double* P = sm;                              // [R][QR_LD]
+  double* pub = sm + (size_t)R * QR_LD;        // [0] norm^2, [1] alpha, [2..2+B) dots
+  double* gram = pub + 2 + B;                  // [B][B]
+  double* red = gram + B * B;                  // [8]
+  double* rfl = red + 8;                       // tau, scale, beta, dsum[B]
+  const int tid = threadIdx.x;
+  // load the owned rows
+  for (int idx = tid; idx < nr * B; idx += QR_THREADS) {
+    const int r = idx / B, c = idx % B;
+    P[r * QR_LD + c] = a.A[(size_t)(a.row0 + lo + r) * a.ld + a.col0 + c];
+  }
+  __syncthreads();
+  const int nref = min(B, m);
+  for (int j = 0; j < nref; ++j) {
+    // ---- phase 1: norm^2 of column j below row j, alpha = P[j][j]
+    double s = 0.0;
+    for (int r = tid; r < nr; r += QR_THREADS) {
+      const int gr = lo + r;
+      if (gr > j) {
+        const double x = P[r * QR_LD + j];
+        s += x * x;
+      }
+    }
+    s = cta_sum(s, red);
+    if (tid == 0) {
+      pub[0] = s;
+      pub[1] = (j >= lo && j < hi) ? P[(j - lo) * QR_LD + j] : 0.0;
+    }
+    cl.sync();
+    if (tid == 0) {
+      double xn2 = 0.0, alpha = 0.0;
+      for (int q = 0; q < C; ++q) {
+        const double* rp = cl.map_shared_rank(pub, q);
+        xn2 += rp[0];
+        alpha += rp[1];
+      }
+      double tau = 0.0, scale = 0.0, beta = alpha;
+      if (xn2 > 0.0) {
+        beta = -copysign(sqrt(alpha * alpha + xn2), alpha);
+        tau = (beta - alpha) / beta;
+        scale = 1.0 / (alpha - beta);
+      }
+      rfl[0] = tau;
+      rfl[1] = scale;
+      rfl[2] = beta;
+      if (rank == 0) a.tau[j] = tau;
+    }
+    __syncthreads();
+    const double tau = rfl[0], scale = rfl[1];
+    // ---- phase 2: v (in place below row j), dots d_c = v^T P[:, c], c > j
+    for (int r = tid; r < nr; r += QR_THREADS)
+      if (lo + r > j) P[r * QR_LD + j] *= scale;
+    __syncthreads();
+    {
+      // thread -> (column c = tid % 32, row phase = tid / 32)
+      const int c = tid % 32, ph = tid / 32;
+      double d = 0.0;
+      if (c > j)
+        for (int r = ph; r < nr; r += QR_THREADS / 32) {
+          const int gr = lo + r;
+          if (gr >= j) d += (gr == j ? 1.0 : P[r * QR_LD + j]) * P[r * QR_LD + c];
+        }
+      // reduce over the 8 row phases through shared memory (gram as scratch)
+      gram[ph * 32 + c] = d;
+      __syncthreads();
+      if (tid < 32) {
+        double t = 0.0;
+#pragma unroll
+        for (int q = 0; q < QR_THREADS / 32; ++q) t += gram[q * 32 + tid];
+        pub[2 + tid] = t;
+      }
+    }
+    cl.sync();
+    if (tid < 32) {
+      double t = 0.0;
+      if (tid > j)
+        for (int q = 0; q < C; ++q) t += cl.map_shared_rank(pub, q)[2 + tid];
+      rfl[3 + tid] = t;
+    }
+    __syncthreads();
+    if (tau != 0.0) {
+      for (int idx = tid; idx < nr * B; idx += QR_THREADS) {
+        const int r = idx / B, c = idx % B;
+        const int gr = lo + r;
+        if (c > j && gr >= j) {
+          const double v = (gr == j) ? 1.0 : P[r * QR_LD + j];
+          P[r * QR_LD + c] -= tau * v * rfl[3 + c];
+        }
+      }
+    }
+    if (tid == 0 && j >= lo && j < hi) P[(j - lo) * QR_LD + j] = rfl[2];
+    __syncthreads();
+  }
+  // ---- Gram matrix G = V^T V (V unit lower trapezoidal), summed over the cluster
+  for (int e = tid; e < B * B; e += QR_THREADS) {
+    const int p = e / B, q = e % B;
+    double g = 0.0;
+    for (int r = 0; r < nr; ++r) {
+      const int gr = lo + r;
+      const double vp = gr > p ? P[r * QR_LD + p] : (gr == p ? 1.0 : 0.0);
+      const double vq = gr > q ? P[r * QR_LD + q] : (gr == q ? 1.0 : 0.0);
+      g += vp * vq;
+    }
+    gram[e] = g;
+  }
+  // write R (upper part, the band) and V (explicit) back
+  for (int idx = tid; idx < nr * B; idx += QR_THREADS) {
+    const int r = idx / B, c = idx % B;
+    const int gr = lo + r;
+    const double x = P[r * QR_LD + c];
+    if (gr <= c) a.A[(size_t)(a.row0 + gr) * a.ld + a.col0 + c] = x;
+    a.V[(size_t)gr * B + c] = gr > c ? x : (gr == c ? 1.0 : 0.0);
+  }
+  cl.sync();
+  if (rank == 0) {
+    // T (upper triangular): T[j][j] = tau_j, T[0:j, j] = -tau_j T[0:j, 0:j] G[0:j, j]
+    double* G = rfl + 3 + B;       // [B][B] summed Gram
+    double* Tm = G + B * B;        // [B][B]
+    for (int e = tid; e < B * B; e += QR_THREADS) {
+      double g = 0.0;
+      for (int q = 0; q < C; ++q) g += cl.map_shared_rank(gram, q)[e];
+      G[e] = g;
+      Tm[e] = 0.0;
+    }
+    __syncthreads();
+    if (tid < 32) {
+      for (int j = 0; j < B; ++j) {
+        const double tj = (j < nref) ? a.tau[j] : 0.0;
+        double t = 0.0;
+        if (tid < j)
+          for (int l = tid; l < j; ++l) t += Tm[tid * B + l] * G[l * B + j];
+        __syncwarp();
+        if (tid < j) Tm[tid * B + j] = -tj * t;
+        if (tid == j) Tm[j * B + j] = tj;
+        __syncwarp();
+      }
+    }
+    __syncthreads();
+    for (int e = tid; e < B * B; e += QR_THREADS) a.T[e] = Tm[e];
+  }
+  cl.sync();   // no CTA leaves while another may still read its shared memory
+}
+
+// Y partials: Yp[s][r][c] = sum over column tiles J of chunk s of (A22 V)[r][c],
+// row block I = blockIdx.x (64 rows), chunk s = blockIdx.y.  64 threads, 8 x 4
+// outputs each.
+constexpr size_t kSymmSmem = sizeof(double) * (TL * (TL + 1) + TL * (B + 1));
+__global__ void __launch_bounds__(64) symm_kernel(const double* A, int ld, int row0, int m, const double* V,
+                                                  double* Yp, int chunk) {
+  extern __shared__ double dsm[];
+  double (*As)[TL + 1] = reinterpret_cast<double (*)[TL + 1]>(dsm);
+  double (*Vs)[B + 1] = reinterpret_cast<double (*)[B + 1]>(dsm + TL * (TL + 1));
+  const int I = blockIdx.x, s = blockIdx.y;
+  const int nt = (m + TL - 1) / TL;
+  const int J0 = s * chunk, J1 = min(nt, J0 + chunk);
+  const int tid = threadIdx.x;
+  const int r0 = (tid / 8) * 8, c0 = (tid % 8) * 4;
+  double acc[8][4];
+#pragma unroll
+  for (int i = 0; i < 8; ++i)
+#pragma unroll
+    for (int q = 0; q < 4; ++q) acc[i][q] = 0.0;
+  const double* A22 = A + (size_t)row0 * ld + row0;
+  for (int J = J0; J < J1; ++J) {
+    __syncthreads();
+    // tile (I, J) of the symmetric A22 as As[r][k] = A22(I*64 + r, J*64 + k)
+    for (int idx = tid; idx < TL * TL; idx += 64) {
+      const int u = idx / TL, w = idx % TL;   // u: outer (row of the stored tile), w: contiguous
+      double x = 0.0;
+      if (J < I) {
+        const int gr = I * TL + u, gc = J * TL + w;
+        if (gr < m) x = A22[(size_t)gr * ld + gc];
+        As[u][w] = x;
+      } else if (J > I) {
+        const int gr = J * TL + u, gc = I * TL + w;   // stored tile (J, I), transposed into As
+        if (gr < m && gc < m) x = A22[(size_t)gr * ld + gc];
+        As[w][u] = x;
+      } else {
+        // diagonal tile: the stored lower element of (u, w) or of its mirror
+        const int a_ = u >= w ? u : w, b_ = u >= w ? w : u;
+        const int gr = I * TL + a_, gc = I * TL + b_;
+        if (gr < m) x = A22[(size_t)gr * ld + gc];
+        As[u][w] = x;
+      }
+    }
+    for (int idx = tid; idx < TL * B; idx += 64) {
+      const int k = idx / B, c = idx % B;
+      const int gk = J * TL + k;
+      Vs[k][c] = gk < m ? V[(size_t)gk * B + c] : 0.0;
+    }
+    __syncthreads();
+#pragma unroll 4
+    for (int k = 0; k < TL; ++k) {
+      double av[8], vv[4];
+#pragma unroll
+      for (int i = 0; i < 8; ++i) av[i] = As[r0 + i][k];
+#pragma unroll
+      for (int q = 0; q < 4; ++q) vv[q] = Vs[k][c0 + q];
+#pragma unroll
+      for (int i = 0; i < 8; ++i)
+#pragma unroll
+        for (int q = 0; q < 4; ++q) acc[i][q] = fma(av[i], vv[q], acc[i][q]);
+    }
+  }
+  double* out = Yp + (size_t)s * m * B;
+#pragma unroll
+  for (int i = 0; i < 8; ++i) {
+    const int gr = I * TL + r0 + i;
+    if (gr < m)
+#pragma unroll
+      for (int q = 0; q < 4; ++q) out[(size_t)gr * B + c0 + q] = acc[i][q];
+  }
+}
+
+// Y = sum_s Yp[s]; Y <- Y T; Up[I] = V_I^T Y_I (64-row blocks, 256 threads).
+__global__ void __launch_bounds__(256) yred_kernel(const double* Yp, int S, int m, const double* T, const double* V,
+                                                   double* Y, double* Up) {
+  __shared__ double Ts[B][B + 1];
+  __shared__ double Ys[TL][B + 1];
+  __shared__ double Vs[TL][B + 1];
+  const int I = blockIdx.x, tid = threadIdx.x;
+  for (int e = tid; e < B * B; e += 256) Ts[e / B][e % B] = T[e];
+  for (int e = tid; e < TL * B; e += 256) {
+    const int r = e / B, c = e % B, gr = I * TL + r;
+    double y = 0.0, v = 0.0;
+    if (gr < m) {
+      for (int s = 0; s < S; ++s) y += Yp[((size_t)s * m + gr) * B + c];
+      v = V[(size_t)gr * B + c];
+    }
+    Ys[r][c] = y;
+    Vs[r][c] = v;
+  }
+  __syncthreads();
+  double yt[8];
+#pragma unroll
+  for (int t = 0; t < 8; ++t) {
+    const int e = tid + 256 * t, r = e / B, c = e % B;
+    double x = 0.0;
+    for (int l = 0; l <= c; ++l) x += Ys[r][l] * Ts[l][c];
+    yt[t] = x;
+  }
+  __syncthreads();
+#pragma unroll
+  for (int t = 0; t < 8; ++t) {
+    const int e = tid + 256 * t, r = e / B, c = e % B, gr = I * TL + r;
+    Ys[r][c] = yt[t];
+    if (gr < m) Y[(size_t)gr * B + c] = yt[t];
+  }
+  __syncthreads();
+#pragma unroll
+  for (int t = 0; t < 4; ++t) {
+    const int e = tid + 256 * t, p = e / B, c = e % B;
+    double u = 0.0;
+    for (int r = 0; r < TL; ++r) u += Vs[r][p] * Ys[r][c];
+    Up[(size_t)I * B * B + e] = u;
+  }
+}
+
+// M = T^T U, U = sum_I Up[I] (one CTA of B*B threads).
+__global__ void __launch_bounds__(B* B) mform_kernel(const double* Up, int nt, const double* T, double* M) {
+  __shared__ double Us[B][B + 1];
+  __shared__ double Ts[B][B + 1];
+  const int e = threadIdx.x, p = e / B, c = e % B;
+  double u = 0.0;
+  for (int I = 0; I < nt; ++I) u += Up[(size_t)I * B * B + e];
+  Us[p][c] = u;
+  Ts[p][c] = T[e];
+  __syncthreads();
+  double x = 0.0;
+  for (int l = 0; l <= p; ++l) x += Ts[l][p] * Us[l][c];   // (T^T)[p][l] = T[l][p], l <= p
+  M[e] = x;
+}
+
+// Z = Y - 1/2 V M (rows in blocks of 64, 256 threads)
+__global__ void __launch_bounds__(256) zform_kernel(const double* Y, const double* V, const double* M, int m,
+                                                    double* Z) {
+  __shared__ double Ms[B][B + 1];
+  __shared__ double Vs[TL][B + 1];
+  const int I = blockIdx.x, tid = threadIdx.x;
+  for (int e = tid; e < B * B; e += 256) Ms[e / B][e % B] = M[e];
+  for (int e = tid; e < TL * B; e += 256) {
+    const int r = e / B, c = e % B, gr = I * TL + r;
+    Vs[r][c] = gr < m ? V[(size_t)gr * B + c] : 0.0;
+  }
+  __syncthreads();
+  for (int e = tid; e < TL * B; e += 256) {
+    const int r = e / B, c = e % B, gr = I * TL + r;
+    if (gr >= m) continue;
+    double x = 0.0;
+#pragma unroll 8
+    for (int l = 0; l < B; ++l) x += Vs[r][l] * Ms[l][c];
+    Z[(size_t)gr * B + c] = Y[(size_t)gr * B + c] - 0.5 * x;
+  }
+}
+
+// A22 -= V Z^T + Z V^T on lower 64 x 64 tiles; 64 threads, 8 x 8 outputs each.
+constexpr size_t kSyr2kSmem = sizeof(double) * 2 * TL * (2 * B + 1);
+__global__ void __launch_bounds__(64) syr2k_kernel(double* A, int ld, int row0, int m, const double* V,
+                                                   const double* Z) {
+  extern __shared__ double dsm[];
+  double (*Li)[2 * B + 1] = reinterpret_cast<double (*)[2 * B + 1]>(dsm);                  // [V_I | Z_I]
+  double (*Lj)[2 * B + 1] = reinterpret_cast<double (*)[2 * B + 1]>(dsm + TL * (2 * B + 1));  // [Z_J | V_J]
+  int ti = (int)((sqrt(8.0 * blockIdx.x + 1.0) - 1.0) * 0.5);
+  while ((ti + 1) * (ti + 2) / 2 <= (int)blockIdx.x) ++ti;
+  while (ti * (ti + 1) / 2 > (int)blockIdx.x) --ti;
+  const int tj = (int)blockIdx.x - ti * (ti + 1) / 2;
+  const int tid = threadIdx.x;
+  for (int e = tid; e < TL * B; e += 64) {
+    const int r = e / B, c = e % B;
+    const int gi = ti * TL + r, gj = tj * TL + r;
+    const bool li = gi < m, lj = gj < m;
+    Li[r][c] = li ? V[(size_t)gi * B + c] : 0.0;
+    Li[r][B + c] = li ? Z[(size_t)gi * B + c] : 0.0;
+    Lj[r][c] = lj ? Z[(size_t)gj * B + c] : 0.0;
+    Lj[r][B + c] = lj ? V[(size_t)gj * B + c] : 0.0;
+  }
+  __syncthreads();
+  const int r0 = (tid / 8) * 8, c0 = (tid % 8) * 8;
+  double acc[8][8];
+#pragma unroll
+  for (int i = 0; i < 8; ++i)
+#pragma unroll
+    for (int q = 0; q < 8; ++q) acc[i][q] = 0.0;
+#pragma unroll 2
+  for (int k = 0; k < 2 * B; ++k) {
+    double x[8], y[8];
+#pragma unroll
+    for (int i = 0; i < 8; ++i) x[i] = Li[r0 + i][k];
+#pragma unroll
+    for (int q = 0; q < 8; ++q) y[q] = Lj[c0 + q][k];
+#pragma unroll
+    for (int i = 0; i < 8; ++i)
+#pragma unroll
+      for (int q = 0; q < 8; ++q) acc[i][q] = fma(x[i], y[q], acc[i][q]);
+  }
+  double* A22 = A + (size_t)row0 * ld + row0;
+#pragma unroll
+  for (int i = 0; i < 8; ++i) {
+    const int gr = ti * TL + r0 + i;
+    if (gr >= m) continue;
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+      const int gc = tj * TL + c0 + q;
+      if (gc <= gr) {
+        double* p = A22 + (size_t)gr * ld + gc;
+        *p -= acc[i][q];
+      }
+    }
+  }
+}
+
+// Br[r][d] = A(r, r - d) for d <= kBand, 0 for kBand < d <= 2 kBand.
+__global__ void band_copy_kernel(const double* A, int ld, int n, double* Br) {
+  const long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= (long long)n * kBandLd) return;
+  const int r = (int)(idx / kBandLd), d = (int)(idx % kBandLd);
+  double x = 0.0;
+  if (d <= B && r - d >= 0) x = A[(size_t)r * ld + (r - d)];
+  Br[idx] = x;
+}
+
+}  // namespace
+
+size_t qr_panel_smem(int rows_per_cta) {
+  return sizeof(double) * ((size_t)rows_per_cta * QR_LD + 2 + B + B * B + 8 + 3 + B + 2 * B * B);
+}
+
+cudaError_t init_sy2sb_attributes() {
+  cudaError_t e = cudaFuncSetAttribute(qr_panel_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)qr_panel_smem(kPanelMaxRowsPerCta));
+  if (e != cudaSuccess) return e;
+  e = cudaFuncSetAttribute(qr_panel_kernel, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+  if (e != cudaSuccess) return e;
+  e = cudaFuncSetAttribute(symm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSymmSmem);
+  if (e != cudaSuccess) return e;
+  return cudaFuncSetAttribute(syr2k_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSyr2kSmem);
+}
+
+// Largest n whose panels fit the biggest cluster this device can run.
+int sy2sb_max_n() {
+  for (int C = kPanelMaxCluster; C >= 1; C /= 2) {
+    cudaLaunchConfig_t cfg{};
+    cfg.gridDim = dim3(C);
+    cfg.blockDim = dim3(QR_THREADS);
+    cfg.dynamicSmemBytes = qr_panel_smem(kPanelMaxRowsPerCta);
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = C;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    int clusters = 0;
+    if (cudaOccupancyMaxActiveClusters(&clusters, qr_panel_kernel, &cfg) == cudaSuccess && clusters > 0)
+      return C * kPanelMaxRowsPerCta + kBand;
+    cudaGetLastError();
+  }
+  return 0;
+}
+
+size_t sy2sb_workspace_doubles(int n) {
+  const int m = n;
+  const int nt = (m + TL - 1) / TL;
+  return (size_t)m * B * (3 + kSymmMaxSplit) + (size_t)nt * B * B + 3 * B * B + B + 256;
+}
+
+cudaError_t launch_sy2sb(double* A, int ld, int n, double* ws, double* Br, int num_sms, cudaStream_t s) {
+  const int nt_full = (n + TL - 1) / TL;
+  double* V = ws;
+  double* Y = V + (size_t)n * B;
+  double* Z = Y + (size_t)n * B;
+  double* Yp = Z + (size_t)n * B;
+  double* Up = Yp + (size_t)n * B * kSymmMaxSplit;
+  double* T = Up + (size_t)nt_full * B * B;
+  double* M = T + B * B;
+  double* tau = M + B * B;
+  for (int c0 = 0; c0 + B + 1 < n; c0 += B) {
+    const int row0 = c0 + B, m = n - row0;
+    // panel QR in one cluster (a power of two of CTAs)
+    int C = 1;
+    while (C * kPanelMaxRowsPerCta < m) C *= 2;
+    if (C > kPanelMaxCluster) return cudaErrorInvalidValue;   // the caller keeps n <= sy2sb_max_n()
+    const int R = (m + C - 1) / C;
+    PanelArgs pa{A, ld, row0, c0, m, R, V, T, tau};
+    cudaLaunchConfig_t cfg{};
+    cfg.gridDim = dim3(C);
+    cfg.blockDim = dim3(QR_THREADS);
+    cfg.dynamicSmemBytes = qr_panel_smem(R);
+    cfg.stream = s;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = C;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    cudaError_t e = cudaLaunchKernelEx(&cfg, qr_panel_kernel, pa);
+    if (e != cudaSuccess) return e;
+    // two-sided update of the trailing block
+    const int nt = (m + TL - 1) / TL;
+    int S = (4 * num_sms + nt - 1) / nt;
+    S = S < 1 ? 1 : (S > kSymmMaxSplit ? kSymmMaxSplit : S);
+    if (S > nt) S = nt;
+    const int chunk = (nt + S - 1) / S;
+    S = (nt + chunk - 1) / chunk;
+    symm_kernel<<<dim3(nt, S), 64, kSymmSmem, s>>>(A, ld, row0, m, V, Yp, chunk);
+    yred_kernel<<<nt, 256, 0, s>>>(Yp, S, m, T, V, Y, Up);
+    mform_kernel<<<1, B * B, 0, s>>>(Up, nt, T, M);
+    zform_kernel<<<nt, 256, 0, s>>>(Y, V, M, m, Z);
+    syr2k_kernel<<<nt * (nt + 1) / 2, 64, kSyr2kSmem, s>>>(A, ld, row0, m, V, Z);
+  }
+  band_copy_kernel<<<(unsigned)(((long long)n * kBandLd + 255) / 256), 256, 0, s>>>(A, ld, n, Br);
+  return cudaGetLastError();
+}
+
+int sy2sb_launches(int n) {
+  int k = 0;
+  for (int c0 = 0; c0 + B + 1 < n; c0 += B) k += 6;
+  return k + 1;
+}
+
+}  // namespace mbd

@@ -145,6 +145,47 @@ cudaError_t init_eigval_attributes();
 // energy = 0.5*sum_{ev>=0} sqrt(ev)/nsl - 0.5*sum_nonint; out[0]=E, out[1]=sum sqrt, out[2]=nimag
 void launch_energy(const double* ev, int n, int nsl, const double* scalars, double* out,
                    cudaStream_t s);
+// ---- two-stage tridiagonalisation (PDSYEV('N','L') reduction, UTILS.f90:835) ----
+constexpr int kBand = 32;                    // half-bandwidth of the intermediate band
+constexpr int kBandLd = 2 * kBand + 1;       // band row: A(r, r - d), d = 0..2 kBand (room for bulges)
+constexpr int kPanelMaxRowsPerCta = 768;     // panel rows one CTA keeps in shared memory
+constexpr int kPanelMaxCluster = 16;         // CTAs of the panel-QR cluster
+constexpr int kSymmMaxSplit = 16;
+constexpr int kTwoStageMaxN = kPanelMaxRowsPerCta * kPanelMaxCluster;
+struct PanelArgs {
+  double* A;
+  int ld;
+  int row0, col0;          // panel = A[row0 .. row0 + m)[col0 .. col0 + kBand)
+  int m;
+  int rows_per_cta;
+  double* V;               // [m][kBand] out: Householder vectors, unit lower trapezoidal
+  double* T;               // [kBand][kBand] out: compact-WY factor
+  double* tau;             // [kBand] out
+};
+cudaError_t init_sy2sb_attributes();
+int sy2sb_max_n();
+size_t sy2sb_workspace_doubles(int n);
+// Dense (lower, row-major, ld) -> band: A is overwritten; Br[n][kBandLd]
+// receives the band (diagonal d = 0..kBand, zero beyond).  ws: workspace.
+cudaError_t launch_sy2sb(double* A, int ld, int n, double* ws, double* Br, int num_sms, cudaStream_t s);
+int sy2sb_launches(int n);
+// Band -> tridiagonal for a batch of bands in one persistent cooperative
+// launch (bulge chasing, one warp per task of a sweep).
+struct BandJob {
+  double* Br;              // [n][kBandLd], overwritten
+  int n;
+  double* d;               // [n] diagonal out
+  double* e;               // [n-1] subdiagonal out
+};
+// items: (job, sweep) pairs ordered by sweep then job; pred[t] = the item of
+// the same job's previous sweep or -1; progress[n_items] zeroed by the launch.
+struct SweepItem {
+  int job, sweep, pred, pad;
+};
+cudaError_t launch_sb2st(const BandJob* jobs, int n_jobs, const SweepItem* items, int n_items, int* progress,
+                         int* err, int num_sms, int max_n, cudaStream_t s);
+cudaError_t init_sb2st_attributes();
+
 // ---- block-CG relay solve of the MIXED_LEARNED mode (UTILS.f90:469-473) ----
 constexpr int kCgState = 24;   // per-frequency recurrence state (doubles)
 struct CgArgs {

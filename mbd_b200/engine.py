@@ -345,9 +345,10 @@ class Engine:
         return S.reshape(M, 3, 3), grad, loss
 
     def stats(self) -> dict:
-        buf = (ctypes.c_double * 3)()
-        self.lib.mbd_rsscs_last_stats(self.ctx, buf, 3)
-        return {"launches": int(buf[0]), "h2d_bytes": int(buf[1]), "d2h_bytes": int(buf[2])}
+        buf = (ctypes.c_double * 4)()
+        self.lib.mbd_rsscs_last_stats(self.ctx, buf, 4)
+        return {"launches": int(buf[0]), "h2d_bytes": int(buf[1]), "d2h_bytes": int(buf[2]),
+                "graph_replayed": bool(buf[3])}
 
     def stream_handle(self) -> int:
         """cudaStream_t of this context (for recording caller-side events)."""

@@ -113,6 +113,7 @@ def test_graph_replay_matches_direct_launches(engine, mode, monkeypatch):
     runs = []
     for _ in range(3):   # capture, replay, replay
         assert engine.compute(mode) == 0
+        assert engine.stats()["graph_replayed"]
         code, res = engine.download()
         assert code == 0
         runs.append(res)

@@ -132,7 +132,7 @@ def test_repeat_is_deterministic(engine):
     np.testing.assert_array_equal(a.alpha_iw, b.alpha_iw)
 
 
-@pytest.mark.parametrize("n", [1, 2, 5, 64, 130, 700])
+@pytest.mark.parametrize("n", [1, 2, 3, 5, 33, 34, 35, 64, 66, 97, 130, 700, 2000, 6500])
 def test_eigvalsh_matches_lapack(engine, n):
     """The FP64 tridiagonalisation + multisection eigenvalues against LAPACK
     (numpy.linalg.eigvalsh) on random symmetric matrices; the upper triangle
