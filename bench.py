@@ -225,7 +225,8 @@ class _Null:
 def roofline(stage_ms, sizes, mode):
     """Roofline of the dominant stage of the last timed step."""
     peaks, src = load_peaks()
-    stages = {k: v for k, v in stage_ms.items() if k != "total"}
+    stages = {k: v for k, v in stage_ms.items()
+              if k not in ("total", "tridiag_dense_to_band", "tridiag_to_tridiagonal")}
     dom = max(stages, key=stages.get)
     if dom == "tridiag":
         # one read of the trailing lower triangle per column: sum_m m^2/2 * 8 B = n^3/6 * 8 B

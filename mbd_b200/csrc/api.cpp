@@ -346,7 +346,7 @@ int band_to_tridiag_single(mbd_ctx* ctx, double* Br, int n, double* d, double* e
   MBD_CUDA(cudaStreamSynchronize(s));   // the pageable source must outlive the copy
   MBD_CUDA(launch_sb2st(reinterpret_cast<BandJob*>(base), 1, reinterpret_cast<SweepItem*>(base + b_job),
                         (int)items.size(), reinterpret_cast<int*>(base + b_job + b_it), ctx->err_flag,
-                        ctx->num_sms, n, s));
+                        ctx->num_sms, n, n / (2 * kBand) + 1, s));
   ctx->launches += 3;
   return MBD_OK;
 }
@@ -528,6 +528,20 @@ int prepare_batch(mbd_ctx* ctx, bool eigen) {
   ctx->order.clear();
   for (size_t g = 0; g < ctx->geoms.size(); ++g)
     if (ctx->geoms[g]->status_host == MBD_OK) ctx->order.push_back((int)g);
+  // Tridiagonalisation path, one for the whole batch (the one-stage grouped
+  // launch and the band -> tridiagonal launch would run one after the other).
+  // Measured on B200 (one-stage vs two-stage): one matrix n = 1500: 20 vs
+  // 36 ms, n = 3000: 52 vs 77 ms, n = 6000: 195 vs 187 ms; 256 matrices
+  // n <= 1800: 798 vs 733 ms per batch (the band -> tridiagonal launch serves
+  // every matrix at once).  So: two-stage for batches that hold a large
+  // matrix or many matrices.
+  {
+    int nmax = 0;
+    for (int g : ctx->order) nmax = std::max(nmax, ctx->geoms[g]->plan.nH);
+    const bool policy = (int)ctx->order.size() >= kTwoStageMinBatch || nmax >= kTwoStageMinN;
+    ctx->two_stage_batch = ctx->two_stage_force == 1 || (ctx->two_stage_force < 0 && policy);
+    ctx->two_stage_min_n = 1 << 30;
+  }
   std::stable_sort(ctx->order.begin(), ctx->order.end(),
                    [&](int a, int b) { return ctx->geoms[a]->plan.n > ctx->geoms[b]->plan.n; });
   for (int g : ctx->order) {
@@ -646,6 +660,8 @@ int prepare_batch(mbd_ctx* ctx, bool eigen) {
       }
   }
   ctx->n_band_jobs = (int)bjobs.size();
+  ctx->sweeps_in_flight = 0;
+  for (const BandJob& bj : bjobs) ctx->sweeps_in_flight += bj.n / (2 * kBand) + 1;
   ctx->n_sweep_items = (int)items.size();
   MBD_CUDA(ctx->sweep_progress.reserve(sizeof(int) * std::max<size_t>(items.size(), 1)));
   const size_t b_jobs = bytes_of<TridiagJob>(jobs.size());
@@ -746,7 +762,8 @@ int enqueue_batch(mbd_ctx* ctx, int mode) {
   }
   if (ctx->n_band_jobs > 0) {
     MBD_CUDA(launch_sb2st(ctx->band_jobs, ctx->n_band_jobs, ctx->sweep_items, ctx->n_sweep_items,
-                          ctx->sweep_progress.as<int>(), ctx->err_flag, ctx->num_sms, ctx->band_max_n, s));
+                          ctx->sweep_progress.as<int>(), ctx->err_flag, ctx->num_sms, ctx->band_max_n,
+                          ctx->sweeps_in_flight, s));
     ctx->launches += 3;
   }
   record_timing(ctx, ctx->bev[2], s);
@@ -824,11 +841,11 @@ int mbd_rsscs_create(mbd_ctx** out, int device) {
   MBD_CUDA(init_mixed_attributes());
   MBD_CUDA(init_sy2sb_attributes());
   {
-    // the two-stage tridiagonalisation serves the batch pipeline only when
-    // MBD_B200_TWO_STAGE=1 (the standalone eigenvalue call always uses it)
+    // reduction path per batch (prepare_batch): MBD_B200_TWO_STAGE=1 / 0
+    // forces the two-stage / one-stage path, otherwise a measured policy
     const char* ts = std::getenv("MBD_B200_TWO_STAGE");
     ctx->two_stage_max_n = sy2sb_max_n();
-    ctx->two_stage_batch = ts && ts[0] == '1';
+    ctx->two_stage_force = (ts && ts[0] == '1') ? 1 : ((ts && ts[0] == '0') ? 0 : -1);
   }
   MBD_CUDA(init_sb2st_attributes());
   ctx->trd_ctas_per_sm = std::max(1, tridiag_max_ctas_per_sm());
@@ -936,10 +953,13 @@ int mbd_rsscs_download(mbd_ctx* ctx, mbd_result* out) {
   };
   ctx->last_ms[Stage::kTotal] = elapsed(ctx->bev[0], ctx->bev[3]);
   ctx->last_ms[Stage::kTridiag] = elapsed(ctx->bev[1], ctx->bev[2]);
+  ctx->last_band_ms = 0.0;
+  ctx->last_chase_ms = ctx->last_ms[Stage::kTridiag];
   ctx->last_ms[Stage::kEig] = elapsed(ctx->bev[2], ctx->bev[3]);
   for (int g : ctx->order) {
     cudaEvent_t* evs = ctx->events.data() + (size_t)g * kGeomEvents;
     for (int k = 1; k < kGeomEvents; ++k) ctx->last_ms[k] += elapsed(evs[k - 1], evs[k]);   // [6]: dense -> band
+    ctx->last_band_ms += elapsed(evs[5], evs[6]);
   }
   ctx->d2h_bytes = sizeof(int);
   int first = MBD_OK;
@@ -1132,6 +1152,10 @@ void* mbd_rsscs_stream(mbd_ctx* ctx) { return ctx ? (void*)ctx->stream : nullptr
 int mbd_rsscs_last_timings(mbd_ctx* ctx, double* ms, int n) {
   if (!ctx || !ms || n < Stage::kCount) return MBD_ERR_ARG;
   for (int k = 0; k < Stage::kCount; ++k) ms[k] = ctx->last_ms[k];
+  if (n >= Stage::kCount + 2) {
+    ms[Stage::kCount] = ctx->last_band_ms;        // dense -> band, summed over geometries
+    ms[Stage::kCount + 1] = ctx->last_chase_ms;   // band (or dense, one-stage) -> tridiagonal, batch-wide
+  }
   return MBD_OK;
 }
 

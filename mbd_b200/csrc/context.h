@@ -116,6 +116,7 @@ struct mbd_ctx {
   mbd::SweepItem* sweep_items = nullptr;
   mbd::DevBuf sweep_progress;
   int n_band_jobs = 0, n_sweep_items = 0, band_max_n = 0;
+  long long sweeps_in_flight = 0;
   int n_trd_groups = 0, trd_total_ctas = 0, n_eig_jobs = 0, n_eig_batch = 0, eig_batch_max_n = 0;
   double trd_est_ms = 0.0;
   std::vector<int> order;                    // geometries that run, descending relay size
@@ -139,9 +140,12 @@ struct mbd_ctx {
   bool use_graphs = true;
   bool graph_replayed = false;               // the last compute ran as a graph replay
   int two_stage_max_n = 0;                   // largest matrix the two-stage reduction takes on this device
-  bool two_stage_batch = false;              // batches use the two-stage reduction
+  bool two_stage_batch = false;              // the whole batch uses the two-stage reduction
+  int two_stage_force = -1;                  // 1 / 0: forced on / off; -1: policy
+  int two_stage_min_n = 1 << 30;             // otherwise matrices from this size up use it
   bool capturing = false;
   double last_ms[mbd::Stage::kCount] = {0};
+  double last_band_ms = 0.0, last_chase_ms = 0.0;
   double launches = 0, h2d_bytes = 0, d2h_bytes = 0;
   int last_mode = 0;
   bool have_batch = false;
@@ -196,7 +200,11 @@ int reserve_learned(mbd_ctx* ctx);
 int band_to_tridiag_single(mbd_ctx* ctx, double* Br, int n, double* d, double* e, DevBuf& scratch, cudaStream_t s);
 int relay_learned(mbd_ctx* ctx, GeomDev* gd, RelaySlot& sl, size_t mstride, cudaEvent_t ev_net, double** X_out);
 
-// Matrices reduced by the two-stage path (larger ones by the one-stage kernel).
-inline bool two_stage(const mbd_ctx* ctx, int n) { return ctx->two_stage_batch && n <= ctx->two_stage_max_n; }
+// Matrices reduced by the two-stage path (the rest by the one-stage kernel).
+constexpr int kTwoStageMinN = 4500;      // a batch holding a matrix this large
+constexpr int kTwoStageMinBatch = 16;    // or this many geometries
+inline bool two_stage(const mbd_ctx* ctx, int n) {
+  return (ctx->two_stage_batch || n >= ctx->two_stage_min_n) && n <= ctx->two_stage_max_n;
+}
 
 }  // namespace mbd

@@ -21,6 +21,8 @@
 // One warp owns a task: lane l holds row l of D and of O in registers.
 #include <cuda_runtime.h>
 
+#include <algorithm>
+
 #include "kernels.h"
 #include "../../include/mbd_b200.h"
 
@@ -32,13 +34,20 @@ constexpr int LD = kBandLd;
 constexpr int WARPS = 4;
 constexpr long long kSpinCycles = 4000000000LL;   // ~2 s, then the wait gives up
 
-struct WarpSmem {
-  double v[B];        // current reflector
+// Shared memory of one warp pair (one sweep item): the reflector of the
+// current and of the next task (double-buffered by task parity), D-warp and
+// O-warp scratch.
+struct PairSmem {
+  double v[2][B];
   double w[B];
-  double v2[B];       // next reflector
   double s[B];
   double Ot[B][B + 1];
+  int go;             // the O-warp's verdict after its wait, read by both warps
 };
+
+__device__ __forceinline__ void pair_sync(int pair) {
+  asm volatile("bar.sync %0, 64;" ::"r"(pair + 1) : "memory");
+}
 
 __device__ __forceinline__ double warp_sum(double x) {
 #pragma unroll
@@ -60,14 +69,18 @@ __device__ __forceinline__ void st_release(int* p, int v) {
 __device__ bool wait_progress(const int* p, int target, int* err) {
   int ok = 1;
   if ((threadIdx.x & 31) == 0) {
+    // tight polling first (the predecessor is usually one task away), then
+    // exponential back-off so that far-behind warps do not load the L2
     const long long t0 = clock64();
+    unsigned ns = 0;
     while (ld_acquire(p) < target) {
       if (*(volatile int*)err != 0 || clock64() - t0 > kSpinCycles) {
         atomicCAS(err, 0, MBD_ERR_TIMEOUT);
         ok = 0;
         break;
       }
-      __nanosleep(32);
+      if (ns) __nanosleep(ns);
+      ns = ns == 0 ? 16 : (ns < 256 ? 2 * ns : 256);
     }
   }
   ok = __shfl_sync(0xffffffffu, ok, 0);
@@ -93,99 +106,135 @@ __device__ __forceinline__ double make_reflector(double x, int len, double* v, d
   return tau;
 }
 
+// Warp pair p of a CTA owns one sweep item at a time: warp 2p updates the
+// diagonal block D two-sided, warp 2p + 1 the block O below it (right apply,
+// next reflector, left apply); they meet at a named barrier once per task.
+constexpr int PAIRS = WARPS / 2;
 __global__ void __launch_bounds__(WARPS * 32) sb2st_kernel(const BandJob* jobs, const SweepItem* items,
                                                            int n_items, int* progress, int* err) {
-  __shared__ WarpSmem wsm[WARPS];
+  __shared__ PairSmem psm[PAIRS];
   const int warp = threadIdx.x / 32, l = threadIdx.x & 31;
-  WarpSmem& S = wsm[warp];
-  const int W = gridDim.x * WARPS;
-  for (int t = blockIdx.x * WARPS + warp; t < n_items; t += W) {
+  const int pair = warp / 2;
+  const bool owarp = (warp & 1) != 0;
+  PairSmem& S = psm[pair];
+  const int W = gridDim.x * PAIRS;
+  for (int t = blockIdx.x * PAIRS + pair; t < n_items; t += W) {
     const SweepItem it = items[t];
     const BandJob jb = jobs[it.job];
     const int n = jb.n, i = it.sweep;
     double* Br = jb.Br;
     const int K = (n - i - 1 + B - 1) / B;           // tasks of sweep i
     const int Kp = (n - i + B - 1) / B;              // tasks of sweep i - 1
-    double tau = 0.0, vl = 0.0;
+    double tau = 0.0, vl = 0.0;                      // current reflector (O-warp registers)
     for (int k = 0; k < K; ++k) {
-      if (it.pred >= 0 && !wait_progress(progress + it.pred, min(k + 2, Kp), err)) return;
+      // the O-warp waits for the previous sweep and decides for the pair; the
+      // D-warp follows it through the barrier (one verdict, both warps leave
+      // together)
+      if (owarp) {
+        const bool ok = it.pred < 0 || wait_progress(progress + it.pred, min(k + 2, Kp), err);
+        if (l == 0) S.go = ok && *(volatile int*)err == 0;
+      }
+      pair_sync(pair);
+      if (!S.go) return;
       const int r = i + 1 + k * B;
       const int L = min(B, n - r);
       const int rn = r + B;
       const int Ln = max(0, min(B, n - rn));
+      double* vcur = S.v[k & 1];
       if (k == 0) {
-        // reflector from column i: x[l] = A(i + 1 + l, i) = Br[i + 1 + l][1 + l]
-        const double x = (l < L) ? __ldcg(Br + (size_t)(r + l) * LD + 1 + l) : 0.0;
-        double beta;
-        tau = make_reflector(x, L, &vl, &beta);
-        if (l < L) Br[(size_t)(r + l) * LD + 1 + l] = (l == 0) ? beta : (tau != 0.0 ? 0.0 : x);
-      }
-      S.v[l] = vl;
-      // D row l (symmetric, from the lower band) and O row l
-      double dr[B], orow[B];
-#pragma unroll
-      for (int j = 0; j < B; ++j) {
-        double x = 0.0;
-        if (l < L && j < L) x = (j <= l) ? __ldcg(Br + (size_t)(r + l) * LD + (l - j))
-                                         : __ldcg(Br + (size_t)(r + j) * LD + (j - l));
-        dr[j] = x;
-        orow[j] = (l < Ln && j < L) ? __ldcg(Br + (size_t)(rn + l) * LD + (B + l - j)) : 0.0;
-      }
-      __syncwarp();
-      if (tau != 0.0) {
-        // D <- H D H:  w = tau D v - (tau^2 / 2)(v^T D v) v;  D -= v w^T + w v^T
-        double dv = 0.0;
-#pragma unroll
-        for (int j = 0; j < B; ++j) dv += dr[j] * S.v[j];
-        const double vdv = warp_sum(vl * dv);
-        const double wl = tau * dv - 0.5 * tau * tau * vdv * vl;
-        S.w[l] = wl;
-        __syncwarp();
-#pragma unroll
-        for (int j = 0; j < B; ++j) dr[j] -= vl * S.w[j] + wl * S.v[j];
-        // O <- O H = O - tau (O v) v^T
-        double ov = 0.0;
-#pragma unroll
-        for (int j = 0; j < B; ++j) ov += orow[j] * S.v[j];
-#pragma unroll
-        for (int j = 0; j < B; ++j) orow[j] -= tau * ov * S.v[j];
-      }
-      // next reflector from O[:, 0]; O <- H' O
-      double v2 = 0.0, tau2 = 0.0, beta2 = 0.0;
-      if (Ln > 0) {
-        tau2 = make_reflector(orow[0], Ln, &v2, &beta2);
-        if (tau2 != 0.0) {
-          S.v2[l] = v2;
-#pragma unroll
-          for (int j = 0; j < B; ++j) S.Ot[l][j] = orow[j];
-          __syncwarp();
-          double sj = 0.0;
-#pragma unroll
-          for (int q = 0; q < B; ++q) sj += S.v2[q] * S.Ot[q][l];   // lane l: column l of v2^T O
-          S.s[l] = sj;
-          __syncwarp();
-#pragma unroll
-          for (int j = 0; j < B; ++j) orow[j] -= tau2 * v2 * S.s[j];
-          orow[0] = (l == 0) ? beta2 : 0.0;
+        if (owarp) {
+          // reflector from column i: x[l] = A(i + 1 + l, i) = Br[i + 1 + l][1 + l]
+          const double x = (l < L) ? __ldcg(Br + (size_t)(r + l) * LD + 1 + l) : 0.0;
+          double beta;
+          tau = make_reflector(x, L, &vl, &beta);
+          if (l < L) Br[(size_t)(r + l) * LD + 1 + l] = (l == 0) ? beta : (tau != 0.0 ? 0.0 : x);
+          vcur[l] = vl;
+          S.w[0] = tau;   // tau for the D-warp (S.w is free before its first use)
         }
+        pair_sync(pair);
       }
-      // store D (lower part) and O
-      if (l < L) {
+      if (!owarp) {
+        // ---- D <- H D H:  w = tau D v - (tau^2 / 2)(v^T D v) v;  D -= v w^T + w v^T
+        const double tauD = (k == 0) ? S.w[0] : S.w[1];
+        __syncwarp();
+        double* rowD = Br + (size_t)(r + l) * LD + l;
+        double* colD = Br + (size_t)r * LD - l;
+        double dr[B];
 #pragma unroll
-        for (int j = 0; j < B; ++j)
-          if (j <= l) Br[(size_t)(r + l) * LD + (l - j)] = dr[j];
-      }
-      if (l < Ln) {
+        for (int j = 0; j < B; ++j) {
+          double x = 0.0;
+          if (l < L && j < L) x = (j <= l) ? __ldcg(rowD - j) : __ldcg(colD + j * (LD + 1));
+          dr[j] = x;
+        }
+        if (tauD != 0.0) {
+          const double vlD = vcur[l];
+          double dv = 0.0;
 #pragma unroll
-        for (int j = 0; j < B; ++j)
-          if (j < L) Br[(size_t)(rn + l) * LD + (B + l - j)] = orow[j];
+          for (int j = 0; j < B; ++j) dv += dr[j] * vcur[j];
+          const double vdv = warp_sum(vlD * dv);
+          const double wl = tauD * dv - 0.5 * tauD * tauD * vdv * vlD;
+          __syncwarp();
+          S.w[l] = wl;
+          __syncwarp();
+#pragma unroll
+          for (int j = 0; j < B; ++j) dr[j] -= vlD * S.w[j] + wl * vcur[j];
+          if (l < L) {
+#pragma unroll
+            for (int j = 0; j < B; ++j)
+              if (j <= l) rowD[-j] = dr[j];
+          }
+        }
+      } else {
+        // ---- O <- O H;  next reflector from O[:, 0];  O <- H' O
+        double* rowO = Br + (size_t)(rn + l) * LD + B + l;
+        double orow[B];
+#pragma unroll
+        for (int j = 0; j < B; ++j) orow[j] = (l < Ln && j < L) ? __ldcg(rowO - j) : 0.0;
+        if (tau != 0.0) {
+          double ov = 0.0;
+#pragma unroll
+          for (int j = 0; j < B; ++j) ov += orow[j] * vcur[j];
+#pragma unroll
+          for (int j = 0; j < B; ++j) orow[j] -= tau * ov * vcur[j];
+        }
+        double v2 = 0.0, tau2 = 0.0, beta2 = 0.0;
+        if (Ln > 0) {
+          tau2 = make_reflector(orow[0], Ln, &v2, &beta2);
+          if (tau2 != 0.0) {
+#pragma unroll
+            for (int j = 0; j < B; ++j) S.Ot[l][j] = orow[j];
+            S.v[(k + 1) & 1][l] = v2;
+            __syncwarp();
+            double sj = 0.0;
+#pragma unroll
+            for (int q = 0; q < B; ++q) sj += S.v[(k + 1) & 1][q] * S.Ot[q][l];   // column l of v2^T O
+            __syncwarp();
+            S.s[l] = sj;
+            __syncwarp();
+#pragma unroll
+            for (int j = 0; j < B; ++j) orow[j] -= tau2 * v2 * S.s[j];
+            orow[0] = (l == 0) ? beta2 : 0.0;
+          }
+          if (l < Ln) {
+#pragma unroll
+            for (int j = 0; j < B; ++j)
+              if (j < L) rowO[-j] = orow[j];
+          }
+        }
+        S.v[(k + 1) & 1][l] = v2;
+        tau = tau2;
+        vl = v2;
       }
       __threadfence();
-      __syncwarp();
-      if (l == 0) st_release(progress + t, k + 1);
-      tau = tau2;
-      vl = v2;
-      __syncwarp();
+      pair_sync(pair);
+      if (owarp) {
+        // the next task's tau for the D-warp, then publish this task
+        if (l == 0) {
+          S.w[1] = tau;
+          st_release(progress + t, k + 1);
+        }
+      }
+      pair_sync(pair);
     }
   }
 }
@@ -211,13 +260,16 @@ int sb2st_max_ctas(int num_sms) {
 }
 
 cudaError_t launch_sb2st(const BandJob* jobs, int n_jobs, const SweepItem* items, int n_items, int* progress,
-                         int* err, int num_sms, int max_n, cudaStream_t s) {
+                         int* err, int num_sms, int max_n, long long sweeps_in_flight, cudaStream_t s) {
   if (n_jobs < 1) return cudaSuccess;
   if (n_items > 0) {
     cudaError_t e = cudaMemsetAsync(progress, 0, sizeof(int) * (size_t)n_items, s);
     if (e != cudaSuccess) return e;
+    // workers: about three times the sweeps that can be in flight at once (a
+    // matrix keeps about n / (2 kBand) sweeps busy), within co-residency
     int grid = sb2st_max_ctas(num_sms);
-    const int need = (n_items + WARPS - 1) / WARPS;
+    const long long want_pairs = 3LL * sweeps_in_flight + 4 * PAIRS;
+    const int need = (int)((std::min<long long>(want_pairs, n_items) + PAIRS - 1) / PAIRS);
     if (grid > need) grid = need;
     void* args[] = {(void*)&jobs, (void*)&items, (void*)&n_items, (void*)&progress, (void*)&err};
     e = cudaLaunchCooperativeKernel((const void*)sb2st_kernel, dim3(grid), dim3(WARPS * 32), args, 0, s);

@@ -39,21 +39,18 @@ __device__ __forceinline__ double warp_sum(double v) {
   return v;
 }
 
-// CTA-wide sum (QR_THREADS threads); red holds QR_THREADS/32 doubles.
-__device__ double cta_sum(double v, double* red) {
-  v = warp_sum(v);
-  const int w = threadIdx.x / 32, l = threadIdx.x % 32;
-  __syncthreads();
-  if (l == 0) red[w] = v;
-  __syncthreads();
-  double s = 0.0;
-#pragma unroll
-  for (int q = 0; q < QR_THREADS / 32; ++q) s += red[q];
-  return s;
+// Shared layout of qr_panel: P[R][QR_LD] | pubN[2][8] norm partials per warp
+// | pubA[2] alpha | pubD[2][B] dot sums | dw[8][B] per-warp dots | gram[B][B]
+// | G[B][B] | Tm[B][B].  pub* are read by the other CTAs of the cluster
+// (double-buffered by column parity).  Warp w owns the local rows r = w mod 8,
+// lane c column c: a warp's update of its rows and the next column's norm over
+// the same rows need no CTA barrier; per column there is one __syncthreads and
+// two cluster barriers.
+constexpr int QR_WARPS = QR_THREADS / 32;
+__host__ __device__ constexpr size_t qr_panel_doubles(int R) {
+  return (size_t)R * QR_LD + 2 * QR_WARPS + 2 + 2 * B + QR_WARPS * B + 3 * B * B + 8;
 }
 
-// Shared layout of qr_panel: P[rows][QR_LD] | pub[2 + B] (values this CTA
-// publishes to the cluster) | gram[B*B] | misc
 __global__ void __launch_bounds__(QR_THREADS) qr_panel_kernel(PanelArgs a) {
   extern __shared__ double sm[];
   cg::cluster_group cl = cg::this_cluster();
@@ -63,99 +60,91 @@ __global__ void __launch_bounds__(QR_THREADS) qr_panel_kernel(PanelArgs a) {
   const int R = a.rows_per_cta;
   const int lo = rank * R, hi = min(m, lo + R);
   const int nr = max(0, hi - lo);
-  double* P = sm;                              // [R][QR_LD]
-  double* pub = sm + (size_t)R * QR_LD;        // [0] norm^2, [1] alpha, [2..2+B) dots
-  double* gram = pub + 2 + B;                  // [B][B]
-  double* red = gram + B * B;                  // [8]
-  double* rfl = red + 8;                       // tau, scale, beta, dsum[B]
-  const int tid = threadIdx.x;
-  // load the owned rows
+  double* P = sm;
+  double* pubN = P + (size_t)R * QR_LD;      // [2][QR_WARPS]
+  double* pubA = pubN + 2 * QR_WARPS;        // [2]
+  double* pubD = pubA + 2;                   // [2][B]
+  double* dw = pubD + 2 * B;                 // [QR_WARPS][B]
+  double* gram = dw + QR_WARPS * B;          // [B][B]
+  double* G = gram + B * B;
+  double* Tm = G + B * B;
+  const int tid = threadIdx.x, warp = tid / 32, lane = tid % 32;
   for (int idx = tid; idx < nr * B; idx += QR_THREADS) {
     const int r = idx / B, c = idx % B;
     P[r * QR_LD + c] = a.A[(size_t)(a.row0 + lo + r) * a.ld + a.col0 + c];
   }
   __syncthreads();
   const int nref = min(B, m);
-  for (int j = 0; j < nref; ++j) {
-    // ---- phase 1: norm^2 of column j below row j, alpha = P[j][j]
+  // norm partial of column j over this warp's rows below row j (lanes split the rows)
+  auto norm_part = [&](int j) {
     double s = 0.0;
-    for (int r = tid; r < nr; r += QR_THREADS) {
-      const int gr = lo + r;
-      if (gr > j) {
+    for (int r = warp + QR_WARPS * lane; r < nr; r += QR_THREADS) {
+      if (lo + r > j) {
         const double x = P[r * QR_LD + j];
         s += x * x;
       }
     }
-    s = cta_sum(s, red);
-    if (tid == 0) {
-      pub[0] = s;
-      pub[1] = (j >= lo && j < hi) ? P[(j - lo) * QR_LD + j] : 0.0;
-    }
+    return warp_sum(s);
+  };
+  double s_next = norm_part(0);
+  for (int j = 0; j < nref; ++j) {
+    const int par = j & 1;
+    // publish the norm partials and (owner CTA) alpha = P[j][j]
+    // (row j belongs to CTA j / R, warp (j - lo) % 8, which also updated it)
+    if (lane == 0) pubN[par * QR_WARPS + warp] = s_next;
+    if (lane == 0 && j >= lo && j < hi && (j - lo) % QR_WARPS == warp) pubA[par] = P[(j - lo) * QR_LD + j];
     cl.sync();
-    if (tid == 0) {
-      double xn2 = 0.0, alpha = 0.0;
-      for (int q = 0; q < C; ++q) {
-        const double* rp = cl.map_shared_rank(pub, q);
-        xn2 += rp[0];
-        alpha += rp[1];
-      }
-      double tau = 0.0, scale = 0.0, beta = alpha;
-      if (xn2 > 0.0) {
-        beta = -copysign(sqrt(alpha * alpha + xn2), alpha);
-        tau = (beta - alpha) / beta;
-        scale = 1.0 / (alpha - beta);
-      }
-      rfl[0] = tau;
-      rfl[1] = scale;
-      rfl[2] = beta;
-      if (rank == 0) a.tau[j] = tau;
+    double xn2 = 0.0;
+    for (int q = lane; q < C * QR_WARPS; q += 32)
+      xn2 += cl.map_shared_rank(pubN, q / QR_WARPS)[par * QR_WARPS + q % QR_WARPS];
+    xn2 = warp_sum(xn2);
+    double alpha = 0.0;
+    if (lane == 0) alpha = cl.map_shared_rank(pubA, j / R)[par];
+    alpha = __shfl_sync(0xffffffffu, alpha, 0);
+    double tau = 0.0, scale = 0.0, beta = alpha;
+    if (xn2 > 0.0) {
+      beta = -copysign(sqrt(alpha * alpha + xn2), alpha);
+      tau = (beta - alpha) / beta;
+      scale = 1.0 / (alpha - beta);
     }
-    __syncthreads();
-    const double tau = rfl[0], scale = rfl[1];
-    // ---- phase 2: v (in place below row j), dots d_c = v^T P[:, c], c > j
-    for (int r = tid; r < nr; r += QR_THREADS)
-      if (lo + r > j) P[r * QR_LD + j] *= scale;
-    __syncthreads();
-    {
-      // thread -> (column c = tid % 32, row phase = tid / 32)
-      const int c = tid % 32, ph = tid / 32;
-      double d = 0.0;
-      if (c > j)
-        for (int r = ph; r < nr; r += QR_THREADS / 32) {
-          const int gr = lo + r;
-          if (gr >= j) d += (gr == j ? 1.0 : P[r * QR_LD + j]) * P[r * QR_LD + c];
-        }
-      // reduce over the 8 row phases through shared memory (gram as scratch)
-      gram[ph * 32 + c] = d;
-      __syncthreads();
-      if (tid < 32) {
-        double t = 0.0;
-#pragma unroll
-        for (int q = 0; q < QR_THREADS / 32; ++q) t += gram[q * 32 + tid];
-        pub[2 + tid] = t;
-      }
-    }
-    cl.sync();
-    if (tid < 32) {
-      double t = 0.0;
-      if (tid > j)
-        for (int q = 0; q < C; ++q) t += cl.map_shared_rank(pub, q)[2 + tid];
-      rfl[3 + tid] = t;
-    }
-    __syncthreads();
-    if (tau != 0.0) {
-      for (int idx = tid; idx < nr * B; idx += QR_THREADS) {
-        const int r = idx / B, c = idx % B;
+    if (rank == 0 && tid == 0) a.tau[j] = tau;
+    // dots d_c = v^T P[:, c] over this warp's rows (lane c), v_j = 1
+    double d = 0.0;
+    if (tau != 0.0)
+      for (int r = warp; r < nr; r += QR_WARPS) {
         const int gr = lo + r;
-        if (c > j && gr >= j) {
-          const double v = (gr == j) ? 1.0 : P[r * QR_LD + j];
-          P[r * QR_LD + c] -= tau * v * rfl[3 + c];
-        }
+        if (gr < j) continue;
+        const double v = (gr == j) ? 1.0 : P[r * QR_LD + j] * scale;
+        d += v * P[r * QR_LD + lane];
       }
-    }
-    if (tid == 0 && j >= lo && j < hi) P[(j - lo) * QR_LD + j] = rfl[2];
+    dw[warp * B + lane] = d;
     __syncthreads();
+    if (warp == 0) {
+      double t = 0.0;
+#pragma unroll
+      for (int q = 0; q < QR_WARPS; ++q) t += dw[q * B + lane];
+      pubD[par * B + lane] = t;
+    }
+    cl.sync();
+    double dc = 0.0;
+    for (int q = 0; q < C; ++q) dc += cl.map_shared_rank(pubD, q)[par * B + lane];
+    // update the remaining columns of this warp's rows, then store v in column j
+    if (tau != 0.0) {
+      for (int r = warp; r < nr; r += QR_WARPS) {
+        const int gr = lo + r;
+        if (gr < j) continue;
+        const double v = (gr == j) ? 1.0 : P[r * QR_LD + j] * scale;
+        if (lane > j) P[r * QR_LD + lane] -= tau * v * dc;
+      }
+      __syncwarp();
+      for (int r = warp + QR_WARPS * lane; r < nr; r += QR_THREADS)
+        if (lo + r > j) P[r * QR_LD + j] *= scale;
+    }
+    if (j >= lo && j < hi && (j - lo) % QR_WARPS == warp && lane == 0) P[(j - lo) * QR_LD + j] = beta;
+    __syncwarp();
+    if (j + 1 < nref) s_next = norm_part(j + 1);
   }
+  __syncthreads();
   // ---- Gram matrix G = V^T V (V unit lower trapezoidal), summed over the cluster
   for (int e = tid; e < B * B; e += QR_THREADS) {
     const int p = e / B, q = e % B;
@@ -179,8 +168,6 @@ __global__ void __launch_bounds__(QR_THREADS) qr_panel_kernel(PanelArgs a) {
   cl.sync();
   if (rank == 0) {
     // T (upper triangular): T[j][j] = tau_j, T[0:j, j] = -tau_j T[0:j, 0:j] G[0:j, j]
-    double* G = rfl + 3 + B;       // [B][B] summed Gram
-    double* Tm = G + B * B;        // [B][B]
     for (int e = tid; e < B * B; e += QR_THREADS) {
       double g = 0.0;
       for (int q = 0; q < C; ++q) g += cl.map_shared_rank(gram, q)[e];
@@ -206,74 +193,87 @@ __global__ void __launch_bounds__(QR_THREADS) qr_panel_kernel(PanelArgs a) {
   cl.sync();   // no CTA leaves while another may still read its shared memory
 }
 
+// FP64 tensor-core MMA, D = A B + D with A 8x4 (row), B 4x8 (col), D 8x8:
+// a = A[lane/4][lane%4], b = B[lane%4][lane/4], d = D[lane/4][2*(lane%4) + {0,1}].
+__device__ __forceinline__ void dmma(double& d0, double& d1, double a, double b) {
+  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};"
+               : "+d"(d0), "+d"(d1)
+               : "d"(a), "d"(b));
+}
+
+// Shared-memory row stride (doubles) making the 8 x 4 fragment loads of a
+// half-warp hit 16 distinct bank pairs: stride = 4 (mod 16).
+constexpr int FS = TL + 4;   // 68
+
 // Y partials: Yp[s][r][c] = sum over column tiles J of chunk s of (A22 V)[r][c],
-// row block I = blockIdx.x (64 rows), chunk s = blockIdx.y.  64 threads, 8 x 4
-// outputs each.
-constexpr size_t kSymmSmem = sizeof(double) * (TL * (TL + 1) + TL * (B + 1));
-__global__ void __launch_bounds__(64) symm_kernel(const double* A, int ld, int row0, int m, const double* V,
-                                                  double* Yp, int chunk) {
+// row block I = blockIdx.x (64 rows), chunk s = blockIdx.y.  4 warps, each 16
+// rows x 32 columns of the block (2 x 4 MMA tiles).
+constexpr size_t kSymmSmem = sizeof(double) * (TL * FS + B * FS);
+__global__ void __launch_bounds__(128) symm_kernel(const double* A, int ld, int row0, int m, const double* V,
+                                                   double* Yp, int chunk) {
   extern __shared__ double dsm[];
-  double (*As)[TL + 1] = reinterpret_cast<double (*)[TL + 1]>(dsm);
-  double (*Vs)[B + 1] = reinterpret_cast<double (*)[B + 1]>(dsm + TL * (TL + 1));
+  double* As = dsm;              // [64][FS]: As[r][k] = A22(I*64 + r, J*64 + k)
+  double* Vt = dsm + TL * FS;    // [32][FS]: Vt[c][k] = V(J*64 + k, c)
   const int I = blockIdx.x, s = blockIdx.y;
   const int nt = (m + TL - 1) / TL;
   const int J0 = s * chunk, J1 = min(nt, J0 + chunk);
-  const int tid = threadIdx.x;
-  const int r0 = (tid / 8) * 8, c0 = (tid % 8) * 4;
-  double acc[8][4];
+  const int tid = threadIdx.x, warp = tid / 32, lane = tid % 32;
+  const int g = lane >> 2, q4 = lane & 3;
+  double acc[2][4][2];
 #pragma unroll
-  for (int i = 0; i < 8; ++i)
+  for (int i = 0; i < 2; ++i)
 #pragma unroll
-    for (int q = 0; q < 4; ++q) acc[i][q] = 0.0;
+    for (int q = 0; q < 4; ++q) acc[i][q][0] = acc[i][q][1] = 0.0;
   const double* A22 = A + (size_t)row0 * ld + row0;
   for (int J = J0; J < J1; ++J) {
     __syncthreads();
-    // tile (I, J) of the symmetric A22 as As[r][k] = A22(I*64 + r, J*64 + k)
-    for (int idx = tid; idx < TL * TL; idx += 64) {
-      const int u = idx / TL, w = idx % TL;   // u: outer (row of the stored tile), w: contiguous
+    for (int idx = tid; idx < TL * TL; idx += 128) {
+      const int u = idx / TL, w = idx % TL;   // w contiguous in global memory
       double x = 0.0;
       if (J < I) {
         const int gr = I * TL + u, gc = J * TL + w;
         if (gr < m) x = A22[(size_t)gr * ld + gc];
-        As[u][w] = x;
+        As[u * FS + w] = x;
       } else if (J > I) {
         const int gr = J * TL + u, gc = I * TL + w;   // stored tile (J, I), transposed into As
         if (gr < m && gc < m) x = A22[(size_t)gr * ld + gc];
-        As[w][u] = x;
+        As[w * FS + u] = x;
       } else {
-        // diagonal tile: the stored lower element of (u, w) or of its mirror
         const int a_ = u >= w ? u : w, b_ = u >= w ? w : u;
         const int gr = I * TL + a_, gc = I * TL + b_;
         if (gr < m) x = A22[(size_t)gr * ld + gc];
-        As[u][w] = x;
+        As[u * FS + w] = x;
       }
     }
-    for (int idx = tid; idx < TL * B; idx += 64) {
+    for (int idx = tid; idx < TL * B; idx += 128) {
       const int k = idx / B, c = idx % B;
       const int gk = J * TL + k;
-      Vs[k][c] = gk < m ? V[(size_t)gk * B + c] : 0.0;
+      Vt[c * FS + k] = gk < m ? V[(size_t)gk * B + c] : 0.0;
     }
     __syncthreads();
 #pragma unroll 4
-    for (int k = 0; k < TL; ++k) {
-      double av[8], vv[4];
+    for (int k0 = 0; k0 < TL; k0 += 4) {
+      double af[2], bf[4];
 #pragma unroll
-      for (int i = 0; i < 8; ++i) av[i] = As[r0 + i][k];
+      for (int i = 0; i < 2; ++i) af[i] = As[(warp * 16 + i * 8 + g) * FS + k0 + q4];
 #pragma unroll
-      for (int q = 0; q < 4; ++q) vv[q] = Vs[k][c0 + q];
+      for (int q = 0; q < 4; ++q) bf[q] = Vt[(q * 8 + g) * FS + k0 + q4];
 #pragma unroll
-      for (int i = 0; i < 8; ++i)
+      for (int i = 0; i < 2; ++i)
 #pragma unroll
-        for (int q = 0; q < 4; ++q) acc[i][q] = fma(av[i], vv[q], acc[i][q]);
+        for (int q = 0; q < 4; ++q) dmma(acc[i][q][0], acc[i][q][1], af[i], bf[q]);
     }
   }
   double* out = Yp + (size_t)s * m * B;
 #pragma unroll
-  for (int i = 0; i < 8; ++i) {
-    const int gr = I * TL + r0 + i;
+  for (int i = 0; i < 2; ++i) {
+    const int gr = I * TL + warp * 16 + i * 8 + g;
     if (gr < m)
 #pragma unroll
-      for (int q = 0; q < 4; ++q) out[(size_t)gr * B + c0 + q] = acc[i][q];
+      for (int q = 0; q < 4; ++q) {
+        out[(size_t)gr * B + q * 8 + 2 * q4] = acc[i][q][0];
+        out[(size_t)gr * B + q * 8 + 2 * q4 + 1] = acc[i][q][1];
+      }
   }
 }
 
@@ -358,59 +358,64 @@ __global__ void __launch_bounds__(256) zform_kernel(const double* Y, const doubl
   }
 }
 
-// A22 -= V Z^T + Z V^T on lower 64 x 64 tiles; 64 threads, 8 x 8 outputs each.
-constexpr size_t kSyr2kSmem = sizeof(double) * 2 * TL * (2 * B + 1);
-__global__ void __launch_bounds__(64) syr2k_kernel(double* A, int ld, int row0, int m, const double* V,
-                                                   const double* Z) {
+// A22 -= V Z^T + Z V^T on lower 64 x 64 tiles: [V_I | Z_I] [Z_J | V_J]^T
+// (K = 64) on FP64 MMAs; 4 warps, each a 32 x 32 quarter (4 x 4 MMA tiles).
+constexpr size_t kSyr2kSmem = sizeof(double) * 2 * TL * FS;
+__global__ void __launch_bounds__(128) syr2k_kernel(double* A, int ld, int row0, int m, const double* V,
+                                                    const double* Z) {
   extern __shared__ double dsm[];
-  double (*Li)[2 * B + 1] = reinterpret_cast<double (*)[2 * B + 1]>(dsm);                  // [V_I | Z_I]
-  double (*Lj)[2 * B + 1] = reinterpret_cast<double (*)[2 * B + 1]>(dsm + TL * (2 * B + 1));  // [Z_J | V_J]
+  double* Li = dsm;              // [64][FS]: [V_I | Z_I]
+  double* Lj = dsm + TL * FS;    // [64][FS]: [Z_J | V_J]
   int ti = (int)((sqrt(8.0 * blockIdx.x + 1.0) - 1.0) * 0.5);
   while ((ti + 1) * (ti + 2) / 2 <= (int)blockIdx.x) ++ti;
   while (ti * (ti + 1) / 2 > (int)blockIdx.x) --ti;
   const int tj = (int)blockIdx.x - ti * (ti + 1) / 2;
-  const int tid = threadIdx.x;
-  for (int e = tid; e < TL * B; e += 64) {
+  const int tid = threadIdx.x, warp = tid / 32, lane = tid % 32;
+  const int g = lane >> 2, q4 = lane & 3;
+  for (int e = tid; e < TL * B; e += 128) {
     const int r = e / B, c = e % B;
     const int gi = ti * TL + r, gj = tj * TL + r;
     const bool li = gi < m, lj = gj < m;
-    Li[r][c] = li ? V[(size_t)gi * B + c] : 0.0;
-    Li[r][B + c] = li ? Z[(size_t)gi * B + c] : 0.0;
-    Lj[r][c] = lj ? Z[(size_t)gj * B + c] : 0.0;
-    Lj[r][B + c] = lj ? V[(size_t)gj * B + c] : 0.0;
+    Li[r * FS + c] = li ? V[(size_t)gi * B + c] : 0.0;
+    Li[r * FS + B + c] = li ? Z[(size_t)gi * B + c] : 0.0;
+    Lj[r * FS + c] = lj ? Z[(size_t)gj * B + c] : 0.0;
+    Lj[r * FS + B + c] = lj ? V[(size_t)gj * B + c] : 0.0;
   }
   __syncthreads();
-  const int r0 = (tid / 8) * 8, c0 = (tid % 8) * 8;
-  double acc[8][8];
+  const int r0 = (warp / 2) * 32, c0 = (warp % 2) * 32;
+  if (ti == tj && c0 > r0) return;   // strictly upper quarter of a diagonal tile
+  double acc[4][4][2];
 #pragma unroll
-  for (int i = 0; i < 8; ++i)
+  for (int i = 0; i < 4; ++i)
 #pragma unroll
-    for (int q = 0; q < 8; ++q) acc[i][q] = 0.0;
+    for (int q = 0; q < 4; ++q) acc[i][q][0] = acc[i][q][1] = 0.0;
 #pragma unroll 2
-  for (int k = 0; k < 2 * B; ++k) {
-    double x[8], y[8];
+  for (int k0 = 0; k0 < 2 * B; k0 += 4) {
+    double af[4], bf[4];
 #pragma unroll
-    for (int i = 0; i < 8; ++i) x[i] = Li[r0 + i][k];
+    for (int i = 0; i < 4; ++i) af[i] = Li[(r0 + i * 8 + g) * FS + k0 + q4];
 #pragma unroll
-    for (int q = 0; q < 8; ++q) y[q] = Lj[c0 + q][k];
+    for (int q = 0; q < 4; ++q) bf[q] = Lj[(c0 + q * 8 + g) * FS + k0 + q4];
 #pragma unroll
-    for (int i = 0; i < 8; ++i)
+    for (int i = 0; i < 4; ++i)
 #pragma unroll
-      for (int q = 0; q < 8; ++q) acc[i][q] = fma(x[i], y[q], acc[i][q]);
+      for (int q = 0; q < 4; ++q) dmma(acc[i][q][0], acc[i][q][1], af[i], bf[q]);
   }
   double* A22 = A + (size_t)row0 * ld + row0;
 #pragma unroll
-  for (int i = 0; i < 8; ++i) {
-    const int gr = ti * TL + r0 + i;
+  for (int i = 0; i < 4; ++i) {
+    const int gr = ti * TL + r0 + i * 8 + g;
     if (gr >= m) continue;
 #pragma unroll
-    for (int q = 0; q < 8; ++q) {
-      const int gc = tj * TL + c0 + q;
-      if (gc <= gr) {
-        double* p = A22 + (size_t)gr * ld + gc;
-        *p -= acc[i][q];
+    for (int q = 0; q < 4; ++q)
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        const int gc = tj * TL + c0 + q * 8 + 2 * q4 + h;
+        if (gc <= gr) {
+          double* p = A22 + (size_t)gr * ld + gc;
+          *p -= acc[i][q][h];
+        }
       }
-    }
   }
 }
 
@@ -426,9 +431,7 @@ __global__ void band_copy_kernel(const double* A, int ld, int n, double* Br) {
 
 }  // namespace
 
-size_t qr_panel_smem(int rows_per_cta) {
-  return sizeof(double) * ((size_t)rows_per_cta * QR_LD + 2 + B + B * B + 8 + 3 + B + 2 * B * B);
-}
+size_t qr_panel_smem(int rows_per_cta) { return sizeof(double) * qr_panel_doubles(rows_per_cta); }
 
 cudaError_t init_sy2sb_attributes() {
   cudaError_t e = cudaFuncSetAttribute(qr_panel_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -441,8 +444,8 @@ cudaError_t init_sy2sb_attributes() {
   return cudaFuncSetAttribute(syr2k_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSyr2kSmem);
 }
 
-// Largest n whose panels fit the biggest cluster this device can run.
-int sy2sb_max_n() {
+// Largest panel-QR cluster this device can run (0: none), probed once.
+int probe_max_cluster() {
   for (int C = kPanelMaxCluster; C >= 1; C /= 2) {
     cudaLaunchConfig_t cfg{};
     cfg.gridDim = dim3(C);
@@ -456,11 +459,23 @@ int sy2sb_max_n() {
     cfg.attrs = attr;
     cfg.numAttrs = 1;
     int clusters = 0;
-    if (cudaOccupancyMaxActiveClusters(&clusters, qr_panel_kernel, &cfg) == cudaSuccess && clusters > 0)
-      return C * kPanelMaxRowsPerCta + kBand;
+    if (cudaOccupancyMaxActiveClusters(&clusters, qr_panel_kernel, &cfg) == cudaSuccess && clusters > 0) return C;
     cudaGetLastError();
   }
   return 0;
+}
+
+int g_max_cluster = -1;
+
+int sy2sb_max_cluster() {
+  if (g_max_cluster < 0) g_max_cluster = probe_max_cluster();
+  return g_max_cluster;
+}
+
+// Largest n whose panels fit the biggest cluster this device can run.
+int sy2sb_max_n() {
+  const int C = sy2sb_max_cluster();
+  return C > 0 ? C * kPanelMaxRowsPerCta + kBand : 0;
 }
 
 size_t sy2sb_workspace_doubles(int n) {
@@ -470,6 +485,7 @@ size_t sy2sb_workspace_doubles(int n) {
 }
 
 cudaError_t launch_sy2sb(double* A, int ld, int n, double* ws, double* Br, int num_sms, cudaStream_t s) {
+  const int max_cluster = sy2sb_max_cluster();
   const int nt_full = (n + TL - 1) / TL;
   double* V = ws;
   double* Y = V + (size_t)n * B;
@@ -483,6 +499,7 @@ cudaError_t launch_sy2sb(double* A, int ld, int n, double* ws, double* Br, int n
     const int row0 = c0 + B, m = n - row0;
     // panel QR in one cluster (a power of two of CTAs)
     int C = 1;
+    while (C * kPanelRowsTarget < m && C < max_cluster) C *= 2;
     while (C * kPanelMaxRowsPerCta < m) C *= 2;
     if (C > kPanelMaxCluster) return cudaErrorInvalidValue;   // the caller keeps n <= sy2sb_max_n()
     const int R = (m + C - 1) / C;
@@ -508,11 +525,11 @@ cudaError_t launch_sy2sb(double* A, int ld, int n, double* ws, double* Br, int n
     if (S > nt) S = nt;
     const int chunk = (nt + S - 1) / S;
     S = (nt + chunk - 1) / chunk;
-    symm_kernel<<<dim3(nt, S), 64, kSymmSmem, s>>>(A, ld, row0, m, V, Yp, chunk);
+    symm_kernel<<<dim3(nt, S), 128, kSymmSmem, s>>>(A, ld, row0, m, V, Yp, chunk);
     yred_kernel<<<nt, 256, 0, s>>>(Yp, S, m, T, V, Y, Up);
     mform_kernel<<<1, B * B, 0, s>>>(Up, nt, T, M);
     zform_kernel<<<nt, 256, 0, s>>>(Y, V, M, m, Z);
-    syr2k_kernel<<<nt * (nt + 1) / 2, 64, kSyr2kSmem, s>>>(A, ld, row0, m, V, Z);
+    syr2k_kernel<<<nt * (nt + 1) / 2, 128, kSyr2kSmem, s>>>(A, ld, row0, m, V, Z);
   }
   band_copy_kernel<<<(unsigned)(((long long)n * kBandLd + 255) / 256), 256, 0, s>>>(A, ld, n, Br);
   return cudaGetLastError();

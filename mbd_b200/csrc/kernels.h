@@ -149,6 +149,7 @@ void launch_energy(const double* ev, int n, int nsl, const double* scalars, doub
 constexpr int kBand = 32;                    // half-bandwidth of the intermediate band
 constexpr int kBandLd = 2 * kBand + 1;       // band row: A(r, r - d), d = 0..2 kBand (room for bulges)
 constexpr int kPanelMaxRowsPerCta = 768;     // panel rows one CTA keeps in shared memory
+constexpr int kPanelRowsTarget = 384;        // fewer rows per CTA while the cluster can grow
 constexpr int kPanelMaxCluster = 16;         // CTAs of the panel-QR cluster
 constexpr int kSymmMaxSplit = 16;
 constexpr int kTwoStageMaxN = kPanelMaxRowsPerCta * kPanelMaxCluster;
@@ -164,6 +165,7 @@ struct PanelArgs {
 };
 cudaError_t init_sy2sb_attributes();
 int sy2sb_max_n();
+int sy2sb_max_cluster();
 size_t sy2sb_workspace_doubles(int n);
 // Dense (lower, row-major, ld) -> band: A is overwritten; Br[n][kBandLd]
 // receives the band (diagonal d = 0..kBand, zero beyond).  ws: workspace.
@@ -182,8 +184,10 @@ struct BandJob {
 struct SweepItem {
   int job, sweep, pred, pad;
 };
+// sweeps_in_flight: sum over jobs of n / (2 kBand), the concurrency the
+// sweep pipeline offers (sizes the worker count).
 cudaError_t launch_sb2st(const BandJob* jobs, int n_jobs, const SweepItem* items, int n_items, int* progress,
-                         int* err, int num_sms, int max_n, cudaStream_t s);
+                         int* err, int num_sms, int max_n, long long sweeps_in_flight, cudaStream_t s);
 cudaError_t init_sb2st_attributes();
 
 // ---- block-CG relay solve of the MIXED_LEARNED mode (UTILS.f90:469-473) ----

@@ -355,8 +355,8 @@ class Engine:
         return int(self.lib.mbd_rsscs_stream(self.ctx) or 0)
 
     def timings(self) -> dict:
-        buf = (ctypes.c_double * 8)()
-        self.lib.mbd_rsscs_last_timings(self.ctx, buf, 8)
+        buf = (ctypes.c_double * 10)()
+        self.lib.mbd_rsscs_last_timings(self.ctx, buf, 10)
         keys = ["total", "setup", "relay_build", "relay_factor", "relay_solve", "cfdm_build",
-                "tridiag", "eig_energy"]
+                "tridiag", "eig_energy", "tridiag_dense_to_band", "tridiag_to_tridiagonal"]
         return dict(zip(keys, list(buf)))
