@@ -94,9 +94,16 @@ __global__ void __launch_bounds__(QR_THREADS) qr_panel_kernel(PanelArgs a) {
     if (lane == 0) pubN[par * QR_WARPS + warp] = s_next;
     if (lane == 0 && j >= lo && j < hi && (j - lo) % QR_WARPS == warp) pubA[par] = P[(j - lo) * QR_LD + j];
     cl.sync();
+    // all remote loads first (independent), then the sums
+    double xparts[kPanelMaxCluster * QR_WARPS / 32];
+#pragma unroll
+    for (int u = 0; u < kPanelMaxCluster * QR_WARPS / 32; ++u) {
+      const int q = lane + 32 * u;
+      xparts[u] = (q < C * QR_WARPS) ? cl.map_shared_rank(pubN, q / QR_WARPS)[par * QR_WARPS + q % QR_WARPS] : 0.0;
+    }
     double xn2 = 0.0;
-    for (int q = lane; q < C * QR_WARPS; q += 32)
-      xn2 += cl.map_shared_rank(pubN, q / QR_WARPS)[par * QR_WARPS + q % QR_WARPS];
+#pragma unroll
+    for (int u = 0; u < kPanelMaxCluster * QR_WARPS / 32; ++u) xn2 += xparts[u];
     xn2 = warp_sum(xn2);
     double alpha = 0.0;
     if (lane == 0) alpha = cl.map_shared_rank(pubA, j / R)[par];
@@ -110,13 +117,23 @@ __global__ void __launch_bounds__(QR_THREADS) qr_panel_kernel(PanelArgs a) {
     if (rank == 0 && tid == 0) a.tau[j] = tau;
     // dots d_c = v^T P[:, c] over this warp's rows (lane c), v_j = 1
     double d = 0.0;
-    if (tau != 0.0)
-      for (int r = warp; r < nr; r += QR_WARPS) {
-        const int gr = lo + r;
-        if (gr < j) continue;
-        const double v = (gr == j) ? 1.0 : P[r * QR_LD + j] * scale;
-        d += v * P[r * QR_LD + lane];
+    if (tau != 0.0) {
+      double d1 = 0.0;   // two accumulation chains
+      int r = warp;
+      for (; r + QR_WARPS < nr; r += 2 * QR_WARPS) {
+        const int g0 = lo + r, g1 = g0 + QR_WARPS;
+        const double v0 = g0 < j ? 0.0 : (g0 == j ? 1.0 : P[r * QR_LD + j] * scale);
+        const double v1 = g1 < j ? 0.0 : (g1 == j ? 1.0 : P[(r + QR_WARPS) * QR_LD + j] * scale);
+        d += v0 * P[r * QR_LD + lane];
+        d1 += v1 * P[(r + QR_WARPS) * QR_LD + lane];
       }
+      if (r < nr) {
+        const int g0 = lo + r;
+        const double v0 = g0 < j ? 0.0 : (g0 == j ? 1.0 : P[r * QR_LD + j] * scale);
+        d += v0 * P[r * QR_LD + lane];
+      }
+      d += d1;
+    }
     dw[warp * B + lane] = d;
     __syncthreads();
     if (warp == 0) {
@@ -126,8 +143,12 @@ __global__ void __launch_bounds__(QR_THREADS) qr_panel_kernel(PanelArgs a) {
       pubD[par * B + lane] = t;
     }
     cl.sync();
+    double dparts[kPanelMaxCluster];
+#pragma unroll
+    for (int q = 0; q < kPanelMaxCluster; ++q) dparts[q] = (q < C) ? cl.map_shared_rank(pubD, q)[par * B + lane] : 0.0;
     double dc = 0.0;
-    for (int q = 0; q < C; ++q) dc += cl.map_shared_rank(pubD, q)[par * B + lane];
+#pragma unroll
+    for (int q = 0; q < kPanelMaxCluster; ++q) dc += dparts[q];
     // update the remaining columns of this warp's rows, then store v in column j
     if (tau != 0.0) {
       for (int r = warp; r < nr; r += QR_WARPS) {
