@@ -21,6 +21,8 @@
 #include <cooperative_groups.h>
 #include <cuda_runtime.h>
 
+#include <cstdlib>
+
 #include "kernels.h"
 
 namespace cg = cooperative_groups;
@@ -507,6 +509,12 @@ size_t sy2sb_workspace_doubles(int n) {
 
 cudaError_t launch_sy2sb(double* A, int ld, int n, double* ws, double* Br, int num_sms, cudaStream_t s) {
   const int max_cluster = sy2sb_max_cluster();
+  // panel rows per CTA the cluster size aims at (MBD_B200_PANEL_ROWS overrides)
+  static const int rows_target = [] {
+    const char* e = std::getenv("MBD_B200_PANEL_ROWS");
+    const int v = e ? std::atoi(e) : 0;
+    return (v >= 32 && v <= kPanelMaxRowsPerCta) ? v : kPanelRowsTarget;
+  }();
   const int nt_full = (n + TL - 1) / TL;
   double* V = ws;
   double* Y = V + (size_t)n * B;
@@ -520,7 +528,7 @@ cudaError_t launch_sy2sb(double* A, int ld, int n, double* ws, double* Br, int n
     const int row0 = c0 + B, m = n - row0;
     // panel QR in one cluster (a power of two of CTAs)
     int C = 1;
-    while (C * kPanelRowsTarget < m && C < max_cluster) C *= 2;
+    while (C * rows_target < m && C < max_cluster) C *= 2;
     while (C * kPanelMaxRowsPerCta < m) C *= 2;
     if (C > kPanelMaxCluster) return cudaErrorInvalidValue;   // the caller keeps n <= sy2sb_max_n()
     const int R = (m + C - 1) / C;
