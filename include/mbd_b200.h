@@ -172,7 +172,9 @@ int mbd_rsscs_last_timings(mbd_ctx* ctx, double* ms, int n);
  * by mbd_rsscs_compute, [1] host->device bytes copied by mbd_rsscs_upload,
  * [2] device->host bytes copied by mbd_rsscs_download, [3] (n >= 4) 1 when
  * the last compute replayed the batch's captured CUDA graph, 0 when it
- * launched the kernels one by one.  n must be >= 3. */
+ * launched the kernels one by one (the first compute of an uploaded batch in
+ * a mode launches directly; the second captures the graph and replays it
+ * from then on).  n must be >= 3. */
 int mbd_rsscs_last_stats(mbd_ctx* ctx, double* out, int n);
 
 /* The CUDA stream (cudaStream_t) every kernel of this context runs on, so a

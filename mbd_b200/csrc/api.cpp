@@ -525,6 +525,7 @@ int plan_slots(mbd_ctx* ctx) {
 // the device job tables of the uploaded batch.
 int prepare_batch(mbd_ctx* ctx, bool eigen) {
   drop_graphs(ctx);
+  for (int& k : ctx->mode_runs) k = 0;
   ctx->order.clear();
   for (size_t g = 0; g < ctx->geoms.size(); ++g)
     if (ctx->geoms[g]->status_host == MBD_OK) ctx->order.push_back((int)g);
@@ -927,8 +928,11 @@ int mbd_rsscs_compute(mbd_ctx* ctx, int mode) {
     if (st != MBD_OK) return st;
   }
   ctx->last_mode = mode;
-  // replay the captured graph of this batch and mode (capture it first)
-  if (ctx->use_graphs && !ctx->graph[mode] && !capture_batch(ctx, mode)) ctx->use_graphs = false;
+  // From the second compute of a batch in a mode on, capture the batch into a
+  // CUDA graph once and replay it; a batch computed once (energy_batch, an
+  // upload per call) is launched directly and does not pay for the capture.
+  const bool repeat = ctx->mode_runs[mode]++ > 0;
+  if (ctx->use_graphs && repeat && !ctx->graph[mode] && !capture_batch(ctx, mode)) ctx->use_graphs = false;
   if (ctx->use_graphs && ctx->graph[mode]) {
     ctx->launches = ctx->graph_launches[mode];
     ctx->graph_replayed = true;

@@ -144,6 +144,7 @@ struct mbd_ctx {
   int two_stage_force = -1;                  // 1 / 0: forced on / off; -1: policy
   int two_stage_min_n = 1 << 30;             // otherwise matrices from this size up use it
   bool capturing = false;
+  int mode_runs[3] = {0, 0, 0};              // computes of the uploaded batch, per mode
   double last_ms[mbd::Stage::kCount] = {0};
   double last_band_ms = 0.0, last_chase_ms = 0.0;
   double launches = 0, h2d_bytes = 0, d2h_bytes = 0;

@@ -143,12 +143,15 @@ __global__ void __launch_bounds__(192) cg_tile_kernel(CgArgs a, const double* in
   const int tid = threadIdx.x;
   const bool diag = ti == tj;
   const int n = a.n;
-  for (int idx = tid; idx < CT * CT; idx += blockDim.x) {
-    const int r = idx / CT, c = idx % CT;
+  // 16-byte loads (rows start 16-byte aligned: ld is a multiple of 32; the
+  // second element of a pair may lie in the row padding, masked below)
+  for (int idx = tid; idx < CT * CT / 2; idx += blockDim.x) {
+    const int r = idx / (CT / 2), c = 2 * (idx % (CT / 2));
     const int gr = ti * CT + r, gc = tj * CT + c;
-    double v = 0.0;
-    if (gr < n && gc < n && (!diag || c <= r)) v = A[(size_t)gr * a.ld + gc];
-    Ts[r][c] = v;
+    double2 v = make_double2(0.0, 0.0);
+    if (gr < n && gc < n && (!diag || c <= r)) v = *reinterpret_cast<const double2*>(A + (size_t)gr * a.ld + gc);
+    Ts[r][c] = v.x;
+    Ts[r][c + 1] = (gc + 1 < n && (!diag || c + 1 <= r)) ? v.y : 0.0;
   }
   for (int idx = tid; idx < CT * 3; idx += blockDim.x) {
     const int r = idx / 3, q = idx % 3;
