@@ -37,12 +37,16 @@ sys.path.insert(0, ROOT)
 
 METRIC = "MBD energies/s, mixed+batched+learned vs plain FP64 on 1 B200, |dE|<=1e-6 Ha"
 SIZES = (500, 1000, 2000)
+BOX_SIZES = (2000, 4000, 6000)
 FP64_NOMINAL_TFLOPS = 148 * 64 * 2 * 1.965e9 / 1e12   # 148 SMs x 64 DFMA/clk x 2 x 1965 MHz
+TWO_STAGE_MAX_N = 768 * 16 + 32   # largest Hamiltonian the two-stage reduction takes (panel rows x cluster CTAs + a panel)
 
 
 WORKLOADS = {
     "clusters": "isolated {H,C,N,O} clusters N in {500,1000,2000} (seeds 0,1,2), 21 freqs",
     "batched": "256 isolated {H,C,N,O} clusters N ~ U{20..600} (seed 0), 21 freqs, one batch",
+    "boxes": "periodic cubic {H,C,N,O} boxes N in {2000,4000,6000} (seeds 0,1,2) at 0.1 atoms/A^3, "
+             "cut-offs 120/100/25 A, 21 freqs",
 }
 WORKLOAD = "clusters"
 
@@ -51,6 +55,8 @@ def workload():
     from mbd_b200 import synthetic as sy
     if WORKLOAD == "batched":
         return sy.cluster_batch(256)
+    if WORKLOAD == "boxes":
+        return [sy.periodic_box(n, seed=k) for k, n in enumerate(BOX_SIZES)]
     return [sy.cluster(n, seed=k) for k, n in enumerate(SIZES)]
 
 
@@ -69,10 +75,10 @@ def load_peaks():
 
 
 def load_traffic():
-    """Per-launch DRAM traffic of the dominant kernel from the committed ncu summary."""
+    """Per-launch DRAM traffic of the workload's dominant kernels from the committed ncu summaries."""
     try:
         with open(os.path.join(ROOT, "profiles", "traffic.json")) as fh:
-            return json.load(fh)
+            return json.load(fh).get(WORKLOAD, {})
     except OSError:
         return {}
 
@@ -225,17 +231,29 @@ class _Null:
 def roofline(stage_ms, sizes, mode):
     """Roofline of the dominant stage of the last timed step."""
     peaks, src = load_peaks()
-    stages = {k: v for k, v in stage_ms.items()
-              if k not in ("total", "tridiag_dense_to_band", "tridiag_to_tridiagonal")}
+    sub = ("total", "tridiag_dense_to_band", "tridiag_to_tridiagonal", "tridiag_one_stage_launch",
+           "tridiag_band_chase_launch")
+    stages = {k: v for k, v in stage_ms.items() if k not in sub}
     dom = max(stages, key=stages.get)
-    if dom == "tridiag" and stage_ms.get("tridiag_dense_to_band", 0.0) > 0.0:
+    one_ms = stage_ms.get("tridiag_one_stage_launch", 0.0)
+    chase_ms = stage_ms.get("tridiag_band_chase_launch", stage_ms.get("tridiag_to_tridiagonal", 0.0))
+    two_stage = stage_ms.get("tridiag_dense_to_band", 0.0) > 0.0
+    if two_stage and one_ms > 0.05:
+        # both launches ran: the matrices above the two-stage limit took the one-stage one
+        big = [n for n in sizes if 3 * n > TWO_STAGE_MAX_N]
+        sizes_two = [n for n in sizes if 3 * n <= TWO_STAGE_MAX_N]
+        if one_ms >= chase_ms:
+            two_stage, sizes, stages["tridiag"] = False, big, one_ms
+        else:
+            sizes = sizes_two
+    if dom == "tridiag" and two_stage:
         # two-stage path: the batch-wide bulge-chasing launch (timed alone by
         # the stage events).  Per task it reads and writes its diagonal block and
         # the block below it (2 x 32 x 32 FP64 each way); sweep i of an n x n
         # band has ceil((n - i - 1) / 32) tasks, sweeps i = 0 .. n - 3.
         def tasks(n):
             return sum((n - i - 1 + 31) // 32 for i in range(0, n - 2))
-        t_ms = stage_ms["tridiag_to_tridiagonal"]
+        t_ms = chase_ms
         nbytes = sum(tasks(3 * n) for n in sizes) * 4 * 32 * 32 * 8.0
         achieved = nbytes / (t_ms / 1000.0) / 1e9
         return {"bound": "hbm", "kernel": "sb2st_kernel (band -> tridiagonal bulge chasing, one launch per batch)",
@@ -286,18 +304,22 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--mode", default="mixed_learned", choices=["plain", "mixed", "mixed_learned"])
-    ap.add_argument("--train-geoms", type=int, default=160,
-                    help="clusters (N ~ U{50..400}) the learned warm start is trained on before timing")
+    ap.add_argument("--train-geoms", type=int, default=None,
+                    help="geometries (N ~ U{50..400}, clusters or, for --workload boxes, periodic boxes) the "
+                         "learned warm start is trained on before timing (default 160; 2000 for boxes)")
     ap.add_argument("--train-epochs", type=int, default=12)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-plain", action="store_true", help="skip the plain FP64 comparison run")
     ap.add_argument("--workload", default="clusters", choices=sorted(WORKLOADS),
-                    help="clusters: the three-cluster headline workload; batched: 256 uneven clusters")
+                    help="clusters: the three-cluster headline workload; batched: 256 uneven clusters; "
+                         "boxes: three periodic boxes of 2000-6000 atoms")
     ap.add_argument("--sizes", default=None,
                     help="comma-separated cluster sizes replacing 500,1000,2000 (profiling runs only)")
     args = ap.parse_args()
     WORKLOAD = args.workload
+    if args.train_geoms is None:
+        args.train_geoms = 2000 if WORKLOAD == "boxes" else 160
     if args.sizes:
         SIZES = tuple(int(x) for x in args.sizes.split(","))
     warmup = max(3, args.warmup)
@@ -327,12 +349,14 @@ def main():
         # solutions of clusters from the same generator (other seeds)
         from mbd_b200 import synthetic as sy
         rng = np.random.default_rng(12345)
-        train = [sy.cluster(int(n), seed=100000 + k) for k, n in
+        gen = sy.periodic_box if WORKLOAD == "boxes" else sy.cluster
+        train = [gen(int(n), seed=100000 + k) for k, n in
                  enumerate(rng.integers(50, 401, size=args.train_geoms))]
         t0 = time.perf_counter()
         loss = eng.learned_train([g for g, _ in train], [s for _, s in train], epochs=args.train_epochs, lr=1e-3,
                                  seed=7)
-        learned = {"train_geoms": args.train_geoms, "train_sizes": "clusters N ~ U{50..400}",
+        learned = {"train_geoms": args.train_geoms,
+                   "train_sizes": ("periodic boxes" if WORKLOAD == "boxes" else "clusters") + " N ~ U{50..400}",
                    "epochs": args.train_epochs, "train_seconds": time.perf_counter() - t0,
                    "loss_first_epoch": float(loss[0]), "loss_last_epoch": float(loss[-1])}
     stream = torch.cuda.ExternalStream(eng.stream_handle(), device=torch.device("cuda", local))
@@ -381,10 +405,12 @@ def main():
             "warmup": warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None,
             "dtype": {"plain": "f64", "mixed": "tf32x3+f64", "mixed_learned": "f64 (CG) + f32 (network)"}[args.mode],
-            "data": "synthetic (seeded {H,C,N,O} clusters; no dataset exists for this path)",
+            "data": "synthetic (seeded {H,C,N,O} " + ("periodic boxes" if WORKLOAD == "boxes" else "clusters")
+                    + "; no dataset exists for this path)",
             "config": {"workload": workload_name(),
                        "mode": args.mode, "parallelism": f"replicas{world}" if world > 1 else "1gpu",
-                       "l2": "working set 0.38-6.1 GB per geometry > 126 MB L2; no flush"},
+                       "l2": "working set 0.38-6.1 GB per geometry > 126 MB L2; no flush" if WORKLOAD != "boxes"
+                             else "working set 6.1-54 GB per geometry > 126 MB L2; no flush"},
             "gpu_launches": stats["launches"] * args.steps,
             "roofline": roofline(stage, [len(g.names) for g, _ in geos], args.mode),
             "energies": [r.energy for r in res][:8],
@@ -416,7 +442,12 @@ def main():
         line["e2e"] = {"value": world * len(geos) * args.steps / t_e2e, "unit": "energies/s",
                        "h2d_bytes_per_step": st2["h2d_bytes"], "d2h_bytes_per_step": st2["d2h_bytes"],
                        "status": [r.status for r in rr]}
-    if rank == 0 and world == 1 and not args.no_cpu_baseline and not args.sizes:
+    if WORKLOAD == "boxes":
+        # one 200-atom box with these cut-offs already takes the oracle about
+        # five minutes (its periodic image sums are numpy loops)
+        line["cpu_baseline"] = {"value": None, "unit": "energies/s", "cores": os.cpu_count(), "kind": "port",
+                                "sample": "not timed: the oracle needs minutes per 200-atom box at these cut-offs"}
+    elif rank == 0 and world == 1 and not args.no_cpu_baseline and not args.sizes:
         cb = cpu_baseline()
         line["cpu_baseline"] = {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")}
     if rank == 0:

@@ -164,8 +164,10 @@ int mbd_rsscs_vdw_params(int z, double* alpha0, double* c6, double* r0);
  * summed over the geometries (their sum can exceed [0]).  [6] is the sum over
  * geometries of the dense -> band reduction (also per geometry, on the same
  * streams) plus the batch-wide band -> tridiagonal launch; [7] is batch-wide.
- * With n >= 10 also [8] the dense -> band part of [6] and [9] the rest.
- * n must be >= 8. */
+ * With n >= 10 also [8] the dense -> band part of [6] and [9] the rest;
+ * with n >= 12 also [10] the one-stage (dense -> tridiagonal) launch of the
+ * matrices that skip the band and [11] the band -> tridiagonal launch, the
+ * two batch-wide launches [9] is made of.  n must be >= 8. */
 int mbd_rsscs_last_timings(mbd_ctx* ctx, double* ms, int n);
 
 /* Counters of the last upload/compute/download: [0] kernel launches issued

@@ -732,7 +732,7 @@ int enqueue_batch(mbd_ctx* ctx, int mode) {
   MBD_CUDA(cudaMemsetAsync(ctx->err_flag, 0, sizeof(int), s));
   record_timing(ctx, ctx->bev[0], s);
   if (ctx->order.empty()) {
-    for (int k = 1; k < 4; ++k) record_timing(ctx, ctx->bev[k], s);
+    for (int k = 1; k < 5; ++k) record_timing(ctx, ctx->bev[k], s);
     return cuda_status(cudaGetLastError());
   }
   // relay and CFDM stages, geometries spread over the slots' streams
@@ -761,6 +761,7 @@ int enqueue_batch(mbd_ctx* ctx, int mode) {
                                    ctx->tridiag_ws.p, ctx->err_flag, s));
     ctx->launches += 2;
   }
+  record_timing(ctx, ctx->bev[4], s);
   if (ctx->n_band_jobs > 0) {
     MBD_CUDA(launch_sb2st(ctx->band_jobs, ctx->n_band_jobs, ctx->sweep_items, ctx->n_sweep_items,
                           ctx->sweep_progress.as<int>(), ctx->err_flag, ctx->num_sms, ctx->band_max_n,
@@ -959,6 +960,8 @@ int mbd_rsscs_download(mbd_ctx* ctx, mbd_result* out) {
   ctx->last_ms[Stage::kTridiag] = elapsed(ctx->bev[1], ctx->bev[2]);
   ctx->last_band_ms = 0.0;
   ctx->last_chase_ms = ctx->last_ms[Stage::kTridiag];
+  ctx->last_onestage_ms = elapsed(ctx->bev[1], ctx->bev[4]);
+  ctx->last_sb2st_ms = elapsed(ctx->bev[4], ctx->bev[2]);
   ctx->last_ms[Stage::kEig] = elapsed(ctx->bev[2], ctx->bev[3]);
   for (int g : ctx->order) {
     cudaEvent_t* evs = ctx->events.data() + (size_t)g * kGeomEvents;
@@ -1159,6 +1162,10 @@ int mbd_rsscs_last_timings(mbd_ctx* ctx, double* ms, int n) {
   if (n >= Stage::kCount + 2) {
     ms[Stage::kCount] = ctx->last_band_ms;        // dense -> band, summed over geometries
     ms[Stage::kCount + 1] = ctx->last_chase_ms;   // band (or dense, one-stage) -> tridiagonal, batch-wide
+  }
+  if (n >= Stage::kCount + 4) {
+    ms[Stage::kCount + 2] = ctx->last_onestage_ms;   // the grouped one-stage launch alone
+    ms[Stage::kCount + 3] = ctx->last_sb2st_ms;      // the bulge-chasing launch alone
   }
   return MBD_OK;
 }

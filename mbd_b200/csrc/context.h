@@ -131,7 +131,8 @@ struct mbd_ctx {
   int* err_flag = nullptr;
   mbd::TridiagJob* job_dev = nullptr;
   std::vector<cudaEvent_t> events;           // kGeomEvents per geometry
-  cudaEvent_t bev[4] = {nullptr, nullptr, nullptr, nullptr};   // start, relay done, tridiag done, end
+  // start, relay done, tridiag done, end, one-stage launch done
+  cudaEvent_t bev[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
   cudaEvent_t fork_ev = nullptr;             // releases the slot streams at the start of a compute
   // one captured graph of mbd_rsscs_compute per mode, valid until the next
   // upload or workspace reallocation
@@ -147,6 +148,7 @@ struct mbd_ctx {
   int mode_runs[3] = {0, 0, 0};              // computes of the uploaded batch, per mode
   double last_ms[mbd::Stage::kCount] = {0};
   double last_band_ms = 0.0, last_chase_ms = 0.0;
+  double last_onestage_ms = 0.0, last_sb2st_ms = 0.0;   // the two batch-wide launches of last_chase_ms
   double launches = 0, h2d_bytes = 0, d2h_bytes = 0;
   int last_mode = 0;
   bool have_batch = false;

@@ -5,11 +5,12 @@
 // For each panel of kBand columns c0 = k*kBand (rows below the band r >= c0 +
 // kBand, m of them):
 //   qr_panel   Householder QR of the m x kBand panel in ONE thread-block
-//              cluster: the panel's rows are spread over the CTAs' shared
-//              memory, cross-CTA sums go through distributed shared memory
-//              and two hardware cluster barriers per column.  Writes R in
-//              place (the band), V explicitly (unit lower trapezoidal) and
-//              the compact-WY factor T (Q = I - V T V^T, dlarft forward).
+//              cluster: the panel's rows are spread over the CTAs' registers
+//              (a lane per column), cross-CTA sums go through distributed
+//              shared memory and two hardware cluster barriers per column.
+//              Writes R in place (the band), V explicitly (unit lower
+//              trapezoidal) and the compact-WY factor T (Q = I - V T V^T,
+//              dlarft forward), whose Gram entries come from the same dots.
 //   symm       Y = A22 V (A22 the trailing m x m lower-stored block), row
 //              blocks of 64 split over S column chunks (fixed-order partials)
 //   yred       Y <- sum of the partials; Y <- Y T; block partials of V^T Y
@@ -31,8 +32,6 @@ namespace mbd {
 namespace {
 
 constexpr int B = kBand;            // 32
-constexpr int QR_THREADS = 256;
-constexpr int QR_LD = B + 1;        // shared-memory row stride of the panel (doubles)
 constexpr int TL = 64;              // tile edge of symm / syr2k
 
 __device__ __forceinline__ double warp_sum(double v) {
@@ -41,7 +40,200 @@ __device__ __forceinline__ double warp_sum(double v) {
   return v;
 }
 
-// Shared layout of qr_panel: P[R][QR_LD] | pubN[2][8] norm partials per warp
+// Panel QR with the panel in registers: warp w of a CTA owns the local rows
+// r = w + NW t (t < RPW), lane c holds column c of them in x[t].  Per column j:
+//   1. every lane has the squared norm of its column below row j (lane j's
+//      is the one needed); warps publish it, the owner of row j publishes
+//      alpha = A(j, j); cluster barrier; every CTA sums the same partials in
+//      the same order, so all compute the same beta, tau.
+//   2. lane j writes v (0 above row j, 1 at row j, x * scale below) to shared
+//      memory for its warp; every lane c forms d_c = v^T x_c over its rows:
+//      for c > j the update's coefficient, for c < j (column c already holds
+//      v_c) the entry (V^T V)[c][j] of the compact-WY Gram matrix.
+//   3. CTA sum of the dots, cluster barrier, cluster sum (fixed order).
+//   4. x_c -= tau v d_c for c > j while every lane accumulates the norm of its
+//      updated column below row j + 1; lane j keeps v, row j gets beta.
+//   5. rank 0, warp 0: T[0:j, j] = -tau_j T[0:j, 0:j] (V^T V)[0:j, j],
+//      T[j][j] = tau_j (dlarft, forward, columnwise) from the same dots.
+// pub* are read by the other CTAs of the cluster (double-buffered by column
+// parity: a buffer is rewritten two columns later, after both barriers of the
+// column in between).
+template <int NW, int RPW>
+__global__ void __launch_bounds__(NW * 32) qr_panel_kernel(PanelArgs a) {
+  constexpr int NT = NW * 32;
+  constexpr unsigned FULL = 0xffffffffu;
+  __shared__ double pubN[2][NW];
+  __shared__ double pubA[2];
+  __shared__ double pubD[2][B];
+  __shared__ double dw[NW][B];
+  __shared__ double vs[NW][RPW];
+  __shared__ double gs[B];
+  __shared__ double Tm[B][B + 1];
+  cg::cluster_group cl = cg::this_cluster();
+  const int rank = (int)cl.block_rank();
+  const int C = (int)cl.num_blocks();
+  const int m = a.m;
+  const int R = a.rows_per_cta;
+  const int lo = rank * R, hi = min(m, lo + R);
+  const int nr = max(0, hi - lo);
+  const int tid = threadIdx.x, warp = tid / 32, lane = tid % 32;
+  const int g0 = lo + warp;   // panel row of x[0]; x[t] holds row g0 + NW t
+  double x[RPW];
+#pragma unroll
+  for (int t = 0; t < RPW; ++t) {
+    const int r = warp + NW * t;
+    x[t] = (r < nr) ? a.A[(size_t)(a.row0 + lo + r) * a.ld + a.col0 + lane] : 0.0;
+  }
+  if (rank == 0)
+    for (int e = tid; e < B * (B + 1); e += NT) (&Tm[0][0])[e] = 0.0;
+  const int nref = min(B, m);
+  // squared norm of this lane's column over the rows below row j
+  double s_own;
+  {
+    double s0 = 0.0, s1 = 0.0;
+#pragma unroll
+    for (int t = 0; t < RPW; ++t) {
+      const double v = (g0 + NW * t > 0) ? x[t] : 0.0;
+      if (t & 1) s1 += v * v;
+      else s0 += v * v;
+    }
+    s_own = s0 + s1;
+  }
+  for (int j = 0; j < nref; ++j) {
+    const int par = j & 1;
+    const double sj = __shfl_sync(FULL, s_own, j);
+    if (lane == 0) pubN[par][warp] = sj;
+    // row j is local row j - lo < 32: warp (j - lo) % NW, slot t = (j - lo) / NW < 4
+    if (j >= lo && j < hi && (j - lo) % NW == warp && lane == j) {
+      const int tj = (j - lo) / NW;
+      double aj = 0.0;
+#pragma unroll
+      for (int t = 0; t < (RPW < 4 ? RPW : 4); ++t)
+        if (t == tj) aj = x[t];
+      pubA[par] = aj;
+    }
+    cl.sync();
+    // all remote loads first (independent), then the sums
+    constexpr int NX = (kPanelMaxCluster * NW + 31) / 32;
+    double xparts[NX];
+#pragma unroll
+    for (int u = 0; u < NX; ++u) {
+      const int q = lane + 32 * u;
+      xparts[u] = (q < C * NW) ? cl.map_shared_rank(&pubN[0][0], q / NW)[par * NW + q % NW] : 0.0;
+    }
+    double xn2 = 0.0;
+#pragma unroll
+    for (int u = 0; u < NX; ++u) xn2 += xparts[u];
+    xn2 = warp_sum(xn2);
+    double alpha = 0.0;
+    if (lane == 0) alpha = cl.map_shared_rank(&pubA[0], j / R)[par];
+    alpha = __shfl_sync(FULL, alpha, 0);
+    double tau = 0.0, scale = 0.0, beta = alpha;
+    if (xn2 > 0.0) {
+      beta = -copysign(sqrt(alpha * alpha + xn2), alpha);
+      tau = (beta - alpha) / beta;
+      scale = 1.0 / (alpha - beta);
+    }
+    if (rank == 0 && tid == 0) a.tau[j] = tau;
+    // v on this warp's rows
+    if (lane == j) {
+      if (g0 > j) {
+#pragma unroll
+        for (int t = 0; t < RPW; ++t) vs[warp][t] = x[t] * scale;
+      } else {
+#pragma unroll
+        for (int t = 0; t < RPW; ++t) {
+          const int g = g0 + NW * t;
+          vs[warp][t] = g < j ? 0.0 : (g == j ? 1.0 : x[t] * scale);
+        }
+      }
+    }
+    __syncwarp();
+    double d0 = 0.0, d1 = 0.0;   // two accumulation chains
+#pragma unroll
+    for (int t = 0; t < RPW; ++t) {
+      if (t & 1) d1 += vs[warp][t] * x[t];
+      else d0 += vs[warp][t] * x[t];
+    }
+    dw[warp][lane] = d0 + d1;
+    __syncthreads();
+    if (warp == 0) {
+      double t = 0.0;
+#pragma unroll
+      for (int q = 0; q < NW; ++q) t += dw[q][lane];
+      pubD[par][lane] = t;
+    }
+    cl.sync();
+    double dparts[kPanelMaxCluster];
+#pragma unroll
+    for (int q = 0; q < kPanelMaxCluster; ++q)
+      dparts[q] = (q < C) ? cl.map_shared_rank(&pubD[0][0], q)[par * B + lane] : 0.0;
+    double dc = 0.0;
+#pragma unroll
+    for (int q = 0; q < kPanelMaxCluster; ++q) dc += dparts[q];
+    // update the columns right of j and the norms below row j + 1
+    const double tdc = (lane > j) ? tau * dc : 0.0;
+    double s0 = 0.0, s1 = 0.0;
+    if (g0 > j + 1) {
+#pragma unroll
+      for (int t = 0; t < RPW; ++t) {
+        x[t] -= vs[warp][t] * tdc;
+        if (t & 1) s1 += x[t] * x[t];
+        else s0 += x[t] * x[t];
+      }
+    } else {
+#pragma unroll
+      for (int t = 0; t < RPW; ++t) {
+        x[t] -= vs[warp][t] * tdc;
+        const double v = (g0 + NW * t > j + 1) ? x[t] : 0.0;
+        if (t & 1) s1 += v * v;
+        else s0 += v * v;
+      }
+    }
+    s_own = s0 + s1;
+    if (lane == j) {
+#pragma unroll
+      for (int t = 0; t < RPW; ++t) {
+        const int g = g0 + NW * t;
+        if (g > j) x[t] = vs[warp][t];
+        else if (g == j) x[t] = beta;
+      }
+    }
+    // compact-WY factor, column j
+    if (rank == 0 && warp == 0) {
+      gs[lane] = dc;
+      __syncwarp();
+      if (lane < j) {
+        double t = 0.0;
+        for (int l = lane; l < j; ++l) t += Tm[lane][l] * gs[l];
+        Tm[lane][j] = -tau * t;
+      }
+      if (lane == j) Tm[j][j] = tau;
+      __syncwarp();
+    }
+  }
+  // write R (rows g <= c: the band) and V (explicit, unit lower trapezoidal)
+#pragma unroll
+  for (int t = 0; t < RPW; ++t) {
+    const int r = warp + NW * t;
+    if (r < nr) {
+      const int g = lo + r;
+      if (g <= lane) a.A[(size_t)(a.row0 + g) * a.ld + a.col0 + lane] = x[t];
+      a.V[(size_t)g * B + lane] = g > lane ? x[t] : (g == lane ? 1.0 : 0.0);
+    }
+  }
+  if (rank == 0) {
+    __syncthreads();
+    for (int e = tid; e < B * B; e += NT) a.T[e] = Tm[e / B][e % B];
+  }
+  cl.sync();   // no CTA leaves while another may still read its shared memory
+}
+
+constexpr int QR_THREADS = 256;
+constexpr int QR_LD = B + 1;        // shared-memory row stride of the panel (doubles)
+// Panels of more than 384 rows per CTA (m > 16 x 384) keep the panel in
+// shared memory instead (the register kernel would spill).
+// Shared layout of qr_panel_smem: P[R][QR_LD] | pubN[2][8] norm partials per warp
 // | pubA[2] alpha | pubD[2][B] dot sums | dw[8][B] per-warp dots | gram[B][B]
 // | G[B][B] | Tm[B][B].  pub* are read by the other CTAs of the cluster
 // (double-buffered by column parity).  Warp w owns the local rows r = w mod 8,
@@ -53,7 +245,7 @@ __host__ __device__ constexpr size_t qr_panel_doubles(int R) {
   return (size_t)R * QR_LD + 2 * QR_WARPS + 2 + 2 * B + QR_WARPS * B + 3 * B * B + 8;
 }
 
-__global__ void __launch_bounds__(QR_THREADS) qr_panel_kernel(PanelArgs a) {
+__global__ void __launch_bounds__(QR_THREADS) qr_panel_smem_kernel(PanelArgs a) {
   extern __shared__ double sm[];
   cg::cluster_group cl = cg::this_cluster();
   const int rank = (int)cl.block_rank();
@@ -215,6 +407,27 @@ __global__ void __launch_bounds__(QR_THREADS) qr_panel_kernel(PanelArgs a) {
   }
   cl.sync();   // no CTA leaves while another may still read its shared memory
 }
+
+// Variants by rows per CTA: (warps, rows per warp); the last one is the
+// shared-memory kernel.
+constexpr int kQrVariants = 4;
+constexpr int kQrWarps[kQrVariants] = {8, 8, 8, QR_THREADS / 32};
+constexpr int kQrRows[kQrVariants] = {12, 24, 48, kPanelMaxRowsPerCta / (QR_THREADS / 32)};
+int qr_variant(int R) {
+  for (int v = 0; v < kQrVariants; ++v)
+    if (R <= kQrWarps[v] * kQrRows[v]) return v;
+  return -1;
+}
+using QrKernel = void (*)(PanelArgs);
+QrKernel qr_kernel(int v) {
+  switch (v) {
+    case 0: return qr_panel_kernel<8, 12>;
+    case 1: return qr_panel_kernel<8, 24>;
+    case 2: return qr_panel_kernel<8, 48>;
+    default: return qr_panel_smem_kernel;
+  }
+}
+size_t qr_smem_bytes(int v) { return v == kQrVariants - 1 ? sizeof(double) * qr_panel_doubles(kPanelMaxRowsPerCta) : 0; }
 
 // FP64 tensor-core MMA, D = A B + D with A 8x4 (row), B 4x8 (col), D 8x8:
 // a = A[lane/4][lane%4], b = B[lane%4][lane/4], d = D[lane/4][2*(lane%4) + {0,1}].
@@ -454,36 +667,44 @@ __global__ void band_copy_kernel(const double* A, int ld, int n, double* Br) {
 
 }  // namespace
 
-size_t qr_panel_smem(int rows_per_cta) { return sizeof(double) * qr_panel_doubles(rows_per_cta); }
-
 cudaError_t init_sy2sb_attributes() {
-  cudaError_t e = cudaFuncSetAttribute(qr_panel_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       (int)qr_panel_smem(kPanelMaxRowsPerCta));
-  if (e != cudaSuccess) return e;
-  e = cudaFuncSetAttribute(qr_panel_kernel, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
-  if (e != cudaSuccess) return e;
-  e = cudaFuncSetAttribute(symm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSymmSmem);
+  for (int v = 0; v < kQrVariants; ++v) {
+    cudaError_t e = cudaFuncSetAttribute(qr_kernel(v), cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+    if (e != cudaSuccess) return e;
+    if (qr_smem_bytes(v) > 0) {
+      e = cudaFuncSetAttribute(qr_kernel(v), cudaFuncAttributeMaxDynamicSharedMemorySize, (int)qr_smem_bytes(v));
+      if (e != cudaSuccess) return e;
+    }
+  }
+  cudaError_t e = cudaFuncSetAttribute(symm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSymmSmem);
   if (e != cudaSuccess) return e;
   return cudaFuncSetAttribute(syr2k_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSyr2kSmem);
 }
 
-// Largest panel-QR cluster this device can run (0: none), probed once.
+// Largest panel-QR cluster this device can run with every variant (0: none),
+// probed once.
 int probe_max_cluster() {
   for (int C = kPanelMaxCluster; C >= 1; C /= 2) {
-    cudaLaunchConfig_t cfg{};
-    cfg.gridDim = dim3(C);
-    cfg.blockDim = dim3(QR_THREADS);
-    cfg.dynamicSmemBytes = qr_panel_smem(kPanelMaxRowsPerCta);
-    cudaLaunchAttribute attr[1];
-    attr[0].id = cudaLaunchAttributeClusterDimension;
-    attr[0].val.clusterDim.x = C;
-    attr[0].val.clusterDim.y = 1;
-    attr[0].val.clusterDim.z = 1;
-    cfg.attrs = attr;
-    cfg.numAttrs = 1;
-    int clusters = 0;
-    if (cudaOccupancyMaxActiveClusters(&clusters, qr_panel_kernel, &cfg) == cudaSuccess && clusters > 0) return C;
-    cudaGetLastError();
+    bool ok = true;
+    for (int v = 0; v < kQrVariants && ok; ++v) {
+      cudaLaunchConfig_t cfg{};
+      cfg.gridDim = dim3(C);
+      cfg.blockDim = dim3(kQrWarps[v] * 32);
+      cfg.dynamicSmemBytes = qr_smem_bytes(v);
+      cudaLaunchAttribute attr[1];
+      attr[0].id = cudaLaunchAttributeClusterDimension;
+      attr[0].val.clusterDim.x = C;
+      attr[0].val.clusterDim.y = 1;
+      attr[0].val.clusterDim.z = 1;
+      cfg.attrs = attr;
+      cfg.numAttrs = 1;
+      int clusters = 0;
+      if (cudaOccupancyMaxActiveClusters(&clusters, qr_kernel(v), &cfg) != cudaSuccess || clusters < 1) {
+        cudaGetLastError();
+        ok = false;
+      }
+    }
+    if (ok) return C;
   }
   return 0;
 }
@@ -532,11 +753,13 @@ cudaError_t launch_sy2sb(double* A, int ld, int n, double* ws, double* Br, int n
     while (C * kPanelMaxRowsPerCta < m) C *= 2;
     if (C > kPanelMaxCluster) return cudaErrorInvalidValue;   // the caller keeps n <= sy2sb_max_n()
     const int R = (m + C - 1) / C;
+    const int qv = qr_variant(R);
+    if (qv < 0) return cudaErrorInvalidValue;
     PanelArgs pa{A, ld, row0, c0, m, R, V, T, tau};
     cudaLaunchConfig_t cfg{};
     cfg.gridDim = dim3(C);
-    cfg.blockDim = dim3(QR_THREADS);
-    cfg.dynamicSmemBytes = qr_panel_smem(R);
+    cfg.blockDim = dim3(kQrWarps[qv] * 32);
+    cfg.dynamicSmemBytes = qv == kQrVariants - 1 ? sizeof(double) * qr_panel_doubles(R) : 0;
     cfg.stream = s;
     cudaLaunchAttribute attr[1];
     attr[0].id = cudaLaunchAttributeClusterDimension;
@@ -545,7 +768,7 @@ cudaError_t launch_sy2sb(double* A, int ld, int n, double* ws, double* Br, int n
     attr[0].val.clusterDim.z = 1;
     cfg.attrs = attr;
     cfg.numAttrs = 1;
-    cudaError_t e = cudaLaunchKernelEx(&cfg, qr_panel_kernel, pa);
+    cudaError_t e = cudaLaunchKernelEx(&cfg, qr_kernel(qv), pa);
     if (e != cudaSuccess) return e;
     // two-sided update of the trailing block
     const int nt = (m + TL - 1) / TL;

@@ -355,8 +355,9 @@ class Engine:
         return int(self.lib.mbd_rsscs_stream(self.ctx) or 0)
 
     def timings(self) -> dict:
-        buf = (ctypes.c_double * 10)()
-        self.lib.mbd_rsscs_last_timings(self.ctx, buf, 10)
+        buf = (ctypes.c_double * 12)()
+        self.lib.mbd_rsscs_last_timings(self.ctx, buf, 12)
         keys = ["total", "setup", "relay_build", "relay_factor", "relay_solve", "cfdm_build",
-                "tridiag", "eig_energy", "tridiag_dense_to_band", "tridiag_to_tridiagonal"]
+                "tridiag", "eig_energy", "tridiag_dense_to_band", "tridiag_to_tridiagonal",
+                "tridiag_one_stage_launch", "tridiag_band_chase_launch"]
         return dict(zip(keys, list(buf)))

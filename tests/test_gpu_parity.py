@@ -144,3 +144,38 @@ def test_eigvalsh_matches_lapack(engine, n):
     w = engine.eigvalsh(H)
     ref = np.linalg.eigvalsh(S)
     np.testing.assert_allclose(w, ref, rtol=0, atol=1e-12 * max(1.0, np.abs(ref).max()) * n)
+
+
+def _known_spectrum(n, seed):
+    """Symmetric H = P2 P1 diag(lam) P1 P2 with two Householder reflectors
+    P = I - 2 p p^T: dense, with exactly the eigenvalues lam (up to the
+    rounding of forming H), built row block by row block in O(n^2)."""
+    rng = np.random.default_rng(seed)
+    lam = rng.uniform(-1.0, 4.0, n)
+    lam[: n // 10] = 1.5                      # a cluster of equal eigenvalues
+    u = rng.standard_normal(n)
+    u /= np.linalg.norm(u)
+    w = rng.standard_normal(n)
+    w /= np.linalg.norm(w)
+    c = float(np.dot(lam, u * u))
+    # H1 = P1 D P1: H1_ij = lam_i d_ij - 2 u_i u_j (lam_i + lam_j - 2c); y = H1 w
+    y = lam * w - 2.0 * u * (np.dot(u * lam, w) + (lam - 2.0 * c) * np.dot(u, w))
+    s = float(np.dot(w, y))
+    H = np.empty((n, n))
+    for r0 in range(0, n, 1024):
+        r = slice(r0, min(n, r0 + 1024))
+        H[r] = (-2.0 * u[r, None] * u[None, :] * (lam[r, None] + lam[None, :] - 2.0 * c)
+                - 2.0 * w[r, None] * y[None, :] - 2.0 * y[r, None] * w[None, :] + 4.0 * s * w[r, None] * w[None, :])
+    H[np.arange(n), np.arange(n)] += lam
+    return H, np.sort(lam)
+
+
+@pytest.mark.parametrize("n", [12000, 13000, 18000])
+def test_eigvalsh_known_spectrum_large(engine, n):
+    """Matrices of the size of a 4000- and 6000-atom box's Hamiltonian
+    (n = 3N): 12000 takes the two-stage reduction at its largest panel,
+    13000 and 18000 the one-stage reduction and the bisection that reads
+    d and e^2 from global memory."""
+    H, lam = _known_spectrum(n, seed=n)
+    w = engine.eigvalsh(H)
+    np.testing.assert_allclose(w, lam, rtol=0, atol=1e-12 * 4.0 * n)
