@@ -18,7 +18,10 @@
 // Work items are (matrix, sweep) pairs ordered by sweep, then matrix; warp w
 // takes items w, w + W, ...  Every wait points to an item of lower index, so
 // the lowest unfinished item always progresses (all CTAs are co-resident).
-// One warp owns a task: lane l holds row l of D and of O in registers.
+// Lane l of a warp holds row l of D (D-warp) or of O (O-warp) in registers;
+// the blocks move between the band and shared memory a band row per load or
+// store instruction (coalesced), and between shared memory and registers a
+// matrix row per lane.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -41,7 +44,8 @@ struct PairSmem {
   double v[2][B];
   double w[B];
   double s[B];
-  double Ot[B][B + 1];
+  double Ot[B][B + 1];   // O-warp: the O block, row-major (row l at Ot[l])
+  double Ds[B][B];       // D-warp: band rows of D, Ds[i][d] = A(r + i, r + i - d)
   int go;             // the O-warp's verdict after its wait, read by both warps
 };
 
@@ -157,15 +161,15 @@ __global__ void __launch_bounds__(WARPS * 32) sb2st_kernel(const BandJob* jobs, 
         // ---- D <- H D H:  w = tau D v - (tau^2 / 2)(v^T D v) v;  D -= v w^T + w v^T
         const double tauD = (k == 0) ? S.w[0] : S.w[1];
         __syncwarp();
-        double* rowD = Br + (size_t)(r + l) * LD + l;
-        double* colD = Br + (size_t)r * LD - l;
-        double dr[B];
+        // band rows r .. r + L - 1, diagonals d <= row (the lower triangle of D)
+        const double* rowsD = Br + (size_t)r * LD + l;
 #pragma unroll
-        for (int j = 0; j < B; ++j) {
-          double x = 0.0;
-          if (l < L && j < L) x = (j <= l) ? __ldcg(rowD - j) : __ldcg(colD + j * (LD + 1));
-          dr[j] = x;
-        }
+        for (int i = 0; i < B; ++i) S.Ds[i][l] = (i < L && l <= i) ? __ldcg(rowsD + (size_t)i * LD) : 0.0;
+        __syncwarp();
+        double dr[B];   // dr[j] = D(l, j): Ds[l][l - j] below the diagonal, Ds[j][j - l] above
+        const double* ds = &S.Ds[0][0];
+#pragma unroll
+        for (int j = 0; j < B; ++j) dr[j] = ds[(j <= l) ? (B + 1) * l - j : (B + 1) * j - l];
         if (tauD != 0.0) {
           const double vlD = vcur[l];
           double dv = 0.0;
@@ -178,18 +182,28 @@ __global__ void __launch_bounds__(WARPS * 32) sb2st_kernel(const BandJob* jobs, 
           __syncwarp();
 #pragma unroll
           for (int j = 0; j < B; ++j) dr[j] -= vlD * S.w[j] + wl * vcur[j];
-          if (l < L) {
 #pragma unroll
-            for (int j = 0; j < B; ++j)
-              if (j <= l) rowD[-j] = dr[j];
-          }
+          for (int j = 0; j < B; ++j)
+            if (j <= l) S.Ds[l][l - j] = dr[j];
+          __syncwarp();
+          double* rowsW = Br + (size_t)r * LD + l;
+#pragma unroll
+          for (int i = 0; i < B; ++i)
+            if (i < L && l <= i) rowsW[(size_t)i * LD] = S.Ds[i][l];
         }
       } else {
         // ---- O <- O H;  next reflector from O[:, 0];  O <- H' O
-        double* rowO = Br + (size_t)(rn + l) * LD + B + l;
+        // band row rn + q holds O(q, j) at diagonal B + q - j: lane l reads j = B - 1 - l
+        const double* rowsO = Br + (size_t)rn * LD + 1 + l;
+        const bool jin = (B - 1 - l) < L;
+#pragma unroll
+        for (int q = 0; q < B; ++q)
+          S.Ot[q][B - 1 - l] = (q < Ln && jin) ? __ldcg(rowsO + (size_t)q * (LD + 1)) : 0.0;
+        __syncwarp();
         double orow[B];
 #pragma unroll
-        for (int j = 0; j < B; ++j) orow[j] = (l < Ln && j < L) ? __ldcg(rowO - j) : 0.0;
+        for (int j = 0; j < B; ++j) orow[j] = S.Ot[l][j];
+        __syncwarp();
         if (tau != 0.0) {
           double ov = 0.0;
 #pragma unroll
@@ -215,24 +229,26 @@ __global__ void __launch_bounds__(WARPS * 32) sb2st_kernel(const BandJob* jobs, 
             for (int j = 0; j < B; ++j) orow[j] -= tau2 * v2 * S.s[j];
             orow[0] = (l == 0) ? beta2 : 0.0;
           }
-          if (l < Ln) {
+          // the rows of O back to the band
 #pragma unroll
-            for (int j = 0; j < B; ++j)
-              if (j < L) rowO[-j] = orow[j];
-          }
+          for (int j = 0; j < B; ++j) S.Ot[l][j] = orow[j];
+          __syncwarp();
+          double* rowsOW = Br + (size_t)rn * LD + 1 + l;
+#pragma unroll
+          for (int q = 0; q < B; ++q)
+            if (q < Ln && jin) rowsOW[(size_t)q * (LD + 1)] = S.Ot[q][B - 1 - l];
         }
         S.v[(k + 1) & 1][l] = v2;
         tau = tau2;
         vl = v2;
       }
-      __threadfence();
+      // both warps' stores are ordered before the barrier; one lane then
+      // fences at GPU scope and publishes the task (the grid-barrier pattern)
       pair_sync(pair);
-      if (owarp) {
-        // the next task's tau for the D-warp, then publish this task
-        if (l == 0) {
-          S.w[1] = tau;
-          st_release(progress + t, k + 1);
-        }
+      if (owarp && l == 0) {
+        S.w[1] = tau;   // the next task's tau for the D-warp
+        __threadfence();
+        st_release(progress + t, k + 1);
       }
       pair_sync(pair);
     }
