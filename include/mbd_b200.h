@@ -8,8 +8,9 @@
  * atom_name, hirshfeld_volume, lattice_vector, cut-offs, vacuum axes, flag_xc)
  * and leaves the energy, alpha_eff, C6_eff and coupled_atom_pol behind.  The
  * calls below take the same data explicitly.  Every pointer is HOST memory
- * owned by the caller (except in mbd_rsscs_compute_resident's device path),
- * arrays follow Fortran column-major order, and every argument type maps to
+ * owned by the caller (except those of mbd_rsscs_eigvalsh_noalloc, which are
+ * device pointers), arrays follow Fortran column-major order, atoms keep the
+ * caller's order in every result, and every argument type maps to
  * iso_c_binding (c_int, c_double, c_ptr, c_char).
  *
  * Threading: one context per host thread.  A context owns its device

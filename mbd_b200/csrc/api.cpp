@@ -1033,15 +1033,22 @@ int mbd_rsscs_download(mbd_ctx* ctx, mbd_result* out) {
       r.energy_Ha = std::nan("");
       r.nimag = 0;
     }
+    // per-atom results back in the caller's atom order
+    const std::vector<int>& pm = gd->plan.perm;
     if (r.alpha_iw)   // column-major alpha(f, i): element (f, i) at f + 21 i
-      for (int i = 0; i < N; ++i)
-        for (int f = 0; f < 21; ++f) r.alpha_iw[f + 21 * (size_t)i] = aiw[(size_t)f * N + i];
+      for (int q = 0; q < N; ++q)
+        for (int f = 0; f < 21; ++f) r.alpha_iw[f + 21 * (size_t)pm[q]] = aiw[(size_t)f * N + q];
+    std::vector<double> tmp;
     if (r.alpha_eff) {
-      MBD_CUDA(cudaMemcpy(r.alpha_eff, gd->alpha_eff, sizeof(double) * N, cudaMemcpyDeviceToHost));
+      tmp.resize(N);
+      MBD_CUDA(cudaMemcpy(tmp.data(), gd->alpha_eff, sizeof(double) * N, cudaMemcpyDeviceToHost));
+      for (int q = 0; q < N; ++q) r.alpha_eff[pm[q]] = tmp[q];
       ctx->d2h_bytes += sizeof(double) * N;
     }
     if (r.c6_eff) {
-      MBD_CUDA(cudaMemcpy(r.c6_eff, gd->c6_eff, sizeof(double) * N, cudaMemcpyDeviceToHost));
+      tmp.resize(N);
+      MBD_CUDA(cudaMemcpy(tmp.data(), gd->c6_eff, sizeof(double) * N, cudaMemcpyDeviceToHost));
+      for (int q = 0; q < N; ++q) r.c6_eff[pm[q]] = tmp[q];
       ctx->d2h_bytes += sizeof(double) * N;
     }
     if (r.molpol_eig)

@@ -3,20 +3,24 @@
 // the solve of get_screened_alpha (UTILS.f90:469-473) by iteration instead of
 // PDPOTRF/PDPOTRS, for the MIXED_LEARNED mode.
 //
-// Preconditioner M^-1: the exact inverses of the 3x3 diagonal blocks of A
-// (block Jacobi).  Iteration (O'Leary's block CG, 3 right-hand sides, one
+// Preconditioner M^-1: the exact inverses of the 64 x 64 diagonal tiles of A
+// (block Jacobi over tiles; the atoms are in spatial order, so a tile holds
+// about 21 neighbouring atoms and their strongest couplings).  Iteration (O'Leary's block CG, 3 right-hand sides, one
 // recurrence per frequency):
 //   Q = A P;  alpha = (P^T Q)^-1 (Z^T R);  X += P alpha;  R -= Q alpha
 //   Z = M^-1 R;  beta = (Z_old^T R_old)^-1 (Z^T R);  P = Z + P beta
 // Four launches per iteration, all frequencies at once (grid.y = f):
 //   cg_tile    tile partials of A P (64 x 64 lower tiles serve both triangles)
 //   cg_rows    Q = sum of the partials of each 64-row block; partials of P^T Q
-//   cg_update  alpha; X, R, Z of 64 atoms per CTA; partials of Z^T R, R^T R
+//   cg_update  alpha; X, R, Z = M^-1 R of one 64-row tile per CTA; partials
+//              of Z^T R, R^T R
 //   cg_dir     beta; P; convergence test ||R||_F^2 <= tol2, after which every
 //              later launch returns at once for that frequency
 // The 3x3 sums are added in one fixed order by every CTA, so all CTAs of a
 // launch take the same decisions.
 #include <cuda_runtime.h>
+
+#include <algorithm>
 
 #include "kernels.h"
 
@@ -107,75 +111,123 @@ __device__ void cta_record(const double* vals, double* sm /* [kRed][32] */, doub
 
 __device__ __forceinline__ bool stopped(const CgArgs& a, int f) { return a.state[f * kCgState] != 0.0; }
 
-// Dinv[f][i] = inverse of the diagonal 3x3 block of atom i.
-__global__ void __launch_bounds__(256) cg_jacobi_kernel(CgArgs a) {
-  const int f = blockIdx.y;
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= a.N) return;
+// Minv[f][I] = inverse of the diagonal tile A_II (rows beyond n: the
+// identity): Cholesky L L^T = A_II in place, W = L^-1 column by column (W's
+// column c kept as row c of the upper triangle, its diagonal in wd), then
+// Minv = W^T W.  A tile that is not positive definite gets the identity (the
+// iteration then cannot converge and the residual gate sends the geometry to
+// the direct solve).
+__global__ void __launch_bounds__(256) cg_tile_inv_kernel(CgArgs a) {
+  __shared__ double T[CT][CT + 1];
+  __shared__ double wd[CT];
+  __shared__ int s_bad;
+  const int I = blockIdx.x, f = blockIdx.y, tid = threadIdx.x;
   const double* A = a.A + (size_t)f * a.a_stride;
-  double m[9], inv[9];
-#pragma unroll
-  for (int r = 0; r < 3; ++r)
-#pragma unroll
-    for (int c = 0; c < 3; ++c) {
-      const int rr = 3 * i + (r > c ? r : c), cc = 3 * i + (r > c ? c : r);
-      m[3 * r + c] = A[(size_t)rr * a.ld + cc];
-    }
-  if (!inv3(m, inv)) {
-#pragma unroll
-    for (int q = 0; q < 9; ++q) inv[q] = (q % 4 == 0) ? 1.0 : 0.0;
+  for (int e = tid; e < CT * CT; e += blockDim.x) {
+    const int r = e / CT, c = e % CT;
+    const int gr = I * CT + r, gc = I * CT + c;
+    double v = (r == c) ? 1.0 : 0.0;
+    if (gr < a.n && gc < a.n) v = (c <= r) ? A[(size_t)gr * a.ld + gc] : A[(size_t)gc * a.ld + gr];
+    T[r][c] = v;
   }
-  double* out = a.Dinv + ((size_t)f * a.N + i) * 9;
-#pragma unroll
-  for (int q = 0; q < 9; ++q) out[q] = inv[q];
+  if (tid == 0) s_bad = 0;
+  __syncthreads();
+  for (int k = 0; k < CT; ++k) {
+    if (tid == 0) {
+      const double d = T[k][k];
+      if (!(d > 0.0) || !isfinite(d)) s_bad = 1;
+      T[k][k] = sqrt(fmax(d, 1e-300));
+    }
+    __syncthreads();
+    const double lkk = T[k][k];
+    for (int i = k + 1 + tid; i < CT; i += blockDim.x) T[i][k] /= lkk;
+    __syncthreads();
+    const int w = CT - k - 1;
+    for (int e = tid; e < w * w; e += blockDim.x) {
+      const int i = k + 1 + e / w, j = k + 1 + e % w;
+      if (j <= i) T[i][j] -= T[i][k] * T[j][k];
+    }
+    __syncthreads();
+  }
+  if (tid < CT) {
+    // W(i, c) = (delta_ic - sum_{c <= k < i} L(i, k) W(k, c)) / L(i, i); W(k, c) at T[c][k] (k > c)
+    const int c = tid;
+    const double wcc = 1.0 / T[c][c];
+    wd[c] = wcc;
+    for (int i = c + 1; i < CT; ++i) {
+      double sum = T[i][c] * wcc;
+      for (int k = c + 1; k < i; ++k) sum += T[i][k] * T[c][k];
+      T[c][i] = -sum / T[i][i];
+    }
+  }
+  __syncthreads();
+  double* M = a.Minv + ((size_t)f * a.nt + I) * CT * CT;
+  for (int e = tid; e < CT * CT; e += blockDim.x) {
+    const int i = e / CT, j = e % CT;
+    double sum = 0.0;
+    if (s_bad) {
+      sum = (i == j) ? 1.0 : 0.0;
+    } else {
+      // (W^T W)(i, j) = sum_{k >= max(i, j)} W(k, i) W(k, j)
+      const int k0 = i > j ? i : j;
+      for (int k = k0; k < CT; ++k) sum += (k == i ? wd[i] : T[i][k]) * (k == j ? wd[j] : T[j][k]);
+    }
+    M[e] = sum;
+  }
 }
 
 // partial[f][I][J][64 x 3] = A_IJ v_J, and A_IJ^T v_I into [J][I] (I > J).
+// Grid-stride over (tile, frequency) items, so that the launches after every
+// frequency has converged cost a few microseconds.
 __global__ void __launch_bounds__(192) cg_tile_kernel(CgArgs a, const double* in) {
-  const int f = blockIdx.y;
-  if (stopped(a, f)) return;
   __shared__ double Ts[CT][CT + 1];
   __shared__ double xI[CT][3], xJ[CT][3];
-  int ti, tj;
-  cg_tri(blockIdx.x, &ti, &tj);
-  const double* A = a.A + (size_t)f * a.a_stride;
-  const double* x = in + (size_t)f * a.ystride;
+  const int ntiles = a.nt * (a.nt + 1) / 2;
   const int tid = threadIdx.x;
-  const bool diag = ti == tj;
   const int n = a.n;
-  // 16-byte loads (rows start 16-byte aligned: ld is a multiple of 32; the
-  // second element of a pair may lie in the row padding, masked below)
-  for (int idx = tid; idx < CT * CT / 2; idx += blockDim.x) {
-    const int r = idx / (CT / 2), c = 2 * (idx % (CT / 2));
-    const int gr = ti * CT + r, gc = tj * CT + c;
-    double2 v = make_double2(0.0, 0.0);
-    if (gr < n && gc < n && (!diag || c <= r)) v = *reinterpret_cast<const double2*>(A + (size_t)gr * a.ld + gc);
-    Ts[r][c] = v.x;
-    Ts[r][c + 1] = (gc + 1 < n && (!diag || c + 1 <= r)) ? v.y : 0.0;
-  }
-  for (int idx = tid; idx < CT * 3; idx += blockDim.x) {
-    const int r = idx / 3, q = idx % 3;
-    const int gi = ti * CT + r, gj = tj * CT + r;
-    xI[r][q] = gi < n ? x[(size_t)gi * 3 + q] : 0.0;
-    xJ[r][q] = gj < n ? x[(size_t)gj * 3 + q] : 0.0;
-  }
-  __syncthreads();
-  const int r = tid / 3, q = tid % 3;
-  double rs = 0.0, cs = 0.0;
+  for (long long item = blockIdx.x; item < (long long)ntiles * a.batch; item += gridDim.x) {
+    const int f = (int)(item / ntiles);
+    if (stopped(a, f)) continue;   // uniform over the CTA
+    int ti, tj;
+    cg_tri((int)(item % ntiles), &ti, &tj);
+    __syncthreads();   // the previous item's reads of Ts / xI / xJ are done
+    const double* A = a.A + (size_t)f * a.a_stride;
+    const double* x = in + (size_t)f * a.ystride;
+    const bool diag = ti == tj;
+    // 16-byte loads (rows start 16-byte aligned: ld is a multiple of 32; the
+    // second element of a pair may lie in the row padding, masked below)
+    for (int idx = tid; idx < CT * CT / 2; idx += blockDim.x) {
+      const int r = idx / (CT / 2), c = 2 * (idx % (CT / 2));
+      const int gr = ti * CT + r, gc = tj * CT + c;
+      double2 v = make_double2(0.0, 0.0);
+      if (gr < n && gc < n && (!diag || c <= r)) v = *reinterpret_cast<const double2*>(A + (size_t)gr * a.ld + gc);
+      Ts[r][c] = v.x;
+      Ts[r][c + 1] = (gc + 1 < n && (!diag || c + 1 <= r)) ? v.y : 0.0;
+    }
+    for (int idx = tid; idx < CT * 3; idx += blockDim.x) {
+      const int r = idx / 3, q = idx % 3;
+      const int gi = ti * CT + r, gj = tj * CT + r;
+      xI[r][q] = gi < n ? x[(size_t)gi * 3 + q] : 0.0;
+      xJ[r][q] = gj < n ? x[(size_t)gj * 3 + q] : 0.0;
+    }
+    __syncthreads();
+    const int r = tid / 3, q = tid % 3;
+    double rs = 0.0, cs = 0.0;
 #pragma unroll 8
-  for (int c = 0; c < CT; ++c) rs += Ts[r][c] * xJ[c][q];
-  if (!diag) {
+    for (int c = 0; c < CT; ++c) rs += Ts[r][c] * xJ[c][q];
+    if (!diag) {
 #pragma unroll 8
-    for (int c = 0; c < CT; ++c) cs += Ts[c][r] * xI[c][q];
-  } else {
-    for (int c = r + 1; c < CT; ++c) cs += Ts[c][r] * xI[c][q];
-  }
-  double* pr = a.partial + (size_t)f * a.nt * a.nt * CT * 3;
-  if (!diag) {
-    pr[((size_t)ti * a.nt + tj) * CT * 3 + tid] = rs;
-    pr[((size_t)tj * a.nt + ti) * CT * 3 + tid] = cs;
-  } else {
-    pr[((size_t)ti * a.nt + ti) * CT * 3 + tid] = rs + cs;
+      for (int c = 0; c < CT; ++c) cs += Ts[c][r] * xI[c][q];
+    } else {
+      for (int c = r + 1; c < CT; ++c) cs += Ts[c][r] * xI[c][q];
+    }
+    double* pr = a.partial + (size_t)f * a.nt * a.nt * CT * 3;
+    if (!diag) {
+      pr[((size_t)ti * a.nt + tj) * CT * 3 + tid] = rs;
+      pr[((size_t)tj * a.nt + ti) * CT * 3 + tid] = cs;
+    } else {
+      pr[((size_t)ti * a.nt + ti) * CT * 3 + tid] = rs + cs;
+    }
   }
 }
 
@@ -215,35 +267,60 @@ __device__ __forceinline__ void load_block(const double* v, size_t base, int i, 
   for (int k = 0; k < 9; ++k) out[k] = v[base + (size_t)9 * i + k];
 }
 
-// init: Z = M^-1 R, P = Z; partials of Z^T R and R^T R into red2.
-__global__ void __launch_bounds__(AT) cg_init_atoms_kernel(CgArgs a) {
-  const int f = blockIdx.y;
-  if (stopped(a, f)) return;
-  __shared__ double sm[kRed * 32];
-  const int i = blockIdx.x * AT + threadIdx.x;
+// Shared memory of the per-tile preconditioner step.
+struct TileSmem {
+  double Ms[CT][CT + 1];   // M^-1 of the tile
+  double Rs[CT][3], Zs[CT][3];
+  double red[kRed * 32];
+};
+
+// Thread (r, q) of a 192-thread CTA on 64-row tile I of frequency f holds
+// R(64 I + r, q) in rv (0 beyond n): Z = M^-1 R on the tile (written to a.Z,
+// and to a.P when also_p), then the CTA's partials of Z^T R and R^T R.
+__device__ void tile_precondition(const CgArgs& a, int f, int I, double rv, bool also_p, TileSmem& S) {
+  const int tid = threadIdx.x, r = tid / 3, q = tid % 3;
+  const double* Mg = a.Minv + ((size_t)f * a.nt + I) * CT * CT;
+  for (int e = tid; e < CT * CT / 2; e += blockDim.x) {
+    const double2 v = reinterpret_cast<const double2*>(Mg)[e];
+    const int rr = (2 * e) / CT, cc = (2 * e) % CT;
+    S.Ms[rr][cc] = v.x;
+    S.Ms[rr][cc + 1] = v.y;
+  }
+  S.Rs[r][q] = rv;
+  __syncthreads();
+  double z0 = 0.0, z1 = 0.0;   // two accumulation chains
+#pragma unroll 8
+  for (int k = 0; k < CT; k += 2) {
+    z0 += S.Ms[r][k] * S.Rs[k][q];
+    z1 += S.Ms[r][k + 1] * S.Rs[k + 1][q];
+  }
+  const double z = z0 + z1;
+  S.Zs[r][q] = z;
+  const int gr = I * CT + r;
+  if (gr < a.n) {
+    const size_t o = (size_t)f * a.ystride + (size_t)gr * 3 + q;
+    a.Z[o] = z;
+    if (also_p) a.P[o] = z;
+  }
+  __syncthreads();
   double vals[kRed];
 #pragma unroll
   for (int k = 0; k < kRed; ++k) vals[k] = 0.0;
-  if (i < a.N) {
-    const size_t base = (size_t)f * a.ystride;
-    double R[9], D[9], Z[9];
-    load_block(a.R, base, i, R);
-    load_block(a.Dinv, (size_t)f * a.N * 9, i, D);
-    mul3(D, R, Z);
+  // (Z^T R)(c, q) = sum_rows Z[row][c] R[row][q]
 #pragma unroll
-    for (int k = 0; k < 9; ++k) {
-      a.Z[base + 9 * (size_t)i + k] = Z[k];
-      a.P[base + 9 * (size_t)i + k] = Z[k];
-    }
-    // (Z^T R)(c, d) = sum_rows Z[row][c] R[row][d]
-#pragma unroll
-    for (int c = 0; c < 3; ++c)
-#pragma unroll
-      for (int d = 0; d < 3; ++d) vals[3 * c + d] = Z[c] * R[d] + Z[3 + c] * R[3 + d] + Z[6 + c] * R[6 + d];
-#pragma unroll
-    for (int k = 0; k < 9; ++k) vals[9] += R[k] * R[k];
-  }
-  cta_record(vals, sm, a.red2 + ((size_t)f * gridDim.x + blockIdx.x) * kRed);
+  for (int c = 0; c < 3; ++c) vals[3 * c + q] = S.Zs[r][c] * rv;
+  vals[9] = rv * rv;
+  cta_record(vals, S.red, a.red2 + ((size_t)f * a.nt + I) * kRed);
+}
+
+// init: Z = M^-1 R, P = Z on one 64-row tile; partials of Z^T R and R^T R.
+__global__ void __launch_bounds__(192) cg_init_tiles_kernel(CgArgs a) {
+  const int I = blockIdx.x, f = blockIdx.y;
+  if (stopped(a, f)) return;
+  __shared__ TileSmem S;
+  const int r = threadIdx.x / 3, q = threadIdx.x % 3, gr = I * CT + r;
+  const double rv = gr < a.n ? a.R[(size_t)f * a.ystride + (size_t)gr * 3 + q] : 0.0;
+  tile_precondition(a, f, I, rv, true, S);
 }
 
 // init: Z^T R and R^T R into the state; stop when already converged.
@@ -261,14 +338,14 @@ __global__ void cg_init_final_kernel(CgArgs a, int nb) {
   }
 }
 
-// alpha = (P^T Q)^-1 (Z^T R); X += P alpha; R -= Q alpha; Z = M^-1 R;
-// partials of Z^T R (new) and R^T R into red2.
-__global__ void __launch_bounds__(AT) cg_update_kernel(CgArgs a, int it) {
-  const int f = blockIdx.y;
+// alpha = (P^T Q)^-1 (Z^T R); X += P alpha; R -= Q alpha on one 64-row
+// tile; Z = M^-1 R; partials of Z^T R (new) and R^T R into red2.
+__global__ void __launch_bounds__(192) cg_update_kernel(CgArgs a, int it) {
+  const int I = blockIdx.x, f = blockIdx.y;
   if (stopped(a, f)) return;
   __shared__ double tot[kRed];
-  __shared__ double sm[kRed * 32];
   __shared__ double s_alpha[9];
+  __shared__ TileSmem S;
   sum_records(a.red + (size_t)f * a.nt * kRed, a.nt, tot);
   if (threadIdx.x == 0) {
     const double* zr = a.state + f * kCgState + kZR0 + 9 * (it & 1);
@@ -282,39 +359,21 @@ __global__ void __launch_bounds__(AT) cg_update_kernel(CgArgs a, int it) {
     for (int k = 0; k < 9; ++k) s_alpha[k] = al[k];
   }
   __syncthreads();
-  const int i = blockIdx.x * AT + threadIdx.x;
-  double vals[kRed];
+  const int r = threadIdx.x / 3, q = threadIdx.x % 3, gr = I * CT + r;
+  double rv = 0.0;
+  if (gr < a.n) {
+    const size_t o = (size_t)f * a.ystride + (size_t)gr * 3;
+    double x = a.X[o + q], rr = a.R[o + q];
 #pragma unroll
-  for (int k = 0; k < kRed; ++k) vals[k] = 0.0;
-  if (i < a.N) {
-    const size_t base = (size_t)f * a.ystride;
-    double X[9], R[9], P[9], Q[9], D[9], Z[9], t[9];
-    load_block(a.X, base, i, X);
-    load_block(a.R, base, i, R);
-    load_block(a.P, base, i, P);
-    load_block(a.Q, base, i, Q);
-    load_block(a.Dinv, (size_t)f * a.N * 9, i, D);
-    mul3(P, s_alpha, t);
-#pragma unroll
-    for (int k = 0; k < 9; ++k) X[k] += t[k];
-    mul3(Q, s_alpha, t);
-#pragma unroll
-    for (int k = 0; k < 9; ++k) R[k] -= t[k];
-    mul3(D, R, Z);
-#pragma unroll
-    for (int k = 0; k < 9; ++k) {
-      a.X[base + 9 * (size_t)i + k] = X[k];
-      a.R[base + 9 * (size_t)i + k] = R[k];
-      a.Z[base + 9 * (size_t)i + k] = Z[k];
+    for (int c = 0; c < 3; ++c) {
+      x += a.P[o + c] * s_alpha[3 * c + q];
+      rr -= a.Q[o + c] * s_alpha[3 * c + q];
     }
-#pragma unroll
-    for (int c = 0; c < 3; ++c)
-#pragma unroll
-      for (int d = 0; d < 3; ++d) vals[3 * c + d] = Z[c] * R[d] + Z[3 + c] * R[3 + d] + Z[6 + c] * R[6 + d];
-#pragma unroll
-    for (int k = 0; k < 9; ++k) vals[9] += R[k] * R[k];
+    a.X[o + q] = x;
+    a.R[o + q] = rr;
+    rv = rr;
   }
-  cta_record(vals, sm, a.red2 + ((size_t)f * gridDim.x + blockIdx.x) * kRed);
+  tile_precondition(a, f, I, rv, false, S);
 }
 
 // beta = (Z^T R)_old^-1 (Z^T R)_new; P = Z + P beta; convergence test.
@@ -324,7 +383,7 @@ __global__ void __launch_bounds__(AT) cg_dir_kernel(CgArgs a, int it) {
   __shared__ double tot[kRed];
   __shared__ double s_beta[9];
   __shared__ int s_done;
-  sum_records(a.red2 + (size_t)f * gridDim.x * kRed, gridDim.x, tot);
+  sum_records(a.red2 + (size_t)f * a.nt * kRed, a.nt, tot);   // one record per 64-row tile
   double* st = a.state + f * kCgState;
   if (threadIdx.x == 0) {
     const double* zr_old = st + kZR0 + 9 * (it & 1);
@@ -372,6 +431,24 @@ __global__ void __launch_bounds__(AT) cg_dir_kernel(CgArgs a, int it) {
 
 }  // namespace
 
+size_t cg_minv_doubles(int n, int batch) {
+  const int nt = (n + CT - 1) / CT;
+  return (size_t)batch * nt * CT * CT;
+}
+
+// CTAs of the grid-stride tile launch: every resident slot of the device.
+int cg_tile_grid() {
+  static int grid = 0;
+  if (grid == 0) {
+    int dev = 0, sms = 0, per_sm = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, cg_tile_kernel, 192, 0);
+    grid = (sms > 0 ? sms : 148) * (per_sm > 0 ? per_sm : 1);
+  }
+  return grid;
+}
+
 size_t cg_partial_doubles(int n, int batch) {
   const int nt = (n + CT - 1) / CT;
   return (size_t)batch * nt * nt * CT * 3;
@@ -384,20 +461,23 @@ size_t cg_red_doubles(int n, int batch) {
 }
 
 void launch_cg_setup(const CgArgs& a, cudaStream_t s) {
-  const int nb = (a.N + AT - 1) / AT;
+  const long long items = (long long)a.nt * (a.nt + 1) / 2 * a.batch;
+  const int tgrid = (int)std::min<long long>(cg_tile_grid(), items);
   cudaMemsetAsync(a.state, 0, sizeof(double) * kCgState * a.batch, s);
-  cg_jacobi_kernel<<<dim3((a.N + 255) / 256, a.batch), 256, 0, s>>>(a);
-  cg_tile_kernel<<<dim3(a.nt * (a.nt + 1) / 2, a.batch), 192, 0, s>>>(a, a.X);
+  cg_tile_inv_kernel<<<dim3(a.nt, a.batch), 256, 0, s>>>(a);
+  cg_tile_kernel<<<tgrid, 192, 0, s>>>(a, a.X);
   cg_rows_kernel<<<dim3(a.nt, a.batch), 192, 0, s>>>(a, 1);
-  cg_init_atoms_kernel<<<dim3(nb, a.batch), AT, 0, s>>>(a);
-  cg_init_final_kernel<<<a.batch, 32, 0, s>>>(a, nb);
+  cg_init_tiles_kernel<<<dim3(a.nt, a.batch), 192, 0, s>>>(a);
+  cg_init_final_kernel<<<a.batch, 32, 0, s>>>(a, a.nt);
 }
 
 void launch_cg_iteration(const CgArgs& a, int it, cudaStream_t s) {
   const int nb = (a.N + AT - 1) / AT;
-  cg_tile_kernel<<<dim3(a.nt * (a.nt + 1) / 2, a.batch), 192, 0, s>>>(a, a.P);
+  const long long items = (long long)a.nt * (a.nt + 1) / 2 * a.batch;
+  const int tgrid = (int)std::min<long long>(cg_tile_grid(), items);
+  cg_tile_kernel<<<tgrid, 192, 0, s>>>(a, a.P);
   cg_rows_kernel<<<dim3(a.nt, a.batch), 192, 0, s>>>(a, 0);
-  cg_update_kernel<<<dim3(nb, a.batch), AT, 0, s>>>(a, it);
+  cg_update_kernel<<<dim3(a.nt, a.batch), 192, 0, s>>>(a, it);
   cg_dir_kernel<<<dim3(nb, a.batch), AT, 0, s>>>(a, it);
 }
 

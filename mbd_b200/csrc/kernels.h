@@ -199,7 +199,7 @@ struct CgArgs {
   int batch;               // frequencies
   double *X, *R, *Z, *P, *Q;   // [batch][n][3]; X holds the start on entry
   size_t ystride;          // n * 3
-  double* Dinv;            // [batch][N][9] block-Jacobi inverses
+  double* Minv;            // [batch][nt][64][64] inverses of the 64 x 64 diagonal tiles
   double* partial;         // cg_partial_doubles
   double* red;             // cg_red_doubles (row-block partials)
   double* red2;            // cg_red_doubles (atom-block partials)
@@ -207,8 +207,9 @@ struct CgArgs {
   double tol2;             // stop when ||R||_F^2 <= tol2
 };
 size_t cg_partial_doubles(int n, int batch);
+size_t cg_minv_doubles(int n, int batch);
 size_t cg_red_doubles(int n, int batch);
-// Jacobi blocks, R = B - A X, Z, P and Z^T R for every frequency.
+// Tile inverses, R = B - A X, Z, P and Z^T R for every frequency.
 void launch_cg_setup(const CgArgs& a, cudaStream_t s);
 // One iteration (iteration index it = 0, 1, ...); a converged frequency skips it.
 void launch_cg_iteration(const CgArgs& a, int it, cudaStream_t s);

@@ -180,7 +180,7 @@ const int* graph_species(const GeomDev* gd) {
 
 size_t cg_doubles(const GeomPlan& p) {
   const size_t ys = (size_t)p.n * 3;
-  return 5 * kNFreq * ys + (size_t)kNFreq * p.N * 9 + cg_partial_doubles(p.n, kNFreq) +
+  return cg_minv_doubles(p.n, kNFreq) + 5 * kNFreq * ys + cg_partial_doubles(p.n, kNFreq) +
          2 * cg_red_doubles(p.n, kNFreq) + 64;
 }
 
@@ -268,14 +268,14 @@ int relay_learned(mbd_ctx* ctx, GeomDev* gd, RelaySlot& sl, size_t mstride, cuda
   a.N = N;
   a.nt = (n + 63) / 64;
   a.batch = kNFreq;
-  a.X = base;
+  a.Minv = base;   // first: its 16-byte loads need the buffer's alignment
+  a.X = a.Minv + cg_minv_doubles(n, kNFreq);
   a.R = a.X + kNFreq * ys;
   a.Z = a.R + kNFreq * ys;
   a.P = a.Z + kNFreq * ys;
   a.Q = a.P + kNFreq * ys;
   a.ystride = ys;
-  a.Dinv = a.Q + kNFreq * ys;
-  a.partial = a.Dinv + (size_t)kNFreq * N * 9;
+  a.partial = a.Q + kNFreq * ys;
   a.red = a.partial + cg_partial_doubles(n, kNFreq);
   a.red2 = a.red + cg_red_doubles(n, kNFreq);
   a.state = gd->cgstate;

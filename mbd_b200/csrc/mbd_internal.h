@@ -65,6 +65,9 @@ struct GeomPlan {
   // per-atom free-atom data
   std::vector<double> alpha0, c6free, r0, hirsh;
   std::vector<double> coords;           // 3N, xyz per atom (bohr)
+  // Per-atom arrays above are in an internal spatial order: internal atom q
+  // is the caller's atom perm[q] (results are scattered back on download).
+  std::vector<int> perm;
 };
 
 // Builds the plan; returns an MBD_* status.

@@ -2,7 +2,10 @@
 // the translation lists the tensor-build kernels iterate over.
 #include <algorithm>
 #include <cmath>
+#include <cstdint>
 #include <cstring>
+#include <utility>
+#include <vector>
 
 #include "mbd_internal.h"
 
@@ -77,6 +80,35 @@ const Entry kTable[] = {
 constexpr int kTableSize = sizeof(kTable) / sizeof(kTable[0]);
 
 double norm3(const double* v) { return std::sqrt(v[0] * v[0] + v[1] * v[1] + v[2] * v[2]); }
+
+// Atoms in Morton (Z-curve) order of their coordinates: perm[p] = the
+// caller's index of internal atom p.  Consecutive internal atoms are then
+// spatial neighbours, so a 64-row diagonal tile of the relay matrix holds the
+// strongest couplings of its ~21 atoms (the block-CG preconditioner of the
+// MIXED_LEARNED mode inverts those tiles).  Ties keep the input order.
+void spatial_order(const double* xyz, int N, std::vector<int>* perm) {
+  double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
+  for (int i = 0; i < N; ++i)
+    for (int c = 0; c < 3; ++c) {
+      lo[c] = std::min(lo[c], xyz[3 * i + c]);
+      hi[c] = std::max(hi[c], xyz[3 * i + c]);
+    }
+  const double ext = std::max(std::max(hi[0] - lo[0], hi[1] - lo[1]), std::max(hi[2] - lo[2], 1e-300));
+  std::vector<std::pair<uint32_t, int>> key(N);
+  for (int i = 0; i < N; ++i) {
+    uint32_t code = 0;
+    uint32_t q[3];
+    for (int c = 0; c < 3; ++c) q[c] = (uint32_t)std::min(1023.0, std::floor((xyz[3 * i + c] - lo[c]) / ext * 1024.0));
+    for (int b = 0; b < 10; ++b)
+      for (int c = 0; c < 3; ++c) code |= ((q[c] >> b) & 1u) << (3 * b + c);
+    key[i] = {code, i};
+  }
+  std::stable_sort(key.begin(), key.end(), [](const std::pair<uint32_t, int>& a, const std::pair<uint32_t, int>& b) {
+    return a.first < b.first;
+  });
+  perm->resize(N);
+  for (int p = 0; p < N; ++p) (*perm)[p] = key[p].second;
+}
 
 // Upper bound of every entry of the short-range tensor at distance r
 // (gaussian_dipole_tensor, UTILS.f90:637-696):
@@ -159,20 +191,29 @@ int build_plan(const mbd_geom& g, GeomPlan* p) {
   p->alpha0.resize(N);
   p->c6free.resize(N);
   p->r0.resize(N);
-  p->hirsh.assign(g.hirshfeld, g.hirshfeld + N);
-  p->coords.assign(g.coords_bohr, g.coords_bohr + 3 * N);
+  p->hirsh.resize(N);
+  p->coords.resize(3 * N);
   for (int k = 0; k < 3; ++k) p->vac[k] = (g.n_periodic != 0 && g.vacuum[k]) ? 1 : 0;
   p->species.resize(N);
   for (int i = 0; i < N; ++i) {
     VdwParam v;
     if (!vdw_param(g.z[i], &v)) return MBD_ERR_UNKNOWN_ELEMENT;
-    p->species[i] = g.z[i] == 1 ? 0 : g.z[i] == 6 ? 1 : g.z[i] == 7 ? 2 : g.z[i] == 8 ? 3 : 4;
-    p->alpha0[i] = v.alpha0;
-    p->c6free[i] = v.c6;
-    p->r0[i] = v.r0;
     if (!(g.hirshfeld[i] > 0.0) || !std::isfinite(g.hirshfeld[i])) return MBD_ERR_ARG;
     for (int c = 0; c < 3; ++c)
       if (!std::isfinite(g.coords_bohr[3 * i + c])) return MBD_ERR_ARG;
+  }
+  // every per-atom array in the internal (spatial) order
+  spatial_order(g.coords_bohr, N, &p->perm);
+  for (int q = 0; q < N; ++q) {
+    const int i = p->perm[q];
+    VdwParam v;
+    vdw_param(g.z[i], &v);
+    p->species[q] = g.z[i] == 1 ? 0 : g.z[i] == 6 ? 1 : g.z[i] == 7 ? 2 : g.z[i] == 8 ? 3 : 4;
+    p->alpha0[q] = v.alpha0;
+    p->c6free[q] = v.c6;
+    p->r0[q] = v.r0;
+    p->hirsh[q] = g.hirshfeld[i];
+    for (int c = 0; c < 3; ++c) p->coords[3 * q + c] = g.coords_bohr[3 * i + c];
   }
 
   // Supercell (get_supercell, UTILS.f90:1252-1283).
