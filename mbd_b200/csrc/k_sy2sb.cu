@@ -441,15 +441,72 @@ __device__ __forceinline__ void dmma(double& d0, double& d1, double a, double b)
 // half-warp hit 16 distinct bank pairs: stride = 4 (mod 16).
 constexpr int FS = TL + 4;   // 68
 
+// 16-byte asynchronous copy global -> shared; src_bytes < 16 zero-fills the rest.
+__device__ __forceinline__ void cp_async16(void* dst, const void* src, int src_bytes) {
+  const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(d), "l"(src), "r"(src_bytes) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int NPEND>
+__device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;" ::"n"(NPEND) : "memory");
+}
+
 // Y partials: Yp[s][r][c] = sum over column tiles J of chunk s of (A22 V)[r][c],
 // row block I = blockIdx.x (64 rows), chunk s = blockIdx.y.  4 warps, each 16
-// rows x 32 columns of the block (2 x 4 MMA tiles).
-constexpr size_t kSymmSmem = sizeof(double) * (TL * FS + B * FS);
+// rows x 32 columns of the block (2 x 4 MMA tiles).  The stored lower tile
+// that holds A22's block (I, J) -- (I, J) itself for J < I, (J, I) for J > I,
+// the diagonal tile for J = I -- and the 64 rows of V of block J are copied to
+// shared memory as they are stored (cp.async, two stages: the next J's copy
+// runs under this J's MMAs); the MMA reads the tile in its orientation.
+constexpr int FV = B + 4;                        // 36: V rows in shared memory (4 mod 16)
+constexpr int kSymmStage = TL * FS + TL * FV;    // doubles per stage
+constexpr size_t kSymmSmem = sizeof(double) * 2 * kSymmStage;
+
+__device__ __forceinline__ void symm_stage(const double* A22, int ld, int m, const double* V, int I, int J,
+                                           double* As, double* Vs) {
+  const int tid = threadIdx.x;
+  const int R0 = (J <= I ? I : J) * TL, C0 = (J <= I ? J : I) * TL;
+  for (int idx = tid; idx < TL * (TL / 2); idx += blockDim.x) {
+    const int u = idx / (TL / 2), w = 2 * (idx % (TL / 2));
+    const int gr = R0 + u, gc = C0 + w;
+    const bool rok = gr < m;
+    const int bytes = rok ? (gc + 1 < m ? 16 : (gc < m ? 8 : 0)) : 0;
+    cp_async16(As + u * FS + w, A22 + (size_t)(rok ? gr : 0) * ld + (bytes ? gc : 0), bytes);
+  }
+  for (int idx = tid; idx < TL * (B / 2); idx += blockDim.x) {
+    const int k = idx / (B / 2), c = 2 * (idx % (B / 2));
+    const int gk = J * TL + k;
+    cp_async16(Vs + k * FV + c, V + (size_t)(gk < m ? gk : 0) * B + c, gk < m ? 16 : 0);
+  }
+}
+
+// MODE 0: block (I, J) stored as is; 1: stored transposed; 2: diagonal tile (lower).
+template <int MODE>
+__device__ __forceinline__ void symm_mma(const double* As, const double* Vs, int warp, int g, int q4,
+                                         double (&acc)[2][4][2]) {
+#pragma unroll 4
+  for (int k0 = 0; k0 < TL; k0 += 4) {
+    double af[2], bf[4];
+#pragma unroll
+    for (int i = 0; i < 2; ++i) {
+      const int r = warp * 16 + i * 8 + g, k = k0 + q4;
+      if (MODE == 0) af[i] = As[r * FS + k];
+      else if (MODE == 1) af[i] = As[k * FS + r];
+      else af[i] = As[(r > k ? r : k) * FS + (r > k ? k : r)];
+    }
+#pragma unroll
+    for (int q = 0; q < 4; ++q) bf[q] = Vs[(k0 + q4) * FV + q * 8 + g];
+#pragma unroll
+    for (int i = 0; i < 2; ++i)
+#pragma unroll
+      for (int q = 0; q < 4; ++q) dmma(acc[i][q][0], acc[i][q][1], af[i], bf[q]);
+  }
+}
+
 __global__ void __launch_bounds__(128) symm_kernel(const double* A, int ld, int row0, int m, const double* V,
                                                    double* Yp, int chunk) {
-  extern __shared__ double dsm[];
-  double* As = dsm;              // [64][FS]: As[r][k] = A22(I*64 + r, J*64 + k)
-  double* Vt = dsm + TL * FS;    // [32][FS]: Vt[c][k] = V(J*64 + k, c)
+  extern __shared__ __align__(16) double dsm[];
   const int I = blockIdx.x, s = blockIdx.y;
   const int nt = (m + TL - 1) / TL;
   const int J0 = s * chunk, J1 = min(nt, J0 + chunk);
@@ -461,44 +518,22 @@ __global__ void __launch_bounds__(128) symm_kernel(const double* A, int ld, int 
 #pragma unroll
     for (int q = 0; q < 4; ++q) acc[i][q][0] = acc[i][q][1] = 0.0;
   const double* A22 = A + (size_t)row0 * ld + row0;
+  if (J0 < J1) symm_stage(A22, ld, m, V, I, J0, dsm, dsm + TL * FS);
+  cp_async_commit();
   for (int J = J0; J < J1; ++J) {
+    const double* As = dsm + ((J - J0) & 1) * kSymmStage;
+    const double* Vs = As + TL * FS;
+    if (J + 1 < J1) {
+      double* An = dsm + ((J + 1 - J0) & 1) * kSymmStage;
+      symm_stage(A22, ld, m, V, I, J + 1, An, An + TL * FS);
+    }
+    cp_async_commit();
+    cp_async_wait<1>();   // this J's stage has landed (the next may be in flight)
     __syncthreads();
-    for (int idx = tid; idx < TL * TL; idx += 128) {
-      const int u = idx / TL, w = idx % TL;   // w contiguous in global memory
-      double x = 0.0;
-      if (J < I) {
-        const int gr = I * TL + u, gc = J * TL + w;
-        if (gr < m) x = A22[(size_t)gr * ld + gc];
-        As[u * FS + w] = x;
-      } else if (J > I) {
-        const int gr = J * TL + u, gc = I * TL + w;   // stored tile (J, I), transposed into As
-        if (gr < m && gc < m) x = A22[(size_t)gr * ld + gc];
-        As[w * FS + u] = x;
-      } else {
-        const int a_ = u >= w ? u : w, b_ = u >= w ? w : u;
-        const int gr = I * TL + a_, gc = I * TL + b_;
-        if (gr < m) x = A22[(size_t)gr * ld + gc];
-        As[u * FS + w] = x;
-      }
-    }
-    for (int idx = tid; idx < TL * B; idx += 128) {
-      const int k = idx / B, c = idx % B;
-      const int gk = J * TL + k;
-      Vt[c * FS + k] = gk < m ? V[(size_t)gk * B + c] : 0.0;
-    }
-    __syncthreads();
-#pragma unroll 4
-    for (int k0 = 0; k0 < TL; k0 += 4) {
-      double af[2], bf[4];
-#pragma unroll
-      for (int i = 0; i < 2; ++i) af[i] = As[(warp * 16 + i * 8 + g) * FS + k0 + q4];
-#pragma unroll
-      for (int q = 0; q < 4; ++q) bf[q] = Vt[(q * 8 + g) * FS + k0 + q4];
-#pragma unroll
-      for (int i = 0; i < 2; ++i)
-#pragma unroll
-        for (int q = 0; q < 4; ++q) dmma(acc[i][q][0], acc[i][q][1], af[i], bf[q]);
-    }
+    if (J < I) symm_mma<0>(As, Vs, warp, g, q4, acc);
+    else if (J > I) symm_mma<1>(As, Vs, warp, g, q4, acc);
+    else symm_mma<2>(As, Vs, warp, g, q4, acc);
+    __syncthreads();      // the stage is read before the copy two steps on reuses it
   }
   double* out = Yp + (size_t)s * m * B;
 #pragma unroll
@@ -596,62 +631,74 @@ __global__ void __launch_bounds__(256) zform_kernel(const double* Y, const doubl
 
 // A22 -= V Z^T + Z V^T on lower 64 x 64 tiles: [V_I | Z_I] [Z_J | V_J]^T
 // (K = 64) on FP64 MMAs; 4 warps, each a 32 x 32 quarter (4 x 4 MMA tiles).
-constexpr size_t kSyr2kSmem = sizeof(double) * 2 * TL * FS;
+// The two operand blocks and the A22 tile itself are copied to shared memory
+// together (cp.async), the products are subtracted there and the tile goes
+// back a row per warp instruction (coalesced).
+constexpr size_t kSyr2kSmem = sizeof(double) * 3 * TL * FS;
 __global__ void __launch_bounds__(128) syr2k_kernel(double* A, int ld, int row0, int m, const double* V,
                                                     const double* Z) {
-  extern __shared__ double dsm[];
-  double* Li = dsm;              // [64][FS]: [V_I | Z_I]
-  double* Lj = dsm + TL * FS;    // [64][FS]: [Z_J | V_J]
+  extern __shared__ __align__(16) double dsm[];
+  double* Li = dsm;                // [64][FS]: [V_I | Z_I]
+  double* Lj = dsm + TL * FS;      // [64][FS]: [Z_J | V_J]
+  double* Cs = dsm + 2 * TL * FS;  // [64][FS]: the A22 tile (I, J)
   int ti = (int)((sqrt(8.0 * blockIdx.x + 1.0) - 1.0) * 0.5);
   while ((ti + 1) * (ti + 2) / 2 <= (int)blockIdx.x) ++ti;
   while (ti * (ti + 1) / 2 > (int)blockIdx.x) --ti;
   const int tj = (int)blockIdx.x - ti * (ti + 1) / 2;
   const int tid = threadIdx.x, warp = tid / 32, lane = tid % 32;
   const int g = lane >> 2, q4 = lane & 3;
-  for (int e = tid; e < TL * B; e += 128) {
-    const int r = e / B, c = e % B;
+  double* A22 = A + (size_t)row0 * ld + row0;
+  for (int e = tid; e < TL * (B / 2); e += 128) {
+    const int r = e / (B / 2), c = 2 * (e % (B / 2));
     const int gi = ti * TL + r, gj = tj * TL + r;
-    const bool li = gi < m, lj = gj < m;
-    Li[r * FS + c] = li ? V[(size_t)gi * B + c] : 0.0;
-    Li[r * FS + B + c] = li ? Z[(size_t)gi * B + c] : 0.0;
-    Lj[r * FS + c] = lj ? Z[(size_t)gj * B + c] : 0.0;
-    Lj[r * FS + B + c] = lj ? V[(size_t)gj * B + c] : 0.0;
+    const int bi = gi < m ? 16 : 0, bj = gj < m ? 16 : 0;
+    const size_t oi = (size_t)(gi < m ? gi : 0) * B + c, oj = (size_t)(gj < m ? gj : 0) * B + c;
+    cp_async16(Li + r * FS + c, V + oi, bi);
+    cp_async16(Li + r * FS + B + c, Z + oi, bi);
+    cp_async16(Lj + r * FS + c, Z + oj, bj);
+    cp_async16(Lj + r * FS + B + c, V + oj, bj);
   }
+  for (int e = tid; e < TL * (TL / 2); e += 128) {
+    const int r = e / (TL / 2), c = 2 * (e % (TL / 2));
+    const int gr = ti * TL + r, gc = tj * TL + c;
+    const bool rok = gr < m;
+    const int bytes = rok ? (gc + 1 < m ? 16 : (gc < m ? 8 : 0)) : 0;
+    cp_async16(Cs + r * FS + c, A22 + (size_t)(rok ? gr : 0) * ld + (bytes ? gc : 0), bytes);
+  }
+  cp_async_commit();
+  cp_async_wait<0>();
   __syncthreads();
   const int r0 = (warp / 2) * 32, c0 = (warp % 2) * 32;
-  if (ti == tj && c0 > r0) return;   // strictly upper quarter of a diagonal tile
-  double acc[4][4][2];
-#pragma unroll
-  for (int i = 0; i < 4; ++i)
-#pragma unroll
-    for (int q = 0; q < 4; ++q) acc[i][q][0] = acc[i][q][1] = 0.0;
-#pragma unroll 2
-  for (int k0 = 0; k0 < 2 * B; k0 += 4) {
-    double af[4], bf[4];
-#pragma unroll
-    for (int i = 0; i < 4; ++i) af[i] = Li[(r0 + i * 8 + g) * FS + k0 + q4];
-#pragma unroll
-    for (int q = 0; q < 4; ++q) bf[q] = Lj[(c0 + q * 8 + g) * FS + k0 + q4];
+  if (!(ti == tj && c0 > r0)) {   // the strictly upper quarter of a diagonal tile is not stored
+    double acc[4][4][2];
 #pragma unroll
     for (int i = 0; i < 4; ++i)
 #pragma unroll
-      for (int q = 0; q < 4; ++q) dmma(acc[i][q][0], acc[i][q][1], af[i], bf[q]);
+      for (int q = 0; q < 4; ++q) acc[i][q][0] = acc[i][q][1] = 0.0;
+#pragma unroll 2
+    for (int k0 = 0; k0 < 2 * B; k0 += 4) {
+      double af[4], bf[4];
+#pragma unroll
+      for (int i = 0; i < 4; ++i) af[i] = Li[(r0 + i * 8 + g) * FS + k0 + q4];
+#pragma unroll
+      for (int q = 0; q < 4; ++q) bf[q] = Lj[(c0 + q * 8 + g) * FS + k0 + q4];
+#pragma unroll
+      for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int q = 0; q < 4; ++q) dmma(acc[i][q][0], acc[i][q][1], af[i], bf[q]);
+    }
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+      for (int q = 0; q < 4; ++q)
+#pragma unroll
+        for (int h = 0; h < 2; ++h) Cs[(r0 + i * 8 + g) * FS + c0 + q * 8 + 2 * q4 + h] -= acc[i][q][h];
   }
-  double* A22 = A + (size_t)row0 * ld + row0;
-#pragma unroll
-  for (int i = 0; i < 4; ++i) {
-    const int gr = ti * TL + r0 + i * 8 + g;
-    if (gr >= m) continue;
-#pragma unroll
-    for (int q = 0; q < 4; ++q)
-#pragma unroll
-      for (int h = 0; h < 2; ++h) {
-        const int gc = tj * TL + c0 + q * 8 + 2 * q4 + h;
-        if (gc <= gr) {
-          double* p = A22 + (size_t)gr * ld + gc;
-          *p -= acc[i][q][h];
-        }
-      }
+  __syncthreads();
+  for (int e = tid; e < TL * TL; e += 128) {
+    const int r = e / TL, c = e % TL;
+    const int gr = ti * TL + r, gc = tj * TL + c;
+    if (gr < m && gc < m && (ti != tj || c <= r)) A22[(size_t)gr * ld + gc] = Cs[r * FS + c];
   }
 }
 
@@ -772,7 +819,7 @@ cudaError_t launch_sy2sb(double* A, int ld, int n, double* ws, double* Br, int n
     if (e != cudaSuccess) return e;
     // two-sided update of the trailing block
     const int nt = (m + TL - 1) / TL;
-    int S = (4 * num_sms + nt - 1) / nt;
+    int S = (2 * num_sms + nt - 1) / nt;   // one wave at two CTAs per SM
     S = S < 1 ? 1 : (S > kSymmMaxSplit ? kSymmMaxSplit : S);
     if (S > nt) S = nt;
     const int chunk = (nt + S - 1) / S;
