@@ -178,55 +178,110 @@ __global__ void __launch_bounds__(256) cg_tile_inv_kernel(CgArgs a) {
 
 // partial[f][I][J][64 x 3] = A_IJ v_J, and A_IJ^T v_I into [J][I] (I > J).
 // Grid-stride over (tile, frequency) items, so that the launches after every
-// frequency has converged cost a few microseconds.
-__global__ void __launch_bounds__(192) cg_tile_kernel(CgArgs a, const double* in) {
-  __shared__ double Ts[CT][CT + 1];
-  __shared__ double xI[CT][3], xJ[CT][3];
+// frequency has converged cost a few microseconds.  Thread (ty, tx) of 16 x 16
+// holds the 16 tile entries of rows ty + 16 i and columns {2 tx, 2 tx + 1,
+// 32 + 2 tx, 33 + 2 tx} in registers (16-byte loads, a warp reads two 256-byte
+// row segments per instruction), forms their row and column products with v
+// (6 FMAs per entry) and the 16 partial sums of every output meet in shared
+// memory (fixed order).
+constexpr int TT = 256;           // threads of cg_tile
+constexpr int RP = CT * 3 + 1;    // row stride of the partial-sum buffer (bank spread)
+__global__ void __launch_bounds__(TT, 3) cg_tile_kernel(CgArgs a, const double* in) {
+  __shared__ __align__(16) double xI[CT * 3], xJ[CT * 3];
+  __shared__ double buf[16 * RP];
   const int ntiles = a.nt * (a.nt + 1) / 2;
-  const int tid = threadIdx.x;
+  const int tid = threadIdx.x, tx = tid & 15, ty = tid >> 4;
   const int n = a.n;
-  for (long long item = blockIdx.x; item < (long long)ntiles * a.batch; item += gridDim.x) {
+  const long long items = (long long)ntiles * a.batch;
+  for (long long item = blockIdx.x; item < items; item += gridDim.x) {
     const int f = (int)(item / ntiles);
-    if (stopped(a, f)) continue;   // uniform over the CTA
+    if (stopped(a, f)) {
+      // skip to this CTA's first item of the next frequency (uniform over the CTA)
+      const long long next = (long long)(f + 1) * ntiles;
+      item += (next - item - 1) / gridDim.x * gridDim.x;
+      continue;
+    }
     int ti, tj;
     cg_tri((int)(item % ntiles), &ti, &tj);
-    __syncthreads();   // the previous item's reads of Ts / xI / xJ are done
+    const bool diag = ti == tj;
     const double* A = a.A + (size_t)f * a.a_stride;
     const double* x = in + (size_t)f * a.ystride;
-    const bool diag = ti == tj;
-    // 16-byte loads (rows start 16-byte aligned: ld is a multiple of 32; the
-    // second element of a pair may lie in the row padding, masked below)
-    for (int idx = tid; idx < CT * CT / 2; idx += blockDim.x) {
-      const int r = idx / (CT / 2), c = 2 * (idx % (CT / 2));
-      const int gr = ti * CT + r, gc = tj * CT + c;
-      double2 v = make_double2(0.0, 0.0);
-      if (gr < n && gc < n && (!diag || c <= r)) v = *reinterpret_cast<const double2*>(A + (size_t)gr * a.ld + gc);
-      Ts[r][c] = v.x;
-      Ts[r][c + 1] = (gc + 1 < n && (!diag || c + 1 <= r)) ? v.y : 0.0;
+    // the 16 entries (16-byte loads; rows start 16-byte aligned, ld a multiple
+    // of 32; an entry beyond n or above the diagonal reads as zero)
+    double t[4][4];
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+      const int r = ty + 16 * i, gr = ti * CT + r;
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        const int c = 2 * tx + 32 * h, gc = tj * CT + c;
+        double2 v = make_double2(0.0, 0.0);
+        if (gr < n && gc < n && (!diag || c <= r)) v = *reinterpret_cast<const double2*>(A + (size_t)gr * a.ld + gc);
+        t[i][2 * h] = v.x;
+        t[i][2 * h + 1] = (gc + 1 < n && (!diag || c + 1 <= r)) ? v.y : 0.0;
+      }
     }
-    for (int idx = tid; idx < CT * 3; idx += blockDim.x) {
-      const int r = idx / 3, q = idx % 3;
-      const int gi = ti * CT + r, gj = tj * CT + r;
-      xI[r][q] = gi < n ? x[(size_t)gi * 3 + q] : 0.0;
-      xJ[r][q] = gj < n ? x[(size_t)gj * 3 + q] : 0.0;
+    __syncthreads();   // the previous item's reads of xI / xJ / buf are done
+    for (int idx = tid; idx < CT * 3; idx += TT) {
+      const int gi = ti * CT + idx / 3, gj = tj * CT + idx / 3;
+      xI[idx] = gi < n ? x[(size_t)ti * CT * 3 + idx] : 0.0;
+      xJ[idx] = gj < n ? x[(size_t)tj * CT * 3 + idx] : 0.0;
     }
     __syncthreads();
-    const int r = tid / 3, q = tid % 3;
-    double rs = 0.0, cs = 0.0;
-#pragma unroll 8
-    for (int c = 0; c < CT; ++c) rs += Ts[r][c] * xJ[c][q];
-    if (!diag) {
-#pragma unroll 8
-      for (int c = 0; c < CT; ++c) cs += Ts[c][r] * xI[c][q];
-    } else {
-      for (int c = r + 1; c < CT; ++c) cs += Ts[c][r] * xI[c][q];
+    double rs[4][3], cs[4][3];
+#pragma unroll
+    for (int k = 0; k < 4; ++k)
+#pragma unroll
+      for (int q = 0; q < 3; ++q) rs[k][q] = cs[k][q] = 0.0;
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+      const int r = ty + 16 * i;
+      double xi[3];
+#pragma unroll
+      for (int q = 0; q < 3; ++q) xi[q] = xI[3 * r + q];
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        const int c = 2 * tx + 32 * (j >> 1) + (j & 1);
+        const double e = t[i][j];
+        const double ec = (!diag || c < r) ? e : 0.0;   // the diagonal counts once (row side)
+#pragma unroll
+        for (int q = 0; q < 3; ++q) {
+          rs[i][q] += e * xJ[3 * c + q];
+          cs[j][q] += ec * xi[q];
+        }
+      }
     }
     double* pr = a.partial + (size_t)f * a.nt * a.nt * CT * 3;
-    if (!diag) {
-      pr[((size_t)ti * a.nt + tj) * CT * 3 + tid] = rs;
-      pr[((size_t)tj * a.nt + ti) * CT * 3 + tid] = cs;
-    } else {
-      pr[((size_t)ti * a.nt + ti) * CT * 3 + tid] = rs + cs;
+    // row sums: the 16 column groups of each row
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+      for (int q = 0; q < 3; ++q) buf[tx * RP + 3 * (ty + 16 * i) + q] = rs[i][q];
+    __syncthreads();
+    double y = 0.0;
+    if (tid < CT * 3) {
+#pragma unroll
+      for (int k = 0; k < 16; ++k) y += buf[k * RP + tid];
+    }
+    __syncthreads();
+    // column sums: the 16 row groups of each column
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      const int c = 2 * tx + 32 * (j >> 1) + (j & 1);
+#pragma unroll
+      for (int q = 0; q < 3; ++q) buf[ty * RP + 3 * c + q] = cs[j][q];
+    }
+    __syncthreads();
+    if (tid < CT * 3) {
+      double z = 0.0;
+#pragma unroll
+      for (int k = 0; k < 16; ++k) z += buf[k * RP + tid];
+      if (!diag) {
+        pr[((size_t)ti * a.nt + tj) * CT * 3 + tid] = y;
+        pr[((size_t)tj * a.nt + ti) * CT * 3 + tid] = z;
+      } else {
+        pr[((size_t)ti * a.nt + ti) * CT * 3 + tid] = y + z;
+      }
     }
   }
 }
@@ -443,7 +498,7 @@ int cg_tile_grid() {
     int dev = 0, sms = 0, per_sm = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, cg_tile_kernel, 192, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, cg_tile_kernel, TT, 0);
     grid = (sms > 0 ? sms : 148) * (per_sm > 0 ? per_sm : 1);
   }
   return grid;
@@ -465,7 +520,7 @@ void launch_cg_setup(const CgArgs& a, cudaStream_t s) {
   const int tgrid = (int)std::min<long long>(cg_tile_grid(), items);
   cudaMemsetAsync(a.state, 0, sizeof(double) * kCgState * a.batch, s);
   cg_tile_inv_kernel<<<dim3(a.nt, a.batch), 256, 0, s>>>(a);
-  cg_tile_kernel<<<tgrid, 192, 0, s>>>(a, a.X);
+  cg_tile_kernel<<<tgrid, TT, 0, s>>>(a, a.X);
   cg_rows_kernel<<<dim3(a.nt, a.batch), 192, 0, s>>>(a, 1);
   cg_init_tiles_kernel<<<dim3(a.nt, a.batch), 192, 0, s>>>(a);
   cg_init_final_kernel<<<a.batch, 32, 0, s>>>(a, a.nt);
@@ -475,7 +530,7 @@ void launch_cg_iteration(const CgArgs& a, int it, cudaStream_t s) {
   const int nb = (a.N + AT - 1) / AT;
   const long long items = (long long)a.nt * (a.nt + 1) / 2 * a.batch;
   const int tgrid = (int)std::min<long long>(cg_tile_grid(), items);
-  cg_tile_kernel<<<tgrid, 192, 0, s>>>(a, a.P);
+  cg_tile_kernel<<<tgrid, TT, 0, s>>>(a, a.P);
   cg_rows_kernel<<<dim3(a.nt, a.batch), 192, 0, s>>>(a, 0);
   cg_update_kernel<<<dim3(a.nt, a.batch), 192, 0, s>>>(a, it);
   cg_dir_kernel<<<dim3(nb, a.batch), AT, 0, s>>>(a, it);

@@ -74,17 +74,23 @@ __device__ bool wait_progress(const int* p, int target, int* err) {
   int ok = 1;
   if ((threadIdx.x & 31) == 0) {
     // tight polling first (the predecessor is usually one task away), then
-    // exponential back-off so that far-behind warps do not load the L2
+    // exponential back-off so that far-behind warps do not load the L2; the
+    // error flag and the clock are read every 64 polls (an extra load per poll
+    // would sit behind the acquire and double the detection latency)
     const long long t0 = clock64();
-    unsigned ns = 0;
+    unsigned ns = 0, polls = 0;
     while (ld_acquire(p) < target) {
-      if (*(volatile int*)err != 0 || clock64() - t0 > kSpinCycles) {
-        atomicCAS(err, 0, MBD_ERR_TIMEOUT);
-        ok = 0;
-        break;
+      if ((++polls & 63u) == 0) {
+        if (*(volatile int*)err != 0 || clock64() - t0 > kSpinCycles) {
+          atomicCAS(err, 0, MBD_ERR_TIMEOUT);
+          ok = 0;
+          break;
+        }
       }
-      if (ns) __nanosleep(ns);
-      ns = ns == 0 ? 16 : (ns < 256 ? 2 * ns : 256);
+      if (polls > 256) {
+        __nanosleep(ns);
+        ns = min(2 * ns + 16, 256u);
+      }
     }
   }
   ok = __shfl_sync(0xffffffffu, ok, 0);
@@ -136,7 +142,7 @@ __global__ void __launch_bounds__(WARPS * 32) sb2st_kernel(const BandJob* jobs, 
       // together)
       if (owarp) {
         const bool ok = it.pred < 0 || wait_progress(progress + it.pred, min(k + 2, Kp), err);
-        if (l == 0) S.go = ok && *(volatile int*)err == 0;
+        if (l == 0) S.go = ok;
       }
       pair_sync(pair);
       if (!S.go) return;
@@ -244,13 +250,13 @@ __global__ void __launch_bounds__(WARPS * 32) sb2st_kernel(const BandJob* jobs, 
       }
       // both warps' stores are ordered before the barrier; one lane then
       // fences at GPU scope and publishes the task (the grid-barrier pattern)
+      // (the next task's first barrier orders S.w[1] before the D-warp reads it)
       pair_sync(pair);
       if (owarp && l == 0) {
         S.w[1] = tau;   // the next task's tau for the D-warp
         __threadfence();
         st_release(progress + t, k + 1);
       }
-      pair_sync(pair);
     }
   }
 }
