@@ -529,20 +529,14 @@ int prepare_batch(mbd_ctx* ctx, bool eigen) {
   ctx->order.clear();
   for (size_t g = 0; g < ctx->geoms.size(); ++g)
     if (ctx->geoms[g]->status_host == MBD_OK) ctx->order.push_back((int)g);
-  // Tridiagonalisation path, one for the whole batch (the one-stage grouped
-  // launch and the band -> tridiagonal launch would run one after the other).
-  // Measured on B200 (one-stage vs two-stage): one matrix n = 1500: 20 vs
-  // 36 ms, n = 3000: 52 vs 77 ms, n = 6000: 195 vs 187 ms; 256 matrices
-  // n <= 1800: 798 vs 733 ms per batch (the band -> tridiagonal launch serves
-  // every matrix at once).  So: two-stage for batches that hold a large
-  // matrix or many matrices.
-  {
-    int nmax = 0;
-    for (int g : ctx->order) nmax = std::max(nmax, ctx->geoms[g]->plan.nH);
-    const bool policy = (int)ctx->order.size() >= kTwoStageMinBatch || nmax >= kTwoStageMinN;
-    ctx->two_stage_batch = ctx->two_stage_force == 1 || (ctx->two_stage_force < 0 && policy);
-    ctx->two_stage_min_n = 1 << 30;
-  }
+  // Tridiagonalisation path.  Measured on B200 (mixed mode, one geometry,
+  // reduction + eigenvalues, one-stage vs two-stage): n = 300: 7.6 vs 3.7 ms,
+  // n = 1050: 15.0 vs 14.2, n = 1500: 22.4 vs 20.9, n = 3000: 54.8 vs 47.3;
+  // a batch of 8 geometries n = 270 .. 1800: step 50.3 vs 38.6 ms.  So every
+  // matrix the two-stage reduction can take goes through it; larger ones
+  // (n above the panel cluster's rows) take the one-stage grouped launch.
+  ctx->two_stage_batch = ctx->two_stage_force != 0;
+  ctx->two_stage_min_n = 1 << 30;
   std::stable_sort(ctx->order.begin(), ctx->order.end(),
                    [&](int a, int b) { return ctx->geoms[a]->plan.n > ctx->geoms[b]->plan.n; });
   for (int g : ctx->order) {
@@ -843,8 +837,8 @@ int mbd_rsscs_create(mbd_ctx** out, int device) {
   MBD_CUDA(init_mixed_attributes());
   MBD_CUDA(init_sy2sb_attributes());
   {
-    // reduction path per batch (prepare_batch): MBD_B200_TWO_STAGE=1 / 0
-    // forces the two-stage / one-stage path, otherwise a measured policy
+    // reduction path (prepare_batch): MBD_B200_TWO_STAGE=0 forces the
+    // one-stage path; otherwise two-stage wherever it applies
     const char* ts = std::getenv("MBD_B200_TWO_STAGE");
     ctx->two_stage_max_n = sy2sb_max_n();
     ctx->two_stage_force = (ts && ts[0] == '1') ? 1 : ((ts && ts[0] == '0') ? 0 : -1);

@@ -204,8 +204,6 @@ int band_to_tridiag_single(mbd_ctx* ctx, double* Br, int n, double* d, double* e
 int relay_learned(mbd_ctx* ctx, GeomDev* gd, RelaySlot& sl, size_t mstride, cudaEvent_t ev_net, double** X_out);
 
 // Matrices reduced by the two-stage path (the rest by the one-stage kernel).
-constexpr int kTwoStageMinN = 4500;      // a batch holding a matrix this large
-constexpr int kTwoStageMinBatch = 16;    // or this many geometries
 inline bool two_stage(const mbd_ctx* ctx, int n) {
   return (ctx->two_stage_batch || n >= ctx->two_stage_min_n) && n <= ctx->two_stage_max_n;
 }

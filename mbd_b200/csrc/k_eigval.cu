@@ -87,10 +87,10 @@ __device__ __forceinline__ void bisect_block(const double* d, const double* e, c
   const int q = gid % kLanesPerEig;
   const int lane = threadIdx.x % 32;
   const int base = lane & ~(kLanesPerEig - 1);
-  const unsigned gmask = 0xffu << base;
-  if (k >= n) return;   // whole 8-lane groups leave together
+  const unsigned gmask = ((1u << kLanesPerEig) - 1u) << base;
+  if (k >= n) return;   // whole lane groups leave together
   // invariant: count(lo) <= k < count(hi)
-  for (int it = 0; it < 40; ++it) {
+  for (int it = 0; it < 64; ++it) {
     const double wdt = hi - lo;
     if (wdt <= 2.0 * 1.1102230246251565e-16 * fmax(fabs(lo), fabs(hi))) break;
     const double x = lo + wdt * (double)(q + 1) / (double)(kLanesPerEig + 1);

@@ -1,10 +1,12 @@
 """GPU parity of batched runs: many geometries of uneven size in one call.
 
 A batch runs the relay stages of its geometries concurrently on several
-streams and reduces all CFDM Hamiltonians in one grouped launch, so these
-tests cover the group planning (one matrix per CTA group, several matrices
-per group when geometries outnumber CTAs, groups of different widths) and the
-batched eigenvalue / energy launches against the FP64 oracle.
+streams and reduces all CFDM Hamiltonians together (the two-stage path: one
+bulge-chasing launch for every band; the one-stage path: one grouped launch),
+so these tests cover the batch planning (one matrix per CTA group, several
+matrices per group when geometries outnumber CTAs, groups of different
+widths) and the batched eigenvalue / energy launches against the FP64
+oracle.
 """
 import numpy as np
 import pytest
@@ -125,3 +127,23 @@ def test_graph_replay_matches_direct_launches(engine, mode, monkeypatch):
         for a, b in zip(res, ref):
             assert a.energy == b.energy
             np.testing.assert_array_equal(a.alpha_iw, b.alpha_iw)
+
+
+@pytest.mark.parametrize("sizes", [(25, 140, 60, 300, 12), tuple(range(20, 20 + 7 * 40, 7))])
+def test_one_stage_reduction_matches_two_stage(engine, sizes, monkeypatch):
+    """The grouped one-stage tridiagonalisation (MBD_B200_TWO_STAGE=0; the
+    default takes it only for matrices above the two-stage limit) against the
+    default two-stage path on the same batches: CTA groups of different
+    widths, several matrices per group when geometries outnumber CTAs."""
+    from mbd_b200 import Engine
+    from mbd_b200 import synthetic as sy
+    items = [sy.cluster(n, seed=70 + k) for k, n in enumerate(sizes)]
+    geos, sets = [g for g, _ in items], [s for _, s in items]
+    two = engine.energy_batch(geos, sets, "plain")
+    monkeypatch.setenv("MBD_B200_TWO_STAGE", "0")
+    with Engine(0) as one_stage:
+        one = one_stage.energy_batch(geos, sets, "plain")
+    for a, b in zip(one, two):
+        assert a.status == 0 and b.status == 0
+        assert abs(a.energy - b.energy) <= PLAIN_E_TOL, (a.energy, b.energy)
+        assert a.nimag == b.nimag
