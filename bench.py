@@ -39,7 +39,7 @@ METRIC = "MBD energies/s, mixed+batched+learned vs plain FP64 on 1 B200, |dE|<=1
 SIZES = (500, 1000, 2000)
 BOX_SIZES = (2000, 4000, 6000)
 FP64_NOMINAL_TFLOPS = 148 * 64 * 2 * 1.965e9 / 1e12   # 148 SMs x 64 DFMA/clk x 2 x 1965 MHz
-TWO_STAGE_MAX_N = 768 * 16 + 32   # largest Hamiltonian the two-stage reduction takes (panel rows x cluster CTAs + a panel)
+TWO_STAGE_MAX_N = 1152 * 16 + 32   # largest Hamiltonian the two-stage reduction takes (panel rows x cluster CTAs + a panel)
 
 
 WORKLOADS = {
@@ -292,8 +292,13 @@ def roofline(stage_ms, sizes, mode):
                 "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak, "traffic": None,
                 "peak_source": f"{src} bf16 cuBLAS / 2 (dense TF32 rate)",
                 "algorithmic": "3 x 21*(3N)^3/3 TF32 flop per energy", "stage_ms": stages}
+    note = None
+    if dom == "relay_solve" and mode == "mixed_learned":
+        note = ("block-CG over the slots' overlapping streams (the stage time is summed over geometries); no "
+                "per-launch timing of its matrix pass cg_tile_kernel here -- ncu: 4.72 TB/s, 72 % of the measured "
+                "copy bandwidth (profiles/cg_tile_kernel_n3000.md)")
     return {"bound": "hbm", "kernel": dom, "achieved": None, "peak": peaks.get("hbm_gbs"), "unit": "GB/s",
-            "frac": None, "traffic": None, "peak_source": src, "stage_ms": stages}
+            "frac": None, "traffic": None, "peak_source": src, "note": note, "stage_ms": stages}
 
 
 def main():

@@ -22,6 +22,7 @@
 #include <cooperative_groups.h>
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cstdlib>
 
 #include "kernels.h"
@@ -291,8 +292,15 @@ __global__ void __launch_bounds__(NW * 32) qr_panel_kernel(PanelArgs a) {
 // (no downdate).  For 48 rows per warp it measured faster than the one-barrier
 // form (196 against 220 us for an m = 5296 panel): the extra sums of the
 // downdate cost more than the barrier they save once the rows per warp grow.
-template <int NW, int RPW>
+// HYB: local rows beyond NW x RPW (up to kPanelMaxRowsPerCta) live in dynamic
+// shared memory, Ps[i][c] for local row NW * RPW + i (row i belongs to warp
+// i % NW as in the registers); they lie below row 383 of the panel, so they
+// never meet the diagonal rows j, j + 1 < 32 and need no masks.
+template <int NW, int RPW, bool HYB>
 __global__ void __launch_bounds__(NW * 32) qr_panel2_kernel(PanelArgs a) {
+  extern __shared__ __align__(16) double Ps[];   // HYB: [R - NW * RPW][QR_LD2]
+  constexpr int QR_LD2 = B + 1;
+  constexpr int RREG = NW * RPW;
   constexpr int NT = NW * 32;
   constexpr unsigned FULL = 0xffffffffu;
   __shared__ double pubN[2][NW];
@@ -317,6 +325,9 @@ __global__ void __launch_bounds__(NW * 32) qr_panel2_kernel(PanelArgs a) {
     const int r = warp + NW * t;
     x[t] = (r < nr) ? a.A[(size_t)(a.row0 + lo + r) * a.ld + a.col0 + lane] : 0.0;
   }
+  if (HYB)
+    for (int i = warp; RREG + i < nr; i += NW)
+      Ps[i * QR_LD2 + lane] = a.A[(size_t)(a.row0 + lo + RREG + i) * a.ld + a.col0 + lane];
   if (rank == 0)
     for (int e = tid; e < B * (B + 1); e += NT) (&Tm[0][0])[e] = 0.0;
   const int nref = min(B, m);
@@ -330,6 +341,11 @@ __global__ void __launch_bounds__(NW * 32) qr_panel2_kernel(PanelArgs a) {
       if (t & 1) s1 += v * v;
       else s0 += v * v;
     }
+    if (HYB)
+      for (int i = warp; RREG + i < nr; i += NW) {
+        const double v = Ps[i * QR_LD2 + lane];
+        s0 += v * v;
+      }
     s_own = s0 + s1;
   }
   for (int j = 0; j < nref; ++j) {
@@ -388,6 +404,8 @@ __global__ void __launch_bounds__(NW * 32) qr_panel2_kernel(PanelArgs a) {
       if (t & 1) d1 += vs[warp][t] * x[t];
       else d0 += vs[warp][t] * x[t];
     }
+    if (HYB)
+      for (int i = warp; RREG + i < nr; i += NW) d0 += (Ps[i * QR_LD2 + j] * scale) * Ps[i * QR_LD2 + lane];
     dw[warp][lane] = d0 + d1;
     __syncthreads();
     if (warp == 0) {
@@ -423,6 +441,18 @@ __global__ void __launch_bounds__(NW * 32) qr_panel2_kernel(PanelArgs a) {
         else s0 += v * v;
       }
     }
+    if (HYB) {
+      // lane j's column is read by every lane here and scaled to v after
+      for (int i = warp; RREG + i < nr; i += NW) {
+        double* pr = Ps + i * QR_LD2;
+        const double y = pr[lane] - (pr[j] * scale) * tdc;
+        if (lane > j) pr[lane] = y;
+        s0 += y * y;
+      }
+      __syncwarp();
+      if (lane == j)
+        for (int i = warp; RREG + i < nr; i += NW) Ps[i * QR_LD2 + j] *= scale;
+    }
     s_own = s0 + s1;
     if (lane == j) {
 #pragma unroll
@@ -455,6 +485,8 @@ __global__ void __launch_bounds__(NW * 32) qr_panel2_kernel(PanelArgs a) {
       a.V[(size_t)g * B + lane] = g > lane ? x[t] : (g == lane ? 1.0 : 0.0);
     }
   }
+  if (HYB)   // rows below 383: V only
+    for (int i = warp; RREG + i < nr; i += NW) a.V[(size_t)(lo + RREG + i) * B + lane] = Ps[i * QR_LD2 + lane];
   if (rank == 0) {
     __syncthreads();
     for (int e = tid; e < B * B; e += NT) a.T[e] = Tm[e / B][e % B];
@@ -462,190 +494,12 @@ __global__ void __launch_bounds__(NW * 32) qr_panel2_kernel(PanelArgs a) {
   cl.sync();   // no CTA leaves while another may still read its shared memory
 }
 
-constexpr int QR_THREADS = 256;
-constexpr int QR_LD = B + 1;        // shared-memory row stride of the panel (doubles)
-// Panels of more than 384 rows per CTA (m > 16 x 384) keep the panel in
-// shared memory instead (the register kernel would spill).
-// Shared layout of qr_panel_smem: P[R][QR_LD] | pubN[2][8] norm partials per warp
-// | pubA[2] alpha | pubD[2][B] dot sums | dw[8][B] per-warp dots | gram[B][B]
-// | G[B][B] | Tm[B][B].  pub* are read by the other CTAs of the cluster
-// (double-buffered by column parity).  Warp w owns the local rows r = w mod 8,
-// lane c column c: a warp's update of its rows and the next column's norm over
-// the same rows need no CTA barrier; per column there is one __syncthreads and
-// two cluster barriers.
-constexpr int QR_WARPS = QR_THREADS / 32;
-__host__ __device__ constexpr size_t qr_panel_doubles(int R) {
-  return (size_t)R * QR_LD + 2 * QR_WARPS + 2 + 2 * B + QR_WARPS * B + 3 * B * B + 8;
-}
-
-__global__ void __launch_bounds__(QR_THREADS) qr_panel_smem_kernel(PanelArgs a) {
-  extern __shared__ double sm[];
-  cg::cluster_group cl = cg::this_cluster();
-  const int rank = (int)cl.block_rank();
-  const int C = (int)cl.num_blocks();
-  const int m = a.m;
-  const int R = a.rows_per_cta;
-  const int lo = rank * R, hi = min(m, lo + R);
-  const int nr = max(0, hi - lo);
-  double* P = sm;
-  double* pubN = P + (size_t)R * QR_LD;      // [2][QR_WARPS]
-  double* pubA = pubN + 2 * QR_WARPS;        // [2]
-  double* pubD = pubA + 2;                   // [2][B]
-  double* dw = pubD + 2 * B;                 // [QR_WARPS][B]
-  double* gram = dw + QR_WARPS * B;          // [B][B]
-  double* G = gram + B * B;
-  double* Tm = G + B * B;
-  const int tid = threadIdx.x, warp = tid / 32, lane = tid % 32;
-  for (int idx = tid; idx < nr * B; idx += QR_THREADS) {
-    const int r = idx / B, c = idx % B;
-    P[r * QR_LD + c] = a.A[(size_t)(a.row0 + lo + r) * a.ld + a.col0 + c];
-  }
-  __syncthreads();
-  const int nref = min(B, m);
-  // norm partial of column j over this warp's rows below row j (lanes split the rows)
-  auto norm_part = [&](int j) {
-    double s = 0.0;
-    for (int r = warp + QR_WARPS * lane; r < nr; r += QR_THREADS) {
-      if (lo + r > j) {
-        const double x = P[r * QR_LD + j];
-        s += x * x;
-      }
-    }
-    return warp_sum(s);
-  };
-  double s_next = norm_part(0);
-  for (int j = 0; j < nref; ++j) {
-    const int par = j & 1;
-    // publish the norm partials and (owner CTA) alpha = P[j][j]
-    // (row j belongs to CTA j / R, warp (j - lo) % 8, which also updated it)
-    if (lane == 0) pubN[par * QR_WARPS + warp] = s_next;
-    if (lane == 0 && j >= lo && j < hi && (j - lo) % QR_WARPS == warp) pubA[par] = P[(j - lo) * QR_LD + j];
-    cl.sync();
-    // all remote loads first (independent), then the sums
-    double xparts[kPanelMaxCluster * QR_WARPS / 32];
-#pragma unroll
-    for (int u = 0; u < kPanelMaxCluster * QR_WARPS / 32; ++u) {
-      const int q = lane + 32 * u;
-      xparts[u] = (q < C * QR_WARPS) ? cl.map_shared_rank(pubN, q / QR_WARPS)[par * QR_WARPS + q % QR_WARPS] : 0.0;
-    }
-    double xn2 = 0.0;
-#pragma unroll
-    for (int u = 0; u < kPanelMaxCluster * QR_WARPS / 32; ++u) xn2 += xparts[u];
-    xn2 = warp_sum(xn2);
-    double alpha = 0.0;
-    if (lane == 0) alpha = cl.map_shared_rank(pubA, j / R)[par];
-    alpha = __shfl_sync(0xffffffffu, alpha, 0);
-    double tau = 0.0, scale = 0.0, beta = alpha;
-    if (xn2 > 0.0) {
-      beta = -copysign(sqrt(alpha * alpha + xn2), alpha);
-      tau = (beta - alpha) / beta;
-      scale = 1.0 / (alpha - beta);
-    }
-    if (rank == 0 && tid == 0) a.tau[j] = tau;
-    // dots d_c = v^T P[:, c] over this warp's rows (lane c), v_j = 1
-    double d = 0.0;
-    if (tau != 0.0) {
-      double d1 = 0.0;   // two accumulation chains
-      int r = warp;
-      for (; r + QR_WARPS < nr; r += 2 * QR_WARPS) {
-        const int g0 = lo + r, g1 = g0 + QR_WARPS;
-        const double v0 = g0 < j ? 0.0 : (g0 == j ? 1.0 : P[r * QR_LD + j] * scale);
-        const double v1 = g1 < j ? 0.0 : (g1 == j ? 1.0 : P[(r + QR_WARPS) * QR_LD + j] * scale);
-        d += v0 * P[r * QR_LD + lane];
-        d1 += v1 * P[(r + QR_WARPS) * QR_LD + lane];
-      }
-      if (r < nr) {
-        const int g0 = lo + r;
-        const double v0 = g0 < j ? 0.0 : (g0 == j ? 1.0 : P[r * QR_LD + j] * scale);
-        d += v0 * P[r * QR_LD + lane];
-      }
-      d += d1;
-    }
-    dw[warp * B + lane] = d;
-    __syncthreads();
-    if (warp == 0) {
-      double t = 0.0;
-#pragma unroll
-      for (int q = 0; q < QR_WARPS; ++q) t += dw[q * B + lane];
-      pubD[par * B + lane] = t;
-    }
-    cl.sync();
-    double dparts[kPanelMaxCluster];
-#pragma unroll
-    for (int q = 0; q < kPanelMaxCluster; ++q) dparts[q] = (q < C) ? cl.map_shared_rank(pubD, q)[par * B + lane] : 0.0;
-    double dc = 0.0;
-#pragma unroll
-    for (int q = 0; q < kPanelMaxCluster; ++q) dc += dparts[q];
-    // update the remaining columns of this warp's rows, then store v in column j
-    if (tau != 0.0) {
-      for (int r = warp; r < nr; r += QR_WARPS) {
-        const int gr = lo + r;
-        if (gr < j) continue;
-        const double v = (gr == j) ? 1.0 : P[r * QR_LD + j] * scale;
-        if (lane > j) P[r * QR_LD + lane] -= tau * v * dc;
-      }
-      __syncwarp();
-      for (int r = warp + QR_WARPS * lane; r < nr; r += QR_THREADS)
-        if (lo + r > j) P[r * QR_LD + j] *= scale;
-    }
-    if (j >= lo && j < hi && (j - lo) % QR_WARPS == warp && lane == 0) P[(j - lo) * QR_LD + j] = beta;
-    __syncwarp();
-    if (j + 1 < nref) s_next = norm_part(j + 1);
-  }
-  __syncthreads();
-  // ---- Gram matrix G = V^T V (V unit lower trapezoidal), summed over the cluster
-  for (int e = tid; e < B * B; e += QR_THREADS) {
-    const int p = e / B, q = e % B;
-    double g = 0.0;
-    for (int r = 0; r < nr; ++r) {
-      const int gr = lo + r;
-      const double vp = gr > p ? P[r * QR_LD + p] : (gr == p ? 1.0 : 0.0);
-      const double vq = gr > q ? P[r * QR_LD + q] : (gr == q ? 1.0 : 0.0);
-      g += vp * vq;
-    }
-    gram[e] = g;
-  }
-  // write R (upper part, the band) and V (explicit) back
-  for (int idx = tid; idx < nr * B; idx += QR_THREADS) {
-    const int r = idx / B, c = idx % B;
-    const int gr = lo + r;
-    const double x = P[r * QR_LD + c];
-    if (gr <= c) a.A[(size_t)(a.row0 + gr) * a.ld + a.col0 + c] = x;
-    a.V[(size_t)gr * B + c] = gr > c ? x : (gr == c ? 1.0 : 0.0);
-  }
-  cl.sync();
-  if (rank == 0) {
-    // T (upper triangular): T[j][j] = tau_j, T[0:j, j] = -tau_j T[0:j, 0:j] G[0:j, j]
-    for (int e = tid; e < B * B; e += QR_THREADS) {
-      double g = 0.0;
-      for (int q = 0; q < C; ++q) g += cl.map_shared_rank(gram, q)[e];
-      G[e] = g;
-      Tm[e] = 0.0;
-    }
-    __syncthreads();
-    if (tid < 32) {
-      for (int j = 0; j < B; ++j) {
-        const double tj = (j < nref) ? a.tau[j] : 0.0;
-        double t = 0.0;
-        if (tid < j)
-          for (int l = tid; l < j; ++l) t += Tm[tid * B + l] * G[l * B + j];
-        __syncwarp();
-        if (tid < j) Tm[tid * B + j] = -tj * t;
-        if (tid == j) Tm[j * B + j] = tj;
-        __syncwarp();
-      }
-    }
-    __syncthreads();
-    for (int e = tid; e < B * B; e += QR_THREADS) a.T[e] = Tm[e];
-  }
-  cl.sync();   // no CTA leaves while another may still read its shared memory
-}
-
-// Variants by rows per CTA: (warps, rows per warp); the last one is the
-// shared-memory kernel.
+// Variants by rows per CTA: (warps, rows per warp); the last one keeps 384
+// rows in registers and the rest in shared memory.
 constexpr int kQrVariants = 4;
-constexpr int kQrWarps[kQrVariants] = {8, 8, 8, QR_THREADS / 32};
-constexpr int kQrRows[kQrVariants] = {12, 24, 48, kPanelMaxRowsPerCta / (QR_THREADS / 32)};
+constexpr int kQrWarps[kQrVariants] = {8, 8, 8, 8};
+constexpr int kQrRows[kQrVariants] = {12, 24, 48, kPanelMaxRowsPerCta / 8};
+constexpr int kQrRegRows = 8 * 48;
 int qr_variant(int R) {
   for (int v = 0; v < kQrVariants; ++v)
     if (R <= kQrWarps[v] * kQrRows[v]) return v;
@@ -656,11 +510,14 @@ QrKernel qr_kernel(int v) {
   switch (v) {
     case 0: return qr_panel_kernel<8, 12>;
     case 1: return qr_panel_kernel<8, 24>;
-    case 2: return qr_panel2_kernel<8, 48>;
-    default: return qr_panel_smem_kernel;
+    case 2: return qr_panel2_kernel<8, 48, false>;
+    default: return qr_panel2_kernel<8, 48, true>;
   }
 }
-size_t qr_smem_bytes(int v) { return v == kQrVariants - 1 ? sizeof(double) * qr_panel_doubles(kPanelMaxRowsPerCta) : 0; }
+// dynamic shared memory of variant v for R rows per CTA
+size_t qr_smem_bytes(int v, int R) {
+  return v == kQrVariants - 1 ? sizeof(double) * (B + 1) * (size_t)std::max(0, R - kQrRegRows) : 0;
+}
 
 // FP64 tensor-core MMA, D = A B + D with A 8x4 (row), B 4x8 (col), D 8x8:
 // a = A[lane/4][lane%4], b = B[lane%4][lane/4], d = D[lane/4][2*(lane%4) + {0,1}].
@@ -951,8 +808,9 @@ cudaError_t init_sy2sb_attributes() {
   for (int v = 0; v < kQrVariants; ++v) {
     cudaError_t e = cudaFuncSetAttribute(qr_kernel(v), cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
     if (e != cudaSuccess) return e;
-    if (qr_smem_bytes(v) > 0) {
-      e = cudaFuncSetAttribute(qr_kernel(v), cudaFuncAttributeMaxDynamicSharedMemorySize, (int)qr_smem_bytes(v));
+    if (qr_smem_bytes(v, kPanelMaxRowsPerCta) > 0) {
+      e = cudaFuncSetAttribute(qr_kernel(v), cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               (int)qr_smem_bytes(v, kPanelMaxRowsPerCta));
       if (e != cudaSuccess) return e;
     }
   }
@@ -970,7 +828,7 @@ int probe_max_cluster() {
       cudaLaunchConfig_t cfg{};
       cfg.gridDim = dim3(C);
       cfg.blockDim = dim3(kQrWarps[v] * 32);
-      cfg.dynamicSmemBytes = qr_smem_bytes(v);
+      cfg.dynamicSmemBytes = qr_smem_bytes(v, kPanelMaxRowsPerCta);
       cudaLaunchAttribute attr[1];
       attr[0].id = cudaLaunchAttributeClusterDimension;
       attr[0].val.clusterDim.x = C;
@@ -1039,7 +897,7 @@ cudaError_t launch_sy2sb(double* A, int ld, int n, double* ws, double* Br, int n
     cudaLaunchConfig_t cfg{};
     cfg.gridDim = dim3(C);
     cfg.blockDim = dim3(kQrWarps[qv] * 32);
-    cfg.dynamicSmemBytes = qv == kQrVariants - 1 ? sizeof(double) * qr_panel_doubles(R) : 0;
+    cfg.dynamicSmemBytes = qr_smem_bytes(qv, R);
     cfg.stream = s;
     cudaLaunchAttribute attr[1];
     attr[0].id = cudaLaunchAttributeClusterDimension;

@@ -170,12 +170,13 @@ def _known_spectrum(n, seed):
     return H, np.sort(lam)
 
 
-@pytest.mark.parametrize("n", [12000, 13000, 18000])
+@pytest.mark.parametrize("n", [12000, 13000, 18000, 19000])
 def test_eigvalsh_known_spectrum_large(engine, n):
     """Matrices of the size of a 4000- and 6000-atom box's Hamiltonian
-    (n = 3N): 12000 takes the two-stage reduction at its largest panel,
-    13000 and 18000 the one-stage reduction and the bisection that reads
-    d and e^2 from global memory."""
+    (n = 3N) and beyond: up to 18464 the two-stage reduction (12000 with
+    panels of up to 384 rows per CTA in registers, 13000 and 18000 with the
+    rows beyond 384 in shared memory), 19000 the one-stage reduction; above
+    12800 the bisection reads d and e^2 from global memory."""
     H, lam = _known_spectrum(n, seed=n)
     w = engine.eigvalsh(H)
     np.testing.assert_allclose(w, lam, rtol=0, atol=1e-12 * 4.0 * n)
