@@ -2,19 +2,25 @@
 """MBD energies/s on one B200 (replicas on N GPUs).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--mode MODE]
+                    [--workload clusters|batched|boxes]
 
-Workload (one step): the MBD@rsSCS energy of three isolated {H,C,N,O}
-clusters of N = 500, 1000 and 2000 atoms (seeded random sequential packing at
-0.1 atoms/A^3, Hirshfeld ratios U(0.6,1.0); synthetic stand-ins, no dataset),
-each with all 21 imaginary frequencies.  Working set per step: 0.38 / 1.5 /
-6.1 GB of relay matrices, far larger than the 126 MB L2, so no L2 flush is
-inserted between steps.
+Workload (one step, default): the MBD@rsSCS energy of three isolated
+{H,C,N,O} clusters of N = 500, 1000 and 2000 atoms (seeded random sequential
+packing at 0.1 atoms/A^3, Hirshfeld ratios U(0.6,1.0); synthetic stand-ins,
+no dataset), each with all 21 imaginary frequencies.  Working set per step:
+0.38 / 1.5 / 6.1 GB of relay matrices, far larger than the 126 MB L2, so no
+L2 flush is inserted between steps.  --workload batched: 256 clusters of
+N ~ U{20..600} in one batch; --workload boxes: periodic boxes of 2000, 4000
+and 6000 atoms.
 
-value : energies/s of the headline mode (mixed: 3xTF32 tensor-core relay
-        factorisation + FP64 refinement, FP64 eigensolve) with inputs resident
-        in HBM (mbd_rsscs_compute only), device-timed with CUDA events on the
-        library's stream, max over ranks.
-plain_fp64 : the same workload in the plain FP64 mode, timed the same way.
+value : energies/s of the headline mode (mixed_learned: block-CG relay solve
+        started from the network's prediction, preconditioned by 64-row tile
+        inverses, FP64 eigensolve; the network is trained before timing) with
+        inputs resident in HBM (mbd_rsscs_compute only), device-timed with
+        CUDA events on the library's stream, max over ranks.
+plain_fp64 : the same workload in the plain FP64 mode, timed the same way;
+mixed_direct / learned_no_network : the 3xTF32 direct relay solve and the
+        block-CG without the network, timed the same way.
 e2e   : the headline mode through mbd_rsscs_energy_batch with host buffers
         (upload + compute + download every step), wall clock.
 Multi-GPU: replicas only (each rank runs the whole workload on its GPU;
@@ -191,6 +197,24 @@ def run_reference(args, rank, world):
             "e2e": {"value": value, "unit": "energies/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
     return 0
+
+
+def max_over_ranks_of(x, dist, device):
+    """The largest x over the ranks of the process group (x itself without
+    one): every replica times its own copy of the workload, the job takes as
+    long as the slowest."""
+    if not dist:
+        return x
+    import torch
+    t = torch.tensor([float(x)], device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def replica_rate(world, energies_per_step, steps, ms):
+    """Whole-job energies/s of `world` replicas that each compute
+    energies_per_step energies per step, `steps` steps in `ms` (max over ranks)."""
+    return world * energies_per_step * steps / (ms / 1000.0)
 
 
 def time_mode(eng, stream, mode, steps, warmup, clocks=None):
@@ -370,11 +394,7 @@ def main():
         raise SystemExit(f"upload failed: {code}")
 
     def max_over_ranks(x):
-        if not dist:
-            return x
-        t = torch.tensor([x], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+        return max_over_ranks_of(x, dist, "cuda")
 
     plain = None
     extra = {}
@@ -389,7 +409,7 @@ def main():
             xms, _, xres, xstage = time_mode(eng, stream, mode, args.steps, warmup)
             eng.use_network(True)
             xms = max_over_ranks(xms)
-            extra[name] = {"value": world * len(geos) * args.steps / (xms / 1000.0), "ms_per_step": xms / args.steps,
+            extra[name] = {"value": replica_rate(world, len(geos), args.steps, xms), "ms_per_step": xms / args.steps,
                            "stage_ms": dict(xstage), "refine_iters": [r.refine_iters for r in xres][:8]}
     if args.mode != "plain" and not args.no_plain:
         if dist:
@@ -397,14 +417,14 @@ def main():
         pms, _, pres, pstage = time_mode(eng, stream, "plain", args.steps, warmup)
         plain_res = pres
         pms = max_over_ranks(pms)
-        plain = {"value": world * len(geos) * args.steps / (pms / 1000.0), "ms_per_step": pms / args.steps,
+        plain = {"value": replica_rate(world, len(geos), args.steps, pms), "ms_per_step": pms / args.steps,
                  "energies": [r.energy for r in pres][:8], "stage_ms": {k: v for k, v in pstage.items()}}
     if dist:
         dist.barrier()
     clk = ClockSampler(local)
     ms, stats, res, stage = time_mode(eng, stream, args.mode, args.steps, warmup, clocks=clk)
     ms = max_over_ranks(ms)
-    value = world * len(geos) * args.steps / (ms / 1000.0)
+    value = replica_rate(world, len(geos), args.steps, ms)
 
     line = {"metric": METRIC, "value": value, "unit": "energies/s", "n_gpus": world, "steps": args.steps,
             "warmup": warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
@@ -444,7 +464,7 @@ def main():
             rr = eng.energy_batch(gl, sl, args.mode)
         t_e2e = max_over_ranks(time.perf_counter() - t0)
         st2 = eng.stats()
-        line["e2e"] = {"value": world * len(geos) * args.steps / t_e2e, "unit": "energies/s",
+        line["e2e"] = {"value": replica_rate(world, len(geos), args.steps, 1000.0 * t_e2e), "unit": "energies/s",
                        "h2d_bytes_per_step": st2["h2d_bytes"], "d2h_bytes_per_step": st2["d2h_bytes"],
                        "status": [r.status for r in rr]}
     if WORKLOAD == "boxes":
