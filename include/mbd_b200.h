@@ -46,8 +46,9 @@ enum {
     MBD_MODE_PLAIN_FP64 = 0,      /* FP64 tensor build, FP64 Cholesky, FP64 eigensolve */
     MBD_MODE_MIXED = 1,           /* FP32 relay copy factorised on tcgen05 tensor cores
                                      (3xTF32), FP64 iterative refinement to 1e-10 */
-    MBD_MODE_MIXED_LEARNED = 2    /* relay solved by block-CG (block-Jacobi preconditioned,
-                                     FP64) started from a message-passing network's
+    MBD_MODE_MIXED_LEARNED = 2    /* relay solved by block-CG (FP64, preconditioned by the
+                                     inverses of the 64x64 diagonal tiles of the relay
+                                     matrix) started from a message-passing network's
                                      prediction of every atom's screened-polarizability
                                      block; direct FP64 fallback on a residual miss */
 };
