@@ -178,7 +178,8 @@ int mbd_rsscs_last_timings(mbd_ctx* ctx, double* ms, int n);
  * the last compute replayed the batch's captured CUDA graph, 0 when it
  * launched the kernels one by one (the first compute of an uploaded batch in
  * a mode launches directly; the second captures the graph and replays it
- * from then on).  n must be >= 3. */
+ * from then on; a change of network or of device buffers starts over).
+ * n must be >= 3. */
 int mbd_rsscs_last_stats(mbd_ctx* ctx, double* out, int n);
 
 /* The CUDA stream (cudaStream_t) every kernel of this context runs on, so a

@@ -329,6 +329,10 @@ void drop_graphs(mbd_ctx* ctx) {
       cudaGraphExecDestroy(g);
       g = nullptr;
     }
+  // the next compute of each mode launches directly again (and reads back
+  // the CG iterations), the one after it captures
+  for (auto& gd : ctx->geoms) gd->cg_iters_seen = 0;
+  for (int& k : ctx->mode_runs) k = 0;
 }
 
 int band_to_tridiag_single(mbd_ctx* ctx, double* Br, int n, double* d, double* e, DevBuf& scratch, cudaStream_t s) {
@@ -525,7 +529,6 @@ int plan_slots(mbd_ctx* ctx) {
 // the device job tables of the uploaded batch.
 int prepare_batch(mbd_ctx* ctx, bool eigen) {
   drop_graphs(ctx);
-  for (int& k : ctx->mode_runs) k = 0;
   ctx->order.clear();
   for (size_t g = 0; g < ctx->geoms.size(); ++g)
     if (ctx->geoms[g]->status_host == MBD_OK) ctx->order.push_back((int)g);
@@ -998,6 +1001,7 @@ int mbd_rsscs_download(mbd_ctx* ctx, mbd_result* out) {
         double most = 0.0;
         for (int f = 0; f < kNFreq; ++f) most = std::max(most, cs[(size_t)f * kCgState + 1]);
         r.refine_iters = (int)most;
+        gd->cg_iters_seen = (worst <= kResidualGate) ? (int)most : 0;
       }
       if (!(worst <= kResidualGate)) {
         int st = run_front(ctx, gd, (int)g, MBD_MODE_PLAIN_FP64);

@@ -62,6 +62,12 @@ struct GeomDev {
   // learned warm start: neighbour graph (built on first use), training data
   DevBuf graph;      // off, nbr, src, species (int); dvec, efeat, eproj (float)
   int n_edges = -1;  // -1 until the graph is built
+  // Block-CG iterations (max over frequencies) of this geometry's last
+  // MIXED_LEARNED compute, as read back by download; 0: unknown.  A captured
+  // graph runs this many iterations plus a margin instead of the full
+  // schedule (the same inputs and network converge identically; a miss
+  // would still be caught by the residual gate).  Forgotten with the graphs.
+  int cg_iters_seen = 0;
   GnnGraph gnn{};    // device views into `graph` (x set per use)
   DevBuf train;      // x [21N][8] and S_true [21N][9] of a training batch
 };

@@ -22,6 +22,7 @@ namespace mbd {
 namespace {
 
 constexpr int kCgMaxIters = 64;
+constexpr int kCgSlack = 4;       // iterations a captured graph adds to the count last seen
 constexpr double kCgTol = 3e-11;   // relative residual the iteration stops at (gate: 1e-10)
 
 // Neighbour lists within the network's cut-off, including periodic images
@@ -298,8 +299,12 @@ int relay_learned(mbd_ctx* ctx, GeomDev* gd, RelaySlot& sl, size_t mstride, cuda
   record_timing(ctx, ev_net, s);
   launch_cg_setup(a, s);
   ctx->launches += 5;
-  for (int it = 0; it < kCgMaxIters; ++it) launch_cg_iteration(a, it, s);
-  ctx->launches += 4 * kCgMaxIters;
+  // the full schedule, or in a captured graph the iterations this geometry
+  // took on its last compute plus a margin
+  const int iters = (ctx->capturing && gd->cg_iters_seen > 0) ? std::min(kCgMaxIters, gd->cg_iters_seen + kCgSlack)
+                                                               : kCgMaxIters;
+  for (int it = 0; it < iters; ++it) launch_cg_iteration(a, it, s);
+  ctx->launches += 4 * iters;
   // the gate's residual, recomputed from X: R = B - A X
   launch_relay_residual(sl.relay64.as<double>(), mstride, p.ld, n, kNFreq, a.X, nullptr, a.R, ys,
                         sl.res_ws.as<double>(), gd->rnorm2, s);

@@ -103,25 +103,34 @@ def test_batched_workload_mixed_vs_plain(engine):
         _assert_close(mixed[k], ref, "mixed")
 
 
-@pytest.mark.parametrize("mode", ["plain", "mixed"])
+@pytest.mark.parametrize("mode", ["plain", "mixed", "mixed_learned"])
 def test_graph_replay_matches_direct_launches(engine, mode, monkeypatch):
     """compute() launches a new batch directly, captures it into a CUDA graph
     on its second call and replays it afterwards; every run equals a context
-    that always launches directly."""
+    that always launches directly.  In the learned mode (block-CG from zero
+    here, no network) the graph runs the CG iterations the first compute
+    took plus a margin instead of the full schedule."""
     from mbd_b200 import Engine
     from mbd_b200 import synthetic as sy
     items = [sy.cluster(n, seed=40 + n) for n in (25, 140, 60)]
     geos, sets = [g for g, _ in items], [s for _, s in items]
+    engine.use_network(False)
     assert engine.upload(geos, sets) == 0
-    runs = []
+    runs, launches = [], []
     for k in range(3):   # direct launches, capture + replay, replay
         assert engine.compute(mode) == 0
-        assert engine.stats()["graph_replayed"] == (k > 0)
+        st = engine.stats()
+        assert st["graph_replayed"] == (k > 0)
+        launches.append(st["launches"])
         code, res = engine.download()
         assert code == 0
         runs.append(res)
+    if mode == "mixed_learned":
+        assert launches[1] < launches[0]   # the trimmed CG schedule
+        assert [r.refine_iters for r in runs[1]] == [r.refine_iters for r in runs[0]]
     monkeypatch.setenv("MBD_B200_NO_GRAPHS", "1")
     with Engine(0) as direct:
+        direct.use_network(False)
         ref = direct.energy_batch(geos, sets, mode)
     for res in runs:
         for a, b in zip(res, ref):
