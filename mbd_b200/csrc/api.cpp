@@ -539,7 +539,6 @@ int prepare_batch(mbd_ctx* ctx, bool eigen) {
   // matrix the two-stage reduction can take goes through it; larger ones
   // (n above the panel cluster's rows) take the one-stage grouped launch.
   ctx->two_stage_batch = ctx->two_stage_force != 0;
-  ctx->two_stage_min_n = 1 << 30;
   std::stable_sort(ctx->order.begin(), ctx->order.end(),
                    [&](int a, int b) { return ctx->geoms[a]->plan.n > ctx->geoms[b]->plan.n; });
   for (int g : ctx->order) {

@@ -147,9 +147,8 @@ struct mbd_ctx {
   bool use_graphs = true;
   bool graph_replayed = false;               // the last compute ran as a graph replay
   int two_stage_max_n = 0;                   // largest matrix the two-stage reduction takes on this device
-  bool two_stage_batch = false;              // the whole batch uses the two-stage reduction
+  bool two_stage_batch = false;              // two-stage reduction for the matrices it can take
   int two_stage_force = -1;                  // 1 / 0: forced on / off; -1: policy
-  int two_stage_min_n = 1 << 30;             // otherwise matrices from this size up use it
   bool capturing = false;
   int mode_runs[3] = {0, 0, 0};              // computes of the uploaded batch, per mode
   double last_ms[mbd::Stage::kCount] = {0};
@@ -211,7 +210,7 @@ int relay_learned(mbd_ctx* ctx, GeomDev* gd, RelaySlot& sl, size_t mstride, cuda
 
 // Matrices reduced by the two-stage path (the rest by the one-stage kernel).
 inline bool two_stage(const mbd_ctx* ctx, int n) {
-  return (ctx->two_stage_batch || n >= ctx->two_stage_min_n) && n <= ctx->two_stage_max_n;
+  return ctx->two_stage_batch && n <= ctx->two_stage_max_n;
 }
 
 }  // namespace mbd

@@ -152,7 +152,6 @@ constexpr int kPanelMaxRowsPerCta = 1152;    // panel rows one CTA keeps (384 in
 constexpr int kPanelRowsTarget = 192;        // fewer rows per CTA while the cluster can grow
 constexpr int kPanelMaxCluster = 16;         // CTAs of the panel-QR cluster
 constexpr int kSymmMaxSplit = 16;
-constexpr int kTwoStageMaxN = kPanelMaxRowsPerCta * kPanelMaxCluster;
 struct PanelArgs {
   double* A;
   int ld;
