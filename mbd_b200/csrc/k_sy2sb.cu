@@ -303,9 +303,13 @@ __global__ void __launch_bounds__(NW * 32) qr_panel2_kernel(PanelArgs a) {
   constexpr int RREG = NW * RPW;
   constexpr int NT = NW * 32;
   constexpr unsigned FULL = 0xffffffffu;
-  __shared__ double pubN[2][NW];
-  __shared__ double pubA[2];
-  __shared__ double pubD[2][B];
+  // receive buffers (double-buffered by column parity): every CTA pushes its
+  // partial sums into every CTA's buffers with remote stores before the
+  // cluster barrier and reads its own buffers after it
+  __shared__ double recvN[2][kPanelMaxCluster];      // CTA norm partials, by rank
+  __shared__ double recvA[2];                        // alpha from the owner of row j
+  __shared__ double recvD[2][kPanelMaxCluster][B];   // CTA dot sums, by rank
+  __shared__ double wn[NW];
   __shared__ double dw[NW][B];
   __shared__ double vs[NW][RPW];
   __shared__ double gs[B];
@@ -351,32 +355,29 @@ __global__ void __launch_bounds__(NW * 32) qr_panel2_kernel(PanelArgs a) {
   for (int j = 0; j < nref; ++j) {
     const int par = j & 1;
     const double sj = __shfl_sync(FULL, s_own, j);
-    if (lane == 0) pubN[par][warp] = sj;
-    // row j is local row j - lo < 32: warp (j - lo) % NW, slot t = (j - lo) / NW < 4
-    if (j >= lo && j < hi && (j - lo) % NW == warp && lane == j) {
+    if (lane == 0) wn[warp] = sj;
+    // row j is local row j - lo < 32: warp (j - lo) % NW, slot t = (j - lo) / NW < 4;
+    // the owner warp pushes alpha = A(j, j) to every CTA
+    if (j >= lo && j < hi && (j - lo) % NW == warp) {
       const int tj = (j - lo) / NW;
       double aj = 0.0;
 #pragma unroll
       for (int t = 0; t < (RPW < 4 ? RPW : 4); ++t)
         if (t == tj) aj = x[t];
-      pubA[par] = aj;
+      aj = __shfl_sync(FULL, aj, j);
+      if (lane < C) cl.map_shared_rank(&recvA[0], lane)[par] = aj;
+    }
+    __syncthreads();
+    if (warp == 0) {
+      double t = 0.0;
+#pragma unroll
+      for (int q = 0; q < NW; ++q) t += wn[q];
+      if (lane < C) cl.map_shared_rank(&recvN[0][0], lane)[par * kPanelMaxCluster + rank] = t;
     }
     cl.sync();
-    // all remote loads first (independent), then the sums
-    constexpr int NX = (kPanelMaxCluster * NW + 31) / 32;
-    double xparts[NX];
-#pragma unroll
-    for (int u = 0; u < NX; ++u) {
-      const int q = lane + 32 * u;
-      xparts[u] = (q < C * NW) ? cl.map_shared_rank(&pubN[0][0], q / NW)[par * NW + q % NW] : 0.0;
-    }
     double xn2 = 0.0;
-#pragma unroll
-    for (int u = 0; u < NX; ++u) xn2 += xparts[u];
-    xn2 = warp_sum(xn2);
-    double alpha = 0.0;
-    if (lane == 0) alpha = cl.map_shared_rank(&pubA[0], j / R)[par];
-    alpha = __shfl_sync(FULL, alpha, 0);
+    for (int q = 0; q < C; ++q) xn2 += recvN[par][q];
+    const double alpha = recvA[par];
     double tau = 0.0, scale = 0.0, beta = alpha;
     if (xn2 > 0.0) {
       beta = -copysign(sqrt(alpha * alpha + xn2), alpha);
@@ -408,20 +409,17 @@ __global__ void __launch_bounds__(NW * 32) qr_panel2_kernel(PanelArgs a) {
       for (int i = warp; RREG + i < nr; i += NW) d0 += (Ps[i * QR_LD2 + j] * scale) * Ps[i * QR_LD2 + lane];
     dw[warp][lane] = d0 + d1;
     __syncthreads();
-    if (warp == 0) {
+    {
+      // every warp forms the CTA's dot vector and pushes it to C / NW ranks
       double t = 0.0;
 #pragma unroll
       for (int q = 0; q < NW; ++q) t += dw[q][lane];
-      pubD[par][lane] = t;
+      for (int q = warp; q < C; q += NW)
+        cl.map_shared_rank(&recvD[0][0][0], q)[(par * kPanelMaxCluster + rank) * B + lane] = t;
     }
     cl.sync();
-    double dparts[kPanelMaxCluster];
-#pragma unroll
-    for (int q = 0; q < kPanelMaxCluster; ++q)
-      dparts[q] = (q < C) ? cl.map_shared_rank(&pubD[0][0], q)[par * B + lane] : 0.0;
     double dc = 0.0;
-#pragma unroll
-    for (int q = 0; q < kPanelMaxCluster; ++q) dc += dparts[q];
+    for (int q = 0; q < C; ++q) dc += recvD[par][q][lane];
     // update the columns right of j and the norms below row j + 1
     const double tdc = (lane > j) ? tau * dc : 0.0;
     double s0 = 0.0, s1 = 0.0;
