@@ -69,11 +69,15 @@ template <int NW, int RPW>
 __global__ void __launch_bounds__(NW * 32) qr_panel_kernel(PanelArgs a) {
   constexpr int NT = NW * 32;
   constexpr unsigned FULL = 0xffffffffu;
-  __shared__ double pubN[2][NW];     // exact norm partials (first column, recomputes)
-  __shared__ double pubA0;           // alpha of the first column (owner CTA)
-  __shared__ double pubD[2][B];      // dot sums of this CTA
-  __shared__ double pubS[2][4];      // S_xx, S_vx, S_vv of this CTA for the next column
-  __shared__ double pubR[2][2];      // owner of row j + 1: x_{j+1}(j + 1), v(j + 1)
+  // receive buffers (double-buffered by column parity): every CTA pushes its
+  // partial sums into every CTA's buffers with remote stores before the
+  // cluster barrier and reads its own buffers after it
+  __shared__ double recvN[2][kPanelMaxCluster];      // exact norm partials (first column, recomputes)
+  __shared__ double recvA0;                          // alpha of the first column
+  __shared__ double recvD[2][kPanelMaxCluster][B];   // dot sums, by rank
+  __shared__ double recvS[2][kPanelMaxCluster][4];   // S_xx, S_vx, S_vv for the next column, by rank
+  __shared__ double recvR[2][2];                     // from the owner of row j + 1: x_{j+1}(j + 1), v(j + 1)
+  __shared__ double wn[NW];
   __shared__ double dw[NW][B];
   __shared__ double ds[NW][3];
   __shared__ double vs[NW][RPW];
@@ -98,7 +102,7 @@ __global__ void __launch_bounds__(NW * 32) qr_panel_kernel(PanelArgs a) {
     for (int e = tid; e < B * (B + 1); e += NT) (&Tm[0][0])[e] = 0.0;
   const int nref = min(B, m);
   // exact ||x_c below row jr||^2 of column c = jr (lane jr's value), summed
-  // over the cluster through pubN[par] (one barrier)
+  // over the cluster through recvN[par] (one barrier)
   auto exact_norm = [&](int jr, int par) -> double {
     double s0 = 0.0, s1 = 0.0;
 #pragma unroll
@@ -108,19 +112,18 @@ __global__ void __launch_bounds__(NW * 32) qr_panel_kernel(PanelArgs a) {
       else s0 += v * v;
     }
     const double sj = __shfl_sync(FULL, s0 + s1, jr);
-    if (lane == 0) pubN[par][warp] = sj;
-    cl.sync();
-    constexpr int NX = (kPanelMaxCluster * NW + 31) / 32;
-    double xparts[NX];
+    if (lane == 0) wn[warp] = sj;
+    __syncthreads();
+    if (warp == 0) {
+      double t = 0.0;
 #pragma unroll
-    for (int u = 0; u < NX; ++u) {
-      const int q = lane + 32 * u;
-      xparts[u] = (q < C * NW) ? cl.map_shared_rank(&pubN[0][0], q / NW)[par * NW + q % NW] : 0.0;
+      for (int q = 0; q < NW; ++q) t += wn[q];
+      if (lane < C) cl.map_shared_rank(&recvN[0][0], lane)[par * kPanelMaxCluster + rank] = t;
     }
+    cl.sync();
     double xn = 0.0;
-#pragma unroll
-    for (int u = 0; u < NX; ++u) xn += xparts[u];
-    return warp_sum(xn);
+    for (int q = 0; q < C; ++q) xn += recvN[par][q];
+    return xn;
   };
   // row jr's entry of this lane's column (valid in the owner warp; jr - lo < 32)
   auto own_entry = [&](int jr) -> double {
@@ -131,12 +134,13 @@ __global__ void __launch_bounds__(NW * 32) qr_panel_kernel(PanelArgs a) {
       if (t == tj) v = x[t];
     return v;
   };
-  // column 0: exact norm and alpha
-  if (0 >= lo && 0 < hi && (0 - lo) % NW == warp && lane == 0) pubA0 = own_entry(0);
-  double xn2 = exact_norm(0, 0);
-  double alpha = 0.0;
-  if (lane == 0) alpha = cl.map_shared_rank(&pubA0, 0)[0];
-  alpha = __shfl_sync(FULL, alpha, 0);
+  // column 0: exact norm and alpha (rank 0, warp 0 owns row 0)
+  if (rank == 0 && warp == 0) {
+    const double a0 = __shfl_sync(FULL, own_entry(0), 0);
+    if (lane < C) *cl.map_shared_rank(&recvA0, lane) = a0;
+  }
+  double xn2 = exact_norm(0, 0);   // its barrier also delivers alpha
+  double alpha = recvA0;
   for (int j = 0; j < nref; ++j) {
     const int par = j & 1;
     double tau = 0.0, scale = 0.0, beta = alpha;
@@ -195,48 +199,41 @@ __global__ void __launch_bounds__(NW * 32) qr_panel_kernel(PanelArgs a) {
         ds[warp][2] = a2;
       }
     }
-    if (j + 1 < nref && j + 1 >= lo && j + 1 < hi && (j + 1 - lo) % NW == warp && lane == j + 1) {
-      pubR[par][0] = own_entry(j + 1);
-      pubR[par][1] = vs[warp][(j + 1 - lo) / NW];
+    if (j + 1 < nref && j + 1 >= lo && j + 1 < hi && (j + 1 - lo) % NW == warp) {
+      // the owner warp of row j + 1 pushes x_{j+1}(j + 1) and v(j + 1) to every CTA
+      const double ex = __shfl_sync(FULL, own_entry(j + 1), j + 1);
+      const double ev = vs[warp][(j + 1 - lo) / NW];
+      if (lane < C) {
+        double* pr = cl.map_shared_rank(&recvR[0][0], lane) + par * 2;
+        pr[0] = ex;
+        pr[1] = ev;
+      }
     }
     __syncthreads();
-    if (warp == 0) {
+    {
+      // every warp forms the CTA's sums and pushes them to C / NW ranks
       double t = 0.0;
 #pragma unroll
       for (int q = 0; q < NW; ++q) t += dw[q][lane];
-      pubD[par][lane] = t;
-      if (lane < 3) {
-        double u = 0.0;
+      double u = 0.0;
+      if (lane < 3)
 #pragma unroll
         for (int q = 0; q < NW; ++q) u += ds[q][lane];
-        pubS[par][lane] = u;
+      for (int q = warp; q < C; q += NW) {
+        cl.map_shared_rank(&recvD[0][0][0], q)[(par * kPanelMaxCluster + rank) * B + lane] = t;
+        if (lane < 3) cl.map_shared_rank(&recvS[0][0][0], q)[(par * kPanelMaxCluster + rank) * 4 + lane] = u;
       }
     }
     cl.sync();
-    // cluster sums: dots (lane c), next-column sums (lanes < C, then a warp sum)
-    double dparts[kPanelMaxCluster];
-#pragma unroll
-    for (int q = 0; q < kPanelMaxCluster; ++q)
-      dparts[q] = (q < C) ? cl.map_shared_rank(&pubD[0][0], q)[par * B + lane] : 0.0;
-    double s3[3] = {0.0, 0.0, 0.0};
-    if (lane < C) {
-      const double* ps = cl.map_shared_rank(&pubS[0][0], lane) + par * 4;
-      s3[0] = ps[0];
-      s3[1] = ps[1];
-      s3[2] = ps[2];
+    // cluster sums in rank order
+    double dc = 0.0, Sxx = 0.0, Svx = 0.0, Svv = 0.0;
+    for (int q = 0; q < C; ++q) {
+      dc += recvD[par][q][lane];
+      Sxx += recvS[par][q][0];
+      Svx += recvS[par][q][1];
+      Svv += recvS[par][q][2];
     }
-    double rx = 0.0, rv = 0.0;
-    if (j + 1 < nref && lane == 0) {
-      const double* pr = cl.map_shared_rank(&pubR[0][0], (j + 1) / R) + par * 2;
-      rx = pr[0];
-      rv = pr[1];
-    }
-    double dc = 0.0;
-#pragma unroll
-    for (int q = 0; q < kPanelMaxCluster; ++q) dc += dparts[q];
-    const double Sxx = warp_sum(s3[0]), Svx = warp_sum(s3[1]), Svv = warp_sum(s3[2]);
-    rx = __shfl_sync(FULL, rx, 0);
-    rv = __shfl_sync(FULL, rv, 0);
+    const double rx = recvR[par][0], rv = recvR[par][1];
     // update the columns right of j
     const double tdc = (lane > j) ? tau * dc : 0.0;
 #pragma unroll
