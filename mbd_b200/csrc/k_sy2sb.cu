@@ -6,11 +6,13 @@
 // kBand, m of them):
 //   qr_panel   Householder QR of the m x kBand panel in ONE thread-block
 //              cluster: the panel's rows are spread over the CTAs' registers
-//              (a lane per column), cross-CTA sums go through distributed
-//              shared memory and two hardware cluster barriers per column.
-//              Writes R in place (the band), V explicitly (unit lower
-//              trapezoidal) and the compact-WY factor T (Q = I - V T V^T,
-//              dlarft forward), whose Gram entries come from the same dots.
+//              (a lane per column; past 384 rows per CTA also shared
+//              memory), cross-CTA sums are pushed into every CTA's shared
+//              memory ahead of one or two hardware cluster barriers per
+//              column.  Writes R in place (the band), V explicitly (unit
+//              lower trapezoidal) and the compact-WY factor T (Q = I - V T
+//              V^T, dlarft forward), whose Gram entries come from the same
+//              dots.
 //   symm       Y = A22 V (A22 the trailing m x m lower-stored block), row
 //              blocks of 64 split over S column chunks (fixed-order partials)
 //   yred       Y <- sum of the partials; Y <- Y T; block partials of V^T Y
@@ -62,9 +64,10 @@ __device__ __forceinline__ double warp_sum(double v) {
 //      below 0.19 and the downdate matched the exact sum to 1.1e-15.
 //   6. rank 0, warp 0: T[0:j, j] = -tau_j T[0:j, 0:j] (V^T V)[0:j, j],
 //      T[j][j] = tau_j (dlarft, forward, columnwise) from the same dots.
-// pub* are read by the other CTAs of the cluster (double-buffered by column
-// parity: a buffer is rewritten two columns later, after the barrier of the
-// column in between).
+// recv* are written by the other CTAs of the cluster (remote stores before
+// the barrier) and read locally after it; double-buffered by column parity,
+// a buffer is rewritten two columns later, after every CTA has passed the
+// barrier of the column in between, so after its reads.
 template <int NW, int RPW>
 __global__ void __launch_bounds__(NW * 32) qr_panel_kernel(PanelArgs a) {
   constexpr int NT = NW * 32;
