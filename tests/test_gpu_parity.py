@@ -180,3 +180,25 @@ def test_eigvalsh_known_spectrum_large(engine, n):
     H, lam = _known_spectrum(n, seed=n)
     w = engine.eigvalsh(H)
     np.testing.assert_allclose(w, lam, rtol=0, atol=1e-12 * 4.0 * n)
+
+
+@pytest.mark.parametrize("xc", [2, 3, 9])
+def test_xc_range_separation(engine, xc):
+    """flag_xc other than PBE (get_beta, UTILS.f90:353-372): PBE0 and HSE take
+    beta = 0.85 (a REAL*4 literal), any other value beta = 1; plain FP64
+    against the oracle on the benzene ring and a 60-atom cluster."""
+    import dataclasses
+
+    from mbd_b200 import synthetic as sy
+    from oracle import mbd_oracle as mo
+    for geo, st in (sy.benzene(), sy.cluster(60, seed=3)):
+        st = dataclasses.replace(st, xc=xc)
+        res = engine.energy(geo, st, "plain")
+        og = mo.Geometry(list(geo.names), geo.coords.copy(), geo.hirshfeld.copy(), geo.lattice.copy(), geo.n_periodic)
+        ref = mo.mbd_at_rsscs(og, mo.Settings(xc=xc, mbd_supercell_cutoff=st.mbd_supercell_cutoff,
+                                              mbd_cfdm_dip_cutoff=st.mbd_cfdm_dip_cutoff,
+                                              mbd_scs_dip_cutoff=st.mbd_scs_dip_cutoff,
+                                              mbd_scs_vacuum_axis=tuple(st.mbd_scs_vacuum_axis)))
+        assert res.status == 0
+        assert abs(res.energy - ref.energy) <= PLAIN_E_TOL, (xc, res.energy, ref.energy)
+        np.testing.assert_allclose(res.c6_eff, ref.c6_eff, rtol=PLAIN_RTOL, atol=0)
