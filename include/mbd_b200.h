@@ -152,6 +152,11 @@ int mbd_rsscs_eigvalsh_noalloc(double* H, int n, int ld, double* w, void* stream
 
 /* Fortran-friendly helpers. */
 int mbd_rsscs_element_z(const char* symbol);   /* "C" -> 6; 0 if no vdW parameters (UTILS.f90:1336-1701) */
+/* The 21 imaginary frequencies (Hartree; omega = 0 first) and Casimir-Polder
+ * weights the engine integrates with: gauss_legendre_grid (UTILS.f90:1188-1211,
+ * REAL*4 literals widened to double), as the report prints them
+ * (UTILS.f90:278).  weight may be NULL; n must be >= MBD_N_FREQ. */
+int mbd_rsscs_frequency_grid(double* omega, double* weight, int n);
 const char* mbd_rsscs_strerror(int code);
 /* Free-atom table entry: alpha0, C6, R0 as the reference stores them
  * (REAL*4 literals widened to double).  Returns MBD_ERR_UNKNOWN_ELEMENT for

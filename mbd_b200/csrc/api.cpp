@@ -1121,6 +1121,15 @@ int mbd_rsscs_eigvalsh(mbd_ctx* ctx, const double* H, int n, int ld, double* w) 
 
 int mbd_rsscs_element_z(const char* symbol) { return element_z(symbol); }
 
+int mbd_rsscs_frequency_grid(double* omega, double* weight, int n) {
+  if (!omega || n < kNFreq) return MBD_ERR_ARG;
+  for (int f = 0; f < kNFreq; ++f) {
+    omega[f] = kCasimirOmega[f];
+    if (weight) weight[f] = kCasimirWeight[f];
+  }
+  return MBD_OK;
+}
+
 int mbd_rsscs_vdw_params(int z, double* alpha0, double* c6, double* r0) {
   VdwParam v;
   if (!vdw_param(z, &v)) return MBD_ERR_UNKNOWN_ELEMENT;

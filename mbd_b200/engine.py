@@ -112,6 +112,9 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
     lib.mbd_rsscs_strerror.restype = ctypes.c_char_p
     lib.mbd_rsscs_vdw_params.argtypes = [ctypes.c_int] + [ctypes.POINTER(ctypes.c_double)] * 3
     lib.mbd_rsscs_vdw_params.restype = ctypes.c_int
+    lib.mbd_rsscs_frequency_grid.argtypes = [ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double),
+                                             ctypes.c_int]
+    lib.mbd_rsscs_frequency_grid.restype = ctypes.c_int
     lib.mbd_rsscs_last_timings.argtypes = [vp, ctypes.POINTER(ctypes.c_double), ctypes.c_int]
     lib.mbd_rsscs_last_timings.restype = ctypes.c_int
     lib.mbd_rsscs_last_stats.argtypes = [vp, ctypes.POINTER(ctypes.c_double), ctypes.c_int]
@@ -147,6 +150,18 @@ def element_z(symbol: str) -> int:
 
 def strerror(code: int) -> str:
     return load_library().mbd_rsscs_strerror(code).decode()
+
+
+def frequency_grid():
+    """(omega, weight): the 21 imaginary frequencies (Hartree) and Casimir-Polder
+    weights the engine integrates with (mbd_rsscs_frequency_grid)."""
+    w = np.zeros(21)
+    wt = np.zeros(21)
+    dp = ctypes.POINTER(ctypes.c_double)
+    code = load_library().mbd_rsscs_frequency_grid(w.ctypes.data_as(dp), wt.ctypes.data_as(dp), 21)
+    if code != MBD_OK:
+        raise MbdError(code, strerror(code))
+    return w, wt
 
 
 @dataclass

@@ -119,30 +119,72 @@ def parse_settings(text: str) -> Settings:
     return s
 
 
+def _fortran_f(v: float, w: int, d: int) -> str:
+    """Fortran Fw.d (asterisks when the number does not fit)."""
+    t = f"{v:{w}.{d}f}"
+    return t if len(t) <= w else "*" * w
+
+
+def _fortran_e(v: float, w: int, d: int) -> str:
+    """Fortran Ew.d: 0.ddd...E+ee (E dropped for a three-digit exponent)."""
+    if v == 0.0 or not np.isfinite(v):
+        body = "0." + "0" * d + "E+00" if v == 0.0 else str(v)
+    else:
+        m, e = f"{abs(v):.{d - 1}E}".split("E")
+        digits = m.replace(".", "")
+        exp = int(e) + 1
+        ee = f"E{exp:+03d}" if abs(exp) <= 99 else f"{exp:+04d}"
+        body = ("-" if v < 0 else "") + "0." + digits + ee
+    return body.rjust(w) if len(body) <= w else "*" * w
+
+
+_RULE = "| ---------------------------------------------------------------------------"
+
+
+def frequency_grid() -> np.ndarray:
+    """The 21 imaginary frequencies of the Casimir-Polder integration (omega = 0
+    and the 20 Gauss-Legendre nodes, gauss_legendre_grid UTILS.f90:1188-1211),
+    in Hartree, as the engine uses them."""
+    from .engine import frequency_grid as grid
+    return grid()[0]
+
+
 def format_report(geo: Geometry, res, omega_grid=None) -> str:
-    """Report fields of MBD_at_rsSCS (UTILS.f90:223-331) for a Result."""
+    """The MBD section of pmbd.x's report (MBD_at_rsSCS UTILS.f90:223-331 and
+    get_mbd_rSCS UTILS.f90:753-755, 861) for a Result, line for line as the
+    reference prints it: every line goes through output_string
+    (UTILS.f90:1708-1714, list-directed WRITE of TRIM(info_str), hence the
+    leading blank) with the reference's edit descriptors."""
     from .engine import N_FREQ
+    grid = frequency_grid() if omega_grid is None else omega_grid
     out = []
-    out.append("  | Many-Body Dispersion (MBD@rsSCS) energy ")
-    out.append("  | System dynamic molecular polarizability alpha(iw) (bohr^3)")
-    out.append("  | ---------------------------------------------------------------------------")
-    out.append("  |  omega(Ha)   alpha_iso      alpha_xx       alpha_yy       alpha_zz")
+
+    def put(text):
+        out.append(" " + text.rstrip())
+
+    put("  | Many-Body Dispersion (MBD@rsSCS) energy ")
+    put("  | System dynamic molecular polarizability alpha(iw) (bohr^3)")
+    put("  " + _RULE)
+    put("  |  omega(Ha)   alpha_iso      alpha_xx       alpha_yy       alpha_zz")
     for f in range(N_FREQ):
         ev = res.mol_pol_eig[f]
-        w = omega_grid[f] if omega_grid is not None else float("nan")
-        out.append("  | %10.6f%15.6E%15.6E%15.6E%15.6E" % (w, ev.sum() / 3.0, ev[0], ev[1], ev[2]))
-    out.append("  | ---------------------------------------------------------------------------")
-    out.append("  | System C6 coefficient    :  %20.8f  hartree bohr^6" % res.c6_mol)
-    out.append("  | ---------------------------------------------------------------------------")
-    out.append("  | Partitioned C6 (hartree bohr^6) | alpha (bohr^3)  of atom in system")
-    out.append("  | ---------------------------------------------------------------------------")
+        vals = (ev.sum() / 3.0, ev[0], ev[1], ev[2])
+        put("  | " + _fortran_f(grid[f], 10, 6) + "".join(_fortran_e(x, 15, 6) for x in vals))
+    put("  " + _RULE)
+    put("  | System C6 coefficient    :  " + _fortran_f(res.c6_mol, 20, 8) + "    hartree bohr^6")
+    put("  " + _RULE)
+    put("  | Partitioned C6 (hartree bohr^6) | alpha (bohr^3)  of atom in system")
+    put("  " + _RULE)
     for i, name in enumerate(geo.names):
-        out.append("  | ATOM %4d  %-2s%12.6f      %12.6f" % (i + 1, name, res.c6_eff[i], res.alpha_eff[i]))
-    out.append("  | ---------------------------------------------------------------------------")
+        put("  | ATOM " + f"{i + 1:4d}" + "  " + f"{name:2.2s}" + _fortran_f(res.c6_eff[i], 12, 6) + " " * 6 +
+            _fortran_f(res.alpha_eff[i], 12, 6))
+    put("  " + _RULE)
     sc = res.supercell
-    out.append("  | Creating super cell of dimension%3d X %3d X %3d in MBD calculation" % tuple(sc))
-    out.append("  | containing%6d  atom" % (len(geo.names) * sc[0] * sc[1] * sc[2]))
+    put("  | Creating super cell of dimension" + f"{sc[0]:3d} X {sc[1]:3d} X {sc[2]:3d}" + " in MBD calculation")
+    put("  | containing" + f"{len(geo.names) * sc[0] * sc[1] * sc[2]:6d}" + "  atom")
     if res.nimag > 0:
-        out.append("***WARNING: found %4d negative eigenvalues in MBD energy calculation." % res.nimag)
-    out.append("  | MBD@rsSCS energy   :%20.9f Ha     %20.9f eV" % (res.energy, res.energy * 27.211))
+        put("***WARNING: found " + f"{res.nimag:4d}" + " negative eigenvalues in MBD energy calculation.")
+    # 27.211 is a REAL*4 literal (UTILS.f90:330)
+    put("  | MBD@rsSCS energy   :" + _fortran_f(res.energy, 20, 9) + " Ha     " +
+        _fortran_f(res.energy * float(np.float32(27.211)), 20, 9) + " eV")
     return "\n".join(out)

@@ -9,10 +9,16 @@ For every example it writes ``<name>.json`` holding
   * the geometry and settings exactly as the reference run read them
     (examples/<name>.in + the settings used for that run),
   * ``printed``: the values the reference printed in examples/<name>.out
-    (C6H6, graphene_111, PBBA), and
+    (C6H6, graphene_111, PBBA), and for the clusters (C6H6, PBBA) the MBD
+    report lines themselves (``report_lines``: from "| Many-Body Dispersion"
+    to the energy line; the graphene output was written by a version of the
+    report code whose headers differ from UTILS.f90:223-331), and
   * ``oracle``: the FP64 oracle's full-precision outputs on the same input
     (used as the parity target for the GPU path; for H2O and TiOCHF, which
     ship no output, this is the only pin).
+
+``--report-only`` adds or refreshes ``report_lines`` in the existing
+fixtures without recomputing the oracle.
 
 The settings of the shipped outputs are taken from the headers of the .out
 files: C6H6 and PBBA used the defaults (the 2000 A box of C6H6 admits no
@@ -39,6 +45,35 @@ CASES = {
     "H2O": (None, False),
     "TiOCHF": ("settings.in", False),
 }
+
+
+REPORT_CASES = ("C6H6", "PBBA")
+
+
+def report_lines(out_text: str) -> list:
+    """The MBD section of a pmbd.x report: the lines from the section header
+    to the energy line that the report code prints (``|`` rows and warnings)."""
+    lines = out_text.splitlines()
+    start = next(i for i, ln in enumerate(lines) if "| Many-Body Dispersion (MBD@rsSCS) energy" in ln)
+    sel = []
+    for ln in lines[start:]:
+        if ln.lstrip().startswith("|") or ln.startswith(" ***WARNING: found"):
+            sel.append(ln)
+            if "| MBD@rsSCS energy" in ln:
+                break
+    return sel
+
+
+def add_report_lines(ref_root: str) -> None:
+    for name in REPORT_CASES:
+        path = os.path.join(HERE, name + ".json")
+        with open(path) as fh:
+            fix = json.load(fh)
+        with open(os.path.join(ref_root, "examples", name + ".out")) as fh:
+            fix["printed"]["report_lines"] = report_lines(fh.read())
+        with open(path, "w") as fh:
+            json.dump(fix, fh, indent=1)
+        print(f"{name}: {len(fix['printed']['report_lines'])} report lines")
 
 
 def main(ref_root: str) -> None:
@@ -80,10 +115,18 @@ def main(ref_root: str) -> None:
                 "atoms": {str(k): v for k, v in rep["atoms"].items()},
                 "pol": rep["pol"],
             }
+            if name in REPORT_CASES:
+                with open(os.path.join(ref_root, "examples", name + ".out")) as fh:
+                    fix["printed"]["report_lines"] = report_lines(fh.read())
         with open(os.path.join(HERE, name + ".json"), "w") as fh:
             json.dump(fix, fh, indent=1)
         print(f"{name}: E={res.energy:.12f} C6={res.c6_mol:.8f} nimag={res.nimag} ({dt:.1f}s)")
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    args = [a for a in sys.argv[1:] if not a.startswith("--")]
+    root = args[0] if args else "/root/reference"
+    if "--report-only" in sys.argv:
+        add_report_lines(root)
+    else:
+        main(root)

@@ -202,3 +202,14 @@ def test_xc_range_separation(engine, xc):
         assert res.status == 0
         assert abs(res.energy - ref.energy) <= PLAIN_E_TOL, (xc, res.energy, ref.energy)
         np.testing.assert_allclose(res.c6_eff, ref.c6_eff, rtol=PLAIN_RTOL, atol=0)
+
+
+@pytest.mark.parametrize("name", ["C6H6", "PBBA"])
+def test_report_from_engine_matches_reference(engine, name):
+    """The engine's results (plain FP64) printed by format_report reproduce the
+    MBD section of the reference's examples/<name>.out byte for byte."""
+    from mbd_b200 import format_report, parse_geometry, parse_settings
+    fix = _fixture(name)
+    geo = parse_geometry(fix["geometry_in"])
+    res = engine.energy(geo, parse_settings(fix["settings_in"]), mode="plain")
+    assert format_report(geo, res).splitlines() == fix["printed"]["report_lines"]

@@ -105,3 +105,42 @@ def test_synthetic_generators():
     assert pb.n_periodic == 3 and np.isclose(pb.lattice[0, 0] ** 3, 3000.0)
     batch = sy.cluster_batch(count=4, seed=0)
     assert all(20 <= len(gg.names) <= 600 for gg, _ in batch)
+
+
+@pytest.mark.parametrize("name", ["C6H6", "PBBA"])
+def test_report_matches_reference_bytes(name):
+    """format_report prints the MBD section of the report with the reference's
+    edit descriptors (UTILS.f90:223-331, 753-755, 861): fed the FP64 oracle's
+    values, it reproduces the lines of examples/<name>.out byte for byte."""
+    import json
+    import types
+
+    from mbd_b200 import format_report, parse_geometry
+    with open(os.path.join(ROOT, "tests", "golden", name + ".json")) as fh:
+        fix = json.load(fh)
+    o = fix["oracle"]
+    res = types.SimpleNamespace(energy=o["energy"], c6_mol=o["c6_mol"], nimag=o["nimag"],
+                                supercell=tuple(o["supercell"]), c6_eff=np.array(o["c6_eff"]),
+                                alpha_eff=np.array(o["alpha_eff"]), mol_pol_eig=np.array(o["mol_pol_eig"]))
+    lines = format_report(parse_geometry(fix["geometry_in"]), res).splitlines()
+    assert lines == fix["printed"]["report_lines"]
+
+
+def test_fortran_edit_descriptors():
+    from mbd_b200 import io
+    assert io._fortran_e(65.6629, 15, 6) == "   0.656629E+02"
+    assert io._fortran_e(0.0212703, 15, 6) == "   0.212703E-01"
+    assert io._fortran_e(-1234.5, 15, 6) == "  -0.123450E+04"
+    assert io._fortran_e(0.0, 15, 6) == "   0.000000E+00"
+    assert io._fortran_e(0.9999999, 15, 6) == "   0.100000E+01"   # rounding carries into the exponent
+    assert io._fortran_f(1622.14013676, 20, 8) == "       1622.14013676"
+    assert io._fortran_f(123456.0, 5, 1) == "*****"
+
+
+def test_frequency_grid_matches_oracle():
+    from mbd_b200.engine import frequency_grid
+    from oracle import mbd_oracle as mo
+    w, wt = frequency_grid()
+    np.testing.assert_array_equal(w, mo.CASIMIR_OMEGA)
+    np.testing.assert_array_equal(wt, mo.CASIMIR_WEIGHT)
+    assert w[0] == 0.0 and wt[0] == 0.0
