@@ -183,6 +183,11 @@ def run_reference(args, rank, world):
     this image, so its CPU path is the FP64 oracle port on the host cores."""
     if rank != 0:
         return 0
+    if WORKLOAD == "boxes":
+        print(json.dumps({"impl": "reference", "metric": METRIC, "config": {"workload": workload_name()},
+                          "unavailable": "the FP64 oracle needs minutes per 200-atom box at these cut-offs; "
+                                         "not timed"}), flush=True)
+        return 0
     vals, cb = [], None
     for _ in range(max(1, args.steps)):
         cb = cpu_baseline()

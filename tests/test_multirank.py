@@ -62,3 +62,18 @@ def test_reference_arm_runs_on_rank_0_only(capsys):
     args = argparse.Namespace(steps=1, warmup=0, gpus=2)
     assert bench.run_reference(args, 1, 2) == 0
     assert capsys.readouterr().out == ""
+
+
+def test_reference_arm_declines_boxes(capsys):
+    import argparse
+    import json
+
+    import bench
+    old = bench.WORKLOAD
+    bench.WORKLOAD = "boxes"
+    try:
+        assert bench.run_reference(argparse.Namespace(steps=1, warmup=0, gpus=1), 0, 1) == 0
+    finally:
+        bench.WORKLOAD = old
+    line = json.loads(capsys.readouterr().out)
+    assert line["impl"] == "reference" and "unavailable" in line
