@@ -149,7 +149,7 @@ void launch_energy(const double* ev, int n, int nsl, const double* scalars, doub
 constexpr int kBand = 32;                    // half-bandwidth of the intermediate band
 constexpr int kBandLd = 2 * kBand + 1;       // band row: A(r, r - d), d = 0..2 kBand (room for bulges)
 constexpr int kPanelMaxRowsPerCta = 1152;    // panel rows one CTA keeps (384 in registers, the rest in shared memory)
-constexpr int kPanelRowsTarget = 192;        // fewer rows per CTA while the cluster can grow
+constexpr int kPanelRowsTarget = 96;         // fewer rows per CTA while the cluster can grow
 constexpr int kPanelMaxCluster = 16;         // CTAs of the panel-QR cluster
 constexpr int kSymmMaxSplit = 16;
 struct PanelArgs {
