@@ -144,3 +144,21 @@ def test_frequency_grid_matches_oracle():
     np.testing.assert_array_equal(w, mo.CASIMIR_OMEGA)
     np.testing.assert_array_equal(wt, mo.CASIMIR_WEIGHT)
     assert w[0] == 0.0 and wt[0] == 0.0
+
+
+def test_report_warning_and_supercell_lines():
+    """The NIMAG warning (UTILS.f90:861, '(A,I4,A)') and the supercell lines
+    (UTILS.f90:753-755) as output_string prints them."""
+    import types
+
+    from mbd_b200 import format_report, parse_geometry
+    geo = parse_geometry("2\n\nC 0 0 0 0.8\nH 0 0 1.1 0.6\n")
+    res = types.SimpleNamespace(energy=-0.5, c6_mol=10.0, nimag=3, supercell=(2, 2, 1),
+                                c6_eff=np.array([1.0, 2.0]), alpha_eff=np.array([3.0, 4.0]),
+                                mol_pol_eig=np.ones((21, 3)))
+    lines = format_report(geo, res, omega_grid=np.zeros(21)).splitlines()
+    assert "   | Creating super cell of dimension  2 X   2 X   1 in MBD calculation" in lines
+    assert "   | containing     8  atom" in lines
+    assert " ***WARNING: found    3 negative eigenvalues in MBD energy calculation." in lines
+    assert lines[-1].startswith("   | MBD@rsSCS energy   :")
+    assert lines.index(" ***WARNING: found    3 negative eigenvalues in MBD energy calculation.") == len(lines) - 2
