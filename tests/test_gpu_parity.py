@@ -4,7 +4,7 @@ Targets: the reference's shipped examples (tests/golden/*.json, whose oracle
 section is pinned to the reference's printed reports) and seeded synthetic
 inputs of every workload at sizes the oracle finishes in seconds.
 
-Bars (north star): |E - E_oracle| <= 1e-6 Ha, screened C6 within 1e-6
+Bars: |E - E_oracle| <= 1e-6 Ha, screened C6 within 1e-6
 relative.  The plain FP64 mode is additionally held to 1e-9 Ha / 1e-9
 relative, which only a faithful FP64 implementation meets.
 """
