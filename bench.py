@@ -53,6 +53,8 @@ WORKLOADS = {
     "batched": "256 isolated {H,C,N,O} clusters N ~ U{20..600} (seed 0), 21 freqs, one batch",
     "boxes": "periodic cubic {H,C,N,O} boxes N in {2000,4000,6000} (seeds 0,1,2) at 0.1 atoms/A^3, "
              "cut-offs 120/100/25 A, 21 freqs",
+    "sheet": "periodic graphene sheet: hexagonal C, a = 2.46 A, 8x8 cells (128 atoms), 20 A along z with "
+             "vacuum axis z, cut-offs 120/100/25 A (2x2x1 supercell, Hamiltonian 1536 wide), 21 freqs",
 }
 WORKLOAD = "clusters"
 
@@ -63,6 +65,8 @@ def workload():
         return sy.cluster_batch(256)
     if WORKLOAD == "boxes":
         return [sy.periodic_box(n, seed=k) for k, n in enumerate(BOX_SIZES)]
+    if WORKLOAD == "sheet":
+        return [sy.graphene_sheet()]
     return [sy.cluster(n, seed=k) for k, n in enumerate(SIZES)]
 
 
@@ -80,13 +84,71 @@ def load_peaks():
         return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0}, "fallback"
 
 
+# DRAM traffic (dram__bytes_read.sum + dram__bytes_write.sum) of one launch of
+# the workload's dominant kernels, from ncu captures of this bench command on
+# a B200 (the summaries are committed under profiles/); a profile constant, not
+# measured by the run that prints it.
+PROFILED_TRAFFIC = {
+    "clusters": {"sb2st_kernel": 14544384, "tridiag_kernel": 210234000000},
+}
+
+
 def load_traffic():
-    """Per-launch DRAM traffic of the workload's dominant kernels from the committed ncu summaries."""
-    try:
-        with open(os.path.join(ROOT, "profiles", "traffic.json")) as fh:
-            return json.load(fh).get(WORKLOAD, {})
-    except OSError:
-        return {}
+    return PROFILED_TRAFFIC.get(WORKLOAD, {})
+
+
+def fp64_step_flops(results):
+    """Algorithmic FP64 work of the reference's method per step: for each
+    energy 21 (3N)^3/3 (Cholesky of the relay matrices) + 126 (3N)^2 (their
+    3-RHS solves) + (4/3) (3N n_SL)^3 (reduction of the CFDM Hamiltonian)."""
+    fl = 0.0
+    for r in results:
+        n = 3.0 * len(r.alpha_eff)
+        nsl = float(np.prod(r.supercell))
+        fl += 21.0 * n ** 3 / 3.0 + 126.0 * n * n + (4.0 / 3.0) * (n * nsl) ** 3
+    return fl
+
+
+def image_terms(geo, st):
+    """(pair, image) terms of the reference's image sums for one energy:
+    short-range (scs_*_block, UTILS.f90:561-579, 610-631: atom pairs i >= j,
+    images in the box +-ceil(cut/|a_k|) with 0 < r <= cut), once per
+    frequency; long-range (supercell_*_block/cfdm_*_block, UTILS.f90:883-1094:
+    lower-triangle (atom, cell) pairs of the supercell, supercell images with
+    r <= cut).  Counted here from the geometry (numpy), for the throughput
+    figure of the periodic sheet workload."""
+    bohr = 0.52917721
+    lat = geo.lattice / bohr
+    xyz = geo.coords / bohr
+
+    def box(cut, L, vac):
+        rng = [0 if (vac[k] or geo.n_periodic == 0) else int(np.ceil(cut / np.linalg.norm(L[k]))) for k in range(3)]
+        g = np.stack(np.meshgrid(*[np.arange(-m, m + 1) for m in rng], indexing="ij"), -1).reshape(-1, 3)
+        return g @ L
+
+    vac = tuple(bool(v) for v in st.mbd_scs_vacuum_axis)
+    scut = st.mbd_scs_dip_cutoff / bohr
+    sh = box(scut, lat, vac)
+    ii, jj = np.tril_indices(len(xyz), 0)
+    sr = 0
+    for s0 in range(0, len(ii), 4096):
+        d = (xyz[ii[s0:s0 + 4096]] - xyz[jj[s0:s0 + 4096]])[:, None, :] + sh[None]
+        r = np.sqrt((d * d).sum(-1))
+        sr += int(np.count_nonzero((r <= scut) & (r > 0.0)))
+    sl = np.array([1 if (vac[k] or geo.n_periodic == 0) else int(np.ceil((st.mbd_supercell_cutoff / bohr)
+                                                                          / np.linalg.norm(lat[k])))
+                   for k in range(3)])
+    cells = np.stack(np.meshgrid(*[np.arange(m) for m in sl], indexing="ij"), -1).reshape(-1, 3) @ lat
+    big = (xyz[:, None, :] + cells[None]).reshape(-1, 3)
+    lcut = st.mbd_cfdm_dip_cutoff / bohr
+    shl = box(lcut, lat * sl[:, None], vac)
+    ii, jj = np.tril_indices(len(big), 0)
+    lr = 0
+    for s0 in range(0, len(ii), 4096):
+        d = (big[ii[s0:s0 + 4096]] - big[jj[s0:s0 + 4096]])[:, None, :] + shl[None]
+        r = np.sqrt((d * d).sum(-1))
+        lr += int(np.count_nonzero((r <= lcut) & (r > 0.0)))
+    return 21 * sr, lr
 
 
 class ClockSampler:
@@ -150,55 +212,67 @@ def _oracle_energy(geo, st):
     return time.perf_counter() - t0
 
 
-def cpu_baseline(budget_s=12.0):
-    """The FP64 oracle (numpy + LAPACK, all host threads) on a bounded sample
-    of the workload.  clusters: one energy of the N=500 and N=1000 clusters,
-    the N=2000 term extrapolated x8 from N=1000 (the n^3 scaling of its dense
-    LAPACK work).  batched: oracle energies of the batch in order until about
-    budget_s seconds, the rest extrapolated by sum N^3."""
+def cpu_baseline():
+    """The FP64 oracle (numpy + LAPACK, all host threads) on the workload, every
+    energy timed (nothing extrapolated).  clusters / sheet: one oracle energy of
+    every geometry of the step.  batched: the first geometries of the batch
+    (a random sample of its size distribution) until about 20 s of CPU time,
+    energies/s over that sample."""
     geos = workload()
     if WORKLOAD == "batched":
         t, done = 0.0, 0
         for geo, st in geos:
             t += _oracle_energy(geo, st)
             done += 1
-            if t >= budget_s:
+            if t >= 20.0:
                 break
-        cost = [len(g.names) ** 3 for g, _ in geos]
-        t_step = t * sum(cost) / sum(cost[:done])
-        sample = (f"oracle energies of the first {done} of {len(geos)} geometries ({t:.1f} s), "
-                  f"extrapolated by sum N^3")
-    else:
-        t500 = _oracle_energy(*geos[0])
-        t1000 = _oracle_energy(*geos[1])
-        t_step = t500 + t1000 + t1000 * 8.0
-        sample = (f"oracle energies of the N=500 ({t500:.2f} s) and N=1000 ({t1000:.2f} s) "
-                  f"clusters; N=2000 extrapolated x8 from N=1000")
-    return {"value": len(geos) / t_step, "unit": "energies/s", "cores": os.cpu_count(), "kind": "port",
-            "sample": sample, "seconds_per_step": t_step, "energies_per_step": len(geos)}
+        return {"value": done / t, "unit": "energies/s", "cores": os.cpu_count(), "kind": "port",
+                "sample": f"oracle energies of the first {done} of the batch's {len(geos)} geometries "
+                          f"(N ~ U{{20..600}}), {t:.1f} s"}
+    times = [_oracle_energy(geo, st) for geo, st in geos]
+    sizes = ",".join(str(len(g.names)) for g, _ in geos)
+    return {"value": len(geos) / sum(times), "unit": "energies/s", "cores": os.cpu_count(), "kind": "port",
+            "sample": f"one oracle energy of each geometry of the step (N = {sizes}): "
+                      + ", ".join(f"{t:.2f} s" for t in times)}
 
 
 def run_reference(args, rank, world):
     """Reference arm: the reference (Fortran/MPI/ScaLAPACK) cannot be built in
-    this image, so its CPU path is the FP64 oracle port on the host cores."""
+    this image, so its CPU path is the FP64 oracle port on the host cores.
+    Each step is one oracle energy, cycling through the workload's geometries
+    in order; energies/s = the workload's energies over the summed mean time
+    of each of its geometries (every energy timed, nothing extrapolated)."""
     if rank != 0:
         return 0
     if WORKLOAD == "boxes":
         print(json.dumps({"impl": "reference", "metric": METRIC, "config": {"workload": workload_name()},
-                          "unavailable": "the FP64 oracle needs minutes per 200-atom box at these cut-offs; "
-                                         "not timed"}), flush=True)
+                          "unavailable": "the FP64 oracle needs hours per 2000-atom box at these cut-offs "
+                                         "(its long-range image sums are numpy loops); not timed"}), flush=True)
         return 0
-    vals, cb = [], None
-    for _ in range(max(1, args.steps)):
-        cb = cpu_baseline()
-        vals.append(cb["seconds_per_step"])
-    t = sum(vals)
-    value = cb["energies_per_step"] * len(vals) / t
+    geos = workload()
+    steps = max(1, args.steps)
+    per = {}
+    t_all = 0.0
+    for k in range(steps):
+        g = k % len(geos)
+        t = _oracle_energy(*geos[g])
+        per.setdefault(g, []).append(t)
+        t_all += t
+    if WORKLOAD == "batched":
+        value = steps / t_all
+        sample = f"oracle energies of the batch's first {min(steps, len(geos))} geometries (N ~ U{{20..600}})"
+    else:
+        mean = [statistics.mean(per[g]) for g in sorted(per)]
+        value = len(per) / sum(mean)
+        sample = ("one oracle energy per step, cycling through the step's geometries: "
+                  + ", ".join(f"N={len(geos[g][0].names)} {len(per[g])}x mean {statistics.mean(per[g]):.2f} s"
+                              for g in sorted(per)))
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "energies/s", "n_gpus": args.gpus,
-            "steps": len(vals), "warmup": 0, "ms_per_step": 1000 * t / len(vals), "higher_is_better": True,
+            "steps": steps, "warmup": 0, "ms_per_step": 1000 * t_all / steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "config": {"workload": workload_name()},
-            "cpu_baseline": {**{k: cb[k] for k in ("unit", "cores", "kind", "sample")}, "value": value},
+            "cpu_baseline": {"unit": "energies/s", "cores": os.cpu_count(), "kind": "port", "sample": sample,
+                             "value": value},
             "e2e": {"value": value, "unit": "energies/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
     return 0
@@ -222,8 +296,11 @@ def replica_rate(world, energies_per_step, steps, ms):
     return world * energies_per_step * steps / (ms / 1000.0)
 
 
-def time_mode(eng, stream, mode, steps, warmup, clocks=None):
-    """Device time of `steps` back-to-back mbd_rsscs_compute calls after warm-up."""
+def time_mode(eng, stream, mode, steps, warmup, clocks=None, flush=None):
+    """Device time of `steps` back-to-back mbd_rsscs_compute calls after
+    warm-up.  With `flush` (a device buffer larger than L2) the buffer is
+    rewritten before every step, outside the timed events, and the steps are
+    timed one by one."""
     import torch
     for _ in range(warmup):
         if eng.compute(mode) != 0:
@@ -232,16 +309,29 @@ def time_mode(eng, stream, mode, steps, warmup, clocks=None):
         if code != 0:
             raise SystemExit(f"compute({mode}) returned status {code}")
     torch.cuda.synchronize()
-    start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     ctx = clocks if clocks is not None else _Null()
     with ctx:
-        start.record(stream)
-        for _ in range(steps):
-            if eng.compute(mode) != 0:
-                raise SystemExit(f"compute({mode}) failed")
-        stop.record(stream)
-        stop.synchronize()
-    ms = start.elapsed_time(stop)
+        if flush is None:
+            start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            start.record(stream)
+            for _ in range(steps):
+                if eng.compute(mode) != 0:
+                    raise SystemExit(f"compute({mode}) failed")
+            stop.record(stream)
+            stop.synchronize()
+            ms = start.elapsed_time(stop)
+        else:
+            evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+                   for _ in range(steps)]
+            with torch.cuda.stream(stream):
+                for a, b in evs:
+                    flush.add_(1.0)
+                    a.record(stream)
+                    if eng.compute(mode) != 0:
+                        raise SystemExit(f"compute({mode}) failed")
+                    b.record(stream)
+            evs[-1][1].synchronize()
+            ms = sum(a.elapsed_time(b) for a, b in evs)
     stats = eng.stats()
     code, res = eng.download()
     if code != 0:
@@ -324,8 +414,8 @@ def roofline(stage_ms, sizes, mode):
     note = None
     if dom == "relay_solve" and mode == "mixed_learned":
         note = ("block-CG over the slots' overlapping streams (the stage time is summed over geometries); no "
-                "per-launch timing of its matrix pass cg_tile_kernel here -- ncu: 4.72 TB/s, 72 % of the measured "
-                "copy bandwidth (profiles/cg_tile_kernel_n3000.md)")
+                "per-launch timing of its matrix pass cg_tile_kernel here (ncu: 4.72 TB/s, 72 % of the measured "
+                "copy bandwidth on an n = 3000 relay batch)")
     return {"bound": "hbm", "kernel": dom, "achieved": None, "peak": peaks.get("hbm_gbs"), "unit": "GB/s",
             "frac": None, "traffic": None, "peak_source": src, "note": note, "stage_ms": stages}
 
@@ -394,6 +484,10 @@ def main():
                    "epochs": args.train_epochs, "train_seconds": time.perf_counter() - t0,
                    "loss_first_epoch": float(loss[0]), "loss_last_epoch": float(loss[-1])}
     stream = torch.cuda.ExternalStream(eng.stream_handle(), device=torch.device("cuda", local))
+    # the sheet's working set (25 MB of relay matrices) fits in the 126 MB L2:
+    # a 512 MB buffer is rewritten before every timed step
+    flush = torch.zeros(64 * 1024 * 1024, dtype=torch.float64, device=torch.device("cuda", local)) \
+        if WORKLOAD == "sheet" else None
     code = eng.upload([g for g, _ in geos], [s for _, s in geos])
     if code != 0:
         raise SystemExit(f"upload failed: {code}")
@@ -411,7 +505,7 @@ def main():
                 dist.barrier()
             if name == "learned_no_network":
                 eng.use_network(False)
-            xms, _, xres, xstage = time_mode(eng, stream, mode, args.steps, warmup)
+            xms, _, xres, xstage = time_mode(eng, stream, mode, args.steps, warmup, flush=flush)
             eng.use_network(True)
             xms = max_over_ranks(xms)
             extra[name] = {"value": replica_rate(world, len(geos), args.steps, xms), "ms_per_step": xms / args.steps,
@@ -419,7 +513,7 @@ def main():
     if args.mode != "plain" and not args.no_plain:
         if dist:
             dist.barrier()
-        pms, _, pres, pstage = time_mode(eng, stream, "plain", args.steps, warmup)
+        pms, _, pres, pstage = time_mode(eng, stream, "plain", args.steps, warmup, flush=flush)
         plain_res = pres
         pms = max_over_ranks(pms)
         plain = {"value": replica_rate(world, len(geos), args.steps, pms), "ms_per_step": pms / args.steps,
@@ -427,10 +521,12 @@ def main():
     if dist:
         dist.barrier()
     clk = ClockSampler(local)
-    ms, stats, res, stage = time_mode(eng, stream, args.mode, args.steps, warmup, clocks=clk)
+    ms, stats, res, stage = time_mode(eng, stream, args.mode, args.steps, warmup, clocks=clk, flush=flush)
     ms = max_over_ranks(ms)
     value = replica_rate(world, len(geos), args.steps, ms)
 
+    step_fl = fp64_step_flops(res)
+    step_tf = step_fl / (ms / args.steps / 1000.0) / 1e12
     line = {"metric": METRIC, "value": value, "unit": "energies/s", "n_gpus": world, "steps": args.steps,
             "warmup": warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None,
@@ -439,15 +535,40 @@ def main():
                     + "; no dataset exists for this path)",
             "config": {"workload": workload_name(),
                        "mode": args.mode, "parallelism": f"replicas{world}" if world > 1 else "1gpu",
-                       "l2": "working set 0.38-6.1 GB per geometry > 126 MB L2; no flush" if WORKLOAD != "boxes"
-                             else "working set 6.1-54 GB per geometry > 126 MB L2; no flush"},
+                       "l2": {"clusters": "working set 0.38-6.1 GB per geometry > 126 MB L2; no flush",
+                              "batched": "working set up to 0.54 GB per geometry, 25 GB per batch > 126 MB L2; "
+                                         "no flush",
+                              "boxes": "working set 6.1-54 GB per geometry > 126 MB L2; no flush",
+                              "sheet": "working set 25 MB < L2: a 512 MB buffer is rewritten before every timed "
+                                       "step (outside the timed events)"}[WORKLOAD]},
             "gpu_launches": stats["launches"] * args.steps,
             "roofline": roofline(stage, [len(g.names) for g, _ in geos], args.mode),
+            "roofline_step": {"bound": "fp64", "achieved": step_tf, "peak": FP64_NOMINAL_TFLOPS, "unit": "TFLOP/s",
+                              "frac": step_tf / FP64_NOMINAL_TFLOPS, "flop_per_step": step_fl,
+                              "algorithmic": "per energy 21 (3N)^3/3 + 126 (3N)^2 + (4/3)(3N n_SL)^3 FP64 flop "
+                                             "(the reference's Cholesky, solves and Hamiltonian reduction) / "
+                                             "device time of the whole step",
+                              "peak_source": "nominal FP64 (148 SM x 64 DFMA/clk x 2 x 1965 MHz); "
+                                             "MEASURED_PEAKS.json has no FP64 entry"},
             "energies": [r.energy for r in res][:8],
             "refine_iters": [r.refine_iters for r in res][:8],
             "stage_ms": dict(stage)}
     if learned is not None:
         line["learned"] = learned
+    if WORKLOAD == "sheet":
+        sr, lr = image_terms(*geos[0])
+        build_ms = stage.get("relay_build", 0.0) + stage.get("cfdm_build", 0.0)
+        line["image_sums"] = {"sr_terms_per_energy": sr, "lr_terms_per_energy": lr,
+                              "build_ms": build_ms,
+                              "build_ms_plain_fp64": (pstage.get("relay_build", 0.0) + pstage.get("cfdm_build", 0.0))
+                              if plain is not None else None,
+                              "build_ms_mixed_direct": (extra["mixed_direct"]["stage_ms"].get("relay_build", 0.0)
+                                                        + extra["mixed_direct"]["stage_ms"].get("cfdm_build", 0.0))
+                              if "mixed_direct" in extra else None,
+                              "terms_per_s": (sr + lr) / (build_ms / 1000.0) if build_ms > 0 else None,
+                              "note": "reference-equivalent (pair, image) terms of the short-range (x 21 "
+                                      "frequencies) and long-range image sums / device time of the relay and "
+                                      "CFDM tensor builds"}
     line.update(extra)
     if plain is not None:
         line["plain_fp64"] = plain

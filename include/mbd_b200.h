@@ -191,6 +191,36 @@ int mbd_rsscs_last_stats(mbd_ctx* ctx, double* out, int n);
  * caller can record its own events around mbd_rsscs_compute. */
 void* mbd_rsscs_stream(mbd_ctx* ctx);
 
+/* ---- options --------------------------------------------------------------
+ * (No counterpart in the reference, which ignores PDPOTRF's info at
+ * UTILS.f90:469 and has no device waits.)  Failure handling of the engine:
+ *   MBD_OPT_RESIDUAL_GATE    relative relay residual ||B - A X||_F / ||B||_F
+ *                            that the MIXED and MIXED_LEARNED solves must reach
+ *                            at every frequency for their result to be used
+ *                            (default 1e-10).  A geometry that misses it is
+ *                            recomputed with the direct FP64 solve, and its
+ *                            mbd_result.refine_iters is -1.  0 sends every
+ *                            geometry to that fallback.
+ *   MBD_OPT_WAIT_LIMIT_S     seconds a bounded device-side wait (flag polls,
+ *                            group barriers, mbarrier waits) may spin before
+ *                            the launch gives up and the compute reports
+ *                            MBD_ERR_TIMEOUT (default 2; 0 < value <= 60).
+ *                            Per device: shared by every context on it.
+ *   MBD_OPT_TEST_STALL_WAIT  1: the batch's band -> tridiagonal launch makes
+ *                            its first sweep wait for a count that no sweep
+ *                            reaches, so that its bounded wait runs out and the
+ *                            compute reports MBD_ERR_TIMEOUT; the context stays
+ *                            usable.  For testing failure detection; 0 (the
+ *                            default) turns it off.
+ * set_option returns MBD_ERR_ARG for an unknown option or a value out of range. */
+enum {
+    MBD_OPT_RESIDUAL_GATE = 1,
+    MBD_OPT_WAIT_LIMIT_S = 2,
+    MBD_OPT_TEST_STALL_WAIT = 3
+};
+int mbd_rsscs_set_option(mbd_ctx* ctx, int option, double value);
+int mbd_rsscs_get_option(mbd_ctx* ctx, int option, double* value);
+
 /* ---- learned warm start of MBD_MODE_MIXED_LEARNED -----------------------
  * (No counterpart in the reference, which solves the relay system directly
  * at UTILS.f90:469-473.)  A message-passing network (3 layers, 64 hidden,

@@ -350,7 +350,7 @@ int band_to_tridiag_single(mbd_ctx* ctx, double* Br, int n, double* d, double* e
   MBD_CUDA(cudaStreamSynchronize(s));   // the pageable source must outlive the copy
   MBD_CUDA(launch_sb2st(reinterpret_cast<BandJob*>(base), 1, reinterpret_cast<SweepItem*>(base + b_job),
                         (int)items.size(), reinterpret_cast<int*>(base + b_job + b_it), ctx->err_flag,
-                        ctx->num_sms, n, n / (2 * kBand) + 1, s));
+                        ctx->num_sms, n, n / (2 * kBand) + 1, -1, s));
   ctx->launches += 3;
   return MBD_OK;
 }
@@ -761,7 +761,7 @@ int enqueue_batch(mbd_ctx* ctx, int mode) {
   if (ctx->n_band_jobs > 0) {
     MBD_CUDA(launch_sb2st(ctx->band_jobs, ctx->n_band_jobs, ctx->sweep_items, ctx->n_sweep_items,
                           ctx->sweep_progress.as<int>(), ctx->err_flag, ctx->num_sms, ctx->band_max_n,
-                          ctx->sweeps_in_flight, s));
+                          ctx->sweeps_in_flight, ctx->test_stall_wait ? 0 : -1, s));
     ctx->launches += 3;
   }
   record_timing(ctx, ctx->bev[2], s);
@@ -1000,9 +1000,9 @@ int mbd_rsscs_download(mbd_ctx* ctx, mbd_result* out) {
         double most = 0.0;
         for (int f = 0; f < kNFreq; ++f) most = std::max(most, cs[(size_t)f * kCgState + 1]);
         r.refine_iters = (int)most;
-        gd->cg_iters_seen = (worst <= kResidualGate) ? (int)most : 0;
+        gd->cg_iters_seen = (worst <= ctx->residual_gate) ? (int)most : 0;
       }
-      if (!(worst <= kResidualGate)) {
+      if (!(worst <= ctx->residual_gate)) {
         int st = run_front(ctx, gd, (int)g, MBD_MODE_PLAIN_FP64);
         if (st == MBD_OK) st = run_tail_single(ctx, gd, ctx->slots[gd->slot]->stream);
         if (st != MBD_OK) return st;
@@ -1168,6 +1168,53 @@ int mbd_rsscs_last_stats(mbd_ctx* ctx, double* out, int n) {
 }
 
 void* mbd_rsscs_stream(mbd_ctx* ctx) { return ctx ? (void*)ctx->stream : nullptr; }
+
+int mbd_rsscs_set_option(mbd_ctx* ctx, int option, double value) {
+  if (!ctx) return MBD_ERR_ARG;
+  switch (option) {
+    case MBD_OPT_RESIDUAL_GATE:
+      if (!(value >= 0.0)) return MBD_ERR_ARG;
+      ctx->residual_gate = value;
+      return MBD_OK;
+    case MBD_OPT_WAIT_LIMIT_S: {
+      if (!(value > 0.0 && value <= 60.0)) return MBD_ERR_ARG;
+      // clock64 counts SM cycles: seconds x the device's maximum SM clock
+      int khz = 0;
+      MBD_CUDA(cudaSetDevice(ctx->device));
+      MBD_CUDA(cudaDeviceGetAttribute(&khz, cudaDevAttrClockRate, ctx->device));
+      const long long cycles = std::max(1LL, (long long)(value * 1e3 * (double)khz));
+      MBD_CUDA(cudaDeviceSynchronize());   // no launch of this device reads the limit meanwhile
+      MBD_CUDA(set_wait_limit_sb2st(cycles));
+      MBD_CUDA(set_wait_limit_tridiag(cycles));
+      MBD_CUDA(set_wait_limit_mixed(cycles));
+      MBD_CUDA(set_wait_limit_tc3(cycles));
+      ctx->wait_limit_s = value;
+      return MBD_OK;
+    }
+    case MBD_OPT_TEST_STALL_WAIT: {
+      const int on = value != 0.0;
+      if (on != ctx->test_stall_wait) {
+        MBD_CUDA(cudaSetDevice(ctx->device));
+        MBD_CUDA(cudaDeviceSynchronize());
+        drop_graphs(ctx);   // the captured launches carry the old setting
+      }
+      ctx->test_stall_wait = on;
+      return MBD_OK;
+    }
+    default:
+      return MBD_ERR_ARG;
+  }
+}
+
+int mbd_rsscs_get_option(mbd_ctx* ctx, int option, double* value) {
+  if (!ctx || !value) return MBD_ERR_ARG;
+  switch (option) {
+    case MBD_OPT_RESIDUAL_GATE: *value = ctx->residual_gate; return MBD_OK;
+    case MBD_OPT_WAIT_LIMIT_S: *value = ctx->wait_limit_s; return MBD_OK;
+    case MBD_OPT_TEST_STALL_WAIT: *value = ctx->test_stall_wait; return MBD_OK;
+    default: return MBD_ERR_ARG;
+  }
+}
 
 int mbd_rsscs_last_timings(mbd_ctx* ctx, double* ms, int n) {
   if (!ctx || !ms || n < Stage::kCount) return MBD_ERR_ARG;

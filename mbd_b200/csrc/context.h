@@ -157,6 +157,10 @@ struct mbd_ctx {
   double launches = 0, h2d_bytes = 0, d2h_bytes = 0;
   int last_mode = 0;
   bool have_batch = false;
+  // options (mbd_rsscs_set_option)
+  double residual_gate = mbd::kResidualGate;   // accepted ||B - A X||_F / ||B||_F of the fast relay solves
+  double wait_limit_s = 2.0;                   // bounded device waits (per device)
+  int test_stall_wait = 0;                     // 1: the bulge-chasing launch's first wait runs out
 };
 
 namespace mbd {

@@ -13,6 +13,7 @@
 #include <algorithm>
 
 #include "tc3.h"
+#include "wait_limit.cuh"
 #include "../../include/mbd_b200.h"
 
 namespace mbd {
@@ -20,7 +21,6 @@ namespace {
 
 constexpr int NB = kMixNB;   // 128
 constexpr int LDS = NB + 1;
-constexpr long long kSpinCycles = 4000000000LL;
 
 __device__ __forceinline__ float tf32_hi(float x) { return __uint_as_float(__float_as_uint(x) & 0xFFFFE000u); }
 
@@ -108,9 +108,10 @@ struct SolveArgs {
 };
 
 __device__ bool wait_flag(const int* f, int epoch, int* err) {
+  const long long lim = wait_limit_cycles();
   const long long t0 = clock64();
   while (*(volatile const int*)f != epoch) {
-    if (*(volatile int*)err != 0 || clock64() - t0 > kSpinCycles) {
+    if (*(volatile int*)err != 0 || clock64() - t0 > lim) {
       atomicCAS(err, 0, MBD_ERR_TIMEOUT);
       return false;
     }
@@ -390,5 +391,7 @@ void launch_relay_residual(const double* A64, size_t a_stride, int ld, int n, in
   res_reduce_kernel<<<dim3(nt, batch), 192, 0, s>>>(partial, nt, n, R, ystride, normpart);
   norm_final_kernel<<<batch, 32, 0, s>>>(normpart, nt, rnorm2);
 }
+
+MBD_WAIT_LIMIT_SETTER(set_wait_limit_mixed)
 
 }  // namespace mbd

@@ -27,6 +27,7 @@
 #include <algorithm>
 
 #include "kernels.h"
+#include "wait_limit.cuh"
 #include "../../include/mbd_b200.h"
 
 namespace mbd {
@@ -35,7 +36,6 @@ namespace {
 constexpr int B = kBand;
 constexpr int LD = kBandLd;
 constexpr int WARPS = 4;
-constexpr long long kSpinCycles = 4000000000LL;   // ~2 s, then the wait gives up
 
 // Shared memory of one warp pair (one sweep item): the reflector of the
 // current and of the next task (double-buffered by task parity), D-warp and
@@ -77,11 +77,12 @@ __device__ bool wait_progress(const int* p, int target, int* err) {
     // exponential back-off so that far-behind warps do not load the L2; the
     // error flag and the clock are read every 64 polls (an extra load per poll
     // would sit behind the acquire and double the detection latency)
+    const long long lim = wait_limit_cycles();
     const long long t0 = clock64();
     unsigned ns = 0, polls = 0;
     while (ld_acquire(p) < target) {
       if ((++polls & 63u) == 0) {
-        if (*(volatile int*)err != 0 || clock64() - t0 > kSpinCycles) {
+        if (*(volatile int*)err != 0 || clock64() - t0 > lim) {
           atomicCAS(err, 0, MBD_ERR_TIMEOUT);
           ok = 0;
           break;
@@ -121,7 +122,8 @@ __device__ __forceinline__ double make_reflector(double x, int len, double* v, d
 // next reflector, left apply); they meet at a named barrier once per task.
 constexpr int PAIRS = WARPS / 2;
 __global__ void __launch_bounds__(WARPS * 32) sb2st_kernel(const BandJob* jobs, const SweepItem* items,
-                                                           int n_items, int* progress, int* err) {
+                                                           int n_items, int* progress, int* err,
+                                                           int stall_item) {
   __shared__ PairSmem psm[PAIRS];
   const int warp = threadIdx.x / 32, l = threadIdx.x & 31;
   const int pair = warp / 2;
@@ -141,7 +143,11 @@ __global__ void __launch_bounds__(WARPS * 32) sb2st_kernel(const BandJob* jobs, 
       // D-warp follows it through the barrier (one verdict, both warps leave
       // together)
       if (owarp) {
-        const bool ok = it.pred < 0 || wait_progress(progress + it.pred, min(k + 2, Kp), err);
+        bool ok;
+        if (t == stall_item && k == 0)   // a count nothing reaches: the wait runs out
+          ok = wait_progress(progress + t, 1 << 30, err);
+        else
+          ok = it.pred < 0 || wait_progress(progress + it.pred, min(k + 2, Kp), err);
         if (l == 0) S.go = ok;
       }
       pair_sync(pair);
@@ -282,7 +288,8 @@ int sb2st_max_ctas(int num_sms) {
 }
 
 cudaError_t launch_sb2st(const BandJob* jobs, int n_jobs, const SweepItem* items, int n_items, int* progress,
-                         int* err, int num_sms, int max_n, long long sweeps_in_flight, cudaStream_t s) {
+                         int* err, int num_sms, int max_n, long long sweeps_in_flight, int stall_item,
+                         cudaStream_t s) {
   if (n_jobs < 1) return cudaSuccess;
   if (n_items > 0) {
     cudaError_t e = cudaMemsetAsync(progress, 0, sizeof(int) * (size_t)n_items, s);
@@ -293,12 +300,14 @@ cudaError_t launch_sb2st(const BandJob* jobs, int n_jobs, const SweepItem* items
     const long long want_pairs = 3LL * sweeps_in_flight + 4 * PAIRS;
     const int need = (int)((std::min<long long>(want_pairs, n_items) + PAIRS - 1) / PAIRS);
     if (grid > need) grid = need;
-    void* args[] = {(void*)&jobs, (void*)&items, (void*)&n_items, (void*)&progress, (void*)&err};
+    void* args[] = {(void*)&jobs, (void*)&items, (void*)&n_items, (void*)&progress, (void*)&err, (void*)&stall_item};
     e = cudaLaunchCooperativeKernel((const void*)sb2st_kernel, dim3(grid), dim3(WARPS * 32), args, 0, s);
     if (e != cudaSuccess) return e;
   }
   extract_kernel<<<dim3((max_n + 255) / 256, n_jobs), 256, 0, s>>>(jobs);
   return cudaGetLastError();
 }
+
+MBD_WAIT_LIMIT_SETTER(set_wait_limit_sb2st)
 
 }  // namespace mbd

@@ -26,6 +26,7 @@
 #include <cstdint>
 
 #include "kernels.h"
+#include "wait_limit.cuh"
 #include "tc3.h"
 #include "../../include/mbd_b200.h"
 
@@ -37,7 +38,6 @@ constexpr int STAGES = 3;                    // 97 KB: two CTAs per SM overlap e
 constexpr int TILE_BYTES = BM * BK * 4;      // 16 KB
 constexpr int STAGE_BYTES = 2 * TILE_BYTES;
 constexpr int TMEM_COLS = 128;
-constexpr long long kWaitCycles = 4000000000LL;
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
   return static_cast<uint32_t>(__cvta_generic_to_shared(p));
@@ -53,6 +53,7 @@ __device__ __forceinline__ void mbar_expect_tx(uint32_t bar, uint32_t bytes) {
 
 // Bounded wait for phase `parity` of an mbarrier.
 __device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, int* err) {
+  const long long lim = wait_limit_cycles();
   const long long t0 = clock64();
   while (true) {
     uint32_t done;
@@ -64,7 +65,7 @@ __device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, int* er
         : "r"(bar), "r"(parity)
         : "memory");
     if (done) return true;
-    if (clock64() - t0 > kWaitCycles || *(volatile int*)err != 0) {
+    if (clock64() - t0 > lim || *(volatile int*)err != 0) {
       atomicCAS(err, 0, MBD_ERR_TIMEOUT);
       return false;
     }
@@ -367,5 +368,7 @@ bool make_tc3_map(CUtensorMap* map, const float* base, int rows, int cols, int l
                   CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
   return r == CUDA_SUCCESS;
 }
+
+MBD_WAIT_LIMIT_SETTER(set_wait_limit_tc3)
 
 }  // namespace mbd

@@ -21,6 +21,7 @@
 #include <cstdint>
 
 #include "kernels.h"
+#include "wait_limit.cuh"
 #include "../../include/mbd_b200.h"
 
 namespace mbd {
@@ -32,7 +33,6 @@ constexpr int THREADS = 512;
 constexpr int NWARP = THREADS / 32;
 constexpr int SLOTS = 2;      // tiles per CTA per round (8 warps x 8 rows each)
 constexpr int TILE_DBL = SLOTS * T * T;   // doubles of one staging buffer (64 KB)
-constexpr long long kSpinCycles = 4000000000LL;   // ~2 s at 2 GHz, then give up
 constexpr int kMaxG = kTridiagMaxGroup;   // largest group (CTAs) the cross-CTA reductions unroll for
 
 struct GroupWS {
@@ -103,12 +103,13 @@ __device__ bool group_sync(unsigned* bar, int G, unsigned& gen, int* err) {
       asm volatile("st.relaxed.gpu.u32 [%0], 0;" ::"l"(bar) : "memory");
       asm volatile("st.release.gpu.u32 [%0], %1;" ::"l"(bar + 1), "r"(target) : "memory");
     } else {
+      const long long lim = wait_limit_cycles();
       const long long t0 = clock64();
       while (true) {
         unsigned cur;
         asm volatile("ld.acquire.gpu.u32 %0, [%1];" : "=r"(cur) : "l"(bar + 1) : "memory");
         if (cur == target) break;
-        if (*(volatile int*)err != 0 || clock64() - t0 > kSpinCycles) {
+        if (*(volatile int*)err != 0 || clock64() - t0 > lim) {
           ok = 0;
           atomicCAS(err, 0, MBD_ERR_TIMEOUT);
           break;
@@ -749,5 +750,7 @@ cudaError_t launch_tridiag_groups(const TridiagJob* jobs_dev, const TridiagGroup
   return cudaLaunchCooperativeKernel((const void*)tridiag_kernel, dim3(total_ctas), dim3(THREADS), args,
                                      kTridiagDynSmem, s);
 }
+
+MBD_WAIT_LIMIT_SETTER(set_wait_limit_tridiag)
 
 }  // namespace mbd

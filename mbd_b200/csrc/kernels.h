@@ -185,8 +185,11 @@ struct SweepItem {
 };
 // sweeps_in_flight: sum over jobs of n / (2 kBand), the concurrency the
 // sweep pipeline offers (sizes the worker count).
+// stall_item >= 0 makes that item's first wait target a count no sweep
+// reaches, so the bounded wait runs out (failure-detection tests only).
 cudaError_t launch_sb2st(const BandJob* jobs, int n_jobs, const SweepItem* items, int n_items, int* progress,
-                         int* err, int num_sms, int max_n, long long sweeps_in_flight, cudaStream_t s);
+                         int* err, int num_sms, int max_n, long long sweeps_in_flight, int stall_item,
+                         cudaStream_t s);
 cudaError_t init_sb2st_attributes();
 
 // ---- block-CG relay solve of the MIXED_LEARNED mode (UTILS.f90:469-473) ----
@@ -226,5 +229,12 @@ constexpr int kEigBatchMaxN = 12800;    // d and e^2 staged in shared memory
 // jobs with n <= kEigBatchMaxN only; max_n the largest n among them.
 void launch_eigen_batch(const EigJob* jobs_dev, int n_jobs, int max_n, cudaStream_t s);
 void launch_energy_batch(const EigJob* jobs_dev, int n_jobs, cudaStream_t s);
+
+// Limit (SM clock cycles) of the bounded device-side waits of each
+// translation unit that has them (wait_limit.cuh); per device.
+cudaError_t set_wait_limit_sb2st(long long cycles);
+cudaError_t set_wait_limit_tridiag(long long cycles);
+cudaError_t set_wait_limit_mixed(long long cycles);
+cudaError_t set_wait_limit_tc3(long long cycles);
 
 }  // namespace mbd

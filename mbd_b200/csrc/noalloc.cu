@@ -80,6 +80,9 @@ extern "C" int mbd_rsscs_eigvalsh_noalloc(double* H, int n, int ld, double* w, v
   if (n > kNoAllocMaxN) return MBD_ERR_TOO_LARGE;
   // 16-byte row starts for the kernel's vector copies
   if ((ld % 2) != 0 || (reinterpret_cast<uintptr_t>(H) % 16) != 0) return MBD_ERR_ARG;
+  // a launch error left behind by the caller's own earlier work is not this
+  // call's: clear it so that the check after the launches sees only ours
+  (void)cudaGetLastError();
   int dev = 0;
   if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return MBD_ERR_DEVICE;
   DeviceSetup* ds = nullptr;
@@ -103,8 +106,10 @@ extern "C" int mbd_rsscs_eigvalsh_noalloc(double* H, int n, int ld, double* w, v
   if (launch_tridiag(job, 1, 1, G, ws, wsb, n, err, s) != cudaSuccess) return MBD_ERR_DEVICE;
   launch_tridiag_eigenvalues_scratch(d, e, n, w, e2, s);
   if (cudaGetLastError() != cudaSuccess) return MBD_ERR_DEVICE;
-  if (cudaStreamSynchronize(s) != cudaSuccess) return MBD_ERR_DEVICE;
+  // the error flag comes back on the caller's stream (a synchronous copy on
+  // the legacy stream would also wait for unrelated work on the device)
   int herr = 0;
-  if (cudaMemcpy(&herr, err, sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess) return MBD_ERR_DEVICE;
+  if (cudaMemcpyAsync(&herr, err, sizeof(int), cudaMemcpyDeviceToHost, s) != cudaSuccess) return MBD_ERR_DEVICE;
+  if (cudaStreamSynchronize(s) != cudaSuccess) return MBD_ERR_DEVICE;
   return herr ? herr : MBD_OK;
 }

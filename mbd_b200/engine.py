@@ -38,7 +38,9 @@ EXPORTED = [
     "mbd_rsscs_stream", "mbd_rsscs_eigvalsh", "mbd_rsscs_eigvalsh_noalloc",
     "mbd_rsscs_learned_param_count", "mbd_rsscs_learned_train", "mbd_rsscs_learned_get_params",
     "mbd_rsscs_learned_set_params", "mbd_rsscs_learned_use_network", "mbd_rsscs_learned_eval",
+    "mbd_rsscs_set_option", "mbd_rsscs_get_option",
 ]
+OPTIONS = {"residual_gate": 1, "wait_limit_s": 2, "test_stall_wait": 3}
 
 
 class MbdError(RuntimeError):
@@ -136,6 +138,10 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
     lib.mbd_rsscs_learned_get_params.restype = ctypes.c_int
     lib.mbd_rsscs_learned_set_params.argtypes = [vp, fp, ctypes.c_int]
     lib.mbd_rsscs_learned_set_params.restype = ctypes.c_int
+    lib.mbd_rsscs_set_option.argtypes = [vp, ctypes.c_int, ctypes.c_double]
+    lib.mbd_rsscs_set_option.restype = ctypes.c_int
+    lib.mbd_rsscs_get_option.argtypes = [vp, ctypes.c_int, ctypes.POINTER(ctypes.c_double)]
+    lib.mbd_rsscs_get_option.restype = ctypes.c_int
     lib.mbd_rsscs_learned_use_network.argtypes = [vp, ctypes.c_int]
     lib.mbd_rsscs_learned_use_network.restype = ctypes.c_int
     lib.mbd_rsscs_learned_eval.argtypes = [vp, fp, ctypes.c_int, ctypes.c_int, ip, ip, fp, fp, fp, fp, fp, dp]
@@ -326,6 +332,19 @@ class Engine:
                                                      p.size)
         if code != MBD_OK:
             raise MbdError(code, strerror(code))
+
+    def set_option(self, name: str, value: float) -> None:
+        """mbd_rsscs_set_option: residual_gate, wait_limit_s, test_stall_wait."""
+        code = self.lib.mbd_rsscs_set_option(self.ctx, OPTIONS[name], float(value))
+        if code != MBD_OK:
+            raise MbdError(code, strerror(code))
+
+    def get_option(self, name: str) -> float:
+        v = ctypes.c_double()
+        code = self.lib.mbd_rsscs_get_option(self.ctx, OPTIONS[name], ctypes.byref(v))
+        if code != MBD_OK:
+            raise MbdError(code, strerror(code))
+        return v.value
 
     def use_network(self, on: bool) -> None:
         self.lib.mbd_rsscs_learned_use_network(self.ctx, 1 if on else 0)

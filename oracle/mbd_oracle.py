@@ -8,9 +8,13 @@ and has no CPU fallback.
 It restates, in vectorised numpy + LAPACK (scipy), the algorithm of
 ``UTILS.f90:153-1320`` (the reference's ``MBD_at_rsSCS``) literally:
 
-* every periodic image inside the box ``ceil(cutoff/|a_k|)`` is visited and
-  tested against ``r <= cutoff`` (``UTILS.f90:561-579``, ``610-631``,
-  ``1016-1035``, ``1073-1092``) -- no damping cut-off, no pruning;
+* every periodic image inside the box ``ceil(cutoff/|a_k|)`` is tested
+  against ``r <= cutoff`` (``UTILS.f90:561-579``, ``610-631``,
+  ``1016-1035``, ``1073-1092``) and summed; the only images left out are
+  short-range ones whose damping factor ``1 - 1/(1 + exp(-6(x - 1)))`` is
+  exactly 0.0 in FP64 (``ZERO_DAMP_X``), which add exact zeros in the
+  reference -- ``tests/test_oracle_golden.py`` checks that leaving them out
+  changes no bit;
 * only the lower triangle of the relay matrix / CFDM Hamiltonian is filled
   (``UTILS.f90:427-431``, ``799-803``) and the dense LAPACK calls read the
   lower triangle (``PDPOTRF('L')``/``PDPOTRS`` at ``UTILS.f90:469,473``,
@@ -326,16 +330,36 @@ def _pair_image_geometry(coords, ii, jj, shifts, cut, self_pairs):
     return p_idx, d[p_idx, s_idx].T, r[p_idx, s_idx]
 
 
+# An image whose Fermi factor 1 - 1/(1 + exp(-6 (r/(beta R) - 1))) rounds to
+# exactly 0.0 in FP64 adds an exact zero to the reference's image sum
+# (UTILS.f90:692): once exp(-6 (x - 1)) < 2^-53, 1 + exp(...) == 1.0.  Beyond
+# x = r/(beta R) > ZERO_DAMP_X, exp(-6 (x - 1)) < exp(-37.5) = 5.2e-17 < 2^-53,
+# so the sum does not change bit for bit when those images are left out.
+ZERO_DAMP_X = 1.0 + 37.5 / 6.0
+
+
 def relay_matrices(sysd: _System, freqs=range(N_FREQ), chunk_elems=4_000_000):
     """Lower-filled relay matrices A(iw_f) = alpha^-1 + T_SR for the given
     frequency indices (get_screened_alpha UTILS.f90:415-441 with
     scs_diag_block 543-587 and scs_offdiag_block 591-633).
+
+    Every image of the reference's box that passes ``r <= cutoff`` is summed,
+    except those whose short-range damping factor is exactly 0.0 in FP64
+    (r > ZERO_DAMP_X * beta * R12): they add exact zeros in the reference.
     Returns (matrices dict f -> (3N,3N) array with lower triangle filled,
     alpha_omega dict f -> (N,))."""
     N = sysd.N
     freqs = list(freqs)
     _, shifts = image_vectors(sysd.scs_rng, sysd.lat)
     cut = sysd.st.mbd_scs_dip_cutoff / BOHR
+    beta = sysd.beta
+    rzero_atom = ZERO_DAMP_X * beta * sysd.rvdw_iso          # half of a pair's zero-damping radius
+    if len(shifts) > 1:
+        # images that can bring any pair inside min(cut, zero-damping radius)
+        span = np.ptp(sysd.coords, axis=0)
+        reach = min(cut, 2.0 * float(np.max(rzero_atom))) + float(np.sqrt(np.sum(span * span)))
+        r_sh = np.sqrt(np.sum(shifts * shifts, axis=1))
+        shifts = shifts[r_sh <= reach]
     alpha_w, sgm = {}, {}
     for f in freqs:
         alpha_w[f], sgm[f] = alpha_and_sigma(sysd.hirsh, sysd.c6free, sysd.alpha0, CASIMIR_OMEGA[f])
@@ -346,11 +370,13 @@ def relay_matrices(sysd: _System, freqs=range(N_FREQ), chunk_elems=4_000_000):
     for s in range(0, len(ii), per):
         pi_, pj_ = ii[s:s + per], jj[s:s + per]
         p_idx, d, r = _pair_image_geometry(sysd.coords, pi_, pj_, shifts, cut, False)
+        keep = r <= rzero_atom[pi_[p_idx]] + rzero_atom[pj_[p_idx]]
+        p_idx, d, r = p_idx[keep], d[:, keep], r[keep]
         gi, gj = pi_[p_idx], pj_[p_idx]
         r12 = sysd.rvdw_iso[gi] + sysd.rvdw_iso[gj]
         for f in freqs:
             s12 = np.sqrt(sgm[f][gi] * sgm[f][gi] + sgm[f][gj] * sgm[f][gj])
-            t6 = gaussian_dipole_tensor6(d, r, s12, r12, sysd.beta)
+            t6 = gaussian_dipole_tensor6(d, r, s12, r12, beta)
             acc = np.zeros((6, len(pi_)))
             for c in range(6):
                 acc[c] = np.bincount(p_idx, weights=t6[c], minlength=len(pi_))
@@ -358,16 +384,19 @@ def relay_matrices(sysd: _System, freqs=range(N_FREQ), chunk_elems=4_000_000):
     # diagonal blocks: images n != 0 of the atom itself, sigma_12 = sigma_i (UTILS.f90:571)
     if len(shifts) > 1:
         r_s = np.sqrt(np.sum(shifts * shifts, axis=1))
-        keep = (r_s <= cut) & (r_s > 0.0)
+        keep = (r_s <= cut) & (r_s > 0.0) & (r_s <= 2.0 * float(np.max(rzero_atom)))
         ds, rs = shifts[keep].T, r_s[keep]
     else:
         ds, rs = np.zeros((3, 0)), np.zeros(0)
+    # (atom, image) pairs inside the atom's own zero-damping radius 2 rzero_i
+    a_idx, s_idx = np.nonzero(rs[None, :] <= 2.0 * rzero_atom[:, None])
+    dd, rr = ds[:, s_idx], rs[s_idx]
     for f in freqs:
         acc = np.zeros((6, N))
-        if len(rs):
-            for i in range(N):
-                t6 = gaussian_dipole_tensor6(ds, rs, sgm[f][i], 2.0 * sysd.rvdw_iso[i], sysd.beta)
-                acc[:, i] = t6.sum(axis=1)
+        if len(rr):
+            t6 = gaussian_dipole_tensor6(dd, rr, sgm[f][a_idx], 2.0 * sysd.rvdw_iso[a_idx], beta)
+            for c in range(6):
+                acc[c] = np.bincount(a_idx, weights=t6[c], minlength=N)
         inv = 1.0 / alpha_w[f]
         acc[0] += inv
         acc[3] += inv

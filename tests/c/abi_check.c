@@ -33,6 +33,12 @@ int main(void) {
     puts("strerror: FAIL");
     bad = 1;
   }
+  double v = 0.0;
+  if (mbd_rsscs_set_option(NULL, MBD_OPT_RESIDUAL_GATE, 0.0) != MBD_ERR_ARG ||
+      mbd_rsscs_get_option(NULL, MBD_OPT_WAIT_LIMIT_S, &v) != MBD_ERR_ARG) {
+    puts("options without a context: FAIL");
+    bad = 1;
+  }
   /* without a GPU the context cannot be created; with one it must be */
   mbd_ctx* ctx = NULL;
   const int st = mbd_rsscs_create(&ctx, 0);

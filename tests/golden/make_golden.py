@@ -1,9 +1,9 @@
 """Generate the golden fixtures under tests/golden/ from the reference tree.
 
-Run once in a container that has the reference checkout (path given as the
-first argument, default /root/reference):
+Run once in a container that has the reference checkout; its root is the
+required first argument:
 
-    python tests/golden/make_golden.py /root/reference
+    python tests/golden/make_golden.py <reference checkout>
 
 For every example it writes ``<name>.json`` holding
   * the geometry and settings exactly as the reference run read them
@@ -125,7 +125,9 @@ def main(ref_root: str) -> None:
 
 if __name__ == "__main__":
     args = [a for a in sys.argv[1:] if not a.startswith("--")]
-    root = args[0] if args else "/root/reference"
+    if not args:
+        sys.exit("usage: make_golden.py <reference checkout> [--report-only]")
+    root = args[0]
     if "--report-only" in sys.argv:
         add_report_lines(root)
     else:

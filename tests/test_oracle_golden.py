@@ -95,3 +95,21 @@ def test_image_ranges_graphene():
     assert list(sysd.scs_rng) == [10, 10, 8]
     assert list(sysd.supercell) == [2, 2, 2]
     assert list(sysd.cfdm_rng) == [5, 4, 4]
+
+
+def test_zero_damping_skip_changes_no_bit(monkeypatch):
+    """Images left out of the short-range sum because their damping factor is
+    exactly 0.0 in FP64 contribute exact zeros: the relay matrices are the same
+    bit for bit with and without the skip (periodic box, every image of the
+    reference's box visited in the second build)."""
+    from mbd_b200 import synthetic as sy
+    g, s = sy.periodic_box(40, seed=7, scs_cut=40.0, cfdm_cut=20.0, sc_cut=5.0)
+    geo = mo.Geometry(list(g.names), g.coords, g.hirshfeld, g.lattice, g.n_periodic)
+    st = mo.Settings(mbd_supercell_cutoff=s.mbd_supercell_cutoff, mbd_cfdm_dip_cutoff=s.mbd_cfdm_dip_cutoff,
+                     mbd_scs_dip_cutoff=s.mbd_scs_dip_cutoff)
+    sysd = mo._System(geo, st)
+    fast, _ = mo.relay_matrices(sysd, freqs=[0, 7])
+    monkeypatch.setattr(mo, "ZERO_DAMP_X", float("inf"))
+    full, _ = mo.relay_matrices(sysd, freqs=[0, 7])
+    for f in (0, 7):
+        assert np.array_equal(fast[f], full[f])

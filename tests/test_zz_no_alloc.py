@@ -16,6 +16,7 @@ import pytest
 
 pytestmark = pytest.mark.gpu
 
+MBD_ERR_ARG = 1
 MBD_ERR_TOO_LARGE = 11
 
 
@@ -36,17 +37,30 @@ def test_noalloc_matches_allocating_entry_point_twice():
     fn.restype = ctypes.c_int
     max_n = 2048
     with Engine(0) as eng:
-        for call, n in enumerate((700, max_n)):
+        # small, largest, then small again (a smaller call after a larger one
+        # must not see the larger call's leftovers in the shared scratch);
+        # the last call uses a padded leading dimension
+        for call, (n, ld) in enumerate(((700, 700), (max_n, max_n), (700, 702))):
             S = _sym(n, seed=100 + call)
             ref = eng.eigvalsh(np.tril(S))                       # allocating entry point
-            H = torch.tensor(S, dtype=torch.float64, device="cuda")   # caller-owned device buffers
+            lapack = np.linalg.eigvalsh(S)                       # LAPACK on the host
+            Hp = np.zeros((n, ld))
+            Hp[:, :n] = S
+            H = torch.tensor(Hp, dtype=torch.float64, device="cuda")   # caller-owned device buffers
             w = torch.empty(n, dtype=torch.float64, device="cuda")
             torch.cuda.synchronize()
-            code = fn(H.data_ptr(), n, n, w.data_ptr(), torch.cuda.current_stream().cuda_stream)
+            code = fn(H.data_ptr(), n, ld, w.data_ptr(), torch.cuda.current_stream().cuda_stream)
             assert code == 0, code
             got = w.cpu().numpy()
             # same tolerance as the eigenvalue parity tests
-            np.testing.assert_allclose(got, ref, rtol=0, atol=1e-12 * max(1.0, np.abs(ref).max()) * n)
+            tol = 1e-12 * max(1.0, np.abs(ref).max()) * n
+            np.testing.assert_allclose(got, ref, rtol=0, atol=tol)
+            np.testing.assert_allclose(got, lapack, rtol=0, atol=tol)
         big = torch.zeros((max_n + 2, max_n + 2), dtype=torch.float64, device="cuda")
         wb = torch.empty(max_n + 2, dtype=torch.float64, device="cuda")
         assert fn(big.data_ptr(), max_n + 2, max_n + 2, wb.data_ptr(), None) == MBD_ERR_TOO_LARGE
+        # an odd leading dimension and a matrix start off the 16-byte grid are refused
+        small = torch.zeros((64, 66), dtype=torch.float64, device="cuda")
+        ws = torch.empty(64, dtype=torch.float64, device="cuda")
+        assert fn(small.data_ptr(), 63, 65, ws.data_ptr(), None) == MBD_ERR_ARG
+        assert fn(small.data_ptr() + 8, 64, 64, ws.data_ptr(), None) == MBD_ERR_ARG
