@@ -16,6 +16,7 @@
 #include <cmath>
 #include <cstdlib>
 #include <cstring>
+#include <limits>
 #include <memory>
 #include <numeric>
 #include <vector>
@@ -336,6 +337,17 @@ void drop_graphs(mbd_ctx* ctx) {
 }
 
 int band_to_tridiag_single(mbd_ctx* ctx, double* Br, int n, double* d, double* e, DevBuf& scratch, cudaStream_t s) {
+  const int C = (ctx->cluster_chase && !ctx->test_stall_wait && n <= sb2st_cluster_max_n())
+                    ? sb2st_cluster_size(n, 1, ctx->num_sms) : 0;
+  if (C > 0) {
+    const BandJob job{Br, n, d, e};
+    MBD_CUDA(scratch.reserve(bytes_of<BandJob>(1)));
+    MBD_CUDA(cudaMemcpyAsync(scratch.p, &job, sizeof(job), cudaMemcpyHostToDevice, s));
+    MBD_CUDA(cudaStreamSynchronize(s));   // the pageable source must outlive the copy
+    MBD_CUDA(launch_sb2st_cluster(scratch.as<BandJob>(), 1, n, C, s));
+    ctx->launches += 1;
+    return MBD_OK;
+  }
   std::vector<SweepItem> items;
   for (int i = 0; i + 3 <= n; ++i) items.push_back(SweepItem{0, i, i - 1, 0});
   const BandJob job{Br, n, d, e};
@@ -638,27 +650,47 @@ int prepare_batch(mbd_ctx* ctx, bool eigen) {
   ctx->n_eig_batch = ctx->n_eig_jobs - (int)ctx->eig_single.size();
   // band -> tridiagonal: one job per two-stage matrix, (job, sweep) items
   // ordered by sweep then job, each pointing at its job's previous sweep
-  std::vector<BandJob> bjobs;
-  ctx->band_max_n = 0;
+  // (the bands that fit a cluster's shared memory first, largest first; the
+  // flag-synchronised chase takes the rest, and all of them while the
+  // failure-detection stall is on: its waits are the ones that can run out)
+  std::vector<BandJob> bjobs, fjobs;
+  const int cap = (ctx->cluster_chase && !ctx->test_stall_wait) ? sb2st_cluster_max_n() : 0;
+  ctx->band_max_n = ctx->band_cluster_max_n = 0;
   for (int g : ctx->order) {
     GeomDev* gd = ctx->geoms[g].get();
     if (!two_stage(ctx, gd->plan.nH)) continue;
-    bjobs.push_back(BandJob{gd->band.as<double>(), gd->plan.nH, gd->d, gd->e});
-    ctx->band_max_n = std::max(ctx->band_max_n, gd->plan.nH);
+    const BandJob bj{gd->band.as<double>(), gd->plan.nH, gd->d, gd->e};
+    if (bj.n <= cap) {
+      bjobs.push_back(bj);
+      ctx->band_cluster_max_n = std::max(ctx->band_cluster_max_n, bj.n);
+    } else {
+      fjobs.push_back(bj);
+      ctx->band_max_n = std::max(ctx->band_max_n, bj.n);
+    }
+  }
+  std::stable_sort(bjobs.begin(), bjobs.end(), [](const BandJob& a, const BandJob& b) { return a.n > b.n; });
+  ctx->n_band_cluster = (int)bjobs.size();
+  ctx->band_cluster_C = sb2st_cluster_size(ctx->band_cluster_max_n, ctx->n_band_cluster, ctx->num_sms);
+  if (ctx->n_band_cluster > 0 && ctx->band_cluster_C < 1) {   // no cluster fits after all
+    fjobs.insert(fjobs.begin(), bjobs.begin(), bjobs.end());
+    for (const BandJob& bj : bjobs) ctx->band_max_n = std::max(ctx->band_max_n, bj.n);
+    bjobs.clear();
+    ctx->n_band_cluster = 0;
   }
   std::vector<SweepItem> items;
   {
-    std::vector<int> last(bjobs.size(), -1);
+    std::vector<int> last(fjobs.size(), -1);
     for (int i = 0; i + 3 <= ctx->band_max_n; ++i)
-      for (size_t j = 0; j < bjobs.size(); ++j) {
-        if (i + 3 > bjobs[j].n) continue;
+      for (size_t j = 0; j < fjobs.size(); ++j) {
+        if (i + 3 > fjobs[j].n) continue;
         items.push_back(SweepItem{(int)j, i, last[j], 0});
         last[j] = (int)items.size() - 1;
       }
   }
+  bjobs.insert(bjobs.end(), fjobs.begin(), fjobs.end());
   ctx->n_band_jobs = (int)bjobs.size();
   ctx->sweeps_in_flight = 0;
-  for (const BandJob& bj : bjobs) ctx->sweeps_in_flight += bj.n / (2 * kBand) + 1;
+  for (const BandJob& bj : fjobs) ctx->sweeps_in_flight += bj.n / (2 * kBand) + 1;
   ctx->n_sweep_items = (int)items.size();
   MBD_CUDA(ctx->sweep_progress.reserve(sizeof(int) * std::max<size_t>(items.size(), 1)));
   const size_t b_jobs = bytes_of<TridiagJob>(jobs.size());
@@ -758,10 +790,15 @@ int enqueue_batch(mbd_ctx* ctx, int mode) {
     ctx->launches += 2;
   }
   record_timing(ctx, ctx->bev[4], s);
-  if (ctx->n_band_jobs > 0) {
-    MBD_CUDA(launch_sb2st(ctx->band_jobs, ctx->n_band_jobs, ctx->sweep_items, ctx->n_sweep_items,
-                          ctx->sweep_progress.as<int>(), ctx->err_flag, ctx->num_sms, ctx->band_max_n,
-                          ctx->sweeps_in_flight, ctx->test_stall_wait ? 0 : -1, s));
+  if (ctx->n_band_cluster > 0) {
+    MBD_CUDA(launch_sb2st_cluster(ctx->band_jobs, ctx->n_band_cluster, ctx->band_cluster_max_n,
+                                  ctx->band_cluster_C, s));
+    ctx->launches += 1;
+  }
+  if (ctx->n_band_jobs > ctx->n_band_cluster) {
+    MBD_CUDA(launch_sb2st(ctx->band_jobs + ctx->n_band_cluster, ctx->n_band_jobs - ctx->n_band_cluster,
+                          ctx->sweep_items, ctx->n_sweep_items, ctx->sweep_progress.as<int>(), ctx->err_flag,
+                          ctx->num_sms, ctx->band_max_n, ctx->sweeps_in_flight, ctx->test_stall_wait ? 0 : -1, s));
     ctx->launches += 3;
   }
   record_timing(ctx, ctx->bev[2], s);
@@ -831,6 +868,8 @@ int mbd_rsscs_create(mbd_ctx** out, int device) {
   {
     const char* ng = std::getenv("MBD_B200_NO_GRAPHS");
     ctx->use_graphs = !(ng && ng[0] && ng[0] != '0');
+    const char* cc = std::getenv("MBD_B200_CLUSTER_CHASE");
+    ctx->cluster_chase = !(cc && cc[0] == '0');
   }
   MBD_CUDA(init_device_constants());
   MBD_CUDA(init_chol_attributes());
@@ -998,8 +1037,15 @@ int mbd_rsscs_download(mbd_ctx* ctx, mbd_result* out) {
         std::vector<double> cs((size_t)kNFreq * kCgState);
         MBD_CUDA(cudaMemcpy(cs.data(), gd->cgstate, sizeof(double) * cs.size(), cudaMemcpyDeviceToHost));
         double most = 0.0;
-        for (int f = 0; f < kNFreq; ++f) most = std::max(most, cs[(size_t)f * kCgState + 1]);
+        bool indefinite = false;
+        for (int f = 0; f < kNFreq; ++f) {
+          most = std::max(most, cs[(size_t)f * kCgState + 1]);
+          indefinite = indefinite || cs[(size_t)f * kCgState + kCgIndefinite] != 0.0;
+        }
         r.refine_iters = (int)most;
+        // a negative curvature proves the relay matrix indefinite: the direct
+        // solve below then reports it (MBD_ERR_RELAY_NOT_SPD)
+        if (indefinite) worst = std::numeric_limits<double>::infinity();
         gd->cg_iters_seen = (worst <= ctx->residual_gate) ? (int)most : 0;
       }
       if (!(worst <= ctx->residual_gate)) {

@@ -122,6 +122,11 @@ struct mbd_ctx {
   mbd::SweepItem* sweep_items = nullptr;
   mbd::DevBuf sweep_progress;
   int n_band_jobs = 0, n_sweep_items = 0, band_max_n = 0;
+  // band jobs [0, n_band_cluster) run in the cluster-resident chase (cluster
+  // size band_cluster_C, largest n band_cluster_max_n), the rest in the
+  // flag-synchronised one
+  int n_band_cluster = 0, band_cluster_C = 0, band_cluster_max_n = 0;
+  bool cluster_chase = true;                 // MBD_B200_CLUSTER_CHASE=0 turns the cluster-resident chase off
   long long sweeps_in_flight = 0;
   int n_trd_groups = 0, trd_total_ctas = 0, n_eig_jobs = 0, n_eig_batch = 0, eig_batch_max_n = 0;
   double trd_est_ms = 0.0;

@@ -30,8 +30,10 @@ namespace {
 constexpr int CT = 64;       // tile edge (rows)
 constexpr int AT = 64;       // atoms per CTA in the per-atom kernels
 constexpr int kRed = 10;     // per-CTA partial sums: a 3x3 matrix and one scalar
-// state[f][kCgState]: [0] stop (0 run, 1 converged, 2 breakdown), [1] iterations,
-// [2..10] Z^T R (even iterations), [11..19] Z^T R (odd), [20] R^T R
+// state[f][kCgState]: [0] stop (0 run, 1 converged, 2 breakdown, 3 negative
+// curvature), [1] iterations, [2..10] Z^T R (even iterations), [11..19] Z^T R
+// (odd), [20] R^T R, [kCgIndefinite] 1 when the relay matrix is shown not to
+// be positive definite
 constexpr int kZR0 = 2, kRR = 20;
 
 __device__ __forceinline__ void cg_tri(int t, int* ti, int* tj) {
@@ -60,6 +62,24 @@ __device__ __forceinline__ bool inv3(const double* m, double* out) {
   out[7] = (m[1] * m[6] - m[0] * m[7]) * id;
   out[8] = (m[0] * m[4] - m[1] * m[3]) * id;
   return true;
+}
+
+// True when the symmetric part of m (3x3, row-major) has a clearly negative
+// pivot in its LDL^T factorisation: some combination p of the search
+// directions has p^T A p < 0, which no positive definite A allows.  Pivots
+// within 1e-10 of the trace count as a (rank) breakdown, not as a proof.
+__device__ __forceinline__ bool negative_curvature(const double* m) {
+  const double a = m[0], b = 0.5 * (m[1] + m[3]), c = 0.5 * (m[2] + m[6]);
+  const double d = m[4], e = 0.5 * (m[5] + m[7]), f = m[8];
+  const double tol = 1e-10 * (fabs(a) + fabs(d) + fabs(f));
+  if (a < -tol) return true;
+  if (!(a > tol)) return false;
+  const double d2 = d - b * b / a;
+  if (d2 < -tol) return true;
+  if (!(d2 > tol)) return false;
+  const double e2 = e - b * c / a;
+  const double d3 = f - c * c / a - e2 * e2 / d2;
+  return d3 < -tol;
 }
 
 __device__ __forceinline__ void mul3(const double* a, const double* b, double* c) {
@@ -400,12 +420,22 @@ __global__ void __launch_bounds__(192) cg_update_kernel(CgArgs a, int it) {
   if (stopped(a, f)) return;
   __shared__ double tot[kRed];
   __shared__ double s_alpha[9];
+  __shared__ int s_indef;
   __shared__ TileSmem S;
   sum_records(a.red + (size_t)f * a.nt * kRed, a.nt, tot);
   if (threadIdx.x == 0) {
     const double* zr = a.state + f * kCgState + kZR0 + 9 * (it & 1);
     double pq[9], ipq[9], al[9];
     for (int k = 0; k < 9; ++k) pq[k] = tot[k];
+    // P^T A P with a negative direction: A is not positive definite (the
+    // reference's unchecked PDPOTRF info, UTILS.f90:469).  Every CTA sees the
+    // same sums and stops; CTA 0 records it and ends this frequency's solve.
+    s_indef = negative_curvature(pq) ? 1 : 0;
+    if (s_indef && I == 0) {
+      double* st = a.state + f * kCgState;
+      st[kCgIndefinite] = 1.0;
+      st[0] = 3.0;
+    }
     if (inv3(pq, ipq)) {
       mul3(ipq, zr, al);
     } else {
@@ -414,6 +444,7 @@ __global__ void __launch_bounds__(192) cg_update_kernel(CgArgs a, int it) {
     for (int k = 0; k < 9; ++k) s_alpha[k] = al[k];
   }
   __syncthreads();
+  if (s_indef) return;
   const int r = threadIdx.x / 3, q = threadIdx.x % 3, gr = I * CT + r;
   double rv = 0.0;
   if (gr < a.n) {

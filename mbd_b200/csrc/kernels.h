@@ -191,9 +191,17 @@ cudaError_t launch_sb2st(const BandJob* jobs, int n_jobs, const SweepItem* items
                          int* err, int num_sms, int max_n, long long sweeps_in_flight, int stall_item,
                          cudaStream_t s);
 cudaError_t init_sb2st_attributes();
+// The same chase with each band held in the distributed shared memory of one
+// thread-block cluster (k_sb2st_cluster.cu): largest n it takes on this
+// device (0 when clusters of this kernel cannot run), the cluster size for a
+// batch (0: none fits), and the launch (jobs with n <= max_n; writes d, e).
+int sb2st_cluster_max_n();
+int sb2st_cluster_size(int max_n, int n_jobs, int num_sms);
+cudaError_t launch_sb2st_cluster(const BandJob* jobs, int n_jobs, int max_n, int C, cudaStream_t s);
 
 // ---- block-CG relay solve of the MIXED_LEARNED mode (UTILS.f90:469-473) ----
 constexpr int kCgState = 24;   // per-frequency recurrence state (doubles)
+constexpr int kCgIndefinite = 21;   // state slot: 1 when a search direction found p^T A p < 0
 struct CgArgs {
   const double* A;         // 21 relay matrices, row-major lower FP64
   size_t a_stride;
