@@ -5,5 +5,6 @@ include/mbd_b200.h; this package holds its ctypes binding (``engine``), the
 geometry.in / setting.in readers and report printer (``io``), the seeded
 synthetic workloads (``synthetic``) and the in-tree build (``build``).
 """
-from .io import Geometry, InputError, Settings, format_report, parse_geometry, parse_settings  # noqa: F401
+from .io import (Geometry, InputError, Settings, format_report, parse_geometry, parse_settings, tile,  # noqa: F401
+                 write_geometry)
 from .engine import EXPORTED, LIB_PATH, Engine, MbdError, Result, load_library  # noqa: F401

@@ -8,7 +8,7 @@
 //   potrf_diag   factor the 64x64 diagonal block in shared memory and store
 //                its inverse Linv (used by the panel and by the solves);
 //   trsm_panel   L[r, k0:k0+64] = A[r, k0:k0+64] Linv^T for rows below;
-//   syrk_lower   A[trail] -= P P^T on the lower 128x128 tiles (DFMA, 8x8 per thread).
+//   syrk_mma     A[trail] -= P P^T on the lower 64x64 tiles (FP64 tensor-core MMA).
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -132,8 +132,8 @@ __global__ void __launch_bounds__(256) trsm_panel_kernel(BatchMat m, int k0, con
 }
 
 // ---------------------------------------------------------------------------
-// SYRK on the trailing lower triangle: C[t0.., t0..] -= P P^T, P = A[t0.., k0:k0+64].
-constexpr int SBM = 128, SBK = 16;
+// SYRK on the trailing lower triangle: C[t0.., t0..] -= P P^T, P = A[t0.., k0:k0+64],
+// on FP64 tensor-core MMAs (mma.sync m8n8k4, FP64 in and out).
 
 __device__ __forceinline__ void tri_index(int t, int* ti, int* tj) {
   int i = (int)((sqrt(8.0 * t + 1.0) - 1.0) * 0.5);
@@ -143,89 +143,91 @@ __device__ __forceinline__ void tri_index(int t, int* ti, int* tj) {
   *tj = t - i * (i + 1) / 2;
 }
 
-__global__ void __launch_bounds__(256) syrk_lower_kernel(BatchMat m, int k0) {
-  extern __shared__ double smem[];
-  double* As = smem;                         // [2][SBK][SBM]
-  double* Bs = smem + 2 * SBK * SBM;         // [2][SBK][SBM]
+// D = A B + D with A 8x4 (row), B 4x8 (col), D 8x8 in FP64:
+// a = A[lane/4][lane%4], b = B[lane%4][lane/4], d = D[lane/4][2*(lane%4) + {0,1}].
+__device__ __forceinline__ void dmma(double& d0, double& d1, double a, double b) {
+  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};"
+               : "+d"(d0), "+d"(d1)
+               : "d"(a), "d"(b));
+}
+
+// 16-byte asynchronous copy global -> shared; src_bytes < 16 zero-fills the rest.
+__device__ __forceinline__ void cp_async16(void* dst, const void* src, int src_bytes) {
+  const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(d), "l"(src), "r"(src_bytes) : "memory");
+}
+
+constexpr int MT = 64;            // tile edge
+constexpr int MFS = MT + 4;       // shared row stride: the 8 x 4 fragment loads of a half-warp hit 16 bank pairs
+constexpr size_t kSyrkSmem = sizeof(double) * 3 * MT * MFS;
+
+// One lower 64 x 64 tile (I, J) of the trailing matrix per CTA, 4 warps each
+// a 32 x 32 quarter (4 x 4 MMA tiles).  The panel rows of block I and J and
+// the tile itself go to shared memory together (cp.async, zero-filled past
+// the matrix), the product is subtracted there and the tile goes back a row
+// per warp instruction.
+__global__ void __launch_bounds__(128) syrk_mma_kernel(BatchMat m, int k0) {
+  extern __shared__ __align__(16) double dsm[];
+  double* Pi = dsm;                // [64][MFS]: P rows of block I
+  double* Pj = dsm + MT * MFS;     // [64][MFS]: P rows of block J
+  double* Cs = dsm + 2 * MT * MFS; // [64][MFS]: the tile (I, J)
   const int b = blockIdx.y;
   double* A = mat_ptr(m, b);
   const int t0 = k0 + NB;
   const int msz = m.n - t0;
   int ti, tj;
   tri_index(blockIdx.x, &ti, &tj);
-  const int rA = t0 + ti * SBM, rB = t0 + tj * SBM;
-  const int tid = threadIdx.x;
-  const int tx = tid % 16, ty = tid / 16;
-  const int nbk = min(NB, m.n - k0);
-
-  // loader: row lr = tid/2 (0..127), k-half kh = (tid%2)*8
-  const int lr = tid / 2, kh = (tid % 2) * 8;
-  double ra[8], rb[8];
-  auto gload = [&](int kc) {
-#pragma unroll
-    for (int u = 0; u < 8; ++u) {
-      int k = kc + kh + u;
-      int rowa = rA + lr, rowb = rB + lr;
-      ra[u] = (rowa < m.n && k < nbk) ? A[(size_t)rowa * m.ld + k0 + k] : 0.0;
-      rb[u] = (rowb < m.n && k < nbk) ? A[(size_t)rowb * m.ld + k0 + k] : 0.0;
-    }
-  };
-  auto sstore = [&](int buf) {
-#pragma unroll
-    for (int u = 0; u < 8; ++u) {
-      As[(buf * SBK + kh + u) * SBM + lr] = ra[u];
-      Bs[(buf * SBK + kh + u) * SBM + lr] = rb[u];
-    }
-  };
-  double acc[8][8];
-#pragma unroll
-  for (int i = 0; i < 8; ++i)
-#pragma unroll
-    for (int j = 0; j < 8; ++j) acc[i][j] = 0.0;
-
-  gload(0);
-  sstore(0);
+  const int tid = threadIdx.x, warp = tid / 32, lane = tid % 32;
+  const int g = lane >> 2, q4 = lane & 3;
+  double* T = A + (size_t)t0 * m.ld;   // row t0 of the matrix
+  for (int e = tid; e < MT * (NB / 2); e += 128) {
+    const int r = e / (NB / 2), c = 2 * (e % (NB / 2));
+    const int gi = ti * MT + r, gj = tj * MT + r;
+    cp_async16(Pi + r * MFS + c, T + (size_t)(gi < msz ? gi : 0) * m.ld + k0 + c, gi < msz ? 16 : 0);
+    cp_async16(Pj + r * MFS + c, T + (size_t)(gj < msz ? gj : 0) * m.ld + k0 + c, gj < msz ? 16 : 0);
+  }
+  for (int e = tid; e < MT * (MT / 2); e += 128) {
+    const int r = e / (MT / 2), c = 2 * (e % (MT / 2));
+    const int gr = ti * MT + r, gc = tj * MT + c;
+    const bool rok = gr < msz;
+    const int bytes = rok ? (gc + 1 < msz ? 16 : (gc < msz ? 8 : 0)) : 0;
+    cp_async16(Cs + r * MFS + c, T + (size_t)(rok ? gr : 0) * m.ld + t0 + (bytes ? gc : 0), bytes);
+  }
+  asm volatile("cp.async.commit_group;" ::: "memory");
+  asm volatile("cp.async.wait_group 0;" ::: "memory");
   __syncthreads();
-  constexpr int NCH = NB / SBK;
-  for (int ch = 0; ch < NCH; ++ch) {
-    const int buf = ch & 1;
-    if (ch + 1 < NCH) gload((ch + 1) * SBK);
+  const int r0 = (warp / 2) * 32, c0 = (warp % 2) * 32;
+  if (!(ti == tj && c0 > r0)) {   // the strictly upper quarter of a diagonal tile is not stored
+    double acc[4][4][2];
 #pragma unroll
-    for (int k = 0; k < SBK; ++k) {
-      double a[8], bb[8];
-      const double2* ap = reinterpret_cast<const double2*>(As + (buf * SBK + k) * SBM + ty * 8);
-      const double2* bp = reinterpret_cast<const double2*>(Bs + (buf * SBK + k) * SBM + tx * 8);
+    for (int i = 0; i < 4; ++i)
 #pragma unroll
-      for (int u = 0; u < 4; ++u) {
-        double2 x = ap[u], y = bp[u];
-        a[2 * u] = x.x; a[2 * u + 1] = x.y;
-        bb[2 * u] = y.x; bb[2 * u + 1] = y.y;
-      }
+      for (int q = 0; q < 4; ++q) acc[i][q][0] = acc[i][q][1] = 0.0;
+#pragma unroll 4
+    for (int kk = 0; kk < NB; kk += 4) {
+      double af[4], bf[4];
 #pragma unroll
-      for (int i = 0; i < 8; ++i)
+      for (int i = 0; i < 4; ++i) af[i] = Pi[(r0 + i * 8 + g) * MFS + kk + q4];
 #pragma unroll
-        for (int j = 0; j < 8; ++j) acc[i][j] = fma(a[i], bb[j], acc[i][j]);
+      for (int q = 0; q < 4; ++q) bf[q] = Pj[(c0 + q * 8 + g) * MFS + kk + q4];
+#pragma unroll
+      for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int q = 0; q < 4; ++q) dmma(acc[i][q][0], acc[i][q][1], af[i], bf[q]);
     }
-    if (ch + 1 < NCH) {
-      sstore(buf ^ 1);
-    }
-    __syncthreads();
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+      for (int q = 0; q < 4; ++q)
+#pragma unroll
+        for (int h = 0; h < 2; ++h) Cs[(r0 + i * 8 + g) * MFS + c0 + q * 8 + 2 * q4 + h] -= acc[i][q][h];
   }
-  // epilogue: C -= acc (lower part only on diagonal tiles)
-#pragma unroll
-  for (int i = 0; i < 8; ++i) {
-    const int r = rA + ty * 8 + i;
-    if (r >= m.n) continue;
-#pragma unroll
-    for (int j = 0; j < 8; ++j) {
-      const int c = rB + tx * 8 + j;
-      if (c < m.n && c <= r) {
-        double* p = A + (size_t)r * m.ld + c;
-        *p -= acc[i][j];
-      }
-    }
+  __syncthreads();
+  for (int e = tid; e < MT * MT; e += 128) {
+    const int r = e / MT, c = e % MT;
+    const int gr = ti * MT + r, gc = tj * MT + c;
+    if (gr < msz && gc < msz && (ti != tj || c <= r)) T[(size_t)gr * m.ld + t0 + gc] = Cs[r * MFS + c];
   }
-  (void)msz;
 }
 
 // ---------------------------------------------------------------------------
@@ -416,8 +418,8 @@ __global__ void __launch_bounds__(256) relay_post_kernel(EpilogueArgs a, const d
 constexpr size_t kPairSmem = 2 * NB * (NB + 1) * sizeof(double);
 
 cudaError_t init_chol_attributes() {
-  cudaError_t e = cudaFuncSetAttribute(syrk_lower_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       (int)(4 * SBK * SBM * sizeof(double)));
+  cudaError_t e = cudaFuncSetAttribute(syrk_mma_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)kSyrkSmem);
   if (e == cudaSuccess)
     e = cudaFuncSetAttribute(potrf_diag_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kPairSmem);
   if (e == cudaSuccess)
@@ -441,10 +443,9 @@ void launch_trsm_panel_f64(const BatchMat& m, int k0, const double* Linv, size_t
 void launch_syrk_lower_f64(const BatchMat& m, int k0, cudaStream_t s) {
   int msz = m.n - k0 - NB;
   if (msz <= 0) return;
-  int nt = (msz + SBM - 1) / SBM;
+  int nt = (msz + MT - 1) / MT;
   dim3 grid(nt * (nt + 1) / 2, m.batch);
-  size_t smem = 4 * SBK * SBM * sizeof(double);
-  syrk_lower_kernel<<<grid, 256, smem, s>>>(m, k0);
+  syrk_mma_kernel<<<grid, 128, kSyrkSmem, s>>>(m, k0);
 }
 
 void launch_init_rhs(double* Y, size_t ystride, int n, int batch, cudaStream_t s) {

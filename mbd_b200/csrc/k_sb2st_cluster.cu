@@ -83,17 +83,129 @@ __device__ __forceinline__ double make_reflector(double x, int len, double* v, d
 
 __device__ __forceinline__ int floor_div(int a, int b) { return a >= 0 ? a / b : -((-a + b - 1) / b); }
 
-// Rows [r, r + 64) of a matrix whose CTAs hold R rows each: row r + q is at
-// base0 + q SLD while r + q < split, at base1 + (r + q - split) SLD after.
-struct RowMap {
+// Rows [r, r + 64) of a task, r in this CTA: row r + q is at base0 + q SLD
+// (this CTA's shared memory) while q < lim, in the next CTA at
+// base1 + (q - lim) SLD after.  LOCAL: every row the task touches is here, so
+// all accesses are plain shared-memory ones (the cluster window is only taken
+// by the few tasks that straddle two CTAs).
+template <bool LOCAL>
+struct Rows {
   double* base0;
   double* base1;
-  int split;   // first row held by the next CTA
-  int r;
+  int lim;
   __device__ __forceinline__ double* row(int q) const {
-    return (r + q < split) ? base0 + q * SLD : base1 + (r + q - split) * SLD;
+    if (LOCAL) return base0 + q * SLD;
+    return (q < lim) ? base0 + q * SLD : base1 + (q - lim) * SLD;
   }
 };
+
+// One task (i, k) at step t on warp pair `pair`: the O-warp builds the
+// reflector (k = 0), updates O and hands H' on; the D-warp updates D.
+template <bool LOCAL>
+__device__ __forceinline__ void chase_task(const Rows<LOCAL>& rm, int n, int r, int i, int k, int t, int R,
+                                           double* refl, double* const* peer_refl, double* pv, double* pw,
+                                           double* ps, int pair, bool owarp) {
+  const int l = threadIdx.x & 31;
+  const int L = min(B, n - r);
+  const int rn = r + B;
+  const int Ln = max(0, min(B, n - rn));
+  // the task's reflector H (v, tau)
+  const double* vsrc;
+  if (k == 0) {
+    if (owarp) {
+      // from column i: x[l] = A(r + l, i), band row r + l at d = l + 1
+      double* xp = rm.row(l) + 1 + l;
+      const double x = (l < L) ? *xp : 0.0;
+      double vl, beta;
+      const double tau0 = make_reflector(x, L, &vl, &beta);
+      if (l < L) *xp = (l == 0) ? beta : (tau0 != 0.0 ? 0.0 : x);
+      pv[l] = vl;
+      if (l == 0) pv[B] = tau0;
+    }
+    pair_sync(pair);
+    vsrc = pv;
+  } else {
+    vsrc = refl + ((t & 1) * kRing + (i % kRing)) * RSLOT;
+  }
+  const double tau = vsrc[B];
+  if (!owarp) {
+    // ---- D <- H D H:  w = tau D v - (tau^2 / 2)(v^T D v) v;  D -= v w^T + w v^T
+    double dr[B];   // dr[j] = D(l, j)
+#pragma unroll
+    for (int j = 0; j < B; ++j) {
+      const int q = (j <= l) ? l : j;
+      dr[j] = (q < L) ? rm.row(q)[(j <= l) ? l - j : j - l] : 0.0;
+    }
+    if (tau != 0.0) {
+      const double vlD = vsrc[l];
+      double dv = 0.0;
+#pragma unroll
+      for (int j = 0; j < B; ++j) dv += dr[j] * vsrc[j];
+      const double vdv = warp_sum(vlD * dv);
+      const double wl = tau * dv - 0.5 * tau * tau * vdv * vlD;
+      pw[l] = wl;
+      __syncwarp();
+#pragma unroll
+      for (int j = 0; j < B; ++j) dr[j] -= vlD * pw[j] + wl * vsrc[j];
+      if (l < L) {
+        double* own = rm.row(l);
+#pragma unroll
+        for (int j = 0; j < B; ++j)
+          if (j <= l) own[l - j] = dr[j];
+      }
+    }
+  } else {
+    // ---- O <- O H;  H' from O[:, 0];  O <- H' O
+    // orow[j] = O(l, j) = A(rn + l, r + j): band row rn + l at d = B + l - j
+    double* orowp = rm.row(B + l) + B + l;
+    double orow[B];
+#pragma unroll
+    for (int j = 0; j < B; ++j) orow[j] = (l < Ln && j < L) ? orowp[-j] : 0.0;
+    if (tau != 0.0) {
+      double ov = 0.0;
+#pragma unroll
+      for (int j = 0; j < B; ++j) ov += orow[j] * vsrc[j];
+#pragma unroll
+      for (int j = 0; j < B; ++j) orow[j] -= tau * ov * vsrc[j];
+    }
+    double v2 = 0.0, tau2 = 0.0, beta2 = 0.0;
+    if (Ln > 0) {
+      tau2 = make_reflector(orow[0], Ln, &v2, &beta2);
+      if (tau2 != 0.0) {
+        // column sums s_l = sum_q v2[q] O(q, l): the rows go to the band
+        // first, then lane l walks column l
+        if (l < Ln) {
+#pragma unroll
+          for (int j = 0; j < B; ++j)
+            if (j < L) orowp[-j] = orow[j];
+        }
+        ps[l] = v2;
+        __syncwarp();
+        double sj = 0.0;
+#pragma unroll
+        for (int q = 0; q < B; ++q) {
+          const double oql = (q < Ln && l < L) ? rm.row(B + q)[B + q - l] : 0.0;
+          sj += ps[q] * oql;
+        }
+        __syncwarp();
+        ps[l] = sj;
+        __syncwarp();
+#pragma unroll
+        for (int j = 0; j < B; ++j) orow[j] -= tau2 * v2 * ps[j];
+        orow[0] = (l == 0) ? beta2 : 0.0;
+      }
+      if (l < Ln) {
+#pragma unroll
+        for (int j = 0; j < B; ++j)
+          if (j < L) orowp[-j] = orow[j];
+      }
+      // H' to the owner of row rn, for task (i, k + 1) at step t + 1
+      double* slot = peer_refl[rn / R] + ((((t + 1) & 1) * kRing) + (i % kRing)) * RSLOT;
+      slot[l] = v2;
+      if (l == 0) slot[B] = tau2;
+    }
+  }
+}
 
 __global__ void __launch_bounds__(THREADS, 1) sb2st_cluster_kernel(const BandJob* jobs, int n_jobs, int rmax) {
   extern __shared__ __align__(16) double sm[];
@@ -102,7 +214,7 @@ __global__ void __launch_bounds__(THREADS, 1) sb2st_cluster_kernel(const BandJob
   cg::cluster_group cl = cg::this_cluster();
   const int C = (int)cl.num_blocks();
   const int rank = (int)cl.block_rank();
-  const int tid = threadIdx.x, warp = tid >> 5, l = tid & 31;
+  const int tid = threadIdx.x, warp = tid >> 5;
   const int pair = warp >> 1;
   const bool owarp = (warp & 1) != 0;
   double* band = sm;
@@ -133,6 +245,7 @@ __global__ void __launch_bounds__(THREADS, 1) sb2st_cluster_kernel(const BandJob
       }
     }
     cl.sync();
+    double* next_band = peer_band[min(rank + 1, C - 1)];
     const int tmax = 2 * (n - 3);
     for (int t = 0; t <= tmax; ++t) {
       // this CTA's tasks at step t: r = 32 t + 1 - 63 i in [lo, hi); pair p
@@ -141,110 +254,12 @@ __global__ void __launch_bounds__(THREADS, 1) sb2st_cluster_kernel(const BandJob
       const int r = 32 * t + 1 - (2 * B - 1) * i;
       const int k = t - 2 * i;
       if (i >= 0 && k >= 0 && r < hi && r < n) {
-        const int L = min(B, n - r);
-        const int rn = r + B;
-        const int Ln = max(0, min(B, n - rn));
-        const int c0 = r / R;
-        RowMap rm;
-        rm.r = r;
-        rm.split = (c0 + 1) * R;
-        rm.base0 = peer_band[c0] + (r - c0 * R) * SLD;
-        rm.base1 = peer_band[min(c0 + 1, C - 1)];
-        // the task's reflector H (v, tau)
-        const double* vsrc;
-        if (k == 0) {
-          if (owarp) {
-            // from column i: x[l] = A(r + l, i), band row r + l at d = l + 1
-            double* xp = rm.row(l) + 1 + l;
-            const double x = (l < L) ? *xp : 0.0;
-            double vl, beta;
-            const double tau0 = make_reflector(x, L, &vl, &beta);
-            if (l < L) *xp = (l == 0) ? beta : (tau0 != 0.0 ? 0.0 : x);
-            pv[l] = vl;
-            if (l == 0) pv[B] = tau0;
-          }
-          pair_sync(pair);
-          vsrc = pv;
+        if (min(n, r + 2 * B) <= hi) {
+          const Rows<true> rm{band + (r - lo) * SLD, nullptr, 0};
+          chase_task(rm, n, r, i, k, t, R, refl, peer_refl, pv, pw, ps, pair, owarp);
         } else {
-          vsrc = refl + ((t & 1) * kRing + (i % kRing)) * RSLOT;
-        }
-        const double tau = vsrc[B];
-        if (!owarp) {
-          // ---- D <- H D H:  w = tau D v - (tau^2 / 2)(v^T D v) v;  D -= v w^T + w v^T
-          double dr[B];   // dr[j] = D(l, j)
-#pragma unroll
-          for (int j = 0; j < B; ++j) {
-            const int q = (j <= l) ? l : j;
-            dr[j] = (q < L) ? rm.row(q)[(j <= l) ? l - j : j - l] : 0.0;
-          }
-          if (tau != 0.0) {
-            const double vlD = vsrc[l];
-            double dv = 0.0;
-#pragma unroll
-            for (int j = 0; j < B; ++j) dv += dr[j] * vsrc[j];
-            const double vdv = warp_sum(vlD * dv);
-            const double wl = tau * dv - 0.5 * tau * tau * vdv * vlD;
-            pw[l] = wl;
-            __syncwarp();
-#pragma unroll
-            for (int j = 0; j < B; ++j) dr[j] -= vlD * pw[j] + wl * vsrc[j];
-            if (l < L) {
-              double* own = rm.row(l);
-#pragma unroll
-              for (int j = 0; j < B; ++j)
-                if (j <= l) own[l - j] = dr[j];
-            }
-          }
-        } else {
-          // ---- O <- O H;  H' from O[:, 0];  O <- H' O
-          // orow[j] = O(l, j) = A(rn + l, r + j): band row rn + l at d = B + l - j
-          double* orowp = rm.row(B + l) + B + l;
-          double orow[B];
-#pragma unroll
-          for (int j = 0; j < B; ++j) orow[j] = (l < Ln && j < L) ? orowp[-j] : 0.0;
-          if (tau != 0.0) {
-            double ov = 0.0;
-#pragma unroll
-            for (int j = 0; j < B; ++j) ov += orow[j] * vsrc[j];
-#pragma unroll
-            for (int j = 0; j < B; ++j) orow[j] -= tau * ov * vsrc[j];
-          }
-          double v2 = 0.0, tau2 = 0.0, beta2 = 0.0;
-          if (Ln > 0) {
-            tau2 = make_reflector(orow[0], Ln, &v2, &beta2);
-            if (tau2 != 0.0) {
-              // column sums s_l = sum_q v2[q] O(q, l): the rows go to the band
-              // first, then lane l walks column l
-              if (l < Ln) {
-#pragma unroll
-                for (int j = 0; j < B; ++j)
-                  if (j < L) orowp[-j] = orow[j];
-              }
-              ps[l] = v2;
-              __syncwarp();
-              double sj = 0.0;
-#pragma unroll
-              for (int q = 0; q < B; ++q) {
-                const double oql = (q < Ln && l < L) ? rm.row(B + q)[B + q - l] : 0.0;
-                sj += ps[q] * oql;
-              }
-              __syncwarp();
-              ps[l] = sj;
-              __syncwarp();
-#pragma unroll
-              for (int j = 0; j < B; ++j) orow[j] -= tau2 * v2 * ps[j];
-              orow[0] = (l == 0) ? beta2 : 0.0;
-            }
-            if (l < Ln) {
-#pragma unroll
-              for (int j = 0; j < B; ++j)
-                if (j < L) orowp[-j] = orow[j];
-            }
-            // H' to the owner of row rn, for task (i, k + 1) at step t + 1
-            double* slot = peer_refl[rn / R] + ((((t + 1) & 1) * kRing) + (i % kRing)) * RSLOT;
-            slot[l] = v2;
-            if (l == 0) slot[B] = tau2;
-          }
+          const Rows<false> rm{band + (r - lo) * SLD, next_band, hi - r};
+          chase_task(rm, n, r, i, k, t, R, refl, peer_refl, pv, pw, ps, pair, owarp);
         }
       }
       cl.sync();

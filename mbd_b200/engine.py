@@ -43,6 +43,40 @@ EXPORTED = [
 OPTIONS = {"residual_gate": 1, "wait_limit_s": 2, "test_stall_wait": 3}
 
 
+NETWORK_MAGIC = b"MBDNET\0\0"
+NETWORK_VERSION = 1
+
+
+def write_network_file(path: str, params) -> None:
+    """Checkpoint of the learned warm start's network: 8-byte magic, uint32
+    format version, uint32 parameter count, the FP32 parameters
+    (little-endian, the layout of mbd_rsscs_learned_get_params) and the
+    SHA-256 of those parameter bytes."""
+    import hashlib
+    import struct
+    p = np.ascontiguousarray(params, dtype="<f4")
+    body = p.tobytes()
+    with open(path, "wb") as fh:
+        fh.write(NETWORK_MAGIC + struct.pack("<II", NETWORK_VERSION, p.size) + body + hashlib.sha256(body).digest())
+
+
+def read_network_file(path: str) -> np.ndarray:
+    import hashlib
+    import struct
+    with open(path, "rb") as fh:
+        data = fh.read()
+    if len(data) < 16 or data[:8] != NETWORK_MAGIC:
+        raise ValueError(f"{path}: not a network checkpoint")
+    version, count = struct.unpack("<II", data[8:16])
+    if version != NETWORK_VERSION:
+        raise ValueError(f"{path}: checkpoint format version {version}, expected {NETWORK_VERSION}")
+    body = data[16:16 + 4 * count]
+    digest = data[16 + 4 * count:]
+    if len(body) != 4 * count or hashlib.sha256(body).digest() != digest:
+        raise ValueError(f"{path}: checkpoint is truncated or corrupted (SHA-256 mismatch)")
+    return np.frombuffer(body, dtype="<f4").astype(np.float32)
+
+
 class MbdError(RuntimeError):
     def __init__(self, code: int, msg: str):
         super().__init__(f"{ERRORS.get(code, code)}: {msg}")
@@ -345,6 +379,15 @@ class Engine:
         if code != MBD_OK:
             raise MbdError(code, strerror(code))
         return v.value
+
+    def save_network(self, path: str) -> None:
+        """Write the context's network to `path` (write_network_file)."""
+        write_network_file(path, self.learned_params())
+
+    def load_network(self, path: str) -> None:
+        """Load a network written by save_network (checked: magic, version,
+        parameter count, SHA-256 of the parameters)."""
+        self.set_learned_params(read_network_file(path))
 
     def use_network(self, on: bool) -> None:
         self.lib.mbd_rsscs_learned_use_network(self.ctx, 1 if on else 0)

@@ -10,6 +10,10 @@
   and ignored: there is no process grid.
 * ``format_report`` prints the fields of MBD_at_rsSCS's report
   (UTILS.f90:223-331).
+* ``write_geometry`` writes a Geometry back in that format and ``tile``
+  replicates a periodic geometry into a supercell (the job of the
+  reference's examples/process.py, which tiles the 60-atom graphene cell
+  into graphene_<i><j>1.in), for any cell and along all three vectors.
 """
 from __future__ import annotations
 
@@ -94,6 +98,43 @@ def parse_geometry(text: str) -> Geometry:
             lat[i] = [_real(t) for t in tok[1:4]]
         geo.lattice = lat
     return geo
+
+
+def write_geometry(geo: Geometry) -> str:
+    """geometry.in text for `geo` as parse_geometry (MBD_rsSCS.f90:66-89)
+    reads it: atom count, a comment line, ``name x y z hirshfeld`` records
+    (Angstrom, full double precision), then the three lattice vectors of a
+    periodic system."""
+    out = [str(len(geo.names)), "geometry written by mbd_b200"]
+    for name, xyz, h in zip(geo.names, geo.coords, geo.hirshfeld):
+        out.append(f"{name:<2s}  {xyz[0]:.17g}  {xyz[1]:.17g}  {xyz[2]:.17g}  {h:.17g}")
+    if geo.n_periodic:
+        for a in geo.lattice:
+            out.append(f"lattice_vector  {a[0]:.17g}  {a[1]:.17g}  {a[2]:.17g}")
+    return "\n".join(out) + "\n"
+
+
+def tile(geo: Geometry, reps) -> Geometry:
+    """Supercell of a periodic geometry: (n1, n2, n3) copies along the three
+    lattice vectors, atoms in the order cell (i, j, k) with k fastest, then
+    atom (examples/process.py:10-18 for the graphene cell, there only along
+    the first two axes with fixed lattice constants); Hirshfeld ratios copied,
+    lattice vectors scaled by the repetitions."""
+    n1, n2, n3 = (int(r) for r in reps)
+    if not geo.n_periodic:
+        raise InputError("tile: the geometry has no lattice vectors")
+    if min(n1, n2, n3) < 1:
+        raise InputError("tile: repetitions must be >= 1")
+    names, xyz, hv = [], [], []
+    for i in range(n1):
+        for j in range(n2):
+            for k in range(n3):
+                shift = i * geo.lattice[0] + j * geo.lattice[1] + k * geo.lattice[2]
+                names += list(geo.names)
+                xyz.append(geo.coords + shift)
+                hv.append(geo.hirshfeld)
+    lat = geo.lattice * np.array([[n1], [n2], [n3]], dtype=np.float64)
+    return Geometry(names, np.concatenate(xyz), np.concatenate(hv), lat, geo.n_periodic)
 
 
 def parse_settings(text: str) -> Settings:
