@@ -212,11 +212,18 @@ void* mbd_rsscs_stream(mbd_ctx* ctx);
  *                            compute reports MBD_ERR_TIMEOUT; the context stays
  *                            usable.  For testing failure detection; 0 (the
  *                            default) turns it off.
+ *   MBD_OPT_FP32_TENSOR_BUILD 1: MIXED and MIXED_LEARNED build the short-range
+ *                            dipole tensors of the relay matrices in FP32
+ *                            arithmetic from FP64 pair displacements (the
+ *                            image set is still selected in FP64); the FP64
+ *                            refinement then solves that FP32-valued system.
+ *                            0 (the default): FP64 arithmetic in every mode.
  * set_option returns MBD_ERR_ARG for an unknown option or a value out of range. */
 enum {
     MBD_OPT_RESIDUAL_GATE = 1,
     MBD_OPT_WAIT_LIMIT_S = 2,
-    MBD_OPT_TEST_STALL_WAIT = 3
+    MBD_OPT_TEST_STALL_WAIT = 3,
+    MBD_OPT_FP32_TENSOR_BUILD = 4
 };
 int mbd_rsscs_set_option(mbd_ctx* ctx, int option, double value);
 int mbd_rsscs_get_option(mbd_ctx* ctx, int option, double* value);

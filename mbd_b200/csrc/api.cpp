@@ -391,6 +391,7 @@ int run_front(mbd_ctx* ctx, GeomDev* gd, int gi, int mode, bool relay_only) {
   RelayBuildArgs rb{N, p.ld, mstride, gd->coords, gd->alpha_w, gd->sgm, gd->rvdw_iso, gd->scs_shifts,
                     (int)p.scs_shifts.size() / 3, p.beta, p.scs_eval_cut, sl.relay64.as<double>(),
                     mixed ? sl.relay32.as<float>() : nullptr};
+  rb.f32_math = (mixed || learned) && ctx->f32_tensor_build;
   launch_relay_build(rb, s);
   ctx->launches += 1;
   mark(2);
@@ -1237,6 +1238,16 @@ int mbd_rsscs_set_option(mbd_ctx* ctx, int option, double value) {
       ctx->wait_limit_s = value;
       return MBD_OK;
     }
+    case MBD_OPT_FP32_TENSOR_BUILD: {
+      const int on = value != 0.0;
+      if (on != ctx->f32_tensor_build) {
+        MBD_CUDA(cudaSetDevice(ctx->device));
+        MBD_CUDA(cudaDeviceSynchronize());
+        drop_graphs(ctx);   // the captured launches carry the old setting
+      }
+      ctx->f32_tensor_build = on;
+      return MBD_OK;
+    }
     case MBD_OPT_TEST_STALL_WAIT: {
       const int on = value != 0.0;
       if (on != ctx->test_stall_wait) {
@@ -1258,6 +1269,7 @@ int mbd_rsscs_get_option(mbd_ctx* ctx, int option, double* value) {
     case MBD_OPT_RESIDUAL_GATE: *value = ctx->residual_gate; return MBD_OK;
     case MBD_OPT_WAIT_LIMIT_S: *value = ctx->wait_limit_s; return MBD_OK;
     case MBD_OPT_TEST_STALL_WAIT: *value = ctx->test_stall_wait; return MBD_OK;
+    case MBD_OPT_FP32_TENSOR_BUILD: *value = ctx->f32_tensor_build; return MBD_OK;
     default: return MBD_ERR_ARG;
   }
 }

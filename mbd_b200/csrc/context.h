@@ -166,6 +166,7 @@ struct mbd_ctx {
   double residual_gate = mbd::kResidualGate;   // accepted ||B - A X||_F / ||B||_F of the fast relay solves
   double wait_limit_s = 2.0;                   // bounded device waits (per device)
   int test_stall_wait = 0;                     // 1: the bulge-chasing launch's first wait runs out
+  int f32_tensor_build = 0;                    // 1: mixed modes build the relay tensors in FP32 arithmetic
 };
 
 namespace mbd {

@@ -5,7 +5,8 @@
 // atom blocks (i >= j) are written (the lower triangle, as the reference's
 // fill at UTILS.f90:427-431 / 799-803).  One thread owns one atom pair
 // (i, j); consecutive threads take consecutive j, so the three 24-byte rows
-// of a 3x3 block written by a warp form contiguous 768-byte runs.
+// of the 3x3 blocks of a warp form contiguous 768-byte runs, which the relay
+// builder writes with 16-byte vector stores.
 #include <cuda_runtime.h>
 
 #include "kernels.h"
@@ -36,59 +37,110 @@ __global__ void atom_freq_kernel(AtomDev a, int N) {
   a.rvdw_iso[i] = pow(h, kOtdD) * a.r0[i];   // UTILS.f90:254
 }
 
-// One thread: pair (i = blockIdx.y, j), frequencies [f0, f0+FCH).
+// Rows of the folded lower-triangle grid: grid row p holds atom rows p and
+// N - 1 - p, whose column blocks (of kBuildThreads atoms) together number
+// about N / kBuildThreads + 1, so nearly every CTA has pairs j <= i to build.
+constexpr int kBuildThreads = 128;
+
+__device__ __forceinline__ bool folded_row(int N, int* i, int* j0) {
+  const int p = blockIdx.y, q = N - 1 - p;
+  const int nb_p = p / kBuildThreads + 1;
+  int jb = blockIdx.x;
+  if (jb < nb_p) {
+    *i = p;
+  } else {
+    jb -= nb_p;
+    if (q == p || jb >= q / kBuildThreads + 1) return false;
+    *i = q;
+  }
+  *j0 = jb * kBuildThreads;
+  return true;
+}
+
+// Value type of the tensor arithmetic: FP64, or FP32 from FP64 displacements
+// (the image set is always selected in FP64: r <= cut exactly as
+// UTILS.f90:574,623 test it).
+template <bool F32>
+struct TensorMath;
+template <>
+struct TensorMath<false> {
+  using T = double;
+  static __device__ __forceinline__ double exp_(double x) { return exp(x); }
+  static __device__ __forceinline__ double erf_(double x) { return erf(x); }
+};
+template <>
+struct TensorMath<true> {
+  using T = float;
+  static __device__ __forceinline__ float exp_(float x) { return expf(x); }
+  static __device__ __forceinline__ float erf_(float x) { return erff(x); }
+};
+
+// One thread: pair (i, j) of the folded grid, frequencies [f0, f0+FCH) (blockIdx.z).
 // gaussian_dipole_tensor (UTILS.f90:637-696) summed over translations
-// (scs_offdiag_block 591-633, scs_diag_block 543-587).
-template <int FCH>
-__global__ void __launch_bounds__(128) relay_build_kernel(RelayBuildArgs a) {
-  const int i = blockIdx.y;
-  const int j = blockIdx.x * blockDim.x + threadIdx.x;
-  if (j > i || j >= a.N) return;
+// (scs_offdiag_block 591-633, scs_diag_block 543-587).  The 3x3 blocks of a
+// warp's 32 consecutive pairs go out through shared memory as whole block
+// rows: 96 contiguous doubles (FP64, double2 stores) or floats (FP32, float4
+// stores) per matrix row.
+template <int FCH, bool F32>
+__global__ void __launch_bounds__(kBuildThreads) relay_build_kernel(RelayBuildArgs a) {
+  using M = TensorMath<F32>;
+  using T = typename M::T;
+  __shared__ __align__(16) double stage[kBuildThreads / 32][3 * 96];
+  int i, j0;
+  if (!folded_row(a.N, &i, &j0)) return;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int j = j0 + threadIdx.x;
+  const int jw = j0 + warp * 32;               // the warp's first pair
+  if (jw > i || jw >= a.N) return;             // whole warps only: none of its pairs exists
+  const bool valid = j <= i && j < a.N;
   const int f0 = blockIdx.z * FCH;
   const int N = a.N;
-  const bool diag = (i == j);
+  const int jj = valid ? j : jw;               // a lane past the end computes a dummy pair
+  const bool diag = (i == jj);
   const double xi = a.coords[3 * i], yi = a.coords[3 * i + 1], zi = a.coords[3 * i + 2];
-  const double d0x = xi - a.coords[3 * j], d0y = yi - a.coords[3 * j + 1], d0z = zi - a.coords[3 * j + 2];
-  const double rv12 = diag ? 2.0 * a.rvdw_iso[i] : a.rvdw_iso[i] + a.rvdw_iso[j];
-  const double inv_brv = 1.0 / (a.beta * rv12);
-  const double c4pi = sqrt(4.0 / kPiD), c16pi = sqrt(16.0 / kPiD);
+  const double d0x = xi - a.coords[3 * jj], d0y = yi - a.coords[3 * jj + 1], d0z = zi - a.coords[3 * jj + 2];
+  const double rv12 = diag ? 2.0 * a.rvdw_iso[i] : a.rvdw_iso[i] + a.rvdw_iso[jj];
+  const T inv_brv = (T)(1.0 / (a.beta * rv12));
+  const T c4pi = (T)sqrt(4.0 / kPiD), c16pi = (T)sqrt(16.0 / kPiD);
 
-  double sg[FCH];
+  T sg[FCH];
 #pragma unroll
   for (int q = 0; q < FCH; ++q) {
     const int f = f0 + q;
     const double si = a.sgm[f * N + i];
     if (diag) {
-      sg[q] = si;                                       // UTILS.f90:571 (sigma_i, not sqrt(2) sigma_i)
+      sg[q] = (T)si;                                     // UTILS.f90:571 (sigma_i, not sqrt(2) sigma_i)
     } else {
-      const double sj = a.sgm[f * N + j];
-      sg[q] = sqrt(si * si + sj * sj);                  // UTILS.f90:620
+      const double sj = a.sgm[f * N + jj];
+      sg[q] = (T)sqrt(si * si + sj * sj);                // UTILS.f90:620
     }
   }
-  double acc[FCH][6];
+  T acc[FCH][6];
 #pragma unroll
   for (int q = 0; q < FCH; ++q)
 #pragma unroll
-    for (int c = 0; c < 6; ++c) acc[q][c] = 0.0;
+    for (int c = 0; c < 6; ++c) acc[q][c] = (T)0;
 
   for (int s = diag ? 1 : 0; s < a.n_shifts; ++s) {
-    const double dx = d0x + a.shifts[3 * s], dy = d0y + a.shifts[3 * s + 1], dz = d0z + a.shifts[3 * s + 2];
-    const double r2 = dx * dx + dy * dy + dz * dz;
-    const double r = sqrt(r2);
-    if (!(r <= a.cut)) continue;
+    const double dxd = d0x + a.shifts[3 * s], dyd = d0y + a.shifts[3 * s + 1], dzd = d0z + a.shifts[3 * s + 2];
+    const double r2d = dxd * dxd + dyd * dyd + dzd * dzd;
+    if (!(sqrt(r2d) <= a.cut)) continue;
+    const T dx = (T)dxd, dy = (T)dyd, dz = (T)dzd;
+    const T r2 = (T)r2d;
+    const T r = F32 ? (T)sqrt(r2d) : sqrt(r2);
     // frequency-independent parts: Fermi damping 1 - 1/(1+exp(-6(r/(beta R)-1)))
-    const double damp = 1.0 - (1.0 / (1.0 + exp(-6.0 * (r * inv_brv - 1.0))));
-    const double inv_r5 = 1.0 / (r2 * r2 * r);
-    const double xx = dx * dx, xy = dx * dy, xz = dx * dz, yy = dy * dy, yz = dy * dz, zz = dz * dz;
+    const T damp = (T)1 - ((T)1 / ((T)1 + M::exp_((T)-6 * (r * inv_brv - (T)1))));
+    const T inv_r5 = (T)1 / (r2 * r2 * r);
+    const T xx = dx * dx, xy = dx * dy, xz = dx * dz, yy = dy * dy, yz = dy * dz, zz = dz * dz;
 #pragma unroll
     for (int q = 0; q < FCH; ++q) {
-      const double ratio = r / sg[q];
-      const double ex = exp(-(ratio * ratio));
-      const double zeta_l = (erf(ratio) - (c4pi * ratio * ex)) * inv_r5;
-      const double zeta_r = (c16pi * ex) / (sg[q] * sg[q] * sg[q] * r2);
+      const T ratio = r / sg[q];
+      const T ex = M::exp_(-(ratio * ratio));
+      const T zeta_l = (M::erf_(ratio) - (c4pi * ratio * ex)) * inv_r5;
+      const T zeta_r = (c16pi * ex) / (sg[q] * sg[q] * sg[q] * r2);
       // -(3 dd - r^2 I) zeta_l + dd zeta_r, damped
-      const double ca = (zeta_r - 3.0 * zeta_l) * damp;
-      const double cb = (r2 * zeta_l) * damp;
+      const T ca = (zeta_r - (T)3 * zeta_l) * damp;
+      const T cb = (r2 * zeta_l) * damp;
       acc[q][0] += ca * xx + cb;
       acc[q][1] += ca * xy;
       acc[q][2] += ca * xz;
@@ -97,25 +149,57 @@ __global__ void __launch_bounds__(128) relay_build_kernel(RelayBuildArgs a) {
       acc[q][5] += ca * zz + cb;
     }
   }
+  const bool full = __all_sync(0xffffffffu, valid);   // all 32 pairs of the warp exist
+  double* st = stage[warp];
 #pragma unroll
   for (int q = 0; q < FCH; ++q) {
     const int f = f0 + q;
+    double t[6];
+#pragma unroll
+    for (int c = 0; c < 6; ++c) t[c] = (double)acc[q][c];
     if (diag) {
       const double inv = 1.0 / a.alpha_w[f * N + i];    // UTILS.f90:583-585
-      acc[q][0] += inv;
-      acc[q][3] += inv;
-      acc[q][5] += inv;
+      t[0] += inv;
+      t[3] += inv;
+      t[5] += inv;
     }
-    const double t[9] = {acc[q][0], acc[q][1], acc[q][2], acc[q][1], acc[q][3],
-                         acc[q][4], acc[q][2], acc[q][4], acc[q][5]};
-    const size_t base = (size_t)f * a.mat_stride + (size_t)(3 * i) * a.ld + 3 * j;
+    const double b9[9] = {t[0], t[1], t[2], t[1], t[3], t[4], t[2], t[4], t[5]};
+    const size_t base = (size_t)f * a.mat_stride + (size_t)(3 * i) * a.ld + 3 * jw;
+    if (full) {
+      // the warp's three block rows, 96 consecutive values each
 #pragma unroll
-    for (int r = 0; r < 3; ++r)
+      for (int r = 0; r < 3; ++r)
 #pragma unroll
-      for (int c = 0; c < 3; ++c) {
-        if (a.A64) a.A64[base + (size_t)r * a.ld + c] = t[3 * r + c];
-        if (a.A32) a.A32[base + (size_t)r * a.ld + c] = (float)t[3 * r + c];
+        for (int c = 0; c < 3; ++c) st[r * 96 + 3 * lane + c] = b9[3 * r + c];
+      __syncwarp();
+#pragma unroll
+      for (int r = 0; r < 3; ++r) {
+        if (a.A64) {
+          double2* dst = reinterpret_cast<double2*>(a.A64 + base + (size_t)r * a.ld);
+          const double2* src = reinterpret_cast<const double2*>(st + r * 96);
+          dst[lane] = src[lane];
+          if (lane < 16) dst[32 + lane] = src[32 + lane];
+        }
+        if (a.A32 && lane < 24) {
+          float4 v;
+          v.x = (float)st[r * 96 + 4 * lane];
+          v.y = (float)st[r * 96 + 4 * lane + 1];
+          v.z = (float)st[r * 96 + 4 * lane + 2];
+          v.w = (float)st[r * 96 + 4 * lane + 3];
+          reinterpret_cast<float4*>(a.A32 + base + (size_t)r * a.ld)[lane] = v;
+        }
       }
+      __syncwarp();
+    } else if (valid) {
+      const size_t pb = base + 3 * (size_t)(j - jw);
+#pragma unroll
+      for (int r = 0; r < 3; ++r)
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+          if (a.A64) a.A64[pb + (size_t)r * a.ld + c] = b9[3 * r + c];
+          if (a.A32) a.A32[pb + (size_t)r * a.ld + c] = (float)b9[3 * r + c];
+        }
+    }
   }
 }
 
@@ -185,8 +269,12 @@ void launch_atom_freq(const AtomDev& a, int N, cudaStream_t s) {
 
 void launch_relay_build(const RelayBuildArgs& a, cudaStream_t s) {
   constexpr int FCH = 7;
-  dim3 grid((a.N + 127) / 128, a.N, 21 / FCH);
-  relay_build_kernel<FCH><<<grid, 128, 0, s>>>(a);
+  // folded rows p and N - 1 - p: at most (N - 1) / 128 + 2 column blocks
+  dim3 grid((a.N - 1) / kBuildThreads + 2, (a.N + 1) / 2, 21 / FCH);
+  if (a.f32_math)
+    relay_build_kernel<FCH, true><<<grid, kBuildThreads, 0, s>>>(a);
+  else
+    relay_build_kernel<FCH, false><<<grid, kBuildThreads, 0, s>>>(a);
 }
 
 void launch_cfdm_build(const CfdmBuildArgs& a, cudaStream_t s) {

@@ -36,6 +36,7 @@ struct RelayBuildArgs {
   double cut;              // min(scs cut-off, damping radius), bohr
   double* A64;             // 21 matrices, row-major lower (may be null)
   float* A32;              // 21 matrices, row-major lower (may be null)
+  int f32_math = 0;        // 1: tensor arithmetic in FP32 from FP64 displacements
 };
 void launch_relay_build(const RelayBuildArgs& a, cudaStream_t s);
 

@@ -40,7 +40,7 @@ EXPORTED = [
     "mbd_rsscs_learned_set_params", "mbd_rsscs_learned_use_network", "mbd_rsscs_learned_eval",
     "mbd_rsscs_set_option", "mbd_rsscs_get_option",
 ]
-OPTIONS = {"residual_gate": 1, "wait_limit_s": 2, "test_stall_wait": 3}
+OPTIONS = {"residual_gate": 1, "wait_limit_s": 2, "test_stall_wait": 3, "fp32_tensor_build": 4}
 
 
 NETWORK_MAGIC = b"MBDNET\0\0"
@@ -368,7 +368,7 @@ class Engine:
             raise MbdError(code, strerror(code))
 
     def set_option(self, name: str, value: float) -> None:
-        """mbd_rsscs_set_option: residual_gate, wait_limit_s, test_stall_wait."""
+        """mbd_rsscs_set_option: residual_gate, wait_limit_s, test_stall_wait, fp32_tensor_build."""
         code = self.lib.mbd_rsscs_set_option(self.ctx, OPTIONS[name], float(value))
         if code != MBD_OK:
             raise MbdError(code, strerror(code))
