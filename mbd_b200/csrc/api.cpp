@@ -338,7 +338,7 @@ void drop_graphs(mbd_ctx* ctx) {
 
 int band_to_tridiag_single(mbd_ctx* ctx, double* Br, int n, double* d, double* e, DevBuf& scratch, cudaStream_t s) {
   const int C = (ctx->cluster_chase && !ctx->test_stall_wait && n <= sb2st_cluster_max_n())
-                    ? sb2st_cluster_size(n, 1, ctx->num_sms) : 0;
+                    ? sb2st_cluster_size(n, 1, ctx->num_sms, tuned_chase_c(ctx, n)) : 0;
   if (C > 0) {
     const BandJob job{Br, n, d, e};
     MBD_CUDA(scratch.reserve(bytes_of<BandJob>(1)));
@@ -450,7 +450,7 @@ int run_front(mbd_ctx* ctx, GeomDev* gd, int gi, int mode, bool relay_only) {
   // 6. dense -> band (stage 1 of the two-stage tridiagonalisation)
   if (two_stage(ctx, p.nH)) {
     MBD_CUDA(launch_sy2sb(gd->hmat.as<double>(), p.ldH, p.nH, sl.trd_ws.as<double>(), gd->band.as<double>(),
-                          ctx->num_sms, s));
+                          ctx->num_sms, s, tuned_rows(ctx, p.nH)));
     ctx->launches += sy2sb_launches(p.nH);
   }
   mark(6);
@@ -671,7 +671,8 @@ int prepare_batch(mbd_ctx* ctx, bool eigen) {
   }
   std::stable_sort(bjobs.begin(), bjobs.end(), [](const BandJob& a, const BandJob& b) { return a.n > b.n; });
   ctx->n_band_cluster = (int)bjobs.size();
-  ctx->band_cluster_C = sb2st_cluster_size(ctx->band_cluster_max_n, ctx->n_band_cluster, ctx->num_sms);
+  ctx->band_cluster_C = sb2st_cluster_size(ctx->band_cluster_max_n, ctx->n_band_cluster, ctx->num_sms,
+                                           tuned_chase_c(ctx, ctx->band_cluster_max_n));
   if (ctx->n_band_cluster > 0 && ctx->band_cluster_C < 1) {   // no cluster fits after all
     fjobs.insert(fjobs.begin(), bjobs.begin(), bjobs.end());
     for (const BandJob& bj : bjobs) ctx->band_max_n = std::max(ctx->band_max_n, bj.n);
@@ -1147,7 +1148,7 @@ int mbd_rsscs_eigvalsh(mbd_ctx* ctx, const double* H, int n, int ld, double* w) 
     MBD_CUDA(ctx->eig_ws.reserve(sizeof(double) * (wsd + (size_t)n * kBandLd)));
     double* ws = ctx->eig_ws.as<double>();
     double* band = ws + wsd;
-    MBD_CUDA(launch_sy2sb(A, ldp, n, ws, band, ctx->num_sms, s));
+    MBD_CUDA(launch_sy2sb(A, ldp, n, ws, band, ctx->num_sms, s, tuned_rows(ctx, n)));
     int st = band_to_tridiag_single(ctx, band, n, d, e, ctx->fb_ws, s);
     if (st != MBD_OK) return st;
   } else {
@@ -1261,6 +1262,29 @@ int mbd_rsscs_set_option(mbd_ctx* ctx, int option, double value) {
     default:
       return MBD_ERR_ARG;
   }
+}
+
+int mbd_rsscs_autotune(mbd_ctx* ctx, int max_n) {
+  if (!ctx || max_n < 1) return MBD_ERR_ARG;
+  MBD_CUDA(cudaSetDevice(ctx->device));
+  MBD_CUDA(cudaDeviceSynchronize());
+  return autotune(ctx, max_n);
+}
+
+int mbd_rsscs_tuning(mbd_ctx* ctx, double* out, int n) {
+  if (!ctx || !out || n < 5 * kTuneClasses) return MBD_ERR_ARG;
+  int filled = 0;
+  for (int k = 0; k < kTuneClasses; ++k) {
+    const TuneChoice& t = ctx->tune[k];
+    double* o = out + 5 * k;
+    o[0] = t.n;
+    o[1] = t.rows;
+    o[2] = t.chase_c;
+    o[3] = t.sy2sb_ms;
+    o[4] = t.chase_ms;
+    if (t.n > 0) filled = k + 1;
+  }
+  return filled;
 }
 
 int mbd_rsscs_get_option(mbd_ctx* ctx, int option, double* value) {

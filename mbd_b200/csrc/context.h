@@ -92,6 +92,16 @@ struct RelaySlot {
   }
 };
 
+// Autotuned launch shapes of the eigen stages per size class n <= 512 * 2^k
+// (tune.cu); 0 = not tuned (the defaults apply).
+constexpr int kTuneClasses = 8;
+struct TuneChoice {
+  int n = 0;            // size the class was timed at
+  int rows = 0;         // panel-QR rows per CTA of the dense -> band reduction
+  int chase_c = 0;      // CTAs of the band -> tridiagonal cluster
+  double sy2sb_ms = 0.0, chase_ms = 0.0;   // the chosen candidates' times
+};
+
 struct Stage {
   enum { kTotal = 0, kSetup, kBuild, kFactor, kSolve, kCfdm, kTridiag, kEig, kCount };
 };
@@ -167,6 +177,7 @@ struct mbd_ctx {
   double wait_limit_s = 2.0;                   // bounded device waits (per device)
   int test_stall_wait = 0;                     // 1: the bulge-chasing launch's first wait runs out
   int f32_tensor_build = 0;                    // 1: mixed modes build the relay tensors in FP32 arithmetic
+  mbd::TuneChoice tune[mbd::kTuneClasses];     // mbd_rsscs_autotune
 };
 
 namespace mbd {
@@ -207,6 +218,11 @@ inline cudaError_t zero_ordered(const mbd_ctx* ctx, void* dst, size_t bytes) {
   return e != cudaSuccess ? e : cudaStreamSynchronize(ctx->stream);
 }
 
+// tune.cu
+int tune_class(int n);
+int autotune(mbd_ctx* ctx, int max_n);
+inline int tuned_rows(const mbd_ctx* ctx, int n) { return ctx->tune[tune_class(n)].rows; }
+inline int tuned_chase_c(const mbd_ctx* ctx, int n) { return ctx->tune[tune_class(n)].chase_c; }
 // api.cpp
 void drop_graphs(mbd_ctx* ctx);
 int run_front(mbd_ctx* ctx, GeomDev* gd, int gi, int mode, bool relay_only = false);

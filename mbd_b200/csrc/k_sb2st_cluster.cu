@@ -311,14 +311,21 @@ int probe_cmax() {
 
 int sb2st_cluster_max_n() { return probe_cmax() * kMaxRows; }
 
-int sb2st_cluster_size(int max_n, int n_jobs, int num_sms) {
+int sb2st_cluster_cmax() { return probe_cmax(); }
+
+int sb2st_cluster_min(int n) { return std::max(1, (n + kMaxRows - 1) / kMaxRows); }
+
+int sb2st_cluster_size(int max_n, int n_jobs, int num_sms, int want_c) {
   const int cmax = probe_cmax();
   if (cmax < 1 || max_n > cmax * kMaxRows) return 0;
-  int C = (max_n + kMaxRows - 1) / kMaxRows;
-  // spare SMs go to wider clusters (fewer tasks per CTA and step), as long as
-  // every CTA keeps at least 64 rows of the largest matrix
-  C = std::max(C, std::min({cmax, num_sms / std::max(1, n_jobs), std::max(1, max_n / (2 * B))}));
-  return std::max(1, std::min(C, cmax));
+  const int cmin = sb2st_cluster_min(max_n);
+  // at most 64 rows per CTA of the largest matrix and no more clusters' worth
+  // of CTAs than the SMs can hold for the batch
+  const int chi = std::max(cmin, std::min({cmax, std::max(1, num_sms / std::max(1, n_jobs)),
+                                            std::max(1, max_n / (2 * B))}));
+  if (want_c > 0) return std::max(cmin, std::min(want_c, chi));
+  // default: spare SMs go to wider clusters (fewer tasks per CTA and step)
+  return chi;
 }
 
 cudaError_t launch_sb2st_cluster(const BandJob* jobs, int n_jobs, int max_n, int C, cudaStream_t s) {

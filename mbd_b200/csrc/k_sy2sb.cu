@@ -905,14 +905,17 @@ size_t sy2sb_workspace_doubles(int n) {
          (kSymmCounters * sizeof(int) + sizeof(double) - 1) / sizeof(double);
 }
 
-cudaError_t launch_sy2sb(double* A, int ld, int n, double* ws, double* Br, int num_sms, cudaStream_t s) {
+cudaError_t launch_sy2sb(double* A, int ld, int n, double* ws, double* Br, int num_sms, cudaStream_t s,
+                         int rows_per_cta) {
   const int max_cluster = sy2sb_max_cluster();
-  // panel rows per CTA the cluster size aims at (MBD_B200_PANEL_ROWS overrides)
-  static const int rows_target = [] {
+  // panel rows per CTA the cluster size aims at: the caller's (autotuned)
+  // choice, else MBD_B200_PANEL_ROWS, else the default
+  static const int rows_env = [] {
     const char* e = std::getenv("MBD_B200_PANEL_ROWS");
     const int v = e ? std::atoi(e) : 0;
     return (v >= 32 && v <= kPanelMaxRowsPerCta) ? v : kPanelRowsTarget;
   }();
+  const int rows_target = (rows_per_cta >= 32 && rows_per_cta <= kPanelMaxRowsPerCta) ? rows_per_cta : rows_env;
   const int nt_full = (n + TL - 1) / TL;
   double* V = ws;
   double* Y = V + (size_t)n * B;

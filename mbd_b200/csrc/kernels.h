@@ -169,7 +169,9 @@ int sy2sb_max_cluster();
 size_t sy2sb_workspace_doubles(int n);
 // Dense (lower, row-major, ld) -> band: A is overwritten; Br[n][kBandLd]
 // receives the band (diagonal d = 0..kBand, zero beyond).  ws: workspace.
-cudaError_t launch_sy2sb(double* A, int ld, int n, double* ws, double* Br, int num_sms, cudaStream_t s);
+// rows_per_cta: panel rows per CTA the QR cluster aims at (0: default).
+cudaError_t launch_sy2sb(double* A, int ld, int n, double* ws, double* Br, int num_sms, cudaStream_t s,
+                         int rows_per_cta = 0);
 int sy2sb_launches(int n);
 // Band -> tridiagonal for a batch of bands in one persistent cooperative
 // launch (bulge chasing, one warp per task of a sweep).
@@ -197,7 +199,11 @@ cudaError_t init_sb2st_attributes();
 // device (0 when clusters of this kernel cannot run), the cluster size for a
 // batch (0: none fits), and the launch (jobs with n <= max_n; writes d, e).
 int sb2st_cluster_max_n();
-int sb2st_cluster_size(int max_n, int n_jobs, int num_sms);
+// want_c > 0: the (autotuned) cluster size to use when it is allowed
+int sb2st_cluster_size(int max_n, int n_jobs, int num_sms, int want_c = 0);
+// smallest and largest cluster size the chase may use for a band of n rows
+int sb2st_cluster_min(int n);
+int sb2st_cluster_cmax();
 cudaError_t launch_sb2st_cluster(const BandJob* jobs, int n_jobs, int max_n, int C, cudaStream_t s);
 
 // ---- block-CG relay solve of the MIXED_LEARNED mode (UTILS.f90:469-473) ----

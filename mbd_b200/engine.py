@@ -38,7 +38,7 @@ EXPORTED = [
     "mbd_rsscs_stream", "mbd_rsscs_eigvalsh", "mbd_rsscs_eigvalsh_noalloc",
     "mbd_rsscs_learned_param_count", "mbd_rsscs_learned_train", "mbd_rsscs_learned_get_params",
     "mbd_rsscs_learned_set_params", "mbd_rsscs_learned_use_network", "mbd_rsscs_learned_eval",
-    "mbd_rsscs_set_option", "mbd_rsscs_get_option",
+    "mbd_rsscs_set_option", "mbd_rsscs_get_option", "mbd_rsscs_autotune", "mbd_rsscs_tuning",
 ]
 OPTIONS = {"residual_gate": 1, "wait_limit_s": 2, "test_stall_wait": 3, "fp32_tensor_build": 4}
 
@@ -176,6 +176,10 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
     lib.mbd_rsscs_set_option.restype = ctypes.c_int
     lib.mbd_rsscs_get_option.argtypes = [vp, ctypes.c_int, ctypes.POINTER(ctypes.c_double)]
     lib.mbd_rsscs_get_option.restype = ctypes.c_int
+    lib.mbd_rsscs_autotune.argtypes = [vp, ctypes.c_int]
+    lib.mbd_rsscs_autotune.restype = ctypes.c_int
+    lib.mbd_rsscs_tuning.argtypes = [vp, ctypes.POINTER(ctypes.c_double), ctypes.c_int]
+    lib.mbd_rsscs_tuning.restype = ctypes.c_int
     lib.mbd_rsscs_learned_use_network.argtypes = [vp, ctypes.c_int]
     lib.mbd_rsscs_learned_use_network.restype = ctypes.c_int
     lib.mbd_rsscs_learned_eval.argtypes = [vp, fp, ctypes.c_int, ctypes.c_int, ip, ip, fp, fp, fp, fp, fp, dp]
@@ -379,6 +383,21 @@ class Engine:
         if code != MBD_OK:
             raise MbdError(code, strerror(code))
         return v.value
+
+    def autotune(self, max_n: int) -> list:
+        """mbd_rsscs_autotune up to Hamiltonians of max_n rows; returns the
+        choices per size class (mbd_rsscs_tuning)."""
+        code = self.lib.mbd_rsscs_autotune(self.ctx, int(max_n))
+        if code != MBD_OK:
+            raise MbdError(code, strerror(code))
+        return self.tuning()
+
+    def tuning(self) -> list:
+        buf = (ctypes.c_double * 40)()
+        k = self.lib.mbd_rsscs_tuning(self.ctx, buf, 40)
+        return [{"n": int(buf[5 * i]), "panel_rows_per_cta": int(buf[5 * i + 1]), "chase_ctas": int(buf[5 * i + 2]),
+                 "dense_to_band_ms": buf[5 * i + 3], "chase_ms": buf[5 * i + 4]} for i in range(max(0, k))
+                if buf[5 * i] > 0]
 
     def save_network(self, path: str) -> None:
         """Write the context's network to `path` (write_network_file)."""

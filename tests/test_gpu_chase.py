@@ -67,3 +67,27 @@ def test_cluster_chase_batch_equals_flag_chase(engines):
         assert ra.status == rb.status == 0
         assert ra.energy == rb.energy
         assert ra.nimag == rb.nimag
+
+
+def test_autotune_choices_and_results():
+    """mbd_rsscs_autotune picks, per size class up to the announced size, a
+    panel-QR rows-per-CTA target among its candidates and a chase cluster size
+    that holds the band; eigenvalues and energies computed afterwards match
+    LAPACK and the oracle fixtures."""
+    from mbd_b200 import Engine
+    with Engine(0) as eng:
+        choices = eng.autotune(3000)
+        assert [c["n"] for c in choices] == [512, 1024, 2048, 3000]
+        for c in choices:
+            assert c["panel_rows_per_cta"] in (48, 96, 192, 384)
+            assert 1 <= c["chase_ctas"] <= 16 and c["chase_ctas"] * 378 >= c["n"]
+            assert c["dense_to_band_ms"] > 0 and c["chase_ms"] > 0
+        S = _sym(3000, seed=77)
+        w = eng.eigvalsh(np.tril(S))
+        ref = np.linalg.eigvalsh(S)
+        np.testing.assert_allclose(w, ref, rtol=0, atol=1e-12 * np.abs(ref).max() * 3000)
+        from tests.golden.make_workload_golden import CASES
+        geo, st = CASES["cluster1000_s1"]()
+        fx = np.load(os.path.join(os.path.dirname(__file__), "golden", "wl_cluster1000_s1.npz"))
+        r = eng.energy(geo, st, mode="plain")
+        assert r.status == 0 and abs(r.energy - float(fx["energy"])) <= 1e-9
