@@ -450,7 +450,7 @@ int run_front(mbd_ctx* ctx, GeomDev* gd, int gi, int mode, bool relay_only) {
   // 6. dense -> band (stage 1 of the two-stage tridiagonalisation)
   if (two_stage(ctx, p.nH)) {
     MBD_CUDA(launch_sy2sb(gd->hmat.as<double>(), p.ldH, p.nH, sl.trd_ws.as<double>(), gd->band.as<double>(),
-                          ctx->num_sms, s, tuned_rows(ctx, p.nH)));
+                          ctx->num_sms, s, tuned_rows(ctx, p.nH), tuned_panel_qr(ctx, p.nH)));
     ctx->launches += sy2sb_launches(p.nH);
   }
   mark(6);
@@ -872,6 +872,8 @@ int mbd_rsscs_create(mbd_ctx** out, int device) {
     ctx->use_graphs = !(ng && ng[0] && ng[0] != '0');
     const char* cc = std::getenv("MBD_B200_CLUSTER_CHASE");
     ctx->cluster_chase = !(cc && cc[0] == '0');
+    const char* pq = std::getenv("MBD_B200_PANEL_QR");
+    ctx->panel_qr_default = (pq && std::strcmp(pq, "tsqr") == 0) ? 1 : 0;
   }
   MBD_CUDA(init_device_constants());
   MBD_CUDA(init_chol_attributes());
@@ -1148,7 +1150,7 @@ int mbd_rsscs_eigvalsh(mbd_ctx* ctx, const double* H, int n, int ld, double* w) 
     MBD_CUDA(ctx->eig_ws.reserve(sizeof(double) * (wsd + (size_t)n * kBandLd)));
     double* ws = ctx->eig_ws.as<double>();
     double* band = ws + wsd;
-    MBD_CUDA(launch_sy2sb(A, ldp, n, ws, band, ctx->num_sms, s, tuned_rows(ctx, n)));
+    MBD_CUDA(launch_sy2sb(A, ldp, n, ws, band, ctx->num_sms, s, tuned_rows(ctx, n), tuned_panel_qr(ctx, n)));
     int st = band_to_tridiag_single(ctx, band, n, d, e, ctx->fb_ws, s);
     if (st != MBD_OK) return st;
   } else {
@@ -1272,16 +1274,17 @@ int mbd_rsscs_autotune(mbd_ctx* ctx, int max_n) {
 }
 
 int mbd_rsscs_tuning(mbd_ctx* ctx, double* out, int n) {
-  if (!ctx || !out || n < 5 * kTuneClasses) return MBD_ERR_ARG;
+  if (!ctx || !out || n < 6 * kTuneClasses) return MBD_ERR_ARG;
   int filled = 0;
   for (int k = 0; k < kTuneClasses; ++k) {
     const TuneChoice& t = ctx->tune[k];
-    double* o = out + 5 * k;
+    double* o = out + 6 * k;
     o[0] = t.n;
     o[1] = t.rows;
     o[2] = t.chase_c;
     o[3] = t.sy2sb_ms;
     o[4] = t.chase_ms;
+    o[5] = t.panel_qr;
     if (t.n > 0) filled = k + 1;
   }
   return filled;

@@ -98,6 +98,7 @@ constexpr int kTuneClasses = 8;
 struct TuneChoice {
   int n = 0;            // size the class was timed at
   int rows = 0;         // panel-QR rows per CTA of the dense -> band reduction
+  int panel_qr = -1;    // panel QR: 0 per-column Householder, 1 TSQR (-1: not tuned)
   int chase_c = 0;      // CTAs of the band -> tridiagonal cluster
   double sy2sb_ms = 0.0, chase_ms = 0.0;   // the chosen candidates' times
 };
@@ -178,6 +179,7 @@ struct mbd_ctx {
   int test_stall_wait = 0;                     // 1: the bulge-chasing launch's first wait runs out
   int f32_tensor_build = 0;                    // 1: mixed modes build the relay tensors in FP32 arithmetic
   mbd::TuneChoice tune[mbd::kTuneClasses];     // mbd_rsscs_autotune
+  int panel_qr_default = 0;                    // MBD_B200_PANEL_QR=tsqr: 1
 };
 
 namespace mbd {
@@ -222,6 +224,10 @@ inline cudaError_t zero_ordered(const mbd_ctx* ctx, void* dst, size_t bytes) {
 int tune_class(int n);
 int autotune(mbd_ctx* ctx, int max_n);
 inline int tuned_rows(const mbd_ctx* ctx, int n) { return ctx->tune[tune_class(n)].rows; }
+inline int tuned_panel_qr(const mbd_ctx* ctx, int n) {
+  const int q = ctx->tune[tune_class(n)].panel_qr;
+  return q >= 0 ? q : ctx->panel_qr_default;
+}
 inline int tuned_chase_c(const mbd_ctx* ctx, int n) { return ctx->tune[tune_class(n)].chase_c; }
 // api.cpp
 void drop_graphs(mbd_ctx* ctx);

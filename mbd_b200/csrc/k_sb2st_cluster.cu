@@ -104,7 +104,7 @@ struct Rows {
 template <bool LOCAL>
 __device__ __forceinline__ void chase_task(const Rows<LOCAL>& rm, int n, int r, int i, int k, int t, int R,
                                            double* refl, double* const* peer_refl, double* pv, double* pw,
-                                           double* ps, int pair, bool owarp) {
+                                           double* ps, int pair, bool owarp, int rank) {
   const int l = threadIdx.x & 31;
   const int L = min(B, n - r);
   const int rn = r + B;
@@ -199,8 +199,10 @@ __device__ __forceinline__ void chase_task(const Rows<LOCAL>& rm, int n, int r, 
         for (int j = 0; j < B; ++j)
           if (j < L) orowp[-j] = orow[j];
       }
-      // H' to the owner of row rn, for task (i, k + 1) at step t + 1
-      double* slot = peer_refl[rn / R] + ((((t + 1) & 1) * kRing) + (i % kRing)) * RSLOT;
+      // H' to the owner of row rn, for task (i, k + 1) at step t + 1 (through
+      // the cluster window only when that is another CTA)
+      const int owner = rn / R;
+      double* slot = (owner == rank ? refl : peer_refl[owner]) + ((((t + 1) & 1) * kRing) + (i % kRing)) * RSLOT;
       slot[l] = v2;
       if (l == 0) slot[B] = tau2;
     }
@@ -256,10 +258,10 @@ __global__ void __launch_bounds__(THREADS, 1) sb2st_cluster_kernel(const BandJob
       if (i >= 0 && k >= 0 && r < hi && r < n) {
         if (min(n, r + 2 * B) <= hi) {
           const Rows<true> rm{band + (r - lo) * SLD, nullptr, 0};
-          chase_task(rm, n, r, i, k, t, R, refl, peer_refl, pv, pw, ps, pair, owarp);
+          chase_task(rm, n, r, i, k, t, R, refl, peer_refl, pv, pw, ps, pair, owarp, rank);
         } else {
           const Rows<false> rm{band + (r - lo) * SLD, next_band, hi - r};
-          chase_task(rm, n, r, i, k, t, R, refl, peer_refl, pv, pw, ps, pair, owarp);
+          chase_task(rm, n, r, i, k, t, R, refl, peer_refl, pv, pw, ps, pair, owarp, rank);
         }
       }
       cl.sync();

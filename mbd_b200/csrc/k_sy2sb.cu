@@ -15,9 +15,8 @@
 //              dots.
 //   symm       Y = A22 V (A22 the trailing m x m lower-stored block), row
 //              blocks of 64 split over S column chunks (fixed-order partials)
-//              then, in the same launch, the last CTA of each row block:
-//              Y <- sum of the partials; Y <- Y T; block partials of V^T Y,
-//              and the last row block: M = T^T (V^T Y)
+//   yred       Y <- sum of the partials; Y <- Y T; block partials of V^T Y
+//   mform      M = T^T (V^T Y)
 //   zform      Z = Y - 1/2 V M
 //   syr2k      A22 -= V Z^T + Z V^T (lower 64 x 64 tiles)
 // so that A22 <- Q^T A22 Q.  Every reduction is summed in a fixed order: the
@@ -551,11 +550,6 @@ __device__ __forceinline__ void cp_async_wait() {
 constexpr int FV = B + 4;                        // 36: V rows in shared memory (4 mod 16)
 constexpr int kSymmStage = TL * FS + TL * FV;    // doubles per stage
 constexpr size_t kSymmSmem = sizeof(double) * 2 * kSymmStage;
-// arrival counters of the fused reductions: one per row block, the last one
-// for the row blocks (n <= 2 * 16 * kPanelMaxRowsPerCta)
-constexpr int kSymmCounters = 1024;
-static_assert(sizeof(double) * 2 * kSymmStage >= sizeof(double) * (3 * TL + B) * (B + 1),
-              "the reductions reuse the stages' shared memory");
 
 __device__ __forceinline__ void symm_stage(const double* A22, int ld, int m, const double* V, int I, int J,
                                            double* As, double* Vs) {
@@ -598,84 +592,8 @@ __device__ __forceinline__ void symm_mma(const double* As, const double* Vs, int
   }
 }
 
-// Y_I = sum_s Yp[s]_I (s in order); Y_I <- Y_I T; Up[I] = V_I^T Y_I, for the
-// 64-row block I, by the 128 threads of one CTA (sm: 3 TL (B + 1) + B (B + 1)
-// doubles).  Partials written by other CTAs of the launch are read past L1.
-__device__ __forceinline__ void yred_block(const double* Yp, int S, int m, const double* T, const double* V,
-                                           double* Y, double* Up, int I, double* sm) {
-  double (*Ts)[B + 1] = reinterpret_cast<double (*)[B + 1]>(sm);
-  double (*Ys)[B + 1] = reinterpret_cast<double (*)[B + 1]>(sm + B * (B + 1));
-  double (*Vs)[B + 1] = reinterpret_cast<double (*)[B + 1]>(sm + (B + TL) * (B + 1));
-  const int tid = threadIdx.x;
-  for (int e = tid; e < B * B; e += 128) Ts[e / B][e % B] = T[e];
-  for (int e = tid; e < TL * B; e += 128) {
-    const int r = e / B, c = e % B, gr = I * TL + r;
-    double y = 0.0, v = 0.0;
-    if (gr < m) {
-      for (int s2 = 0; s2 < S; ++s2) y += __ldcg(Yp + ((size_t)s2 * m + gr) * B + c);
-      v = V[(size_t)gr * B + c];
-    }
-    Ys[r][c] = y;
-    Vs[r][c] = v;
-  }
-  __syncthreads();
-  double yt[16];
-#pragma unroll
-  for (int t = 0; t < 16; ++t) {
-    const int e = tid + 128 * t, r = e / B, c = e % B;
-    double x = 0.0;
-    for (int l = 0; l <= c; ++l) x += Ys[r][l] * Ts[l][c];
-    yt[t] = x;
-  }
-  __syncthreads();
-#pragma unroll
-  for (int t = 0; t < 16; ++t) {
-    const int e = tid + 128 * t, r = e / B, c = e % B, gr = I * TL + r;
-    Ys[r][c] = yt[t];
-    if (gr < m) Y[(size_t)gr * B + c] = yt[t];
-  }
-  __syncthreads();
-#pragma unroll
-  for (int t = 0; t < 8; ++t) {
-    const int e = tid + 128 * t, p = e / B, c = e % B;
-    double u = 0.0;
-    for (int r = 0; r < TL; ++r) u += Vs[r][p] * Ys[r][c];
-    Up[(size_t)I * B * B + e] = u;
-  }
-}
-
-// M = T^T U, U = sum_I Up[I] (I in order), by the 128 threads of one CTA
-// (sm: 2 B (B + 1) doubles).
-__device__ __forceinline__ void mform_block(const double* Up, int nt, const double* T, double* M, double* sm) {
-  double (*Us)[B + 1] = reinterpret_cast<double (*)[B + 1]>(sm);
-  double (*Ts)[B + 1] = reinterpret_cast<double (*)[B + 1]>(sm + B * (B + 1));
-  const int tid = threadIdx.x;
-#pragma unroll
-  for (int t = 0; t < 8; ++t) {
-    const int e = tid + 128 * t, p = e / B, c = e % B;
-    double u = 0.0;
-    for (int I = 0; I < nt; ++I) u += __ldcg(Up + (size_t)I * B * B + e);
-    Us[p][c] = u;
-    Ts[p][c] = T[e];
-  }
-  __syncthreads();
-#pragma unroll
-  for (int t = 0; t < 8; ++t) {
-    const int e = tid + 128 * t, p = e / B, c = e % B;
-    double x = 0.0;
-    for (int l = 0; l <= p; ++l) x += Ts[l][p] * Us[l][c];   // (T^T)[p][l] = T[l][p], l <= p
-    M[e] = x;
-  }
-}
-
-// After its partial, the last of the S CTAs of row block I (an arrival count
-// per block) reduces the block (yred_block), and the last block to finish
-// forms M (mform_block): the reductions run inside this launch, in the same
-// order as separate passes would sum.  The counters are zero on entry and are
-// left zero for the next panel.
 __global__ void __launch_bounds__(128) symm_kernel(const double* A, int ld, int row0, int m, const double* V,
-                                                   double* Yp, int chunk, int S, const double* T, double* Y,
-                                                   double* Up, double* M, int* cnt) {
+                                                   double* Yp, int chunk) {
   extern __shared__ __align__(16) double dsm[];
   const int I = blockIdx.x, s = blockIdx.y;
   const int nt = (m + TL - 1) / TL;
@@ -716,23 +634,65 @@ __global__ void __launch_bounds__(128) symm_kernel(const double* A, int ld, int 
         out[(size_t)gr * B + q * 8 + 2 * q4 + 1] = acc[i][q][1];
       }
   }
-  __shared__ int s_last;
-  __threadfence();   // this CTA's partial is visible before its arrival counts
+}
+
+// Y = sum_s Yp[s]; Y <- Y T; Up[I] = V_I^T Y_I (64-row blocks, 256 threads).
+__global__ void __launch_bounds__(256) yred_kernel(const double* Yp, int S, int m, const double* T, const double* V,
+                                                   double* Y, double* Up) {
+  __shared__ double Ts[B][B + 1];
+  __shared__ double Ys[TL][B + 1];
+  __shared__ double Vs[TL][B + 1];
+  const int I = blockIdx.x, tid = threadIdx.x;
+  for (int e = tid; e < B * B; e += 256) Ts[e / B][e % B] = T[e];
+  for (int e = tid; e < TL * B; e += 256) {
+    const int r = e / B, c = e % B, gr = I * TL + r;
+    double y = 0.0, v = 0.0;
+    if (gr < m) {
+      for (int s = 0; s < S; ++s) y += Yp[((size_t)s * m + gr) * B + c];
+      v = V[(size_t)gr * B + c];
+    }
+    Ys[r][c] = y;
+    Vs[r][c] = v;
+  }
   __syncthreads();
-  if (tid == 0) s_last = atomicAdd(cnt + I, 1) == S - 1;
+  double yt[8];
+#pragma unroll
+  for (int t = 0; t < 8; ++t) {
+    const int e = tid + 256 * t, r = e / B, c = e % B;
+    double x = 0.0;
+    for (int l = 0; l <= c; ++l) x += Ys[r][l] * Ts[l][c];
+    yt[t] = x;
+  }
   __syncthreads();
-  if (!s_last) return;
-  __threadfence();
-  if (tid == 0) cnt[I] = 0;
-  yred_block(Yp, S, m, T, V, Y, Up, I, dsm);
-  __threadfence();
+#pragma unroll
+  for (int t = 0; t < 8; ++t) {
+    const int e = tid + 256 * t, r = e / B, c = e % B, gr = I * TL + r;
+    Ys[r][c] = yt[t];
+    if (gr < m) Y[(size_t)gr * B + c] = yt[t];
+  }
   __syncthreads();
-  if (tid == 0) s_last = atomicAdd(cnt + kSymmCounters - 1, 1) == nt - 1;
+#pragma unroll
+  for (int t = 0; t < 4; ++t) {
+    const int e = tid + 256 * t, p = e / B, c = e % B;
+    double u = 0.0;
+    for (int r = 0; r < TL; ++r) u += Vs[r][p] * Ys[r][c];
+    Up[(size_t)I * B * B + e] = u;
+  }
+}
+
+// M = T^T U, U = sum_I Up[I] (one CTA of B*B threads).
+__global__ void __launch_bounds__(B* B) mform_kernel(const double* Up, int nt, const double* T, double* M) {
+  __shared__ double Us[B][B + 1];
+  __shared__ double Ts[B][B + 1];
+  const int e = threadIdx.x, p = e / B, c = e % B;
+  double u = 0.0;
+  for (int I = 0; I < nt; ++I) u += Up[(size_t)I * B * B + e];
+  Us[p][c] = u;
+  Ts[p][c] = T[e];
   __syncthreads();
-  if (!s_last) return;
-  __threadfence();
-  if (tid == 0) cnt[kSymmCounters - 1] = 0;
-  mform_block(Up, nt, T, M, dsm);
+  double x = 0.0;
+  for (int l = 0; l <= p; ++l) x += Ts[l][p] * Us[l][c];   // (T^T)[p][l] = T[l][p], l <= p
+  M[e] = x;
 }
 
 // Z = Y - 1/2 V M (rows in blocks of 64, 256 threads)
@@ -843,6 +803,10 @@ __global__ void band_copy_kernel(const double* A, int ld, int n, double* Br) {
 }  // namespace
 
 cudaError_t init_sy2sb_attributes() {
+  {
+    cudaError_t e = init_tsqr_attributes();
+    if (e != cudaSuccess) return e;
+  }
   for (int v = 0; v < kQrVariants; ++v) {
     cudaError_t e = cudaFuncSetAttribute(qr_kernel(v), cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
     if (e != cudaSuccess) return e;
@@ -901,12 +865,11 @@ int sy2sb_max_n() {
 size_t sy2sb_workspace_doubles(int n) {
   const int m = n;
   const int nt = (m + TL - 1) / TL;
-  return (size_t)m * B * (3 + kSymmMaxSplit) + (size_t)nt * B * B + 3 * B * B + B + 256 +
-         (kSymmCounters * sizeof(int) + sizeof(double) - 1) / sizeof(double);
+  return (size_t)m * B * (3 + kSymmMaxSplit) + (size_t)nt * B * B + 3 * B * B + B + 256;
 }
 
 cudaError_t launch_sy2sb(double* A, int ld, int n, double* ws, double* Br, int num_sms, cudaStream_t s,
-                         int rows_per_cta) {
+                         int rows_per_cta, int panel_qr) {
   const int max_cluster = sy2sb_max_cluster();
   // panel rows per CTA the cluster size aims at: the caller's (autotuned)
   // choice, else MBD_B200_PANEL_ROWS, else the default
@@ -925,10 +888,6 @@ cudaError_t launch_sy2sb(double* A, int ld, int n, double* ws, double* Br, int n
   double* T = Up + (size_t)nt_full * B * B;
   double* M = T + B * B;
   double* tau = M + B * B;
-  int* cnt = reinterpret_cast<int*>(tau + B + 256);
-  if (nt_full + 1 > kSymmCounters) return cudaErrorInvalidValue;
-  cudaError_t ez = cudaMemsetAsync(cnt, 0, sizeof(int) * kSymmCounters, s);
-  if (ez != cudaSuccess) return ez;
   for (int c0 = 0; c0 + B + 1 < n; c0 += B) {
     const int row0 = c0 + B, m = n - row0;
     // panel QR in one cluster (a power of two of CTAs)
@@ -937,9 +896,14 @@ cudaError_t launch_sy2sb(double* A, int ld, int n, double* ws, double* Br, int n
     while (C * kPanelMaxRowsPerCta < m) C *= 2;
     if (C > kPanelMaxCluster) return cudaErrorInvalidValue;   // the caller keeps n <= sy2sb_max_n()
     const int R = (m + C - 1) / C;
+    PanelArgs pa{A, ld, row0, c0, m, R, V, T, tau};
+    if (panel_qr == 1 && C >= 2 && R >= B && R <= tsqr_max_rows_per_cta()) {
+      // TSQR with Householder reconstruction: three cluster exchanges per panel
+      cudaError_t e = launch_tsqr_panel(pa, C, s);
+      if (e != cudaSuccess) return e;
+    } else {
     const int qv = qr_variant(R);
     if (qv < 0) return cudaErrorInvalidValue;
-    PanelArgs pa{A, ld, row0, c0, m, R, V, T, tau};
     cudaLaunchConfig_t cfg{};
     cfg.gridDim = dim3(C);
     cfg.blockDim = dim3(kQrWarps[qv] * 32);
@@ -954,6 +918,7 @@ cudaError_t launch_sy2sb(double* A, int ld, int n, double* ws, double* Br, int n
     cfg.numAttrs = 1;
     cudaError_t e = cudaLaunchKernelEx(&cfg, qr_kernel(qv), pa);
     if (e != cudaSuccess) return e;
+    }
     // two-sided update of the trailing block
     const int nt = (m + TL - 1) / TL;
     int S = (2 * num_sms + nt - 1) / nt;   // one wave at two CTAs per SM
@@ -961,7 +926,9 @@ cudaError_t launch_sy2sb(double* A, int ld, int n, double* ws, double* Br, int n
     if (S > nt) S = nt;
     const int chunk = (nt + S - 1) / S;
     S = (nt + chunk - 1) / chunk;
-    symm_kernel<<<dim3(nt, S), 128, kSymmSmem, s>>>(A, ld, row0, m, V, Yp, chunk, S, T, Y, Up, M, cnt);
+    symm_kernel<<<dim3(nt, S), 128, kSymmSmem, s>>>(A, ld, row0, m, V, Yp, chunk);
+    yred_kernel<<<nt, 256, 0, s>>>(Yp, S, m, T, V, Y, Up);
+    mform_kernel<<<1, B * B, 0, s>>>(Up, nt, T, M);
     zform_kernel<<<nt, 256, 0, s>>>(Y, V, M, m, Z);
     syr2k_kernel<<<nt * (nt + 1) / 2, 128, kSyr2kSmem, s>>>(A, ld, row0, m, V, Z);
   }
@@ -971,7 +938,7 @@ cudaError_t launch_sy2sb(double* A, int ld, int n, double* ws, double* Br, int n
 
 int sy2sb_launches(int n) {
   int k = 0;
-  for (int c0 = 0; c0 + B + 1 < n; c0 += B) k += 4;
+  for (int c0 = 0; c0 + B + 1 < n; c0 += B) k += 6;
   return k + 1;
 }
 

@@ -169,9 +169,15 @@ int sy2sb_max_cluster();
 size_t sy2sb_workspace_doubles(int n);
 // Dense (lower, row-major, ld) -> band: A is overwritten; Br[n][kBandLd]
 // receives the band (diagonal d = 0..kBand, zero beyond).  ws: workspace.
-// rows_per_cta: panel rows per CTA the QR cluster aims at (0: default).
+// rows_per_cta: panel rows per CTA the QR cluster aims at (0: default);
+// panel_qr: 0 Householder QR with one cluster exchange per column,
+// 1 TSQR with Householder reconstruction (k_tsqr.cu) where it applies.
 cudaError_t launch_sy2sb(double* A, int ld, int n, double* ws, double* Br, int num_sms, cudaStream_t s,
-                         int rows_per_cta = 0);
+                         int rows_per_cta = 0, int panel_qr = 0);
+// TSQR panel QR (k_tsqr.cu): rows per CTA in [32, tsqr_max_rows_per_cta()], C <= 16.
+cudaError_t init_tsqr_attributes();
+int tsqr_max_rows_per_cta();
+cudaError_t launch_tsqr_panel(const PanelArgs& pa, int C, cudaStream_t s);
 int sy2sb_launches(int n);
 // Band -> tridiagonal for a batch of bands in one persistent cooperative
 // launch (bulge chasing, one warp per task of a sweep).

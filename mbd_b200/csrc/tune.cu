@@ -5,9 +5,11 @@
 // For each size class (n <= 512 * 2^k) up to the largest Hamiltonian a
 // caller announces, it times on a synthetic symmetric matrix of the class's
 // size, generated on the device:
-//   * the dense -> band reduction with each panel-QR rows-per-CTA target
-//     (48, 96, 192, 384: the target sets how many CTAs share a panel's QR
-//     cluster, trading cluster-barrier latency against per-CTA work);
+//   * the dense -> band reduction with each panel-QR algorithm (Householder
+//     with one cluster exchange per column, or TSQR with Householder
+//     reconstruction) and rows-per-CTA target (48 .. 384: the target sets how
+//     many CTAs share a panel's QR cluster, trading exchange latency against
+//     per-CTA work);
 //   * the cluster-resident band -> tridiagonal chase with each cluster size
 //     from the smallest that holds the band to the widest allowed (more CTAs:
 //     fewer tasks per CTA and step, a wider barrier);
@@ -89,14 +91,15 @@ int autotune(mbd_ctx* ctx, int max_n) {
                                                                      0x5eedu + (unsigned)k);
     TuneChoice tc;
     tc.n = n;
-    // dense -> band: panel rows per CTA
+    // dense -> band: panel QR algorithm and rows per CTA
     double best = 1e30;
-    for (int rows : {48, 96, 192, 384}) {
+    const int cand[][2] = {{0, 48}, {0, 96}, {0, 192}, {0, 384}, {1, 96}, {1, 192}, {1, 384}};
+    for (const auto& cq : cand) {
       double t = 1e30;
       for (int rep = 0; rep < 2; ++rep) {
         if (fail(cudaMemcpyAsync(a.p, a0.p, mat, cudaMemcpyDeviceToDevice, s)) || fail(cudaEventRecord(e0, s)) ||
             fail(launch_sy2sb(static_cast<double*>(a.p), ld, n, static_cast<double*>(ws.p),
-                              static_cast<double*>(band.p), ctx->num_sms, s, rows)) ||
+                              static_cast<double*>(band.p), ctx->num_sms, s, cq[1], cq[0])) ||
             fail(cudaEventRecord(e1, s)) || fail(cudaEventSynchronize(e1)))
           break;
         float ms = 0.f;
@@ -106,7 +109,8 @@ int autotune(mbd_ctx* ctx, int max_n) {
       if (status != MBD_OK) break;
       if (t < best) {
         best = t;
-        tc.rows = rows;
+        tc.panel_qr = cq[0];
+        tc.rows = cq[1];
       }
     }
     tc.sy2sb_ms = best;

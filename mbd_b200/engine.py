@@ -393,11 +393,12 @@ class Engine:
         return self.tuning()
 
     def tuning(self) -> list:
-        buf = (ctypes.c_double * 40)()
-        k = self.lib.mbd_rsscs_tuning(self.ctx, buf, 40)
-        return [{"n": int(buf[5 * i]), "panel_rows_per_cta": int(buf[5 * i + 1]), "chase_ctas": int(buf[5 * i + 2]),
-                 "dense_to_band_ms": buf[5 * i + 3], "chase_ms": buf[5 * i + 4]} for i in range(max(0, k))
-                if buf[5 * i] > 0]
+        buf = (ctypes.c_double * 48)()
+        k = self.lib.mbd_rsscs_tuning(self.ctx, buf, 48)
+        return [{"n": int(buf[6 * i]), "panel_qr": {0: "householder", 1: "tsqr"}.get(int(buf[6 * i + 5]), "default"),
+                 "panel_rows_per_cta": int(buf[6 * i + 1]), "chase_ctas": int(buf[6 * i + 2]),
+                 "dense_to_band_ms": buf[6 * i + 3], "chase_ms": buf[6 * i + 4]} for i in range(max(0, k))
+                if buf[6 * i] > 0]
 
     def save_network(self, path: str) -> None:
         """Write the context's network to `path` (write_network_file)."""

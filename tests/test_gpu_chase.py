@@ -80,6 +80,7 @@ def test_autotune_choices_and_results():
         assert [c["n"] for c in choices] == [512, 1024, 2048, 3000]
         for c in choices:
             assert c["panel_rows_per_cta"] in (48, 96, 192, 384)
+            assert c["panel_qr"] in ("householder", "tsqr")
             assert 1 <= c["chase_ctas"] <= 16 and c["chase_ctas"] * 378 >= c["n"]
             assert c["dense_to_band_ms"] > 0 and c["chase_ms"] > 0
         S = _sym(3000, seed=77)
