@@ -235,15 +235,16 @@ int mbd_rsscs_get_option(mbd_ctx* ctx, int option, double* value);
  * n <= 512 * 2^k up to max_n (the largest Hamiltonian dimension 3 N n_SL the
  * caller will compute): the dense -> band panel QR (per-column Householder or
  * TSQR with Householder reconstruction) and its rows per CTA (48 .. 384), and
- * the band -> tridiagonal cluster size; keeps the fastest per class
- * in the context for its later computes and eigenvalue calls.  Allocates and
- * frees its own test matrices; takes about a second up to n = 6000.  Call it
- * before upload (a batch uploaded before keeps working: its captured graphs
- * are dropped).
- * mbd_rsscs_tuning writes, per class k = 0 .. 7, out[6k .. 6k+5] = {size
- * timed, panel rows per CTA, chase cluster CTAs, dense -> band ms, chase ms,
- * panel QR (0 Householder, 1 TSQR, -1 not tuned)} (n >= 48) and returns the
- * number of classes up to the last tuned one. */
+ * the band -> tridiagonal chase (flag-synchronised, or cluster-resident at
+ * each cluster size); keeps the fastest per class in the context for its
+ * later computes and eigenvalue calls.  Allocates and frees its own test
+ * matrices; takes a few seconds up to n = 6000.  Call it before upload (a
+ * batch uploaded before keeps working: its captured graphs are dropped).
+ * mbd_rsscs_tuning writes, per class k = 0 .. 7, out[8k .. 8k+7] = {size
+ * timed, panel rows per CTA, chase (cluster CTAs, or -1: flag-synchronised),
+ * dense -> band ms, chase ms, panel QR (0 Householder, 1 TSQR, -1 not tuned),
+ * flag-synchronised chase ms, best cluster-resident chase ms} (n >= 64) and
+ * returns the number of classes up to the last tuned one. */
 int mbd_rsscs_autotune(mbd_ctx* ctx, int max_n);
 int mbd_rsscs_tuning(mbd_ctx* ctx, double* out, int n);
 

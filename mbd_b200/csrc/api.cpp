@@ -337,7 +337,8 @@ void drop_graphs(mbd_ctx* ctx) {
 }
 
 int band_to_tridiag_single(mbd_ctx* ctx, double* Br, int n, double* d, double* e, DevBuf& scratch, cudaStream_t s) {
-  const int C = (ctx->cluster_chase && !ctx->test_stall_wait && n <= sb2st_cluster_max_n())
+  const int C = (ctx->cluster_chase && !ctx->test_stall_wait && n <= sb2st_cluster_max_n() &&
+                 tuned_chase_c(ctx, n) != kChaseFlag)
                     ? sb2st_cluster_size(n, 1, ctx->num_sms, tuned_chase_c(ctx, n)) : 0;
   if (C > 0) {
     const BandJob job{Br, n, d, e};
@@ -661,7 +662,7 @@ int prepare_batch(mbd_ctx* ctx, bool eigen) {
     GeomDev* gd = ctx->geoms[g].get();
     if (!two_stage(ctx, gd->plan.nH)) continue;
     const BandJob bj{gd->band.as<double>(), gd->plan.nH, gd->d, gd->e};
-    if (bj.n <= cap) {
+    if (bj.n <= cap && tuned_chase_c(ctx, bj.n) != kChaseFlag) {
       bjobs.push_back(bj);
       ctx->band_cluster_max_n = std::max(ctx->band_cluster_max_n, bj.n);
     } else {
@@ -1274,17 +1275,19 @@ int mbd_rsscs_autotune(mbd_ctx* ctx, int max_n) {
 }
 
 int mbd_rsscs_tuning(mbd_ctx* ctx, double* out, int n) {
-  if (!ctx || !out || n < 6 * kTuneClasses) return MBD_ERR_ARG;
+  if (!ctx || !out || n < 8 * kTuneClasses) return MBD_ERR_ARG;
   int filled = 0;
   for (int k = 0; k < kTuneClasses; ++k) {
     const TuneChoice& t = ctx->tune[k];
-    double* o = out + 6 * k;
+    double* o = out + 8 * k;
     o[0] = t.n;
     o[1] = t.rows;
     o[2] = t.chase_c;
     o[3] = t.sy2sb_ms;
     o[4] = t.chase_ms;
     o[5] = t.panel_qr;
+    o[6] = t.flag_chase_ms;
+    o[7] = t.cluster_chase_ms;
     if (t.n > 0) filled = k + 1;
   }
   return filled;

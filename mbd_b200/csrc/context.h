@@ -99,9 +99,12 @@ struct TuneChoice {
   int n = 0;            // size the class was timed at
   int rows = 0;         // panel-QR rows per CTA of the dense -> band reduction
   int panel_qr = -1;    // panel QR: 0 per-column Householder, 1 TSQR (-1: not tuned)
-  int chase_c = 0;      // CTAs of the band -> tridiagonal cluster
+  int chase_c = 0;      // band -> tridiagonal: CTAs of the cluster-resident chase
+                        // (0: its default size), or kChaseFlag: the flag-synchronised chase
   double sy2sb_ms = 0.0, chase_ms = 0.0;   // the chosen candidates' times
+  double flag_chase_ms = 0.0, cluster_chase_ms = 0.0;   // the best of each chase kernel
 };
+constexpr int kChaseFlag = -1;
 
 struct Stage {
   enum { kTotal = 0, kSetup, kBuild, kFactor, kSolve, kCfdm, kTridiag, kEig, kCount };

@@ -10,9 +10,11 @@
 //     reconstruction) and rows-per-CTA target (48 .. 384: the target sets how
 //     many CTAs share a panel's QR cluster, trading exchange latency against
 //     per-CTA work);
-//   * the cluster-resident band -> tridiagonal chase with each cluster size
-//     from the smallest that holds the band to the widest allowed (more CTAs:
-//     fewer tasks per CTA and step, a wider barrier);
+//   * the band -> tridiagonal chase: the flag-synchronised kernel (each
+//     sweep waits for its predecessor's progress flag in global memory)
+//     against the cluster-resident kernel (lock-step wavefront steps) with
+//     each cluster size from the smallest that holds the band to the widest
+//     allowed (more CTAs: fewer tasks per CTA and step, a wider barrier);
 // each candidate twice, keeping the faster run, and stores the fastest choice
 // per class in the context.  Later computes and eigenvalue calls of the
 // context use them.  A choice only regroups sums (cluster partials), so the
@@ -114,14 +116,46 @@ int autotune(mbd_ctx* ctx, int max_n) {
       }
     }
     tc.sy2sb_ms = best;
-    // band -> tridiagonal: cluster size (the band stays as the last run left it)
+    // band -> tridiagonal: the flag-synchronised chase (which works on the
+    // band in place, so every run starts from a saved copy) against the
+    // cluster-resident chase at each cluster size (which leaves the band in
+    // global memory untouched)
+    double* d = static_cast<double*>(de.p);
+    const BandJob bj{static_cast<double*>(band.p), n, d, d + n};
+    const size_t band_bytes = sizeof(double) * (size_t)n * kBandLd;
+    std::vector<SweepItem> items;
+    for (int i = 0; i + 3 <= n; ++i) items.push_back(SweepItem{0, i, i - 1, 0});
+    Buf band0, items_d, prog;
+    if (status != MBD_OK || fail(cudaMalloc(&band0.p, band_bytes)) ||
+        fail(cudaMalloc(&items_d.p, sizeof(SweepItem) * std::max<size_t>(1, items.size()))) ||
+        fail(cudaMalloc(&prog.p, sizeof(int) * std::max<size_t>(1, items.size()))) ||
+        fail(cudaMemcpyAsync(band0.p, band.p, band_bytes, cudaMemcpyDeviceToDevice, s)) ||
+        fail(cudaMemcpyAsync(items_d.p, items.data(), sizeof(SweepItem) * items.size(), cudaMemcpyHostToDevice, s)) ||
+        fail(cudaMemcpyAsync(job.p, &bj, sizeof(bj), cudaMemcpyHostToDevice, s)) || fail(cudaStreamSynchronize(s)))
+      break;
+    {
+      double t = 1e30;
+      for (int rep = 0; rep < 2; ++rep) {
+        if (fail(cudaMemcpyAsync(band.p, band0.p, band_bytes, cudaMemcpyDeviceToDevice, s)) ||
+            fail(cudaEventRecord(e0, s)) ||
+            fail(launch_sb2st(static_cast<const BandJob*>(job.p), 1, static_cast<const SweepItem*>(items_d.p),
+                              (int)items.size(), static_cast<int*>(prog.p), ctx->err_flag, ctx->num_sms, n,
+                              n / (2 * kBand) + 1, -1, s)) ||
+            fail(cudaEventRecord(e1, s)) || fail(cudaEventSynchronize(e1)))
+          break;
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, e0, e1);
+        t = std::min(t, (double)ms);
+      }
+      if (status != MBD_OK) break;
+      tc.flag_chase_ms = t;
+      tc.chase_c = kChaseFlag;
+      tc.chase_ms = t;
+      if (fail(cudaMemcpyAsync(band.p, band0.p, band_bytes, cudaMemcpyDeviceToDevice, s))) break;
+    }
     const int cmin = sb2st_cluster_min(n);
     const int chi = sb2st_cluster_size(n, 1, ctx->num_sms, 0);   // 0: no cluster holds this band
     if (status == MBD_OK && chi > 0) {
-      double* d = static_cast<double*>(de.p);
-      const BandJob bj{static_cast<double*>(band.p), n, d, d + n};
-      if (fail(cudaMemcpyAsync(job.p, &bj, sizeof(bj), cudaMemcpyHostToDevice, s)) || fail(cudaStreamSynchronize(s)))
-        break;
       std::vector<int> cands;
       const int step = std::max(1, (chi - cmin + 3) / 4);
       for (int c = cmin; c <= chi; c += step) cands.push_back(c);
@@ -139,12 +173,13 @@ int autotune(mbd_ctx* ctx, int max_n) {
           t = std::min(t, (double)ms);
         }
         if (status != MBD_OK) break;
-        if (t < best) {
-          best = t;
+        if (t < best) best = t;
+        if (t < tc.chase_ms) {
+          tc.chase_ms = t;
           tc.chase_c = c;
         }
       }
-      tc.chase_ms = best < 1e30 ? best : 0.0;
+      tc.cluster_chase_ms = best < 1e30 ? best : 0.0;
     }
     if (status == MBD_OK) ctx->tune[k] = tc;
   }

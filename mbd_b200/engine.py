@@ -393,12 +393,19 @@ class Engine:
         return self.tuning()
 
     def tuning(self) -> list:
-        buf = (ctypes.c_double * 48)()
-        k = self.lib.mbd_rsscs_tuning(self.ctx, buf, 48)
-        return [{"n": int(buf[6 * i]), "panel_qr": {0: "householder", 1: "tsqr"}.get(int(buf[6 * i + 5]), "default"),
-                 "panel_rows_per_cta": int(buf[6 * i + 1]), "chase_ctas": int(buf[6 * i + 2]),
-                 "dense_to_band_ms": buf[6 * i + 3], "chase_ms": buf[6 * i + 4]} for i in range(max(0, k))
-                if buf[6 * i] > 0]
+        buf = (ctypes.c_double * 64)()
+        k = self.lib.mbd_rsscs_tuning(self.ctx, buf, 64)
+        out = []
+        for i in range(max(0, k)):
+            o = buf[8 * i:8 * i + 8]
+            if o[0] <= 0:
+                continue
+            out.append({"n": int(o[0]), "panel_qr": {0: "householder", 1: "tsqr"}.get(int(o[5]), "default"),
+                        "panel_rows_per_cta": int(o[1]),
+                        "chase": "flag" if int(o[2]) < 0 else f"cluster{int(o[2])}",
+                        "dense_to_band_ms": o[3], "chase_ms": o[4],
+                        "flag_chase_ms": o[6], "cluster_chase_ms": o[7]})
+        return out
 
     def save_network(self, path: str) -> None:
         """Write the context's network to `path` (write_network_file)."""

@@ -71,9 +71,10 @@ def test_cluster_chase_batch_equals_flag_chase(engines):
 
 def test_autotune_choices_and_results():
     """mbd_rsscs_autotune picks, per size class up to the announced size, a
-    panel-QR rows-per-CTA target among its candidates and a chase cluster size
-    that holds the band; eigenvalues and energies computed afterwards match
-    LAPACK and the oracle fixtures."""
+    panel-QR rows-per-CTA target among its candidates and the faster chase
+    (flag-synchronised, or cluster-resident at a cluster size that holds the
+    band); eigenvalues and energies computed afterwards match LAPACK and the
+    oracle fixtures."""
     from mbd_b200 import Engine
     with Engine(0) as eng:
         choices = eng.autotune(3000)
@@ -81,8 +82,13 @@ def test_autotune_choices_and_results():
         for c in choices:
             assert c["panel_rows_per_cta"] in (48, 96, 192, 384)
             assert c["panel_qr"] in ("householder", "tsqr")
-            assert 1 <= c["chase_ctas"] <= 16 and c["chase_ctas"] * 378 >= c["n"]
-            assert c["dense_to_band_ms"] > 0 and c["chase_ms"] > 0
+            assert c["dense_to_band_ms"] > 0 and c["flag_chase_ms"] > 0 and c["cluster_chase_ms"] > 0
+            if c["chase"] == "flag":
+                assert c["chase_ms"] == c["flag_chase_ms"] <= c["cluster_chase_ms"]
+            else:
+                ctas = int(c["chase"][len("cluster"):])
+                assert 1 <= ctas <= 16 and ctas * 378 >= c["n"]
+                assert c["chase_ms"] == c["cluster_chase_ms"] < c["flag_chase_ms"]
         S = _sym(3000, seed=77)
         w = eng.eigvalsh(np.tril(S))
         ref = np.linalg.eigvalsh(S)
