@@ -656,13 +656,21 @@ int prepare_batch(mbd_ctx* ctx, bool eigen) {
   // flag-synchronised chase takes the rest, and all of them while the
   // failure-detection stall is on: its waits are the ones that can run out)
   std::vector<BandJob> bjobs, fjobs;
-  const int cap = (ctx->cluster_chase && !ctx->test_stall_wait) ? sb2st_cluster_max_n() : 0;
+  // one chase kernel per batch (the two launches would run one after the
+  // other): the one tuned for the batch's largest band, whose chase sets the
+  // launch's length
+  int big = 0;
+  for (int g : ctx->order)
+    if (two_stage(ctx, ctx->geoms[g]->plan.nH)) big = std::max(big, ctx->geoms[g]->plan.nH);
+  const bool cluster_ok = ctx->cluster_chase && !ctx->test_stall_wait && big > 0 &&
+                          big <= sb2st_cluster_max_n() && tuned_chase_c(ctx, big) != kChaseFlag;
+  const int cap = cluster_ok ? sb2st_cluster_max_n() : 0;
   ctx->band_max_n = ctx->band_cluster_max_n = 0;
   for (int g : ctx->order) {
     GeomDev* gd = ctx->geoms[g].get();
     if (!two_stage(ctx, gd->plan.nH)) continue;
     const BandJob bj{gd->band.as<double>(), gd->plan.nH, gd->d, gd->e};
-    if (bj.n <= cap && tuned_chase_c(ctx, bj.n) != kChaseFlag) {
+    if (bj.n <= cap) {
       bjobs.push_back(bj);
       ctx->band_cluster_max_n = std::max(ctx->band_cluster_max_n, bj.n);
     } else {
@@ -871,8 +879,14 @@ int mbd_rsscs_create(mbd_ctx** out, int device) {
   {
     const char* ng = std::getenv("MBD_B200_NO_GRAPHS");
     ctx->use_graphs = !(ng && ng[0] && ng[0] != '0');
+    // the band -> tridiagonal chase of size classes the autotuner has not
+    // timed: flag-synchronised (measured faster at every size on B200);
+    // MBD_B200_CLUSTER_CHASE=1 makes it the cluster-resident one, =0 rules
+    // the cluster-resident chase out even where the autotuner picks it
     const char* cc = std::getenv("MBD_B200_CLUSTER_CHASE");
     ctx->cluster_chase = !(cc && cc[0] == '0');
+    if (cc && cc[0] == '1')
+      for (TuneChoice& t : ctx->tune) t.chase_c = 0;
     const char* pq = std::getenv("MBD_B200_PANEL_QR");
     ctx->panel_qr_default = (pq && std::strcmp(pq, "tsqr") == 0) ? 1 : 0;
   }

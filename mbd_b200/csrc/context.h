@@ -99,8 +99,8 @@ struct TuneChoice {
   int n = 0;            // size the class was timed at
   int rows = 0;         // panel-QR rows per CTA of the dense -> band reduction
   int panel_qr = -1;    // panel QR: 0 per-column Householder, 1 TSQR (-1: not tuned)
-  int chase_c = 0;      // band -> tridiagonal: CTAs of the cluster-resident chase
-                        // (0: its default size), or kChaseFlag: the flag-synchronised chase
+  int chase_c = -1;     // band -> tridiagonal: CTAs of the cluster-resident chase
+                        // (0: its default size), or kChaseFlag (-1): the flag-synchronised chase
   double sy2sb_ms = 0.0, chase_ms = 0.0;   // the chosen candidates' times
   double flag_chase_ms = 0.0, cluster_chase_ms = 0.0;   // the best of each chase kernel
 };
