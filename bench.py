@@ -86,8 +86,7 @@ def load_peaks():
 
 # DRAM traffic (dram__bytes_read.sum + dram__bytes_write.sum) of one launch of
 # the workload's dominant kernels, from ncu captures of this bench command on
-# a B200 (the summaries are committed under profiles/); a profile constant, not
-# measured by the run that prints it.
+# a B200: a profile constant, not measured by the run that prints it.
 PROFILED_TRAFFIC = {
     "clusters": {"sb2st_kernel": 14544384, "tridiag_kernel": 210234000000},
 }
@@ -391,6 +390,7 @@ def roofline(stage_ms, sizes, mode):
         return {"bound": "hbm", "kernel": "sb2st_kernel (band -> tridiagonal bulge chasing, one launch per batch)",
                 "achieved": achieved, "peak": peaks.get("hbm_gbs"), "unit": "GB/s",
                 "frac": achieved / peaks.get("hbm_gbs"), "traffic": load_traffic().get("sb2st_kernel"),
+                "traffic_source": "ncu capture of one launch of this workload (a profile constant)",
                 "kernel_ms": t_ms,
                 "peak_source": f"{src} copy bandwidth (MEASURED_PEAKS.json hbm_gbs)",
                 "algorithmic": "per bulge-chasing task 2 x 32x32 FP64 blocks read + written; "
@@ -451,6 +451,9 @@ def main():
     ap.add_argument("--workload", default="clusters", choices=sorted(WORKLOADS),
                     help="clusters: the three-cluster headline workload; batched: 256 uneven clusters; "
                          "boxes: three periodic boxes of 2000-6000 atoms")
+    ap.add_argument("--no-autotune", action="store_true",
+                    help="keep the untuned launch shapes (profiling runs: the autotuner's own launches "
+                         "would swamp a launch list)")
     ap.add_argument("--sizes", default=None,
                     help="comma-separated cluster sizes replacing 500,1000,2000 (profiling runs only)")
     args = ap.parse_args()
@@ -500,7 +503,7 @@ def main():
     # sizes before anything is timed (the network's training above used the
     # defaults; the choices apply to the computes below)
     t0 = time.perf_counter()
-    tuned = eng.autotune(max(3 * len(g.names) * _supercell_cells(g, s) for g, s in geos))
+    tuned = [] if args.no_autotune else eng.autotune(max(3 * len(g.names) * _supercell_cells(g, s) for g, s in geos))
     tune_s = time.perf_counter() - t0
     stream = torch.cuda.ExternalStream(eng.stream_handle(), device=torch.device("cuda", local))
     # the sheet's working set (25 MB of relay matrices) fits in the 126 MB L2:

@@ -17,27 +17,55 @@ namespace mbd {
 namespace {
 
 // Number of eigenvalues of the symmetric tridiagonal (d, e) below x; e2 = e^2.
-__device__ int sturm_count(const double* d, const double* e2, int n, double x) {
+// The three-term recurrence is homogeneous in (p, p_prev), so rescaling both
+// by a power of two changes no sign and no count.  CHECK steps run between
+// two magnitude checks; with CHECK = 4 a step's FMA is the only link of the
+// dependency chain (the check and its branch sit on it once per 4 steps).
+// One step grows max(|p|, |p_prev|) by at most G = |d_i - x| + e_{i-1}^2
+// <= 2 tn + tn^2 (tn bounds |d|, |e| and the shifts); the caller takes
+// CHECK = 4 only for tn < 2^32, where G^4 < 2^260: after a check the pair
+// stays below 2^500 (or 2^523 scaled down to 2^23) and 4 steps keep it
+// below 2^783.  Cancellation can shrink p by much more per step, but a tiny
+// p only matters through its sign, which an FMA rounds correctly even below
+// the normal range.
+template <int CHECK>
+__device__ __forceinline__ void sturm_rescale(double& p, double& pm) {
   const double big = 0x1p500, small = 0x1p-500;
+  const double m = fmax(fabs(p), fabs(pm));
+  if (m > big) {
+    p *= small;
+    pm *= small;
+  } else if (m < small && m != 0.0) {
+    p *= big;
+    pm *= big;
+  }
+}
+
+__device__ __forceinline__ void sturm_step(double di, double e2i, double x, double& p, double& pm, bool& neg,
+                                           int& cnt) {
+  const double pn = fma(di - x, p, -e2i * pm);
+  const bool nn = (pn == 0.0) ? !neg : (pn < 0.0);
+  cnt += (nn != neg);
+  neg = nn;
+  pm = p;
+  p = pn;
+}
+
+template <int CHECK>
+__device__ int sturm_count(const double* d, const double* e2, int n, double x) {
   double pm = 1.0;
   double p = d[0] - x;
   bool neg = (p <= 0.0);               // a zero takes the sign opposite to its predecessor (+1)
   int cnt = neg ? 1 : 0;
-  for (int i = 1; i < n; ++i) {
-    const double pn = fma(d[i] - x, p, -e2[i - 1] * pm);
-    const bool nn = (pn == 0.0) ? !neg : (pn < 0.0);
-    cnt += (nn != neg);
-    neg = nn;
-    pm = p;
-    p = pn;
-    const double ap = fabs(p);
-    if (ap > big) {
-      p *= small;
-      pm *= small;
-    } else if (ap < small && ap != 0.0) {
-      p *= big;
-      pm *= big;
-    }
+  int i = 1;
+  for (; i + CHECK <= n; i += CHECK) {
+#pragma unroll
+    for (int u = 0; u < CHECK; ++u) sturm_step(d[i + u], e2[i + u - 1], x, p, pm, neg, cnt);
+    sturm_rescale<CHECK>(p, pm);
+  }
+  for (; i < n; ++i) {
+    sturm_step(d[i], e2[i - 1], x, p, pm, neg, cnt);
+    sturm_rescale<1>(p, pm);
   }
   return cnt;
 }
@@ -82,6 +110,8 @@ __device__ __forceinline__ void bisect_block(const double* d, const double* e, c
   const double tn = fmax(fabs(lo), fabs(hi));
   lo -= 4.0 * 2.2e-16 * tn + 1e-300;
   hi += 4.0 * 2.2e-16 * tn + 1e-300;
+  // |d_i - x| + e_{i-1}^2 <= 2 tn + tn^2 for every shift x in [lo, hi]
+  const bool few_checks = tn < 0x1p32;
   const int gid = block * blockDim.x + threadIdx.x;
   const int k = gid / kLanesPerEig;
   const int q = gid % kLanesPerEig;
@@ -94,7 +124,9 @@ __device__ __forceinline__ void bisect_block(const double* d, const double* e, c
     const double wdt = hi - lo;
     if (wdt <= 2.0 * 1.1102230246251565e-16 * fmax(fabs(lo), fabs(hi))) break;
     const double x = lo + wdt * (double)(q + 1) / (double)(kLanesPerEig + 1);
-    const bool above = (x > lo && x < hi) ? (sturm_count(dd, ee, n, x) > k) : (x >= hi);
+    const bool above = (x > lo && x < hi) ? ((few_checks ? sturm_count<4>(dd, ee, n, x)
+                                                         : sturm_count<1>(dd, ee, n, x)) > k)
+                                          : (x >= hi);
     const unsigned bits = (__ballot_sync(gmask, above) & gmask) >> base;
     const double xprev = __shfl_up_sync(gmask, x, 1, kLanesPerEig);
     const int first = bits ? (__ffs(bits) - 1) : kLanesPerEig;
