@@ -112,8 +112,16 @@ def test_cg_without_network_matches_plain(engine):
 
 
 def test_trained_network_saves_cg_iterations(engine, trained):
-    """Held-out boxes: the network's warm start needs fewer block-CG
-    iterations than a zero start, with the same energies."""
+    """Held-out boxes: the network's warm start needs at least 4 % fewer
+    block-CG iterations in total than a zero start, with the same energies
+    (measured on a B200: 133 against 140 over the six boxes).
+
+    The bar is what a warm start of this accuracy can give: the iteration
+    reduces the error by a roughly constant factor rho ~ 0.5 per step, so a
+    start with relative block error eps saves about log(eps) / log(rho)
+    iterations -- 2 to 3 at the network's ~13 % error (training loss
+    ~0.0165, reached with 160 training geometries and not lowered by 2000
+    or by 30 epochs), of the 20-30 the solves take."""
     test = _train_set(6, 120, 180, seed=11)
     geos, sets = [g for g, _ in test], [s for _, s in test]
     with_net = engine.energy_batch(geos, sets, "mixed_learned")
@@ -129,7 +137,8 @@ def test_trained_network_saves_cg_iterations(engine, trained):
         assert a.status == 0
         assert abs(a.energy - b.energy) <= E_TOL
         assert abs(a.c6_mol - b.c6_mol) <= C6_RTOL * abs(b.c6_mol)
-    assert it_with < it_without, (it_with, it_without)
+    print(f"block-CG iterations with the network {it_with}, without {it_without}")
+    assert it_with <= 0.96 * it_without, (it_with, it_without)
 
 
 def test_learned_mode_vs_oracle(engine, trained):
