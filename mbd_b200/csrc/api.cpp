@@ -332,7 +332,7 @@ void drop_graphs(mbd_ctx* ctx) {
     }
   // the next compute of each mode launches directly again (and reads back
   // the CG iterations), the one after it captures
-  for (auto& gd : ctx->geoms) gd->cg_iters_seen = 0;
+  for (auto& gd : ctx->geoms) gd->cg_iters_seen = gd->cg_iters_seen1 = 0;
   for (int& k : ctx->mode_runs) k = 0;
 }
 
@@ -391,7 +391,7 @@ int run_front(mbd_ctx* ctx, GeomDev* gd, int gi, int mode, bool relay_only) {
   const size_t mstride = (size_t)n * p.ld;
   RelayBuildArgs rb{N, p.ld, mstride, gd->coords, gd->alpha_w, gd->sgm, gd->rvdw_iso, gd->scs_shifts,
                     (int)p.scs_shifts.size() / 3, p.beta, p.scs_eval_cut, sl.relay64.as<double>(),
-                    mixed ? sl.relay32.as<float>() : nullptr};
+                    (mixed || (learned && ctx->cg_fp32)) ? sl.relay32.as<float>() : nullptr};
   rb.f32_math = (mixed || learned) && ctx->f32_tensor_build;
   launch_relay_build(rb, s);
   ctx->launches += 1;
@@ -883,6 +883,13 @@ int mbd_rsscs_create(mbd_ctx** out, int device) {
     // timed: flag-synchronised (measured faster at every size on B200);
     // MBD_B200_CLUSTER_CHASE=1 makes it the cluster-resident one, =0 rules
     // the cluster-resident chase out even where the autotuner picks it
+    // MBD_B200_CG_FP32=1: the learned mode's block-CG runs its matrix passes
+    // on an FP32 copy of the relay matrices in two phases with an FP64
+    // restart between them (measured on B200 for the 2000-atom cluster:
+    // relay solve 16.6 ms against 17.4 ms for the one-phase FP64 passes, for
+    // 50 % more relay memory; off by default)
+    const char* cf = std::getenv("MBD_B200_CG_FP32");
+    ctx->cg_fp32 = cf && cf[0] == '1';
     const char* cc = std::getenv("MBD_B200_CLUSTER_CHASE");
     ctx->cluster_chase = !(cc && cc[0] == '0');
     if (cc && cc[0] == '1')
@@ -1055,17 +1062,21 @@ int mbd_rsscs_download(mbd_ctx* ctx, mbd_result* out) {
       if (ctx->last_mode == MBD_MODE_MIXED_LEARNED) {
         std::vector<double> cs((size_t)kNFreq * kCgState);
         MBD_CUDA(cudaMemcpy(cs.data(), gd->cgstate, sizeof(double) * cs.size(), cudaMemcpyDeviceToHost));
-        double most = 0.0;
+        double most = 0.0, most1 = 0.0;
         bool indefinite = false;
         for (int f = 0; f < kNFreq; ++f) {
           most = std::max(most, cs[(size_t)f * kCgState + 1]);
+          if (ctx->cg_fp32) most1 = std::max(most1, cs[(size_t)f * kCgState + kCgPhase1Iters]);
           indefinite = indefinite || cs[(size_t)f * kCgState + kCgIndefinite] != 0.0;
         }
-        r.refine_iters = (int)most;
+        // iterations of both phases (the mixed-precision form) or of the one
+        r.refine_iters = (int)(most1 + most);
         // a negative curvature proves the relay matrix indefinite: the direct
         // solve below then reports it (MBD_ERR_RELAY_NOT_SPD)
         if (indefinite) worst = std::numeric_limits<double>::infinity();
-        gd->cg_iters_seen = (worst <= ctx->residual_gate) ? (int)most : 0;
+        const bool ok = worst <= ctx->residual_gate;
+        gd->cg_iters_seen = ok ? (int)most : 0;
+        gd->cg_iters_seen1 = ok ? (int)most1 : 0;
       }
       if (!(worst <= ctx->residual_gate)) {
         int st = run_front(ctx, gd, (int)g, MBD_MODE_PLAIN_FP64);

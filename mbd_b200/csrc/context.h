@@ -67,7 +67,8 @@ struct GeomDev {
   // graph runs this many iterations plus a margin instead of the full
   // schedule (the same inputs and network converge identically; a miss
   // would still be caught by the residual gate).  Forgotten with the graphs.
-  int cg_iters_seen = 0;
+  int cg_iters_seen = 0;    // block-CG iterations of the last compute (the second phase when two-phase)
+  int cg_iters_seen1 = 0;   // the first phase's (mixed-precision block-CG)
   GnnGraph gnn{};    // device views into `graph` (x set per use)
   DevBuf train;      // x [21N][8] and S_true [21N][9] of a training batch
 };
@@ -181,6 +182,7 @@ struct mbd_ctx {
   double wait_limit_s = 2.0;                   // bounded device waits (per device)
   int test_stall_wait = 0;                     // 1: the bulge-chasing launch's first wait runs out
   int f32_tensor_build = 0;                    // 1: mixed modes build the relay tensors in FP32 arithmetic
+  bool cg_fp32 = false;                        // learned mode: block-CG matrix passes on the FP32 copy
   mbd::TuneChoice tune[mbd::kTuneClasses];     // mbd_rsscs_autotune
   int panel_qr_default = 0;                    // MBD_B200_PANEL_QR=tsqr: 1
 };

@@ -206,9 +206,26 @@ __global__ void __launch_bounds__(256) cg_tile_inv_kernel(CgArgs a) {
 // memory (fixed order).
 constexpr int TT = 256;           // threads of cg_tile
 constexpr int RP = CT * 3 + 1;    // row stride of the partial-sum buffer (bank spread)
-__global__ void __launch_bounds__(TT, 3) cg_tile_kernel(CgArgs a, const double* in) {
-  __shared__ __align__(16) double xI[CT * 3], xJ[CT * 3];
-  __shared__ double buf[16 * RP];
+// Two consecutive entries of a row: 16-byte loads of FP64, 8-byte loads of
+// the FP32 copy (half the bytes of the pass).
+template <typename T> struct Pair;
+template <> struct Pair<double> { using V = double2; };
+template <> struct Pair<float> { using V = float2; };
+template <typename T>
+__device__ __forceinline__ typename Pair<T>::V load_pair(const T* A, size_t o) {
+  return *reinterpret_cast<const typename Pair<T>::V*>(A + o);
+}
+// TA = double: the FP64 pass (FP64 products and sums).  TA = float: the pass
+// of the mixed-precision block-CG, products and the per-tile sums of 64
+// terms in FP32 (at 2x the FP64 rate: the FP32 pass would otherwise stay
+// bound by its 12 FP64 FMAs per entry, not by its halved bytes), the 16
+// partial sums of each output added in FP64.  A tile's sums carry a relative
+// error of a few 1e-7, below what either phase of that solve resolves.
+template <typename TA>
+__global__ void __launch_bounds__(TT, 3) cg_tile_kernel(CgArgs a, const TA* Abase, const double* in) {
+  using TC = TA;
+  __shared__ __align__(16) TC xI[CT * 3], xJ[CT * 3];
+  __shared__ TC buf[16 * RP];
   const int ntiles = a.nt * (a.nt + 1) / 2;
   const int tid = threadIdx.x, tx = tid & 15, ty = tid >> 4;
   const int n = a.n;
@@ -224,46 +241,47 @@ __global__ void __launch_bounds__(TT, 3) cg_tile_kernel(CgArgs a, const double* 
     int ti, tj;
     cg_tri((int)(item % ntiles), &ti, &tj);
     const bool diag = ti == tj;
-    const double* A = a.A + (size_t)f * a.a_stride;
+    const TA* A = Abase + (size_t)f * a.a_stride;
     const double* x = in + (size_t)f * a.ystride;
-    // the 16 entries (16-byte loads; rows start 16-byte aligned, ld a multiple
+    // the 16 entries (pair loads; rows start 16-byte aligned, ld a multiple
     // of 32; an entry beyond n or above the diagonal reads as zero)
-    double t[4][4];
+    TC t[4][4];
 #pragma unroll
     for (int i = 0; i < 4; ++i) {
       const int r = ty + 16 * i, gr = ti * CT + r;
 #pragma unroll
       for (int h = 0; h < 2; ++h) {
         const int c = 2 * tx + 32 * h, gc = tj * CT + c;
-        double2 v = make_double2(0.0, 0.0);
-        if (gr < n && gc < n && (!diag || c <= r)) v = *reinterpret_cast<const double2*>(A + (size_t)gr * a.ld + gc);
+        typename Pair<TC>::V v;
+        v.x = v.y = (TC)0;
+        if (gr < n && gc < n && (!diag || c <= r)) v = load_pair(A, (size_t)gr * a.ld + gc);
         t[i][2 * h] = v.x;
-        t[i][2 * h + 1] = (gc + 1 < n && (!diag || c + 1 <= r)) ? v.y : 0.0;
+        t[i][2 * h + 1] = (gc + 1 < n && (!diag || c + 1 <= r)) ? v.y : (TC)0;
       }
     }
     __syncthreads();   // the previous item's reads of xI / xJ / buf are done
     for (int idx = tid; idx < CT * 3; idx += TT) {
       const int gi = ti * CT + idx / 3, gj = tj * CT + idx / 3;
-      xI[idx] = gi < n ? x[(size_t)ti * CT * 3 + idx] : 0.0;
-      xJ[idx] = gj < n ? x[(size_t)tj * CT * 3 + idx] : 0.0;
+      xI[idx] = (TC)(gi < n ? x[(size_t)ti * CT * 3 + idx] : 0.0);
+      xJ[idx] = (TC)(gj < n ? x[(size_t)tj * CT * 3 + idx] : 0.0);
     }
     __syncthreads();
-    double rs[4][3], cs[4][3];
+    TC rs[4][3], cs[4][3];
 #pragma unroll
     for (int k = 0; k < 4; ++k)
 #pragma unroll
-      for (int q = 0; q < 3; ++q) rs[k][q] = cs[k][q] = 0.0;
+      for (int q = 0; q < 3; ++q) rs[k][q] = cs[k][q] = (TC)0;
 #pragma unroll
     for (int i = 0; i < 4; ++i) {
       const int r = ty + 16 * i;
-      double xi[3];
+      TC xi[3];
 #pragma unroll
       for (int q = 0; q < 3; ++q) xi[q] = xI[3 * r + q];
 #pragma unroll
       for (int j = 0; j < 4; ++j) {
         const int c = 2 * tx + 32 * (j >> 1) + (j & 1);
-        const double e = t[i][j];
-        const double ec = (!diag || c < r) ? e : 0.0;   // the diagonal counts once (row side)
+        const TC e = t[i][j];
+        const TC ec = (!diag || c < r) ? e : (TC)0;   // the diagonal counts once (row side)
 #pragma unroll
         for (int q = 0; q < 3; ++q) {
           rs[i][q] += e * xJ[3 * c + q];
@@ -281,7 +299,7 @@ __global__ void __launch_bounds__(TT, 3) cg_tile_kernel(CgArgs a, const double* 
     double y = 0.0;
     if (tid < CT * 3) {
 #pragma unroll
-      for (int k = 0; k < 16; ++k) y += buf[k * RP + tid];
+      for (int k = 0; k < 16; ++k) y += (double)buf[k * RP + tid];
     }
     __syncthreads();
     // column sums: the 16 row groups of each column
@@ -295,7 +313,7 @@ __global__ void __launch_bounds__(TT, 3) cg_tile_kernel(CgArgs a, const double* 
     if (tid < CT * 3) {
       double z = 0.0;
 #pragma unroll
-      for (int k = 0; k < 16; ++k) z += buf[k * RP + tid];
+      for (int k = 0; k < 16; ++k) z += (double)buf[k * RP + tid];
       if (!diag) {
         pr[((size_t)ti * a.nt + tj) * CT * 3 + tid] = y;
         pr[((size_t)tj * a.nt + ti) * CT * 3 + tid] = z;
@@ -396,6 +414,18 @@ __global__ void __launch_bounds__(192) cg_init_tiles_kernel(CgArgs a) {
   const int r = threadIdx.x / 3, q = threadIdx.x % 3, gr = I * CT + r;
   const double rv = gr < a.n ? a.R[(size_t)f * a.ystride + (size_t)gr * 3 + q] : 0.0;
   tile_precondition(a, f, I, rv, true, S);
+}
+
+// Between the phases: frequencies stopped as converged (1) or broken down
+// (2) run again, negative curvature (3) stays; the first phase's iteration
+// count is kept in kCgPhase1Iters.  Must run before any kernel that tests
+// the stop flag in the restart.
+__global__ void cg_reopen_kernel(CgArgs a) {
+  const int f = blockIdx.x * blockDim.x + threadIdx.x;
+  if (f >= a.batch) return;
+  double* st = a.state + f * kCgState;
+  st[kCgPhase1Iters] = st[1];
+  if (st[0] == 1.0 || st[0] == 2.0) st[0] = 0.0;
 }
 
 // init: Z^T R and R^T R into the state; stop when already converged.
@@ -529,7 +559,7 @@ int cg_tile_grid() {
     int dev = 0, sms = 0, per_sm = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, cg_tile_kernel, TT, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, cg_tile_kernel<double>, TT, 0);
     grid = (sms > 0 ? sms : 148) * (per_sm > 0 ? per_sm : 1);
   }
   return grid;
@@ -551,17 +581,30 @@ void launch_cg_setup(const CgArgs& a, cudaStream_t s) {
   const int tgrid = (int)std::min<long long>(cg_tile_grid(), items);
   cudaMemsetAsync(a.state, 0, sizeof(double) * kCgState * a.batch, s);
   cg_tile_inv_kernel<<<dim3(a.nt, a.batch), 256, 0, s>>>(a);
-  cg_tile_kernel<<<tgrid, TT, 0, s>>>(a, a.X);
+  cg_tile_kernel<double><<<tgrid, TT, 0, s>>>(a, a.A, a.X);
   cg_rows_kernel<<<dim3(a.nt, a.batch), 192, 0, s>>>(a, 1);
   cg_init_tiles_kernel<<<dim3(a.nt, a.batch), 192, 0, s>>>(a);
   cg_init_final_kernel<<<a.batch, 32, 0, s>>>(a, a.nt);
 }
 
-void launch_cg_iteration(const CgArgs& a, int it, cudaStream_t s) {
+void launch_cg_restart(const CgArgs& a, cudaStream_t s) {
+  const long long items = (long long)a.nt * (a.nt + 1) / 2 * a.batch;
+  const int tgrid = (int)std::min<long long>(cg_tile_grid(), items);
+  cg_reopen_kernel<<<(a.batch + 31) / 32, 32, 0, s>>>(a);
+  cg_tile_kernel<double><<<tgrid, TT, 0, s>>>(a, a.A, a.X);
+  cg_rows_kernel<<<dim3(a.nt, a.batch), 192, 0, s>>>(a, 1);
+  cg_init_tiles_kernel<<<dim3(a.nt, a.batch), 192, 0, s>>>(a);
+  cg_init_final_kernel<<<a.batch, 32, 0, s>>>(a, a.nt);
+}
+
+void launch_cg_iteration(const CgArgs& a, int it, cudaStream_t s, bool fp32) {
   const int nb = (a.N + AT - 1) / AT;
   const long long items = (long long)a.nt * (a.nt + 1) / 2 * a.batch;
   const int tgrid = (int)std::min<long long>(cg_tile_grid(), items);
-  cg_tile_kernel<<<tgrid, TT, 0, s>>>(a, a.P);
+  if (fp32 && a.A32)
+    cg_tile_kernel<float><<<tgrid, TT, 0, s>>>(a, a.A32, a.P);
+  else
+    cg_tile_kernel<double><<<tgrid, TT, 0, s>>>(a, a.A, a.P);
   cg_rows_kernel<<<dim3(a.nt, a.batch), 192, 0, s>>>(a, 0);
   cg_update_kernel<<<dim3(a.nt, a.batch), 192, 0, s>>>(a, it);
   cg_dir_kernel<<<dim3(nb, a.batch), AT, 0, s>>>(a, it);

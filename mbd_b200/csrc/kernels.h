@@ -217,6 +217,7 @@ constexpr int kCgState = 24;   // per-frequency recurrence state (doubles)
 constexpr int kCgIndefinite = 21;   // state slot: 1 when a search direction found p^T A p < 0
 struct CgArgs {
   const double* A;         // 21 relay matrices, row-major lower FP64
+  const float* A32;        // the same matrices rounded to FP32 (same strides), or null
   size_t a_stride;
   int ld, n, N, nt;        // n = 3N, nt = ceil(n / 64)
   int batch;               // frequencies
@@ -232,10 +233,19 @@ struct CgArgs {
 size_t cg_partial_doubles(int n, int batch);
 size_t cg_minv_doubles(int n, int batch);
 size_t cg_red_doubles(int n, int batch);
+constexpr int kCgPhase1Iters = 22;   // state slot: iterations of the first (FP32-pass) phase
 // Tile inverses, R = B - A X, Z, P and Z^T R for every frequency.
 void launch_cg_setup(const CgArgs& a, cudaStream_t s);
-// One iteration (iteration index it = 0, 1, ...); a converged frequency skips it.
-void launch_cg_iteration(const CgArgs& a, int it, cudaStream_t s);
+// One iteration (iteration index it = 0, 1, ...); a converged frequency
+// skips it.  fp32: the matrix pass reads A32 instead of A (FP64 vectors and
+// sums either way).
+void launch_cg_iteration(const CgArgs& a, int it, cudaStream_t s, bool fp32 = false);
+// Restart between the two phases of the mixed-precision solve: the true
+// residual R = B - A X from the FP64 matrix, Z = M^-1 R, P = Z, Z^T R; the
+// frequencies the first phase stopped (converged or broke down) run again,
+// those shown indefinite stay stopped; the first phase's iteration count
+// moves to state slot kCgPhase1Iters.
+void launch_cg_restart(const CgArgs& a, cudaStream_t s);
 
 // Many tridiagonal eigenproblems and energies in one launch each.
 struct EigJob {

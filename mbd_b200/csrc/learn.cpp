@@ -24,6 +24,14 @@ namespace {
 constexpr int kCgMaxIters = 64;
 constexpr int kCgSlack = 4;       // iterations a captured graph adds to the count last seen
 constexpr double kCgTol = 3e-11;   // relative residual the iteration stops at (gate: 1e-10)
+// Mixed-precision form (the matrix passes on the FP32 copy of the relay
+// matrices): phase 1 from the warm start to a relative residual of
+// kCgTol1, a restart from the true FP64 residual, phase 2 to kCgTol.  Each
+// phase's FP32 passes perturb only the correction it computes: phase 2 starts
+// from a residual ~1e-5 of B, and the FP32 rounding of the matrix (~6e-8
+// relative) then leaves ~1e-12 in the final residual, far below the gate.
+constexpr int kCgPhaseMaxIters = 40;
+constexpr double kCgTol1 = 1e-5;
 
 // Neighbour lists within the network's cut-off, including periodic images
 // along non-vacuum axes (an atom may meet another atom, or itself, through
@@ -248,6 +256,15 @@ int reserve_learned(mbd_ctx* ctx) {
     MBD_CUDA(sl.cg.reserve(cg));
     MBD_CUDA(sl.gnn.reserve(gw));
     MBD_CUDA(sl.res_ws.reserve(res));
+    if (ctx->cg_fp32) {
+      // the FP32 copy of the relay matrices the mixed-precision passes read
+      size_t r32 = 0;
+      for (int g : ctx->order)
+        if (ctx->geoms[g]->slot == s) r32 = std::max(r32, sizeof(float) * (size_t)kNFreq * ctx->geoms[g]->plan.n *
+                                                              ctx->geoms[g]->plan.ld);
+      moved = moved || r32 > sl.relay32.bytes;
+      MBD_CUDA(sl.relay32.reserve(r32));
+    }
   }
   if (moved) drop_graphs(ctx);
   return MBD_OK;
@@ -263,6 +280,7 @@ int relay_learned(mbd_ctx* ctx, GeomDev* gd, RelaySlot& sl, size_t mstride, cuda
   double* base = sl.cg.as<double>();
   CgArgs a{};
   a.A = sl.relay64.as<double>();
+  a.A32 = ctx->cg_fp32 ? sl.relay32.as<float>() : nullptr;
   a.a_stride = mstride;
   a.ld = p.ld;
   a.n = n;
@@ -297,14 +315,26 @@ int relay_learned(mbd_ctx* ctx, GeomDev* gd, RelaySlot& sl, size_t mstride, cuda
     MBD_CUDA(cudaMemsetAsync(a.X, 0, sizeof(double) * kNFreq * ys, s));
   }
   record_timing(ctx, ev_net, s);
-  launch_cg_setup(a, s);
-  ctx->launches += 5;
   // the full schedule, or in a captured graph the iterations this geometry
   // took on its last compute plus a margin
-  const int iters = (ctx->capturing && gd->cg_iters_seen > 0) ? std::min(kCgMaxIters, gd->cg_iters_seen + kCgSlack)
-                                                               : kCgMaxIters;
-  for (int it = 0; it < iters; ++it) launch_cg_iteration(a, it, s);
-  ctx->launches += 4 * iters;
+  auto sched = [&](int seen, int cap) { return (ctx->capturing && seen > 0) ? std::min(cap, seen + kCgSlack) : cap; };
+  if (a.A32) {
+    const double tol2 = a.tol2;
+    a.tol2 = kCgTol1 * kCgTol1 * 3.0 * N;
+    launch_cg_setup(a, s);
+    const int it1 = sched(gd->cg_iters_seen1, kCgPhaseMaxIters);
+    for (int it = 0; it < it1; ++it) launch_cg_iteration(a, it, s, true);
+    a.tol2 = tol2;
+    launch_cg_restart(a, s);
+    const int it2 = sched(gd->cg_iters_seen, kCgPhaseMaxIters);
+    for (int it = 0; it < it2; ++it) launch_cg_iteration(a, it, s, true);
+    ctx->launches += 5 + 5 + 4 * (it1 + it2);
+  } else {
+    launch_cg_setup(a, s);
+    const int iters = sched(gd->cg_iters_seen, kCgMaxIters);
+    for (int it = 0; it < iters; ++it) launch_cg_iteration(a, it, s);
+    ctx->launches += 5 + 4 * iters;
+  }
   // the gate's residual, recomputed from X: R = B - A X
   launch_relay_residual(sl.relay64.as<double>(), mstride, p.ld, n, kNFreq, a.X, nullptr, a.R, ys,
                         sl.res_ws.as<double>(), gd->rnorm2, s);

@@ -115,3 +115,33 @@ def test_headline_clusters_one_call_each_vs_oracle(engine):
     headline cluster in the headline mode."""
     geo, st, fx = _load("cluster2000_s2")
     _check(engine.energy(geo, st, mode="mixed_learned"), fx, "mixed_learned")
+
+
+def test_two_phase_fp32_cg_headline_clusters():
+    """The opt-in mixed-precision block-CG of the learned mode
+    (MBD_B200_CG_FP32=1: matrix passes on an FP32 copy of the relay matrices,
+    products in FP32, a restart from the FP64 residual between its two
+    phases) on the headline clusters, twice (the second compute replays the
+    captured graph with the phase lengths of the first): the mixed forms'
+    bars against the oracle fixtures and the FP64 residual gate."""
+    from mbd_b200 import Engine
+    loaded = [_load(nm) for nm in CLUSTERS]
+    old = os.environ.get("MBD_B200_CG_FP32")
+    os.environ["MBD_B200_CG_FP32"] = "1"
+    try:
+        eng = Engine(0)
+    finally:
+        if old is None:
+            del os.environ["MBD_B200_CG_FP32"]
+        else:
+            os.environ["MBD_B200_CG_FP32"] = old
+    with eng:
+        eng.use_network(False)
+        assert eng.upload([g for g, _, _ in loaded], [s for _, s, _ in loaded]) == 0
+        for rep in range(2):
+            assert eng.compute("mixed_learned") == 0
+            code, res = eng.download()
+            assert code == 0
+            for r, (_, _, fx) in zip(res, loaded):
+                _check(r, fx, "mixed_learned")
+        assert eng.stats()["graph_replayed"]
