@@ -107,18 +107,33 @@ struct SolveArgs {
   int* err;
 };
 
+__device__ __forceinline__ int ld_acquire_flag(const int* p) {
+  int v;
+  asm volatile("ld.acquire.gpu.b32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+
+// Thread 0 of the waiting CTA polls with acquire loads; the CTA barrier after
+// it orders the other threads' reads of the block behind the acquire.
 __device__ bool wait_flag(const int* f, int epoch, int* err) {
   const long long lim = wait_limit_cycles();
   const long long t0 = clock64();
-  while (*(volatile const int*)f != epoch) {
+  while (ld_acquire_flag(f) != epoch) {
     if (*(volatile int*)err != 0 || clock64() - t0 > lim) {
       atomicCAS(err, 0, MBD_ERR_TIMEOUT);
       return false;
     }
     __nanosleep(64);
   }
-  __threadfence();
   return true;
+}
+
+// The block's results are written by every thread before the CTA barrier;
+// thread 0 then publishes them with a release store at GPU scope (cumulative
+// over the writes the barrier ordered before it; no separate fence).
+__device__ __forceinline__ void publish_flag(int* f, int epoch) {
+  __syncthreads();
+  if (threadIdx.x == 0) asm volatile("st.release.gpu.b32 [%0], %1;" ::"l"(f), "r"(epoch) : "memory");
 }
 
 // Forward: z_blk = Linv_blk (w_blk - sum_{k<blk} L_{blk,k} z_k).
@@ -191,9 +206,7 @@ __global__ void __launch_bounds__(256) fwd_syncfree_kernel(SolveArgs a) {
     for (int l = 0; l <= rr; ++l) s += ((double)Lh[rr * NB + l] + (double)Ll[rr * NB + l]) * acc_s[l][q];
     if (rr < nbk) a.out[(size_t)b * a.ystride + (size_t)(r0 + rr) * 3 + q] = s;
   }
-  __threadfence();
-  __syncthreads();
-  if (threadIdx.x == 0) atomicExch(a.flags + b * a.nblk + blk, a.epoch);
+  publish_flag(a.flags + b * a.nblk + blk, a.epoch);
 }
 
 // Backward: x_blk = Linv_blk^T (z_blk - sum_{k>blk} L_{k,blk}^T x_k).
@@ -250,9 +263,7 @@ __global__ void __launch_bounds__(256) bwd_syncfree_kernel(SolveArgs a) {
     for (int l = rr; l < NB; ++l) s += ((double)Lh[l * NB + rr] + (double)Ll[l * NB + rr]) * acc_s[l][q];
     if (rr < nbk) a.out[(size_t)b * a.ystride + (size_t)(c0 + rr) * 3 + q] = s;
   }
-  __threadfence();
-  __syncthreads();
-  if (threadIdx.x == 0) atomicExch(a.flags + b * a.nblk + blk, a.epoch);
+  publish_flag(a.flags + b * a.nblk + blk, a.epoch);
 }
 
 // ---------------------------------------------------------------------------
