@@ -886,7 +886,7 @@ int mbd_rsscs_create(mbd_ctx** out, int device) {
     // MBD_B200_CG_FP32=1: the learned mode's block-CG runs its matrix passes
     // on an FP32 copy of the relay matrices in two phases with an FP64
     // restart between them (measured on B200 for the 2000-atom cluster:
-    // relay solve 16.6 ms against 17.4 ms for the one-phase FP64 passes, for
+    // relay solve 15.7 ms against 17.4 ms for the one-phase FP64 passes, for
     // 50 % more relay memory; off by default)
     const char* cf = std::getenv("MBD_B200_CG_FP32");
     ctx->cg_fp32 = cf && cf[0] == '1';

@@ -222,7 +222,8 @@ __device__ __forceinline__ typename Pair<T>::V load_pair(const T* A, size_t o) {
 // partial sums of each output added in FP64.  A tile's sums carry a relative
 // error of a few 1e-7, below what either phase of that solve resolves.
 template <typename TA>
-__global__ void __launch_bounds__(TT, 3) cg_tile_kernel(CgArgs a, const TA* Abase, const double* in) {
+__global__ void __launch_bounds__(TT, sizeof(TA) == 4 ? 4 : 3) cg_tile_kernel(CgArgs a, const TA* Abase,
+                                                                            const double* in) {
   using TC = TA;
   __shared__ __align__(16) TC xI[CT * 3], xJ[CT * 3];
   __shared__ TC buf[16 * RP];
@@ -553,13 +554,14 @@ size_t cg_minv_doubles(int n, int batch) {
 }
 
 // CTAs of the grid-stride tile launch: every resident slot of the device.
+template <typename TA>
 int cg_tile_grid() {
   static int grid = 0;
   if (grid == 0) {
     int dev = 0, sms = 0, per_sm = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, cg_tile_kernel<double>, TT, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, cg_tile_kernel<TA>, TT, 0);
     grid = (sms > 0 ? sms : 148) * (per_sm > 0 ? per_sm : 1);
   }
   return grid;
@@ -578,7 +580,7 @@ size_t cg_red_doubles(int n, int batch) {
 
 void launch_cg_setup(const CgArgs& a, cudaStream_t s) {
   const long long items = (long long)a.nt * (a.nt + 1) / 2 * a.batch;
-  const int tgrid = (int)std::min<long long>(cg_tile_grid(), items);
+  const int tgrid = (int)std::min<long long>(cg_tile_grid<double>(), items);
   cudaMemsetAsync(a.state, 0, sizeof(double) * kCgState * a.batch, s);
   cg_tile_inv_kernel<<<dim3(a.nt, a.batch), 256, 0, s>>>(a);
   cg_tile_kernel<double><<<tgrid, TT, 0, s>>>(a, a.A, a.X);
@@ -589,7 +591,7 @@ void launch_cg_setup(const CgArgs& a, cudaStream_t s) {
 
 void launch_cg_restart(const CgArgs& a, cudaStream_t s) {
   const long long items = (long long)a.nt * (a.nt + 1) / 2 * a.batch;
-  const int tgrid = (int)std::min<long long>(cg_tile_grid(), items);
+  const int tgrid = (int)std::min<long long>(cg_tile_grid<double>(), items);
   cg_reopen_kernel<<<(a.batch + 31) / 32, 32, 0, s>>>(a);
   cg_tile_kernel<double><<<tgrid, TT, 0, s>>>(a, a.A, a.X);
   cg_rows_kernel<<<dim3(a.nt, a.batch), 192, 0, s>>>(a, 1);
@@ -600,9 +602,9 @@ void launch_cg_restart(const CgArgs& a, cudaStream_t s) {
 void launch_cg_iteration(const CgArgs& a, int it, cudaStream_t s, bool fp32) {
   const int nb = (a.N + AT - 1) / AT;
   const long long items = (long long)a.nt * (a.nt + 1) / 2 * a.batch;
-  const int tgrid = (int)std::min<long long>(cg_tile_grid(), items);
+  const int tgrid = (int)std::min<long long>(cg_tile_grid<double>(), items);
   if (fp32 && a.A32)
-    cg_tile_kernel<float><<<tgrid, TT, 0, s>>>(a, a.A32, a.P);
+    cg_tile_kernel<float><<<(int)std::min<long long>(cg_tile_grid<float>(), items), TT, 0, s>>>(a, a.A32, a.P);
   else
     cg_tile_kernel<double><<<tgrid, TT, 0, s>>>(a, a.A, a.P);
   cg_rows_kernel<<<dim3(a.nt, a.batch), 192, 0, s>>>(a, 0);
