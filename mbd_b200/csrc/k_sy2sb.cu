@@ -43,6 +43,11 @@ __device__ __forceinline__ double warp_sum(double v) {
   return v;
 }
 
+// The cluster barrier in its two halves: work a CTA does between its arrive
+// and its wait overlaps the other CTAs' arrival instead of delaying them.
+__device__ __forceinline__ void cluster_arrive() { asm volatile("barrier.cluster.arrive.release.aligned;" ::: "memory"); }
+__device__ __forceinline__ void cluster_wait() { asm volatile("barrier.cluster.wait.acquire.aligned;" ::: "memory"); }
+
 // Panel QR with the panel in registers: warp w of a CTA owns the local rows
 // r = w + NW t (t < RPW), lane c holds column c of them in x[t].  One cluster
 // barrier per column j (given ||x_j below row j||^2 and alpha = A(j, j)):
@@ -87,6 +92,22 @@ __global__ void __launch_bounds__(NW * 32) qr_panel_kernel(PanelArgs a) {
   __shared__ double gs[B];
   __shared__ double Tm[B][B + 1];
   cg::cluster_group cl = cg::this_cluster();
+  // T[0:jc, jc] = -tau_jc T[0:jc, 0:jc] (V^T V)[0:jc, jc], T[jc][jc] = tau_jc
+  // (dlarft, forward, columnwise) from column jc's dots dcj (rank 0, warp 0)
+  int jprev = -1;
+  double dcprev = 0.0, tauprev = 0.0;
+  auto t_column = [&](int jc, double dcj, double tauj) {
+    const int ln = threadIdx.x % 32;
+    gs[ln] = dcj;
+    __syncwarp();
+    if (ln < jc) {
+      double t = 0.0;
+      for (int l = ln; l < jc; ++l) t += Tm[ln][l] * gs[l];
+      Tm[ln][jc] = -tauj * t;
+    }
+    if (ln == jc) Tm[jc][jc] = tauj;
+    __syncwarp();
+  };
   const int rank = (int)cl.block_rank();
   const int C = (int)cl.num_blocks();
   const int m = a.m;
@@ -227,7 +248,9 @@ __global__ void __launch_bounds__(NW * 32) qr_panel_kernel(PanelArgs a) {
         if (lane < 3) cl.map_shared_rank(&recvS[0][0][0], q)[(par * kPanelMaxCluster + rank) * 4 + lane] = u;
       }
     }
-    cl.sync();
+    cluster_arrive();
+    if (rank == 0 && warp == 0 && jprev >= 0) t_column(jprev, dcprev, tauprev);
+    cluster_wait();
     // cluster sums in rank order
     double dc = 0.0, Sxx = 0.0, Svx = 0.0, Svv = 0.0;
     for (int q = 0; q < C; ++q) {
@@ -249,18 +272,12 @@ __global__ void __launch_bounds__(NW * 32) qr_panel_kernel(PanelArgs a) {
         else if (g == j) x[t] = beta;
       }
     }
-    // compact-WY factor, column j
-    if (rank == 0 && warp == 0) {
-      gs[lane] = dc;
-      __syncwarp();
-      if (lane < j) {
-        double t = 0.0;
-        for (int l = lane; l < j; ++l) t += Tm[lane][l] * gs[l];
-        Tm[lane][j] = -tau * t;
-      }
-      if (lane == j) Tm[j][j] = tau;
-      __syncwarp();
-    }
+    // compact-WY factor, column j: built by rank 0's warp 0 inside the next
+    // column's barrier (it needs only this column's dots and the earlier
+    // columns of T), so that no CTA waits for it
+    jprev = j;
+    dcprev = dc;
+    tauprev = tau;
     // the next column's norm and alpha
     if (j + 1 < nref) {
       const double dn = __shfl_sync(FULL, dc, j + 1);
@@ -280,6 +297,7 @@ __global__ void __launch_bounds__(NW * 32) qr_panel_kernel(PanelArgs a) {
       a.V[(size_t)g * B + lane] = g > lane ? x[t] : (g == lane ? 1.0 : 0.0);
     }
   }
+  if (rank == 0 && warp == 0 && jprev >= 0) t_column(jprev, dcprev, tauprev);   // the last column of T
   if (rank == 0) {
     __syncthreads();
     for (int e = tid; e < B * B; e += NT) a.T[e] = Tm[e / B][e % B];
@@ -315,6 +333,22 @@ __global__ void __launch_bounds__(NW * 32) qr_panel2_kernel(PanelArgs a) {
   __shared__ double gs[B];
   __shared__ double Tm[B][B + 1];
   cg::cluster_group cl = cg::this_cluster();
+  // T[0:jc, jc] = -tau_jc T[0:jc, 0:jc] (V^T V)[0:jc, jc], T[jc][jc] = tau_jc
+  // (dlarft, forward, columnwise) from column jc's dots dcj (rank 0, warp 0)
+  int jprev = -1;
+  double dcprev = 0.0, tauprev = 0.0;
+  auto t_column = [&](int jc, double dcj, double tauj) {
+    const int ln = threadIdx.x % 32;
+    gs[ln] = dcj;
+    __syncwarp();
+    if (ln < jc) {
+      double t = 0.0;
+      for (int l = ln; l < jc; ++l) t += Tm[ln][l] * gs[l];
+      Tm[ln][jc] = -tauj * t;
+    }
+    if (ln == jc) Tm[jc][jc] = tauj;
+    __syncwarp();
+  };
   const int rank = (int)cl.block_rank();
   const int C = (int)cl.num_blocks();
   const int m = a.m;
@@ -374,7 +408,9 @@ __global__ void __launch_bounds__(NW * 32) qr_panel2_kernel(PanelArgs a) {
       for (int q = 0; q < NW; ++q) t += wn[q];
       if (lane < C) cl.map_shared_rank(&recvN[0][0], lane)[par * kPanelMaxCluster + rank] = t;
     }
-    cl.sync();
+    cluster_arrive();
+    if (rank == 0 && warp == 0 && jprev >= 0) t_column(jprev, dcprev, tauprev);
+    cluster_wait();
     double xn2 = 0.0;
     for (int q = 0; q < C; ++q) xn2 += recvN[par][q];
     const double alpha = recvA[par];
@@ -460,18 +496,12 @@ __global__ void __launch_bounds__(NW * 32) qr_panel2_kernel(PanelArgs a) {
         else if (g == j) x[t] = beta;
       }
     }
-    // compact-WY factor, column j
-    if (rank == 0 && warp == 0) {
-      gs[lane] = dc;
-      __syncwarp();
-      if (lane < j) {
-        double t = 0.0;
-        for (int l = lane; l < j; ++l) t += Tm[lane][l] * gs[l];
-        Tm[lane][j] = -tau * t;
-      }
-      if (lane == j) Tm[j][j] = tau;
-      __syncwarp();
-    }
+    // compact-WY factor, column j: built by rank 0's warp 0 inside the next
+    // column's barrier (it needs only this column's dots and the earlier
+    // columns of T), so that no CTA waits for it
+    jprev = j;
+    dcprev = dc;
+    tauprev = tau;
   }
   // write R (rows g <= c: the band) and V (explicit, unit lower trapezoidal)
 #pragma unroll
@@ -485,6 +515,7 @@ __global__ void __launch_bounds__(NW * 32) qr_panel2_kernel(PanelArgs a) {
   }
   if (HYB)   // rows below 383: V only
     for (int i = warp; RREG + i < nr; i += NW) a.V[(size_t)(lo + RREG + i) * B + lane] = Ps[i * QR_LD2 + lane];
+  if (rank == 0 && warp == 0 && jprev >= 0) t_column(jprev, dcprev, tauprev);   // the last column of T
   if (rank == 0) {
     __syncthreads();
     for (int e = tid; e < B * B; e += NT) a.T[e] = Tm[e / B][e % B];
