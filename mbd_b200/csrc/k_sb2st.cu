@@ -69,7 +69,10 @@ __device__ __forceinline__ void st_release(int* p, int v) {
   asm volatile("st.release.gpu.b32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
 }
 
-// Lane 0 spins (bounded) until *p >= target; then every lane acquires.
+// Lane 0 spins (bounded) with acquire loads until *p >= target; the warp
+// barrier after it orders every lane's later reads behind that acquire (a
+// second acquire load by every lane would add an L2 round trip to each link
+// of the sweep-to-sweep chain).
 __device__ bool wait_progress(const int* p, int target, int* err) {
   int ok = 1;
   if ((threadIdx.x & 31) == 0) {
@@ -95,7 +98,6 @@ __device__ bool wait_progress(const int* p, int target, int* err) {
     }
   }
   ok = __shfl_sync(0xffffffffu, ok, 0);
-  if (ok) (void)ld_acquire(p);
   __syncwarp();
   return ok != 0;
 }
