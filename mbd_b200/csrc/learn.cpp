@@ -10,6 +10,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cstdlib>
 #include <cmath>
 #include <cstdint>
 #include <cstring>
@@ -317,7 +318,14 @@ int relay_learned(mbd_ctx* ctx, GeomDev* gd, RelaySlot& sl, size_t mstride, cuda
   record_timing(ctx, ev_net, s);
   // the full schedule, or in a captured graph the iterations this geometry
   // took on its last compute plus a margin
-  auto sched = [&](int seen, int cap) { return (ctx->capturing && seen > 0) ? std::min(cap, seen + kCgSlack) : cap; };
+  // MBD_B200_CG_PREDICT=0: captured graphs keep the full schedule too
+  static const bool predict = [] {
+    const char* e = std::getenv("MBD_B200_CG_PREDICT");
+    return !(e && e[0] == '0');
+  }();
+  auto sched = [&](int seen, int cap) {
+    return (predict && ctx->capturing && seen > 0) ? std::min(cap, seen + kCgSlack) : cap;
+  };
   if (a.A32) {
     const double tol2 = a.tol2;
     a.tol2 = kCgTol1 * kCgTol1 * 3.0 * N;
