@@ -183,7 +183,10 @@ int mbd_rsscs_last_timings(mbd_ctx* ctx, double* ms, int n);
  * the last compute replayed the batch's captured CUDA graph, 0 when it
  * launched the kernels one by one (the first compute of an uploaded batch in
  * a mode launches directly; the second captures the graph and replays it
- * from then on; a change of network or of device buffers starts over).
+ * from then on; a change of network or of device buffers starts over),
+ * [4] (n >= 5) the edges of the MIXED_LEARNED network's neighbour lists over
+ * the batch's geometries (pairs within 5 A, periodic images included, both
+ * directions; 0 until a learned compute or training has built them).
  * n must be >= 3. */
 int mbd_rsscs_last_stats(mbd_ctx* ctx, double* out, int n);
 

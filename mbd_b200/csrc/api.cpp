@@ -1240,6 +1240,11 @@ int mbd_rsscs_last_stats(mbd_ctx* ctx, double* out, int n) {
   out[1] = ctx->h2d_bytes;
   out[2] = ctx->d2h_bytes;
   if (n >= 4) out[3] = ctx->graph_replayed ? 1.0 : 0.0;
+  if (n >= 5) {
+    double edges = 0.0;
+    for (const auto& gd : ctx->geoms) edges += std::max(gd->n_edges, 0);
+    out[4] = edges;
+  }
   return MBD_OK;
 }
 

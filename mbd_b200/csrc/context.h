@@ -151,6 +151,7 @@ struct mbd_ctx {
   double* omega_dev = nullptr;               // the 21 imaginary frequencies
   // learned warm start: network parameters, Adam state, training work
   mbd::DevBuf gnn_params, gnn_grad, gnn_m1, gnn_m2, gnn_train_work, gnn_eval;
+  mbd::DevBuf graph_scan;   // edge counts / offsets of the network graphs being built
   bool have_net = false;
   bool use_net = true;
   double* loss_dev = nullptr;

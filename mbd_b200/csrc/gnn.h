@@ -54,6 +54,24 @@ struct GnnWork {
   float *dS, *dh, *dh2, *du, *dm, *ds, *da, *dfilt, *cw, *S_true;
 };
 
+// Radius graph of one geometry (the network's neighbour lists): edges
+// (i, j, t) for the images t = n0 a0 + n1 a1 + n2 a2, |n_k| <= rng[k], with
+// 1e-12 <= |x_j + t - x_i|^2 < rc2, CSR by i, each list in (image, j) order.
+struct GraphBox {
+  double lat[9];         // lattice vectors a_k = lat[3k .. 3k+2], bohr
+  int rng[3];            // image range per axis (0 along vacuum axes and for clusters)
+  double lo[3], hi[3];   // bounding box of the atoms
+  double pad;            // the cut-off plus a rounding margin (image pruning)
+  double rc2;            // squared cut-off, bohr^2
+};
+// cnt[i] = edges of atom i
+void gnn_graph_count(const double* x, int N, const GraphBox& b, int* cnt, cudaStream_t s);
+// cnt[0..N) -> CSR offsets in place, cnt[N] = *E = the edge count
+void gnn_graph_scan(int* cnt_off, int N, int* E, cudaStream_t s);
+// the lists at the offsets off_in (copied to off[0..N])
+void gnn_graph_fill(const double* x, int N, const GraphBox& b, const int* off_in, int* off, int* nbr, int* src,
+                    float* dvec, cudaStream_t s);
+
 size_t gnn_work_floats(int N, int F, int E, bool train);
 GnnWork gnn_work_layout(float* base, int N, int F, int E, bool train);
 void gnn_edges(const float* dvec, int E, float* efeat, float* eproj, cudaStream_t s);

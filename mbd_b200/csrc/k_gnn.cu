@@ -367,6 +367,112 @@ __global__ void targets_kernel(const double* X, size_t ystride, const double* al
   St[idx] = (float)(X[(size_t)f * ystride + (size_t)9 * i + c] / alpha_w[(size_t)f * N + i]);
 }
 
+// ---- the network's neighbour lists (radius graph), built on the device ----
+// Every (atom i, image t, atom j) is tested with one warp per atom i, lanes
+// over j; a ballot orders each warp's edges by (image, j), so the lists come
+// out deterministic.  Coordinates are in bohr; the translations and distances
+// use explicitly rounded FP64 operations (no contraction), so the count pass
+// and the fill pass take the same decisions.
+
+__device__ __forceinline__ void image_shift(const GraphBox& b, int n0, int n1, int n2, double* t) {
+#pragma unroll
+  for (int c = 0; c < 3; ++c)
+    t[c] = __dadd_rn(__dadd_rn(__dmul_rn((double)n0, b.lat[c]), __dmul_rn((double)n1, b.lat[3 + c])),
+                     __dmul_rn((double)n2, b.lat[6 + c]));
+}
+
+// false when no atom of image t can lie within the cut-off of xi (xi outside
+// the image's bounding box widened by the cut-off and a rounding margin)
+__device__ __forceinline__ bool image_near(const GraphBox& b, const double* xi, const double* t) {
+  bool near = true;
+#pragma unroll
+  for (int c = 0; c < 3; ++c) near = near && xi[c] >= b.lo[c] + t[c] - b.pad && xi[c] <= b.hi[c] + t[c] + b.pad;
+  return near;
+}
+
+template <bool FILL>
+__global__ void __launch_bounds__(256) graph_kernel(const double* __restrict__ x, int N, GraphBox b,
+                                                    const int* __restrict__ off_in, int* cnt_or_off,
+                                                    int* __restrict__ nbr, int* __restrict__ src,
+                                                    float* __restrict__ dvec) {
+  const int lane = threadIdx.x & 31;
+  const int i = (int)((blockIdx.x * (unsigned)blockDim.x + threadIdx.x) >> 5);
+  if (i >= N) return;   // whole warps
+  const double xi[3] = {x[3 * i], x[3 * i + 1], x[3 * i + 2]};
+  int pos = FILL ? off_in[i] : 0;
+  if (FILL && lane == 0) {
+    cnt_or_off[i] = pos;
+    if (i == N - 1) cnt_or_off[N] = off_in[N];
+  }
+  for (int n0 = -b.rng[0]; n0 <= b.rng[0]; ++n0)
+    for (int n1 = -b.rng[1]; n1 <= b.rng[1]; ++n1)
+      for (int n2 = -b.rng[2]; n2 <= b.rng[2]; ++n2) {
+        double t[3];
+        image_shift(b, n0, n1, n2, t);
+        if (!image_near(b, xi, t)) continue;   // uniform over the warp
+        for (int j0 = 0; j0 < N; j0 += 32) {
+          const int j = j0 + lane;
+          bool ok = false;
+          double d[3] = {0.0, 0.0, 0.0};
+          if (j < N) {
+#pragma unroll
+            for (int c = 0; c < 3; ++c) d[c] = __dsub_rn(__dadd_rn(x[3 * j + c], t[c]), xi[c]);
+            const double r2 = __dadd_rn(__dadd_rn(__dmul_rn(d[0], d[0]), __dmul_rn(d[1], d[1])), __dmul_rn(d[2], d[2]));
+            ok = r2 < b.rc2 && r2 >= 1e-12;   // the atom itself (zero shift) has r = 0
+          }
+          const unsigned m = __ballot_sync(0xffffffffu, ok);
+          if (FILL && ok) {
+            const int e = pos + __popc(m & ((1u << lane) - 1u));
+            nbr[e] = j;
+            src[e] = i;
+            dvec[3 * (size_t)e] = (float)d[0];
+            dvec[3 * (size_t)e + 1] = (float)d[1];
+            dvec[3 * (size_t)e + 2] = (float)d[2];
+          }
+          pos += __popc(m);
+        }
+      }
+  if (!FILL && lane == 0) cnt_or_off[i] = pos;
+}
+
+// In-place exclusive scan of a[0..N) by one CTA; a[N] = *E = the total.
+__global__ void __launch_bounds__(1024) graph_scan_kernel(int* a, int N, int* E) {
+  __shared__ int wsum[32];
+  const int t = threadIdx.x, lane = t & 31, w = t >> 5;
+  const int chunk = (N + 1023) / 1024;
+  const int b0 = min(N, t * chunk), b1 = min(N, b0 + chunk);
+  int mine = 0;
+  for (int k = b0; k < b1; ++k) mine += a[k];
+  int v = mine;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const int u = __shfl_up_sync(0xffffffffu, v, o);
+    if (lane >= o) v += u;
+  }
+  if (lane == 31) wsum[w] = v;
+  __syncthreads();
+  if (w == 0) {
+    int q = wsum[lane];
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int u = __shfl_up_sync(0xffffffffu, q, o);
+      if (lane >= o) q += u;
+    }
+    wsum[lane] = q;
+  }
+  __syncthreads();
+  int run = v - mine + (w > 0 ? wsum[w - 1] : 0);
+  for (int k = b0; k < b1; ++k) {
+    const int c = a[k];
+    a[k] = run;
+    run += c;
+  }
+  if (t == 0) {
+    a[N] = wsum[31];
+    *E = wsum[31];
+  }
+}
+
 inline unsigned blocks(long long n, int t) { return (unsigned)((n + t - 1) / t); }
 
 void outer(const float* A, int K1, const float* B, int K2, long long rows, long long bmod, float* out,
@@ -419,6 +525,19 @@ GnnWork gnn_work_layout(float* base, int N, int F, int E, bool train) {
     w.S_true = take(9 * M);
   }
   return w;
+}
+
+void gnn_graph_count(const double* x, int N, const GraphBox& b, int* cnt, cudaStream_t s) {
+  graph_kernel<false><<<blocks(32LL * N, 256), 256, 0, s>>>(x, N, b, nullptr, cnt, nullptr, nullptr, nullptr);
+}
+
+void gnn_graph_scan(int* cnt_off, int N, int* E, cudaStream_t s) {
+  graph_scan_kernel<<<1, 1024, 0, s>>>(cnt_off, N, E);
+}
+
+void gnn_graph_fill(const double* x, int N, const GraphBox& b, const int* off_in, int* off, int* nbr, int* src,
+                    float* dvec, cudaStream_t s) {
+  graph_kernel<true><<<blocks(32LL * N, 256), 256, 0, s>>>(x, N, b, off_in, off, nbr, src, dvec);
 }
 
 void gnn_edges(const float* dvec, int E, float* efeat, float* eproj, cudaStream_t s) {

@@ -34,14 +34,14 @@ constexpr double kCgTol = 3e-11;   // relative residual the iteration stops at (
 constexpr int kCgPhaseMaxIters = 40;
 constexpr double kCgTol1 = 1e-5;
 
-// Neighbour lists within the network's cut-off, including periodic images
-// along non-vacuum axes (an atom may meet another atom, or itself, through
-// several images).  Lists are symmetric: edge (i, j + t) implies (j, i - t).
-void build_graph(const GeomPlan& p, std::vector<int>& off, std::vector<int>& nbr, std::vector<int>& src,
-                 std::vector<float>& dvec) {
-  const int N = p.N;
+// Image range and bounding box of the network's neighbour lists (within the
+// cut-off, including periodic images along non-vacuum axes: an atom may meet
+// another atom, or itself, through several images).  The lists are
+// symmetric: edge (i, j + t) implies (j, i - t).
+GraphBox graph_box(const GeomPlan& p) {
+  GraphBox b{};
   const double rc = kGnnCutoffBohr;
-  int rng[3] = {0, 0, 0};
+  for (int k = 0; k < 9; ++k) b.lat[k] = p.lat[k];
   if (p.n_periodic != 0) {
     // images up to the cut-off plus a cell: widths from |a_k| lower-bound nothing,
     // so use the perpendicular width V / |a_i x a_j|
@@ -61,124 +61,83 @@ void build_graph(const GeomPlan& p, std::vector<int>& off, std::vector<int>& nbr
       if (p.vac[k]) continue;
       const double area = std::sqrt(cs[k][0] * cs[k][0] + cs[k][1] * cs[k][1] + cs[k][2] * cs[k][2]);
       const double width = vol > 0.0 ? vol / area : 0.0;
-      rng[k] = width > 0.0 ? (int)std::ceil(rc / width) + 1 : 0;
+      b.rng[k] = width > 0.0 ? (int)std::ceil(rc / width) + 1 : 0;
     }
   }
-  double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
-  for (int i = 0; i < N; ++i)
+  for (int c = 0; c < 3; ++c) {
+    b.lo[c] = 1e300;
+    b.hi[c] = -1e300;
+  }
+  for (int i = 0; i < p.N; ++i)
     for (int c = 0; c < 3; ++c) {
-      lo[c] = std::min(lo[c], p.coords[3 * i + c]);
-      hi[c] = std::max(hi[c], p.coords[3 * i + c]);
+      b.lo[c] = std::min(b.lo[c], p.coords[3 * i + c]);
+      b.hi[c] = std::max(b.hi[c], p.coords[3 * i + c]);
     }
-  // image points near the box: (atom, position)
-  struct Pt {
-    int atom;
-    double x[3];
-  };
-  std::vector<Pt> pts;
-  for (int n0 = -rng[0]; n0 <= rng[0]; ++n0)
-    for (int n1 = -rng[1]; n1 <= rng[1]; ++n1)
-      for (int n2 = -rng[2]; n2 <= rng[2]; ++n2) {
-        double t[3];
-        for (int c = 0; c < 3; ++c) t[c] = n0 * p.lat[c] + n1 * p.lat[3 + c] + n2 * p.lat[6 + c];
-        for (int j = 0; j < N; ++j) {
-          Pt q{j, {p.coords[3 * j] + t[0], p.coords[3 * j + 1] + t[1], p.coords[3 * j + 2] + t[2]}};
-          bool keep = true;
-          for (int c = 0; c < 3; ++c) keep = keep && q.x[c] >= lo[c] - rc && q.x[c] <= hi[c] + rc;
-          if (keep) pts.push_back(q);
-        }
-      }
-  // uniform bins of edge rc over the padded box
-  int nb[3];
-  for (int c = 0; c < 3; ++c) nb[c] = std::max(1, (int)std::ceil((hi[c] - lo[c] + 2 * rc) / rc));
-  auto bin_of = [&](const double* x, int* b) {
-    for (int c = 0; c < 3; ++c) b[c] = std::min(nb[c] - 1, std::max(0, (int)((x[c] - (lo[c] - rc)) / rc)));
-  };
-  const size_t nbins = (size_t)nb[0] * nb[1] * nb[2];
-  std::vector<int> head(nbins + 1, 0);
-  std::vector<int> order(pts.size());
-  std::vector<size_t> pb(pts.size());
-  for (size_t k = 0; k < pts.size(); ++k) {
-    int b[3];
-    bin_of(pts[k].x, b);
-    pb[k] = ((size_t)b[0] * nb[1] + b[1]) * nb[2] + b[2];
-    head[pb[k] + 1]++;
-  }
-  for (size_t k = 0; k < nbins; ++k) head[k + 1] += head[k];
-  {
-    std::vector<int> fill(head.begin(), head.end() - 1);
-    for (size_t k = 0; k < pts.size(); ++k) order[fill[pb[k]]++] = (int)k;
-  }
-  off.assign(N + 1, 0);
-  nbr.clear();
-  src.clear();
-  dvec.clear();
-  const double rc2 = rc * rc;
-  for (int i = 0; i < N; ++i) {
-    const double* xi = &p.coords[3 * i];
-    int b[3];
-    bin_of(xi, b);
-    for (int d0 = -1; d0 <= 1; ++d0)
-      for (int d1 = -1; d1 <= 1; ++d1)
-        for (int d2 = -1; d2 <= 1; ++d2) {
-          const int c0 = b[0] + d0, c1 = b[1] + d1, c2 = b[2] + d2;
-          if (c0 < 0 || c1 < 0 || c2 < 0 || c0 >= nb[0] || c1 >= nb[1] || c2 >= nb[2]) continue;
-          const size_t bin = ((size_t)c0 * nb[1] + c1) * nb[2] + c2;
-          for (int k = head[bin]; k < head[bin + 1]; ++k) {
-            const Pt& q = pts[order[k]];
-            const double dx = q.x[0] - xi[0], dy = q.x[1] - xi[1], dz = q.x[2] - xi[2];
-            const double r2 = dx * dx + dy * dy + dz * dz;
-            if (r2 >= rc2 || r2 < 1e-12) continue;   // the atom itself (zero shift) has r = 0
-            nbr.push_back(q.atom);
-            src.push_back(i);
-            dvec.push_back((float)dx);
-            dvec.push_back((float)dy);
-            dvec.push_back((float)dz);
-          }
-        }
-    off[i + 1] = (int)nbr.size();
-  }
+  b.pad = rc + 1e-6;   // far above the rounding of |coordinates| <= 1e6 bohr
+  b.rc2 = rc * rc;
+  return b;
 }
 
-// Device copy of a graph: [off | nbr | src | species] ints, [dvec | efeat | eproj] floats.
-int upload_graph(mbd_ctx* ctx, GeomDev* gd, cudaStream_t s) {
-  const GeomPlan& p = gd->plan;
-  std::vector<int> off, nbr, src;
-  std::vector<float> dvec;
-  build_graph(p, off, nbr, src, dvec);
-  const int N = p.N, E = (int)nbr.size();
-  const size_t b_off = bytes_of<int>(N + 1), b_e = bytes_of<int>(std::max(E, 1)), b_sp = bytes_of<int>(N);
-  const size_t b_dv = bytes_of<float>(3 * (size_t)std::max(E, 1)), b_ef = bytes_of<float>(kGnnRbf * (size_t)std::max(E, 1));
-  const size_t b_ep = bytes_of<float>(6 * (size_t)std::max(E, 1));
-  const size_t total = b_off + 2 * b_e + b_sp + b_dv + b_ef + b_ep;
-  MBD_CUDA(gd->graph.reserve(total));
-  char* base = gd->graph.as<char>();
-  std::vector<char> host(b_off + 2 * b_e + b_sp + b_dv, 0);
-  std::memcpy(host.data(), off.data(), sizeof(int) * off.size());
-  std::memcpy(host.data() + b_off, nbr.data(), sizeof(int) * nbr.size());
-  std::memcpy(host.data() + b_off + b_e, src.data(), sizeof(int) * src.size());
-  std::memcpy(host.data() + b_off + 2 * b_e, p.species.data(), sizeof(int) * N);
-  std::memcpy(host.data() + b_off + 2 * b_e + b_sp, dvec.data(), sizeof(float) * dvec.size());
-  MBD_CUDA(h2d_ordered(ctx, base, host.data(), host.size()));
-  ctx->h2d_bytes += (double)host.size();
-  GnnGraph& g = gd->gnn;
-  g.N = N;
-  g.F = kNFreq;
-  g.E = E;
-  g.off = reinterpret_cast<const int*>(base);
-  g.nbr = reinterpret_cast<const int*>(base + b_off);
-  g.src = reinterpret_cast<const int*>(base + b_off + b_e);
-  const int* species = reinterpret_cast<const int*>(base + b_off + 2 * b_e);
-  const float* dv = reinterpret_cast<const float*>(base + b_off + 2 * b_e + b_sp);
-  float* ef = reinterpret_cast<float*>(base + b_off + 2 * b_e + b_sp + b_dv);
-  float* ep = reinterpret_cast<float*>(base + b_off + 2 * b_e + b_sp + b_dv + b_ef);
-  g.efeat = ef;
-  g.eproj = ep;
-  g.x = nullptr;
-  gd->n_edges = E;
-  (void)species;
-  gnn_edges(dv, E, ef, ep, s);
-  ctx->launches += E > 0 ? 1 : 0;
+// The network graphs of `todo`, built on the GPU: every geometry's edge
+// counts and offsets, one synchronisation to size the graph buffers, then the
+// lists.  Device copy of a graph: [off | nbr | src | species] ints,
+// [dvec | efeat | eproj] floats.
+int build_graphs(mbd_ctx* ctx, const std::vector<GeomDev*>& todo, cudaStream_t s) {
+  if (todo.empty()) return MBD_OK;
+  const size_t K = todo.size();
+  auto pad64 = [](size_t k) { return (k + 63) & ~size_t(63); };
+  size_t total = pad64(K);
+  for (GeomDev* gd : todo) total += pad64((size_t)gd->plan.N + 1);
+  MBD_CUDA(ctx->graph_scan.reserve(sizeof(int) * total));
+  int* Ed = ctx->graph_scan.as<int>();
+  std::vector<int*> offs(K);
+  std::vector<GraphBox> boxes(K);
+  size_t o = pad64(K);
+  for (size_t k = 0; k < K; ++k) {
+    GeomDev* gd = todo[k];
+    offs[k] = Ed + o;
+    o += pad64((size_t)gd->plan.N + 1);
+    boxes[k] = graph_box(gd->plan);
+    gnn_graph_count(gd->coords, gd->plan.N, boxes[k], offs[k], s);
+    gnn_graph_scan(offs[k], gd->plan.N, Ed + k, s);
+  }
+  std::vector<int> Eh(K);
+  MBD_CUDA(cudaMemcpyAsync(Eh.data(), Ed, sizeof(int) * K, cudaMemcpyDeviceToHost, s));
+  MBD_CUDA(cudaStreamSynchronize(s));
+  for (size_t k = 0; k < K; ++k) {
+    GeomDev* gd = todo[k];
+    const GeomPlan& p = gd->plan;
+    const int N = p.N, E = Eh[k];
+    if (E < 0) return MBD_ERR_DEVICE;
+    const size_t b_off = bytes_of<int>(N + 1), b_e = bytes_of<int>(std::max(E, 1)), b_sp = bytes_of<int>(N);
+    const size_t b_dv = bytes_of<float>(3 * (size_t)std::max(E, 1)), b_ef = bytes_of<float>(kGnnRbf * (size_t)std::max(E, 1));
+    const size_t b_ep = bytes_of<float>(6 * (size_t)std::max(E, 1));
+    MBD_CUDA(gd->graph.reserve(b_off + 2 * b_e + b_sp + b_dv + b_ef + b_ep));
+    char* base = gd->graph.as<char>();
+    int* off = reinterpret_cast<int*>(base);
+    int* nbr = reinterpret_cast<int*>(base + b_off);
+    int* src = reinterpret_cast<int*>(base + b_off + b_e);
+    int* species = reinterpret_cast<int*>(base + b_off + 2 * b_e);
+    float* dv = reinterpret_cast<float*>(base + b_off + 2 * b_e + b_sp);
+    float* ef = reinterpret_cast<float*>(base + b_off + 2 * b_e + b_sp + b_dv);
+    float* ep = reinterpret_cast<float*>(base + b_off + 2 * b_e + b_sp + b_dv + b_ef);
+    MBD_CUDA(cudaMemcpyAsync(species, p.species.data(), sizeof(int) * N, cudaMemcpyHostToDevice, s));
+    ctx->h2d_bytes += (double)sizeof(int) * N;
+    gnn_graph_fill(gd->coords, N, boxes[k], offs[k], off, nbr, src, dv, s);
+    gnn_edges(dv, E, ef, ep, s);
+    ctx->launches += 3 + (E > 0 ? 1 : 0);
+    GnnGraph& g = gd->gnn;
+    g.N = N;
+    g.F = kNFreq;
+    g.E = E;
+    g.off = off;
+    g.nbr = nbr;
+    g.src = src;
+    g.efeat = ef;
+    g.eproj = ep;
+    g.x = nullptr;
+    gd->n_edges = E;
+  }
   return cuda_status(cudaGetLastError());
 }
 
@@ -233,12 +192,12 @@ int reserve_params(mbd_ctx* ctx) {
 
 // Per-slot CG and network buffers and every geometry's graph.
 int reserve_learned(mbd_ctx* ctx) {
-  for (int g : ctx->order) {
-    GeomDev* gd = ctx->geoms[g].get();
-    if (gd->n_edges < 0) {
-      int st = upload_graph(ctx, gd, ctx->stream);
-      if (st != MBD_OK) return st;
-    }
+  {
+    std::vector<GeomDev*> todo;
+    for (int g : ctx->order)
+      if (ctx->geoms[g]->n_edges < 0) todo.push_back(ctx->geoms[g].get());
+    int st = build_graphs(ctx, todo, ctx->stream);
+    if (st != MBD_OK) return st;
   }
   bool moved = false;
   for (int s = 0; s < ctx->n_slots; ++s) {

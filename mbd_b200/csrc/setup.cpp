@@ -246,19 +246,21 @@ int build_plan(const mbd_geom& g, GeomPlan* p) {
   // leaves the FP64 relay matrix unchanged to ~1e-30 relative; the
   // reference's own r <= mbd_scs_dip_cutoff test (UTILS.f90:574,623) still
   // applies inside it.
-  double rmax_iso = 0.0, amax = 0.0, sgm_lo = 1e300, sgm_hi = 0.0;
+  // sigma = (alpha / 3 sqrt(2 / pi))^(1/3) rises with alpha: its extremes
+  // come from the extremes of alpha over atoms and frequencies
+  double rmax_iso = 0.0, amax = 0.0, amin = 1e300;
   for (int i = 0; i < N; ++i) {
     rmax_iso = std::max(rmax_iso, std::pow(p->hirsh[i], kOtd) * p->r0[i]);
     for (int f = 0; f < kNFreq; ++f) {
       double w = kCasimirOmega[f];
       double wp = (4.0 / 3.0) * p->c6free[i] / (p->alpha0[i] * p->alpha0[i]);
       double aw = (p->hirsh[i] * p->alpha0[i]) / (1.0 + (w * w) / (wp * wp));
-      double sg = std::pow((aw / 3.0) * std::sqrt(2.0 / kPi), kOtd);
-      sgm_lo = std::min(sgm_lo, sg);
-      sgm_hi = std::max(sgm_hi, sg * std::sqrt(2.0));
+      amin = std::min(amin, aw);
       amax = std::max(amax, aw);
     }
   }
+  const double sgm_lo = std::pow((amin / 3.0) * std::sqrt(2.0 / kPi), kOtd);
+  const double sgm_hi = std::pow((amax / 3.0) * std::sqrt(2.0 / kPi), kOtd) * std::sqrt(2.0);
   const double beta_rhi = p->beta * 2.0 * rmax_iso;
   const double tau = 1e-30 / amax;
   double r_lo = beta_rhi, r_hi = beta_rhi * 64.0 + 64.0;

@@ -10,6 +10,7 @@ no sm_100 GPU is present, construction raises.
 from __future__ import annotations
 
 import ctypes
+import functools
 import os
 from dataclasses import dataclass
 
@@ -188,6 +189,7 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
     return lib
 
 
+@functools.lru_cache(maxsize=512)
 def element_z(symbol: str) -> int:
     return load_library().mbd_rsscs_element_z(symbol.encode())
 
@@ -449,10 +451,10 @@ class Engine:
         return S.reshape(M, 3, 3), grad, loss
 
     def stats(self) -> dict:
-        buf = (ctypes.c_double * 4)()
-        self.lib.mbd_rsscs_last_stats(self.ctx, buf, 4)
+        buf = (ctypes.c_double * 5)()
+        self.lib.mbd_rsscs_last_stats(self.ctx, buf, 5)
         return {"launches": int(buf[0]), "h2d_bytes": int(buf[1]), "d2h_bytes": int(buf[2]),
-                "graph_replayed": bool(buf[3])}
+                "graph_replayed": bool(buf[3]), "network_edges": int(buf[4])}
 
     def stream_handle(self) -> int:
         """cudaStream_t of this context (for recording caller-side events)."""

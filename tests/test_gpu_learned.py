@@ -111,6 +111,31 @@ def test_cg_without_network_matches_plain(engine):
         assert a.err_est[0] <= 1e-10
 
 
+def test_network_graph_matches_oracle_neighbours(engine):
+    """The network's neighbour lists, built on the GPU at the first learned
+    compute of a batch, have the edges of the oracle's brute-force lists: a
+    cluster, a periodic box and a sheet (vacuum axis) whose cells are narrower
+    than twice the cut-off, so atoms also meet themselves through images."""
+    from mbd_b200 import synthetic as sy
+    from mbd_b200.engine import BOHR
+    items = [sy.cluster(250, seed=4), sy.periodic_box(40, seed=2, scs_cut=20.0, cfdm_cut=15.0, sc_cut=5.0),
+             sy.graphene_sheet(3)]
+    geos, sets = [g for g, _ in items], [s for _, s in items]
+    engine.use_network(False)
+    try:
+        res = engine.energy_batch(geos, sets, "mixed_learned")
+    finally:
+        engine.use_network(True)
+    assert all(r.status == 0 for r in res)
+    expect = []
+    for g, s in items:
+        lat = g.lattice / BOHR if g.n_periodic else None
+        _, nbr, _ = gn.neighbours(g.coords / BOHR, lat, tuple(bool(v) for v in s.mbd_scs_vacuum_axis))
+        expect.append(len(nbr))
+    assert min(expect) > 0
+    assert engine.stats()["network_edges"] == sum(expect), expect
+
+
 def test_trained_network_saves_cg_iterations(engine, trained):
     """Held-out boxes: the network's warm start needs at least 4 % fewer
     block-CG iterations in total than a zero start, with the same energies
