@@ -1007,9 +1007,52 @@ int mbd_rsscs_compute(mbd_ctx* ctx, int mode) {
 int mbd_rsscs_download(mbd_ctx* ctx, mbd_result* out) {
   if (!ctx || !ctx->have_batch || !out) return MBD_ERR_ARG;
   MBD_CUDA(cudaSetDevice(ctx->device));
+  // Every geometry's results in one pass into page-locked memory: the block
+  // alpha_iw .. energy and the block info .. CG state of its results buffer,
+  // queued behind the batch on the context stream, one synchronisation.
+  struct Range {
+    const char* lo;
+    size_t bytes, at;
+  };
+  auto range = [](const void* a, const void* b_end) {
+    const char* lo = static_cast<const char*>(a);
+    return Range{lo, (size_t)(static_cast<const char*>(b_end) - lo), 0};
+  };
+  std::vector<Range> r1(ctx->geoms.size()), r2(ctx->geoms.size());
+  size_t stage = 256;
+  for (size_t g = 0; g < ctx->geoms.size(); ++g) {
+    const GeomDev* gd = ctx->geoms[g].get();
+    if (gd->status_host != MBD_OK) continue;
+    r1[g] = range(gd->alpha_iw, gd->energy + 8);
+    r2[g] = range(gd->info, gd->cgstate + (size_t)kNFreq * kCgState);
+    r1[g].at = stage;
+    stage += (r1[g].bytes + 255) & ~size_t(255);
+    r2[g].at = stage;
+    stage += (r2[g].bytes + 255) & ~size_t(255);
+  }
+  MBD_CUDA(ctx->staging.reserve(stage));
+  char* hs = ctx->staging.as<char>();
+  MBD_CUDA(cudaMemcpyAsync(hs, ctx->err_flag, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+  ctx->d2h_bytes = sizeof(int);
+  auto fetch = [&](size_t g, cudaStream_t s) -> cudaError_t {
+    for (const Range* r : {&r1[g], &r2[g]}) {
+      cudaError_t e = cudaMemcpyAsync(hs + r->at, r->lo, r->bytes, cudaMemcpyDeviceToHost, s);
+      if (e != cudaSuccess) return e;
+      ctx->d2h_bytes += (double)r->bytes;
+    }
+    return cudaSuccess;
+  };
+  for (size_t g = 0; g < ctx->geoms.size(); ++g)
+    if (ctx->geoms[g]->status_host == MBD_OK) MBD_CUDA(fetch(g, ctx->stream));
   MBD_CUDA(cudaStreamSynchronize(ctx->stream));
   int err = 0;
-  MBD_CUDA(cudaMemcpy(&err, ctx->err_flag, sizeof(int), cudaMemcpyDeviceToHost));
+  std::memcpy(&err, hs, sizeof(int));
+  // host copy of a device array inside geometry g's two blocks
+  auto host = [&](size_t g, const void* dev) -> const char* {
+    const char* d = static_cast<const char*>(dev);
+    const Range& r = (d >= r1[g].lo && d < r1[g].lo + r1[g].bytes) ? r1[g] : r2[g];
+    return hs + r.at + (d - r.lo);
+  };
   // stage timings: relay/CFDM stages summed over geometries (they overlap on
   // the slots' streams), the batch-wide stages and the total from batch events
   for (int k = 0; k < Stage::kCount; ++k) ctx->last_ms[k] = 0.0;
@@ -1029,7 +1072,6 @@ int mbd_rsscs_download(mbd_ctx* ctx, mbd_result* out) {
     for (int k = 1; k < kGeomEvents; ++k) ctx->last_ms[k] += elapsed(evs[k - 1], evs[k]);   // [6]: dense -> band
     ctx->last_band_ms += elapsed(evs[5], evs[6]);
   }
-  ctx->d2h_bytes = sizeof(int);
   int first = MBD_OK;
   for (size_t g = 0; g < ctx->geoms.size(); ++g) {
     GeomDev* gd = ctx->geoms[g].get();
@@ -1047,21 +1089,16 @@ int mbd_rsscs_download(mbd_ctx* ctx, mbd_result* out) {
       continue;
     }
     const int N = p.N;
-    std::vector<double> aiw(21 * (size_t)N), molpol(21 * 9);
-    double scal[8], en[8];
-    int info[32];
     if (ctx->last_mode != MBD_MODE_PLAIN_FP64) {
       // residual gate of the mixed relay solve; a miss re-runs this geometry
       // with the direct FP64 solve (the plain path) before reading results
-      double rn[32];
-      MBD_CUDA(cudaMemcpy(rn, gd->rnorm2, sizeof(double) * 21, cudaMemcpyDeviceToHost));
+      const double* rn = reinterpret_cast<const double*>(host(g, gd->rnorm2));
       double worst = 0.0;
       for (int f = 0; f < 21; ++f) worst = std::max(worst, std::sqrt(rn[f] / (3.0 * N)));
       r.err_est[0] = r.err_est[1] = r.err_est[2] = worst;
       r.refine_iters = kRefineIters;
       if (ctx->last_mode == MBD_MODE_MIXED_LEARNED) {
-        std::vector<double> cs((size_t)kNFreq * kCgState);
-        MBD_CUDA(cudaMemcpy(cs.data(), gd->cgstate, sizeof(double) * cs.size(), cudaMemcpyDeviceToHost));
+        const double* cs = reinterpret_cast<const double*>(host(g, gd->cgstate));
         double most = 0.0, most1 = 0.0;
         bool indefinite = false;
         for (int f = 0; f < kNFreq; ++f) {
@@ -1082,16 +1119,17 @@ int mbd_rsscs_download(mbd_ctx* ctx, mbd_result* out) {
         int st = run_front(ctx, gd, (int)g, MBD_MODE_PLAIN_FP64);
         if (st == MBD_OK) st = run_tail_single(ctx, gd, ctx->slots[gd->slot]->stream);
         if (st != MBD_OK) return st;
-        MBD_CUDA(cudaStreamSynchronize(ctx->slots[gd->slot]->stream));
+        const cudaStream_t ss = ctx->slots[gd->slot]->stream;
+        MBD_CUDA(fetch(g, ss));   // the re-run's results replace the staged ones
+        MBD_CUDA(cudaStreamSynchronize(ss));
         r.refine_iters = -1;
       }
     }
-    MBD_CUDA(cudaMemcpy(aiw.data(), gd->alpha_iw, sizeof(double) * 21 * N, cudaMemcpyDeviceToHost));
-    MBD_CUDA(cudaMemcpy(molpol.data(), gd->molpol, sizeof(double) * 21 * 9, cudaMemcpyDeviceToHost));
-    MBD_CUDA(cudaMemcpy(scal, gd->scalars, sizeof(scal), cudaMemcpyDeviceToHost));
-    MBD_CUDA(cudaMemcpy(en, gd->energy, sizeof(en), cudaMemcpyDeviceToHost));
-    MBD_CUDA(cudaMemcpy(info, gd->info, sizeof(info), cudaMemcpyDeviceToHost));
-    ctx->d2h_bytes += sizeof(double) * (21.0 * N + 21 * 9 + 16) + sizeof(info);
+    const double* aiw = reinterpret_cast<const double*>(host(g, gd->alpha_iw));
+    const double* molpol = reinterpret_cast<const double*>(host(g, gd->molpol));
+    const double* scal = reinterpret_cast<const double*>(host(g, gd->scalars));
+    const double* en = reinterpret_cast<const double*>(host(g, gd->energy));
+    const int* info = reinterpret_cast<const int*>(host(g, gd->info));
     int status = MBD_OK;
     for (int f = 0; f < 21; ++f)
       if (info[f] != 0) status = MBD_ERR_RELAY_NOT_SPD;
@@ -1111,23 +1149,18 @@ int mbd_rsscs_download(mbd_ctx* ctx, mbd_result* out) {
     if (r.alpha_iw)   // column-major alpha(f, i): element (f, i) at f + 21 i
       for (int q = 0; q < N; ++q)
         for (int f = 0; f < 21; ++f) r.alpha_iw[f + 21 * (size_t)pm[q]] = aiw[(size_t)f * N + q];
-    std::vector<double> tmp;
     if (r.alpha_eff) {
-      tmp.resize(N);
-      MBD_CUDA(cudaMemcpy(tmp.data(), gd->alpha_eff, sizeof(double) * N, cudaMemcpyDeviceToHost));
-      for (int q = 0; q < N; ++q) r.alpha_eff[pm[q]] = tmp[q];
-      ctx->d2h_bytes += sizeof(double) * N;
+      const double* a = reinterpret_cast<const double*>(host(g, gd->alpha_eff));
+      for (int q = 0; q < N; ++q) r.alpha_eff[pm[q]] = a[q];
     }
     if (r.c6_eff) {
-      tmp.resize(N);
-      MBD_CUDA(cudaMemcpy(tmp.data(), gd->c6_eff, sizeof(double) * N, cudaMemcpyDeviceToHost));
-      for (int q = 0; q < N; ++q) r.c6_eff[pm[q]] = tmp[q];
-      ctx->d2h_bytes += sizeof(double) * N;
+      const double* c = reinterpret_cast<const double*>(host(g, gd->c6_eff));
+      for (int q = 0; q < N; ++q) r.c6_eff[pm[q]] = c[q];
     }
     if (r.molpol_eig)
       for (int f = 0; f < 21; ++f) {
         double e3[3];
-        sym3_eigenvalues_upper(molpol.data() + 9 * f, e3);
+        sym3_eigenvalues_upper(molpol + 9 * f, e3);
         for (int k = 0; k < 3; ++k) r.molpol_eig[f + 21 * k] = e3[k];
       }
     if (status != MBD_OK && first == MBD_OK) first = status;

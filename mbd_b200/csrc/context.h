@@ -42,6 +42,26 @@ struct DevBuf {
   T* as() const { return static_cast<T*>(p); }
 };
 
+// Page-locked host memory (the download's staging area).
+struct HostBuf {
+  void* p = nullptr;
+  size_t bytes = 0;
+  ~HostBuf() {
+    if (p) cudaFreeHost(p);
+  }
+  cudaError_t reserve(size_t b) {
+    if (b <= bytes) return cudaSuccess;
+    if (p) cudaFreeHost(p);
+    p = nullptr;
+    bytes = 0;
+    cudaError_t e = cudaMallocHost(&p, b);
+    if (e == cudaSuccess) bytes = b;
+    return e;
+  }
+  template <class T>
+  T* as() const { return static_cast<T*>(p); }
+};
+
 // Per-geometry device state that must survive until download.
 struct GeomDev {
   GeomPlan plan;
@@ -127,6 +147,7 @@ struct mbd_ctx {
   std::vector<std::unique_ptr<mbd::RelaySlot>> slots;
   int n_slots = 0;                           // slots in use for the current batch
   mbd::DevBuf tridiag_ws, tables, misc, fb_ws;
+  mbd::HostBuf staging;   // download: every geometry's results in one pass
   // standalone eigenvalue call: matrix, (d, e, eigenvalues, scratch), workspace
   mbd::DevBuf eig_a, eig_vec, eig_ws;
   // batch plan (device tables in `tables`)
