@@ -130,6 +130,17 @@ int mbd_rsscs_download(mbd_ctx* ctx, mbd_result* out);
  * buffers come from (and stay with) the context. */
 int mbd_rsscs_eigvalsh(mbd_ctx* ctx, const double* H, int n, int ld, double* w);
 
+/* Eigenvalues and eigenvectors of a real symmetric n x n matrix in FP64: the
+ * PDSYEV call of UTILS.f90:835 with JOBZ = 'V' (the reference passes 'N' and
+ * discards the eigenvector matrix it allocates at UTILS.f90:771).  H as for
+ * mbd_rsscs_eigvalsh (HOST, lower triangle in C row-major order, H(i,j) for
+ * j <= i at H[i*ld + j]).  w (host, n) receives the eigenvalues ascending;
+ * Z (host, row-major, ldz >= n) the orthonormal eigenvectors as columns:
+ * Z[i*ldz + k] is component i of the eigenvector of w[k] (for a Fortran
+ * caller, Z's rows are the eigenvectors).  The sign of each vector, and the
+ * basis inside a degenerate eigenspace, are the engine's choice. */
+int mbd_rsscs_eigh(mbd_ctx* ctx, const double* H, int n, int ld, double* w, double* Z, int ldz);
+
 /* mbd_rsscs_eigvalsh for callers that must not allocate device memory.
  * (No counterpart in the reference: pmbd.x lets ScaLAPACK allocate its work
  * arrays.)  Meant for hosts that own the GPU's memory through their own pool

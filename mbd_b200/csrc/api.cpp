@@ -1228,6 +1228,114 @@ int mbd_rsscs_eigvalsh(mbd_ctx* ctx, const double* H, int n, int ld, double* w) 
   return err ? err : MBD_OK;
 }
 
+int mbd_rsscs_eigh(mbd_ctx* ctx, const double* H, int n, int ld, double* w, double* Z, int ldz) {
+  if (!ctx || !H || !w || !Z || n < 1 || ld < n || ldz < n) return MBD_ERR_ARG;
+  MBD_CUDA(cudaSetDevice(ctx->device));
+  cudaStream_t s = ctx->stream;
+  constexpr int NBW = 128;   // reflectors per compact-WY block of the back-transformation
+  const size_t ldp = round_up(n, 32);
+  const size_t nn = (size_t)n * ldp;
+  const int G = tridiag_group_ctas(ctx, n);
+  const size_t wsb = tridiag_workspace_bytes(n, G);
+  MBD_CUDA(ctx->eig_ws.reserve(wsb));
+  // A, V (reflectors), X, X2 (vectors), Gram; scratch; W, W2 (NBW x n);
+  // S, T (NBW x NBW); tau, d, e, ev (2n); the deviation word
+  size_t off = 0;
+  std::vector<size_t> o;
+  auto add = [&](size_t doubles) { o.push_back(off); off += (doubles + 31) & ~size_t(31); };
+  add(nn);
+  add(nn);
+  add(nn);
+  add(nn);
+  add((size_t)n * n);
+  add(eigh_scratch_doubles(n));
+  add((size_t)NBW * n);
+  add((size_t)NBW * n);
+  add((size_t)NBW * NBW);
+  add((size_t)NBW * NBW);
+  add(n);
+  add(n);
+  add(n);
+  add(2 * (size_t)n);
+  add(4);
+  MBD_CUDA(ctx->eigh_buf.reserve(sizeof(double) * off));
+  double* base = ctx->eigh_buf.as<double>();
+  double* A = base + o[0];
+  double* V = base + o[1];
+  double* X = base + o[2];
+  double* X2 = base + o[3];
+  double* Gm = base + o[4];
+  double* scratch = base + o[5];
+  double* W = base + o[6];
+  double* W2 = base + o[7];
+  double* Sg = base + o[8];
+  double* Tb = base + o[9];
+  double* tau = base + o[10];
+  double* d = base + o[11];
+  double* e = base + o[12];
+  double* ev = base + o[13];
+  unsigned long long* dev = reinterpret_cast<unsigned long long*>(base + o[14]);
+  MBD_CUDA(cudaMemcpy2DAsync(A, sizeof(double) * ldp, H, sizeof(double) * ld, sizeof(double) * n, n,
+                             cudaMemcpyHostToDevice, s));
+  MBD_CUDA(cudaMemsetAsync(V, 0, sizeof(double) * nn, s));
+  MBD_CUDA(cudaMemsetAsync(tau, 0, sizeof(double) * n, s));
+  MBD_CUDA(cudaMemsetAsync(e, 0, sizeof(double) * n, s));
+  MBD_CUDA(cudaMemsetAsync(ctx->err_flag, 0, sizeof(int), s));
+  // A = Q T Q^T, the reflectors of Q kept
+  TridiagJob job{A, n, (int)ldp, d, e};
+  job.vsave = V;
+  job.tau = tau;
+  job.ldv = ldp;
+  MBD_CUDA(cudaMemcpyAsync(ctx->job_dev, &job, sizeof(job), cudaMemcpyHostToDevice, s));
+  MBD_CUDA(launch_tridiag(ctx->job_dev, 1, 1, G, ctx->eig_ws.p, wsb, n, ctx->err_flag, s));
+  launch_tridiag_eigenvalues(d, e, n, ev, s);
+  double ends[2];
+  MBD_CUDA(cudaMemcpyAsync(&ends[0], ev, sizeof(double), cudaMemcpyDeviceToHost, s));
+  MBD_CUDA(cudaMemcpyAsync(&ends[1], ev + n - 1, sizeof(double), cudaMemcpyDeviceToHost, s));
+  MBD_CUDA(cudaStreamSynchronize(s));
+  int err = 0;
+  MBD_CUDA(cudaMemcpy(&err, ctx->err_flag, sizeof(int), cudaMemcpyDeviceToHost));
+  if (err) return err;
+  const double tnorm = std::max(std::fabs(ends[0]), std::fabs(ends[1]));
+  // the tridiagonal's eigenvectors, then Newton-Schulz to orthonormality
+  launch_tri_vectors(d, e, ev, n, tnorm, X, ldp, scratch, s);
+  const double ns_tol = 1e-15 * std::max(10.0, 4.0 * std::sqrt((double)n));
+  for (int step = 0; step < 4; ++step) {
+    dgemm_rm(true, false, n, n, n, 1.0, X, ldp, X, ldp, 0.0, Gm, n, s);   // X^T X
+    MBD_CUDA(cudaMemsetAsync(dev, 0, sizeof(unsigned long long), s));
+    launch_ns_prepare(Gm, n, dev, s);
+    unsigned long long bits = 0;
+    MBD_CUDA(cudaMemcpyAsync(&bits, dev, sizeof(bits), cudaMemcpyDeviceToHost, s));
+    MBD_CUDA(cudaStreamSynchronize(s));
+    double dv;
+    std::memcpy(&dv, &bits, sizeof(dv));
+    if (!(dv > ns_tol)) break;
+    dgemm_rm(false, false, n, n, n, 1.0, X, ldp, Gm, n, 0.0, X2, ldp, s);   // X (3I - X^T X) / 2
+    std::swap(X, X2);
+  }
+  // X <- Q X: blocks of reflectors c0 .. c0 + kb - 1 (rows c0 + 1 .. n - 1),
+  // the last block first; V^T of a block is row-major (kb x m) at
+  // V + c0 * ldp + c0 + 1
+  const int nr = n - 1;
+  for (int c0 = nr > 0 ? ((nr - 1) / NBW) * NBW : -1; c0 >= 0; c0 -= NBW) {
+    const int kb = std::min(NBW, nr - c0);
+    const int m = n - c0 - 1;
+    const double* Vt = V + (size_t)c0 * ldp + c0 + 1;
+    double* Xs = X + (size_t)(c0 + 1) * ldp;
+    dgemm_rm(false, true, kb, kb, m, 1.0, Vt, ldp, Vt, ldp, 0.0, Sg, NBW, s);    // S = V^T V
+    launch_wy_t(Sg, tau + c0, kb, NBW, Tb, s);
+    dgemm_rm(false, false, kb, n, m, 1.0, Vt, ldp, Xs, ldp, 0.0, W, n, s);       // W = V^T X
+    dgemm_rm(false, false, kb, n, kb, 1.0, Tb, NBW, W, n, 0.0, W2, n, s);        // W2 = T W
+    dgemm_rm(true, false, m, n, kb, -1.0, Vt, ldp, W2, n, 1.0, Xs, ldp, s);      // X -= V W2
+  }
+  MBD_CUDA(cudaGetLastError());
+  MBD_CUDA(cudaMemcpyAsync(w, ev, sizeof(double) * n, cudaMemcpyDeviceToHost, s));
+  MBD_CUDA(cudaMemcpy2DAsync(Z, sizeof(double) * ldz, X, sizeof(double) * ldp, sizeof(double) * n, n,
+                             cudaMemcpyDeviceToHost, s));
+  MBD_CUDA(cudaStreamSynchronize(s));
+  return MBD_OK;
+}
+
 int mbd_rsscs_element_z(const char* symbol) { return element_z(symbol); }
 
 int mbd_rsscs_frequency_grid(double* omega, double* weight, int n) {

@@ -150,6 +150,7 @@ struct mbd_ctx {
   mbd::HostBuf staging;   // download: every geometry's results in one pass
   // standalone eigenvalue call: matrix, (d, e, eigenvalues, scratch), workspace
   mbd::DevBuf eig_a, eig_vec, eig_ws;
+  mbd::DevBuf eigh_buf;   // mbd_rsscs_eigh: matrix, reflectors, vectors, Gram, scratch
   // batch plan (device tables in `tables`)
   mbd::TridiagJob* trd_jobs = nullptr;
   mbd::TridiagGroup* trd_groups = nullptr;

@@ -399,6 +399,7 @@ __device__ bool tridiag_one(const TridiagJob& job, const GroupWS& w, int g, int 
         }
         sm.rf = rfl;
         if (g == 0) job.e[c] = rfl.beta;
+        if (g == 0 && job.tau) job.tau[c] = rfl.tau;
       }
     }
     __syncthreads();
@@ -586,6 +587,7 @@ __device__ bool tridiag_one(const TridiagJob& job, const GroupWS& w, int g, int 
         const double wr = (rf.tau != 0.0) ? rf.tau * (y - corr) + alpha2 * vr : 0.0;
         w.W[j * nm + r] = wr;
         w.V[j * nm + r] = vr;
+        if (job.vsave) job.vsave[(size_t)c * job.ldv + r] = vr;
         if (!panel_end) {
           const double x = arc - (upd + vr * sm.wc[j] + wr * sm.vc[j]);
           A[(size_t)r * ld + c1] = x;
@@ -621,6 +623,7 @@ __device__ bool tridiag_one(const TridiagJob& job, const GroupWS& w, int g, int 
         const double wr = (rf.tau != 0.0) ? rf.tau * (y2 - corr) + alpha2 * vr : 0.0;
         w.W[j * nm + r2] = wr;
         w.V[j * nm + r2] = vr;
+        if (job.vsave) job.vsave[(size_t)c * job.ldv + r2] = vr;
         if (!panel_end) {
           const double x = ldg_cg(A + (size_t)r2 * ld + c1) - (upd + vr * sm.wc[j] + wr * sm.vc[j]);
           A[(size_t)r2 * ld + c1] = x;

@@ -110,6 +110,12 @@ struct TridiagJob {
   int n, ld;
   double* d;               // [n]
   double* e;               // [n-1]
+  // optional (eigenvectors): reflector c = 0..n-2, H_c = I - tau[c] v v^T with
+  // v(r) at vsave[c * ldv + r] for r >= c + 1 (v(c + 1) = 1); rows r <= c of
+  // each reflector are left as the caller set them (zero)
+  double* vsave = nullptr;
+  double* tau = nullptr;
+  size_t ldv = 0;
 };
 constexpr int kTrdTile = 64;
 constexpr int kTrdNB = 32;
@@ -143,6 +149,23 @@ void launch_tridiag_eigenvalues(const double* d, const double* e, int n, double*
 void launch_tridiag_eigenvalues_scratch(const double* d, const double* e, int n, double* ev, double* e2,
                                         cudaStream_t s);
 cudaError_t init_eigval_attributes();
+// ---- eigenvectors (k_eigvec.cu) ----
+// C (M x N, row-major) = alpha op(A) op(B) + beta C on FP64 MMA; op(A)(i, k) =
+// ta ? A[k * lda + i] : A[i * lda + k], op(B)(k, j) = tb ? B[j * ldb + k] :
+// B[k * ldb + j]; beta == 0 does not read C.
+void dgemm_rm(bool ta, bool tb, int M, int N, int K, double alpha, const double* A, size_t lda, const double* B,
+              size_t ldb, double beta, double* C, size_t ldc, cudaStream_t s);
+// doubles of the scratch launch_tri_vectors needs
+size_t eigh_scratch_doubles(int n);
+// Eigenvectors of the tridiagonal (d, e) for its ascending eigenvalues ev into
+// the columns of Z (row-major, Z[i * ldz + k] = component i of vector k);
+// tnorm = max |ev| sets the cluster tolerance and the pivot floor.
+void launch_tri_vectors(const double* d, const double* e, const double* ev, int n, double tnorm, double* Z, size_t ldz,
+                        double* scratch, cudaStream_t s);
+// G (n x n) <- 3/2 I - G/2, *dev = max |G - I| as bits (atomic max; zero it first)
+void launch_ns_prepare(double* G, int n, unsigned long long* dev, cudaStream_t s);
+// T (nb x nb row-major upper) of I - V T V^T = H_0 ... H_{kb-1} from S = V^T V (ld nb)
+void launch_wy_t(const double* S, const double* tau, int kb, int nb, double* T, cudaStream_t s);
 // energy = 0.5*sum_{ev>=0} sqrt(ev)/nsl - 0.5*sum_nonint; out[0]=E, out[1]=sum sqrt, out[2]=nimag
 void launch_energy(const double* ev, int n, int nsl, const double* scalars, double* out,
                    cudaStream_t s);

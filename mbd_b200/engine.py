@@ -36,7 +36,7 @@ EXPORTED = [
     "mbd_rsscs_create", "mbd_rsscs_destroy", "mbd_rsscs_energy", "mbd_rsscs_energy_batch",
     "mbd_rsscs_upload", "mbd_rsscs_compute", "mbd_rsscs_download", "mbd_rsscs_element_z",
     "mbd_rsscs_strerror", "mbd_rsscs_vdw_params", "mbd_rsscs_last_timings", "mbd_rsscs_last_stats",
-    "mbd_rsscs_stream", "mbd_rsscs_eigvalsh", "mbd_rsscs_eigvalsh_noalloc",
+    "mbd_rsscs_stream", "mbd_rsscs_eigvalsh", "mbd_rsscs_eigvalsh_noalloc", "mbd_rsscs_eigh",
     "mbd_rsscs_learned_param_count", "mbd_rsscs_learned_train", "mbd_rsscs_learned_get_params",
     "mbd_rsscs_learned_set_params", "mbd_rsscs_learned_use_network", "mbd_rsscs_learned_eval",
     "mbd_rsscs_set_option", "mbd_rsscs_get_option", "mbd_rsscs_autotune", "mbd_rsscs_tuning",
@@ -161,6 +161,9 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
     lib.mbd_rsscs_eigvalsh.argtypes = [vp, ctypes.POINTER(ctypes.c_double), ctypes.c_int, ctypes.c_int,
                                        ctypes.POINTER(ctypes.c_double)]
     lib.mbd_rsscs_eigvalsh.restype = ctypes.c_int
+    lib.mbd_rsscs_eigh.argtypes = [vp, ctypes.POINTER(ctypes.c_double), ctypes.c_int, ctypes.c_int,
+                                   ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double), ctypes.c_int]
+    lib.mbd_rsscs_eigh.restype = ctypes.c_int
     fp = ctypes.POINTER(ctypes.c_float)
     ip = ctypes.POINTER(ctypes.c_int)
     dp = ctypes.POINTER(ctypes.c_double)
@@ -342,6 +345,21 @@ class Engine:
         if code != MBD_OK:
             raise MbdError(code, strerror(code))
         return w
+
+    def eigh(self, H: np.ndarray):
+        """(w, Z): eigenvalues ascending and orthonormal eigenvectors as the
+        columns of Z, H @ Z[:, k] = w[k] Z[:, k] (numpy.linalg.eigh's layout);
+        only the lower triangle of H is read (mbd_rsscs_eigh)."""
+        H = np.ascontiguousarray(H, dtype=np.float64)
+        n = H.shape[0]
+        w = np.zeros(n)
+        Z = np.zeros((n, n))
+        dp = ctypes.POINTER(ctypes.c_double)
+        code = self.lib.mbd_rsscs_eigh(self.ctx, H.ctypes.data_as(dp), n, H.shape[1], w.ctypes.data_as(dp),
+                                       Z.ctypes.data_as(dp), n)
+        if code != MBD_OK:
+            raise MbdError(code, strerror(code))
+        return w, Z
 
     # -- learned warm start (MBD_MODE_MIXED_LEARNED) --------------------------
     def learned_train(self, geos, sts, epochs: int = 20, lr: float = 2e-3, seed: int = 0) -> np.ndarray:
