@@ -1299,7 +1299,10 @@ int mbd_rsscs_eigh(mbd_ctx* ctx, const double* H, int n, int ld, double* w, doub
   const double tnorm = std::max(std::fabs(ends[0]), std::fabs(ends[1]));
   // the tridiagonal's eigenvectors, then Newton-Schulz to orthonormality
   launch_tri_vectors(d, e, ev, n, tnorm, X, ldp, scratch, s);
+  // a step maps a deviation dv of X^T X from I to about 3/4 dv^2: after one
+  // from dv <= ns_one the product is not formed again to check it
   const double ns_tol = 1e-15 * std::max(10.0, 4.0 * std::sqrt((double)n));
+  const double ns_one = std::sqrt(ns_tol);
   for (int step = 0; step < 4; ++step) {
     dgemm_rm(true, false, n, n, n, 1.0, X, ldp, X, ldp, 0.0, Gm, n, s);   // X^T X
     MBD_CUDA(cudaMemsetAsync(dev, 0, sizeof(unsigned long long), s));
@@ -1312,6 +1315,7 @@ int mbd_rsscs_eigh(mbd_ctx* ctx, const double* H, int n, int ld, double* w, doub
     if (!(dv > ns_tol)) break;
     dgemm_rm(false, false, n, n, n, 1.0, X, ldp, Gm, n, 0.0, X2, ldp, s);   // X (3I - X^T X) / 2
     std::swap(X, X2);
+    if (dv <= ns_one) break;
   }
   // X <- Q X: blocks of reflectors c0 .. c0 + kb - 1 (rows c0 + 1 .. n - 1),
   // the last block first; V^T of a block is row-major (kb x m) at
