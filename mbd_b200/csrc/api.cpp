@@ -353,7 +353,7 @@ int band_to_tridiag_single(mbd_ctx* ctx, double* Br, int n, double* d, double* e
   for (int i = 0; i + 3 <= n; ++i) items.push_back(SweepItem{0, i, i - 1, 0});
   const BandJob job{Br, n, d, e};
   const size_t b_job = bytes_of<BandJob>(1), b_it = bytes_of<SweepItem>(std::max<size_t>(items.size(), 1));
-  const size_t b_pr = bytes_of<int>(std::max<size_t>(items.size(), 1));
+  const size_t b_pr = bytes_of<int>(2 * std::max<size_t>(items.size(), 1));
   MBD_CUDA(scratch.reserve(b_job + b_it + b_pr));
   char* base = scratch.as<char>();
   std::vector<char> host(b_job + b_it, 0);
@@ -703,7 +703,7 @@ int prepare_batch(mbd_ctx* ctx, bool eigen) {
   ctx->sweeps_in_flight = 0;
   for (const BandJob& bj : fjobs) ctx->sweeps_in_flight += bj.n / (2 * kBand) + 1;
   ctx->n_sweep_items = (int)items.size();
-  MBD_CUDA(ctx->sweep_progress.reserve(sizeof(int) * std::max<size_t>(items.size(), 1)));
+  MBD_CUDA(ctx->sweep_progress.reserve(2 * sizeof(int) * std::max<size_t>(items.size(), 1)));
   const size_t b_jobs = bytes_of<TridiagJob>(jobs.size());
   const size_t b_groups = bytes_of<TridiagGroup>(groups.size());
   const size_t b_eig = bytes_of<EigJob>(eig.size());

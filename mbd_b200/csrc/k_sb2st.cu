@@ -11,9 +11,20 @@
 //   O   <- O H                (O = A[r_k + kBand .. + kBand, r_k .. + kBand))
 //   H'  from O[:, 0];  O <- H' O;  carry H' to task k + 1.
 // Task (i, k) touches columns [r_k, r_k + kBand) and must follow task
-// (i-1, k+1), the last task of the previous sweep that touches one of them:
-// each sweep's warp publishes its completed task count, the next sweep's
-// warp waits (bounded) until it reaches k + 2.
+// (i-1, k+1), the last task of the previous sweep that touches one of them.
+// Of that task it needs only the diagonal block (its D(0,0) is the last
+// diagonal entry of (i, k)'s D block, its column 0 the last column of
+// (i, k)'s O block) and the corner O(0,0) of its O block (the last entry of
+// (i, k)'s O block): every other entry the two tasks touch is disjoint.  So
+// each sweep publishes two counts: one when its D-warp has stored a task's D
+// block, one as soon as its O-warp has the next reflector's beta and has
+// stored it as O(0,0) (the rest of the O block, which (i, k) does not touch,
+// is stored later).  The two counts share one 64-bit word per sweep item
+// (D-warp count in the low half, O-warp count in the high half, each
+// advanced by a release add), so the next sweep's O-warp polls a single word
+// (bounded) until both halves reach k + 2; its D-warp follows through the
+// pair barrier.  Earlier tasks of sweep i-1 are complete by then: task k + 1
+// started after the pair barrier that closed task k.
 //
 // Work items are (matrix, sweep) pairs ordered by sweep, then matrix; warp w
 // takes items w, w + W, ...  Every wait points to an item of lower index, so
@@ -59,21 +70,27 @@ __device__ __forceinline__ double warp_sum(double x) {
   return x;
 }
 
-__device__ __forceinline__ int ld_acquire(const int* p) {
-  int v;
-  asm volatile("ld.acquire.gpu.b32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+__device__ __forceinline__ unsigned long long ld_acquire(const unsigned long long* p) {
+  unsigned long long v;
+  asm volatile("ld.acquire.gpu.b64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
   return v;
 }
 
-__device__ __forceinline__ void st_release(int* p, int v) {
-  asm volatile("st.release.gpu.b32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+// one published count (low half: D-warp, high half: O-warp)
+__device__ __forceinline__ void add_release(unsigned long long* p, unsigned long long v) {
+  asm volatile("red.release.gpu.global.add.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
+}
+constexpr unsigned long long kCountD = 1ull, kCountO = 1ull << 32;
+
+__device__ __forceinline__ int both_counts(unsigned long long v) {
+  return min((int)(unsigned)(v & 0xffffffffull), (int)(unsigned)(v >> 32));
 }
 
-// Lane 0 spins (bounded) with acquire loads until *p >= target; the warp
-// barrier after it orders every lane's later reads behind that acquire (a
-// second acquire load by every lane would add an L2 round trip to each link
-// of the sweep-to-sweep chain).
-__device__ bool wait_progress(const int* p, int target, int* err) {
+// Lane 0 spins (bounded) with acquire loads until both counts of *p reach
+// target; the warp barrier after it orders every lane's later reads behind
+// that acquire (a second acquire load by every lane would add an L2 round
+// trip to each link of the sweep-to-sweep chain).
+__device__ bool wait_progress(const unsigned long long* p, int target, int* err) {
   int ok = 1;
   if ((threadIdx.x & 31) == 0) {
     // tight polling first (the predecessor is usually one task away), then
@@ -83,7 +100,7 @@ __device__ bool wait_progress(const int* p, int target, int* err) {
     const long long lim = wait_limit_cycles();
     const long long t0 = clock64();
     unsigned ns = 0, polls = 0;
-    while (ld_acquire(p) < target) {
+    while (both_counts(ld_acquire(p)) < target) {
       if ((++polls & 63u) == 0) {
         if (*(volatile int*)err != 0 || clock64() - t0 > lim) {
           atomicCAS(err, 0, MBD_ERR_TIMEOUT);
@@ -124,7 +141,7 @@ __device__ __forceinline__ double make_reflector(double x, int len, double* v, d
 // next reflector, left apply); they meet at a named barrier once per task.
 constexpr int PAIRS = WARPS / 2;
 __global__ void __launch_bounds__(WARPS * 32) sb2st_kernel(const BandJob* jobs, const SweepItem* items,
-                                                           int n_items, int* progress, int* err,
+                                                           int n_items, unsigned long long* progress, int* err,
                                                            int stall_item) {
   __shared__ PairSmem psm[PAIRS];
   const int warp = threadIdx.x / 32, l = threadIdx.x & 31;
@@ -205,6 +222,9 @@ __global__ void __launch_bounds__(WARPS * 32) sb2st_kernel(const BandJob* jobs, 
           for (int i = 0; i < B; ++i)
             if (i < L && l <= i) rowsW[(size_t)i * LD] = S.Ds[i][l];
         }
+        // the warp barrier orders every lane's stores before lane 0's release
+        __syncwarp();
+        if (l == 0) add_release(progress + t, kCountD);
       } else {
         // ---- O <- O H;  next reflector from O[:, 0];  O <- H' O
         // band row rn + q holds O(q, j) at diagonal B + q - j: lane l reads j = B - 1 - l
@@ -228,6 +248,12 @@ __global__ void __launch_bounds__(WARPS * 32) sb2st_kernel(const BandJob* jobs, 
         double v2 = 0.0, tau2 = 0.0, beta2 = 0.0;
         if (Ln > 0) {
           tau2 = make_reflector(orow[0], Ln, &v2, &beta2);
+          // O(0,0) is final now (beta2; the entry itself when there is no
+          // reflection): store it and publish it for the next sweep
+          if (l == 0) {
+            Br[(size_t)rn * LD + B] = beta2;
+            add_release(progress + t, kCountO);
+          }
           if (tau2 != 0.0) {
 #pragma unroll
             for (int j = 0; j < B; ++j) S.Ot[l][j] = orow[j];
@@ -249,23 +275,22 @@ __global__ void __launch_bounds__(WARPS * 32) sb2st_kernel(const BandJob* jobs, 
           __syncwarp();
           double* rowsOW = Br + (size_t)rn * LD + 1 + l;
 #pragma unroll
-          for (int q = 0; q < B; ++q)
-            if (q < Ln && jin) rowsOW[(size_t)q * (LD + 1)] = S.Ot[q][B - 1 - l];
+          for (int q = 0; q < B; ++q)   // O(0,0) (q = 0, lane B - 1) is stored already
+            if (q < Ln && jin && (q > 0 || l != B - 1)) rowsOW[(size_t)q * (LD + 1)] = S.Ot[q][B - 1 - l];
+        } else if (l == 0) {
+          add_release(progress + t, kCountO);   // no O block
         }
         S.v[(k + 1) & 1][l] = v2;
         tau = tau2;
         vl = v2;
       }
-      // both warps' stores are ordered before the barrier; one lane then
-      // publishes the task with a release store at GPU scope, which is
-      // cumulative over the writes the barrier ordered before it (no
-      // separate fence: a __threadfence() before it cost ~7 % of the launch)
-      // (the next task's first barrier orders S.w[1] before the D-warp reads it)
+      // Publication is a release store at GPU scope by one lane, cumulative
+      // over the writes a barrier ordered before it (no separate fence: a
+      // __threadfence() cost ~7 % of the launch).  The barrier below closes
+      // the task for the pair (the next task's first barrier orders S.w[1]
+      // before the D-warp reads it).
       pair_sync(pair);
-      if (owarp && l == 0) {
-        S.w[1] = tau;   // the next task's tau for the D-warp
-        st_release(progress + t, k + 1);
-      }
+      if (owarp && l == 0) S.w[1] = tau;   // the next task's tau for the D-warp
     }
   }
 }
@@ -295,7 +320,7 @@ cudaError_t launch_sb2st(const BandJob* jobs, int n_jobs, const SweepItem* items
                          cudaStream_t s) {
   if (n_jobs < 1) return cudaSuccess;
   if (n_items > 0) {
-    cudaError_t e = cudaMemsetAsync(progress, 0, sizeof(int) * (size_t)n_items, s);
+    cudaError_t e = cudaMemsetAsync(progress, 0, 2 * sizeof(int) * (size_t)n_items, s);
     if (e != cudaSuccess) return e;
     // workers: about three times the sweeps that can be in flight at once (a
     // matrix keeps about n / (2 kBand) sweeps busy), within co-residency
@@ -303,7 +328,8 @@ cudaError_t launch_sb2st(const BandJob* jobs, int n_jobs, const SweepItem* items
     const long long want_pairs = 3LL * sweeps_in_flight + 4 * PAIRS;
     const int need = (int)((std::min<long long>(want_pairs, n_items) + PAIRS - 1) / PAIRS);
     if (grid > need) grid = need;
-    void* args[] = {(void*)&jobs, (void*)&items, (void*)&n_items, (void*)&progress, (void*)&err, (void*)&stall_item};
+    unsigned long long* prog64 = reinterpret_cast<unsigned long long*>(progress);
+    void* args[] = {(void*)&jobs, (void*)&items, (void*)&n_items, (void*)&prog64, (void*)&err, (void*)&stall_item};
     e = cudaLaunchCooperativeKernel((const void*)sb2st_kernel, dim3(grid), dim3(WARPS * 32), args, 0, s);
     if (e != cudaSuccess) return e;
   }

@@ -219,6 +219,7 @@ struct SweepItem {
 // sweep pipeline offers (sizes the worker count).
 // stall_item >= 0 makes that item's first wait target a count no sweep
 // reaches, so the bounded wait runs out (failure-detection tests only).
+// progress: 2 * n_items ints (two published task counts per sweep item).
 cudaError_t launch_sb2st(const BandJob* jobs, int n_jobs, const SweepItem* items, int n_items, int* progress,
                          int* err, int num_sms, int max_n, long long sweeps_in_flight, int stall_item,
                          cudaStream_t s);

@@ -128,7 +128,7 @@ int autotune(mbd_ctx* ctx, int max_n) {
     Buf band0, items_d, prog;
     if (status != MBD_OK || fail(cudaMalloc(&band0.p, band_bytes)) ||
         fail(cudaMalloc(&items_d.p, sizeof(SweepItem) * std::max<size_t>(1, items.size()))) ||
-        fail(cudaMalloc(&prog.p, sizeof(int) * std::max<size_t>(1, items.size()))) ||
+        fail(cudaMalloc(&prog.p, 2 * sizeof(int) * std::max<size_t>(1, items.size()))) ||
         fail(cudaMemcpyAsync(band0.p, band.p, band_bytes, cudaMemcpyDeviceToDevice, s)) ||
         fail(cudaMemcpyAsync(items_d.p, items.data(), sizeof(SweepItem) * items.size(), cudaMemcpyHostToDevice, s)) ||
         fail(cudaMemcpyAsync(job.p, &bj, sizeof(bj), cudaMemcpyHostToDevice, s)) || fail(cudaStreamSynchronize(s)))
