@@ -451,7 +451,8 @@ int run_front(mbd_ctx* ctx, GeomDev* gd, int gi, int mode, bool relay_only) {
   // 6. dense -> band (stage 1 of the two-stage tridiagonalisation)
   if (two_stage(ctx, p.nH)) {
     MBD_CUDA(launch_sy2sb(gd->hmat.as<double>(), p.ldH, p.nH, sl.trd_ws.as<double>(), gd->band.as<double>(),
-                          ctx->num_sms, s, tuned_rows(ctx, p.nH), tuned_panel_qr(ctx, p.nH)));
+                          ctx->num_sms, s, tuned_rows(ctx, p.nH), tuned_panel_qr(ctx, p.nH),
+                          lookahead_for(ctx, sl.la)));
     ctx->launches += sy2sb_launches(p.nH);
   }
   mark(6);
@@ -533,6 +534,7 @@ int plan_slots(mbd_ctx* ctx) {
     std::unique_ptr<RelaySlot> sl(new RelaySlot());
     MBD_CUDA(cudaStreamCreateWithFlags(&sl->stream, cudaStreamNonBlocking));
     MBD_CUDA(cudaEventCreateWithFlags(&sl->done, cudaEventDisableTiming));
+    MBD_CUDA(create_lookahead(&sl->la));
     ctx->slots.push_back(std::move(sl));
   }
   ctx->n_slots = S;
@@ -876,6 +878,7 @@ int mbd_rsscs_create(mbd_ctx** out, int device) {
   MBD_CUDA(cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking));
   for (auto& e : ctx->bev) MBD_CUDA(cudaEventCreate(&e));
   MBD_CUDA(cudaEventCreateWithFlags(&ctx->fork_ev, cudaEventDisableTiming));
+  MBD_CUDA(create_lookahead(&ctx->la_ctx));
   {
     const char* ng = std::getenv("MBD_B200_NO_GRAPHS");
     ctx->use_graphs = !(ng && ng[0] && ng[0] != '0');
@@ -896,6 +899,10 @@ int mbd_rsscs_create(mbd_ctx** out, int device) {
       for (TuneChoice& t : ctx->tune) t.chase_c = 0;
     const char* pq = std::getenv("MBD_B200_PANEL_QR");
     ctx->panel_qr_default = (pq && std::strcmp(pq, "tsqr") == 0) ? 1 : 0;
+    // the dense -> band reduction's look-ahead: each panel's QR beside the
+    // previous panel's trailing update (MBD_B200_LOOKAHEAD=0: one stream)
+    const char* la = std::getenv("MBD_B200_LOOKAHEAD");
+    ctx->lookahead = !(la && la[0] == '0');
   }
   MBD_CUDA(init_device_constants());
   MBD_CUDA(init_chol_attributes());
@@ -935,6 +942,9 @@ void mbd_rsscs_destroy(mbd_ctx* ctx) {
   for (auto e : ctx->bev)
     if (e) cudaEventDestroy(e);
   if (ctx->fork_ev) cudaEventDestroy(ctx->fork_ev);
+  if (ctx->la_ctx.ready) cudaEventDestroy(ctx->la_ctx.ready);
+  if (ctx->la_ctx.done) cudaEventDestroy(ctx->la_ctx.done);
+  if (ctx->la_ctx.aux) cudaStreamDestroy(ctx->la_ctx.aux);
   ctx->geoms.clear();
   ctx->slots.clear();
   if (ctx->stream) cudaStreamDestroy(ctx->stream);
@@ -1209,7 +1219,8 @@ int mbd_rsscs_eigvalsh(mbd_ctx* ctx, const double* H, int n, int ld, double* w) 
     MBD_CUDA(ctx->eig_ws.reserve(sizeof(double) * (wsd + (size_t)n * kBandLd)));
     double* ws = ctx->eig_ws.as<double>();
     double* band = ws + wsd;
-    MBD_CUDA(launch_sy2sb(A, ldp, n, ws, band, ctx->num_sms, s, tuned_rows(ctx, n), tuned_panel_qr(ctx, n)));
+    MBD_CUDA(launch_sy2sb(A, ldp, n, ws, band, ctx->num_sms, s, tuned_rows(ctx, n), tuned_panel_qr(ctx, n),
+                          lookahead_for(ctx, ctx->la_ctx)));
     int st = band_to_tridiag_single(ctx, band, n, d, e, ctx->fb_ws, s);
     if (st != MBD_OK) return st;
   } else {

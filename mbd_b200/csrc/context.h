@@ -98,6 +98,7 @@ struct GeomDev {
 struct RelaySlot {
   cudaStream_t stream = nullptr;
   cudaEvent_t done = nullptr;
+  Sy2sbLookAhead la{};   // the dense -> band look-ahead's stream and events
   DevBuf relay64, linv, rhs;                                  // plain FP64 path
   DevBuf relay32, p_hi, p_lo, l_hi, l_lo, mixv, res_ws, solve_sync;   // mixed path
   DevBuf cg, gnn;                                             // learned path: CG vectors, network work
@@ -105,6 +106,9 @@ struct RelaySlot {
   int solve_epoch = 0;
   ~RelaySlot() {
     if (done) cudaEventDestroy(done);
+    if (la.ready) cudaEventDestroy(la.ready);
+    if (la.done) cudaEventDestroy(la.done);
+    if (la.aux) cudaStreamDestroy(la.aux);
     if (stream) cudaStreamDestroy(stream);
   }
   size_t held() const {
@@ -148,6 +152,8 @@ struct mbd_ctx {
   int n_slots = 0;                           // slots in use for the current batch
   mbd::DevBuf tridiag_ws, tables, misc, fb_ws;
   mbd::HostBuf staging;   // download: every geometry's results in one pass
+  mbd::Sy2sbLookAhead la_ctx{};   // look-ahead stream and events of the context-stream reductions
+  bool lookahead = true;     // dense -> band look-ahead (MBD_B200_LOOKAHEAD=0: off)
   // standalone eigenvalue call: matrix, (d, e, eigenvalues, scratch), workspace
   mbd::DevBuf eig_a, eig_vec, eig_ws;
   mbd::DevBuf eigh_buf;   // mbd_rsscs_eigh: matrix, reflectors, vectors, Gram, scratch
@@ -246,6 +252,21 @@ inline cudaError_t h2d_ordered(const mbd_ctx* ctx, void* dst, const void* src, s
 inline cudaError_t zero_ordered(const mbd_ctx* ctx, void* dst, size_t bytes) {
   cudaError_t e = cudaMemsetAsync(dst, 0, bytes, ctx->stream);
   return e != cudaSuccess ? e : cudaStreamSynchronize(ctx->stream);
+}
+
+// Look-ahead streams: an auxiliary stream at the device's highest priority
+// and its two events.
+inline cudaError_t create_lookahead(Sy2sbLookAhead* la) {
+  int least = 0, greatest = 0;
+  cudaError_t e = cudaDeviceGetStreamPriorityRange(&least, &greatest);
+  if (e == cudaSuccess) e = cudaStreamCreateWithPriority(&la->aux, cudaStreamNonBlocking, greatest);
+  if (e == cudaSuccess) e = cudaEventCreateWithFlags(&la->ready, cudaEventDisableTiming);
+  if (e == cudaSuccess) e = cudaEventCreateWithFlags(&la->done, cudaEventDisableTiming);
+  la->priority = greatest;
+  return e;
+}
+inline const Sy2sbLookAhead* lookahead_for(const mbd_ctx* ctx, const Sy2sbLookAhead& la) {
+  return ctx->lookahead && la.aux ? &la : nullptr;
 }
 
 // tune.cu

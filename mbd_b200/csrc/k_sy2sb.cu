@@ -754,16 +754,28 @@ __global__ void __launch_bounds__(256) zform_kernel(const double* Y, const doubl
 // together (cp.async), the products are subtracted there and the tile goes
 // back a row per warp instruction (coalesced).
 constexpr size_t kSyr2kSmem = sizeof(double) * 3 * TL * FS;
+// part: 0 every lower tile (one CTA each, triangular order), 1 the tiles of
+// tile column 0 (the next panel's columns), 2 the lower tiles right of it.
 __global__ void __launch_bounds__(128) syr2k_kernel(double* A, int ld, int row0, int m, const double* V,
-                                                    const double* Z) {
+                                                    const double* Z, int part) {
   extern __shared__ __align__(16) double dsm[];
   double* Li = dsm;                // [64][FS]: [V_I | Z_I]
   double* Lj = dsm + TL * FS;      // [64][FS]: [Z_J | V_J]
   double* Cs = dsm + 2 * TL * FS;  // [64][FS]: the A22 tile (I, J)
-  int ti = (int)((sqrt(8.0 * blockIdx.x + 1.0) - 1.0) * 0.5);
-  while ((ti + 1) * (ti + 2) / 2 <= (int)blockIdx.x) ++ti;
-  while (ti * (ti + 1) / 2 > (int)blockIdx.x) --ti;
-  const int tj = (int)blockIdx.x - ti * (ti + 1) / 2;
+  int ti, tj;
+  if (part == 1) {
+    ti = (int)blockIdx.x;
+    tj = 0;
+  } else {
+    ti = (int)((sqrt(8.0 * blockIdx.x + 1.0) - 1.0) * 0.5);
+    while ((ti + 1) * (ti + 2) / 2 <= (int)blockIdx.x) ++ti;
+    while (ti * (ti + 1) / 2 > (int)blockIdx.x) --ti;
+    tj = (int)blockIdx.x - ti * (ti + 1) / 2;
+    if (part == 2) {
+      ++ti;
+      ++tj;
+    }
+  }
   const int tid = threadIdx.x, warp = tid / 32, lane = tid % 32;
   const int g = lane >> 2, q4 = lane & 3;
   double* A22 = A + (size_t)row0 * ld + row0;
@@ -896,11 +908,11 @@ int sy2sb_max_n() {
 size_t sy2sb_workspace_doubles(int n) {
   const int m = n;
   const int nt = (m + TL - 1) / TL;
-  return (size_t)m * B * (3 + kSymmMaxSplit) + (size_t)nt * B * B + 3 * B * B + B + 256;
+  return (size_t)m * B * (4 + kSymmMaxSplit) + (size_t)nt * B * B + 3 * B * B + B + 256;
 }
 
 cudaError_t launch_sy2sb(double* A, int ld, int n, double* ws, double* Br, int num_sms, cudaStream_t s,
-                         int rows_per_cta, int panel_qr) {
+                         int rows_per_cta, int panel_qr, const Sy2sbLookAhead* la) {
   const int max_cluster = sy2sb_max_cluster();
   // panel rows per CTA the cluster size aims at: the caller's (autotuned)
   // choice, else MBD_B200_PANEL_ROWS, else the default
@@ -911,17 +923,19 @@ cudaError_t launch_sy2sb(double* A, int ld, int n, double* ws, double* Br, int n
   }();
   const int rows_target = (rows_per_cta >= 32 && rows_per_cta <= kPanelMaxRowsPerCta) ? rows_per_cta : rows_env;
   const int nt_full = (n + TL - 1) / TL;
-  double* V = ws;
-  double* Y = V + (size_t)n * B;
+  double* Vb[2];
+  Vb[0] = ws;
+  double* Y = Vb[0] + (size_t)n * B;
   double* Z = Y + (size_t)n * B;
   double* Yp = Z + (size_t)n * B;
   double* Up = Yp + (size_t)n * B * kSymmMaxSplit;
   double* T = Up + (size_t)nt_full * B * B;
   double* M = T + B * B;
   double* tau = M + B * B;
-  for (int c0 = 0; c0 + B + 1 < n; c0 += B) {
+  Vb[1] = tau + B + 64;   // the next panel's reflectors while this panel's are in use
+  // panel QR of the columns c0 .. c0 + B - 1 in one cluster (a power of two of CTAs)
+  auto panel_qr_launch = [&](int c0, double* V, cudaStream_t st, bool urgent) -> cudaError_t {
     const int row0 = c0 + B, m = n - row0;
-    // panel QR in one cluster (a power of two of CTAs)
     int C = 1;
     while (C * rows_target < m && C < max_cluster) C *= 2;
     while (C * kPanelMaxRowsPerCta < m) C *= 2;
@@ -930,26 +944,36 @@ cudaError_t launch_sy2sb(double* A, int ld, int n, double* ws, double* Br, int n
     PanelArgs pa{A, ld, row0, c0, m, R, V, T, tau};
     if (panel_qr == 1 && C >= 2 && R >= B && R <= tsqr_max_rows_per_cta()) {
       // TSQR with Householder reconstruction: three cluster exchanges per panel
-      cudaError_t e = launch_tsqr_panel(pa, C, s);
-      if (e != cudaSuccess) return e;
-    } else {
+      return launch_tsqr_panel(pa, C, st);
+    }
     const int qv = qr_variant(R);
     if (qv < 0) return cudaErrorInvalidValue;
     cudaLaunchConfig_t cfg{};
     cfg.gridDim = dim3(C);
     cfg.blockDim = dim3(kQrWarps[qv] * 32);
     cfg.dynamicSmemBytes = qr_smem_bytes(qv, R);
-    cfg.stream = s;
-    cudaLaunchAttribute attr[1];
+    cfg.stream = st;
+    cudaLaunchAttribute attr[2];
     attr[0].id = cudaLaunchAttributeClusterDimension;
     attr[0].val.clusterDim.x = C;
     attr[0].val.clusterDim.y = 1;
     attr[0].val.clusterDim.z = 1;
+    attr[1].id = cudaLaunchAttributePriority;
+    attr[1].val.priority = urgent && la ? la->priority : 0;
     cfg.attrs = attr;
-    cfg.numAttrs = 1;
-    cudaError_t e = cudaLaunchKernelEx(&cfg, qr_kernel(qv), pa);
-    if (e != cudaSuccess) return e;
+    cfg.numAttrs = urgent && la ? 2 : 1;
+    return cudaLaunchKernelEx(&cfg, qr_kernel(qv), pa);
+  };
+  bool qr_done = false;   // this panel's QR was launched by the previous panel (look-ahead)
+  int p = 0;
+  for (int c0 = 0; c0 + B + 1 < n; c0 += B, ++p) {
+    const int row0 = c0 + B, m = n - row0;
+    double* V = Vb[p & 1];
+    if (!qr_done) {
+      cudaError_t e = panel_qr_launch(c0, V, s, false);
+      if (e != cudaSuccess) return e;
     }
+    qr_done = false;
     // two-sided update of the trailing block
     const int nt = (m + TL - 1) / TL;
     int S = (2 * num_sms + nt - 1) / nt;   // one wave at two CTAs per SM
@@ -961,7 +985,23 @@ cudaError_t launch_sy2sb(double* A, int ld, int n, double* ws, double* Br, int n
     yred_kernel<<<nt, 256, 0, s>>>(Yp, S, m, T, V, Y, Up);
     mform_kernel<<<1, B * B, 0, s>>>(Up, nt, T, M);
     zform_kernel<<<nt, 256, 0, s>>>(Y, V, M, m, Z);
-    syr2k_kernel<<<nt * (nt + 1) / 2, 128, kSyr2kSmem, s>>>(A, ld, row0, m, V, Z);
+    const int c1 = c0 + B;
+    if (la && c1 + B + 1 < n) {
+      // look-ahead: the next panel's columns (tile column 0) first, then its
+      // QR on the auxiliary stream beside the rest of the update
+      syr2k_kernel<<<nt, 128, kSyr2kSmem, s>>>(A, ld, row0, m, V, Z, 1);
+      cudaError_t e = cudaEventRecord(la->ready, s);
+      if (e == cudaSuccess) e = cudaStreamWaitEvent(la->aux, la->ready, 0);
+      if (e == cudaSuccess) e = panel_qr_launch(c1, Vb[(p + 1) & 1], la->aux, true);
+      if (e == cudaSuccess) e = cudaEventRecord(la->done, la->aux);
+      if (e != cudaSuccess) return e;
+      if (nt > 1) syr2k_kernel<<<nt * (nt - 1) / 2, 128, kSyr2kSmem, s>>>(A, ld, row0, m, V, Z, 2);
+      e = cudaStreamWaitEvent(s, la->done, 0);
+      if (e != cudaSuccess) return e;
+      qr_done = true;
+    } else {
+      syr2k_kernel<<<nt * (nt + 1) / 2, 128, kSyr2kSmem, s>>>(A, ld, row0, m, V, Z, 0);
+    }
   }
   band_copy_kernel<<<(unsigned)(((long long)n * kBandLd + 255) / 256), 256, 0, s>>>(A, ld, n, Br);
   return cudaGetLastError();

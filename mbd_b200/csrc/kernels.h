@@ -195,8 +195,16 @@ size_t sy2sb_workspace_doubles(int n);
 // rows_per_cta: panel rows per CTA the QR cluster aims at (0: default);
 // panel_qr: 0 Householder QR with one cluster exchange per column,
 // 1 TSQR with Householder reconstruction (k_tsqr.cu) where it applies.
+// la (optional): look-ahead -- each panel's update first applies to the next
+// panel's columns, whose QR then runs on la->aux (at la->priority) beside the
+// rest of the update; ready/done order the two streams.
+struct Sy2sbLookAhead {
+  cudaStream_t aux;
+  cudaEvent_t ready, done;
+  int priority;
+};
 cudaError_t launch_sy2sb(double* A, int ld, int n, double* ws, double* Br, int num_sms, cudaStream_t s,
-                         int rows_per_cta = 0, int panel_qr = 0);
+                         int rows_per_cta = 0, int panel_qr = 0, const Sy2sbLookAhead* la = nullptr);
 // TSQR panel QR (k_tsqr.cu): rows per CTA in [32, tsqr_max_rows_per_cta()], C <= 16.
 cudaError_t init_tsqr_attributes();
 int tsqr_max_rows_per_cta();

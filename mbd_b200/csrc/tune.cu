@@ -101,7 +101,8 @@ int autotune(mbd_ctx* ctx, int max_n) {
       for (int rep = 0; rep < 2; ++rep) {
         if (fail(cudaMemcpyAsync(a.p, a0.p, mat, cudaMemcpyDeviceToDevice, s)) || fail(cudaEventRecord(e0, s)) ||
             fail(launch_sy2sb(static_cast<double*>(a.p), ld, n, static_cast<double*>(ws.p),
-                              static_cast<double*>(band.p), ctx->num_sms, s, cq[1], cq[0])) ||
+                              static_cast<double*>(band.p), ctx->num_sms, s, cq[1], cq[0],
+                              lookahead_for(ctx, ctx->la_ctx))) ||
             fail(cudaEventRecord(e1, s)) || fail(cudaEventSynchronize(e1)))
           break;
         float ms = 0.f;
