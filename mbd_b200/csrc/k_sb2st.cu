@@ -157,6 +157,11 @@ __global__ void __launch_bounds__(WARPS * 32) sb2st_kernel(const BandJob* jobs, 
     const int K = (n - i - 1 + B - 1) / B;           // tasks of sweep i
     const int Kp = (n - i + B - 1) / B;              // tasks of sweep i - 1
     double tau = 0.0, vl = 0.0;                      // current reflector (O-warp registers)
+    // D-warp: rows 0 .. B-2 of the next task's D block go into S.Ds during
+    // this task, once the D-warp has stored and published (the D-warp waits
+    // for the O-warp at the end of a task anyway); the next task then loads
+    // only its last row after its wait
+    bool have_pf = false;
     for (int k = 0; k < K; ++k) {
       // the O-warp waits for the previous sweep and decides for the pair; the
       // D-warp follows it through the barrier (one verdict, both warps leave
@@ -194,8 +199,12 @@ __global__ void __launch_bounds__(WARPS * 32) sb2st_kernel(const BandJob* jobs, 
         __syncwarp();
         // band rows r .. r + L - 1, diagonals d <= row (the lower triangle of D)
         const double* rowsD = Br + (size_t)r * LD + l;
+        if (have_pf) {
+          S.Ds[B - 1][l] = (B - 1 < L) ? __ldcg(rowsD + (size_t)(B - 1) * LD) : 0.0;
+        } else {
 #pragma unroll
-        for (int i = 0; i < B; ++i) S.Ds[i][l] = (i < L && l <= i) ? __ldcg(rowsD + (size_t)i * LD) : 0.0;
+          for (int i = 0; i < B; ++i) S.Ds[i][l] = (i < L && l <= i) ? __ldcg(rowsD + (size_t)i * LD) : 0.0;
+        }
         __syncwarp();
         double dr[B];   // dr[j] = D(l, j): Ds[l][l - j] below the diagonal, Ds[j][j - l] above
         const double* ds = &S.Ds[0][0];
@@ -225,6 +234,19 @@ __global__ void __launch_bounds__(WARPS * 32) sb2st_kernel(const BandJob* jobs, 
         // the warp barrier orders every lane's stores before lane 0's release
         __syncwarp();
         if (l == 0) add_release(progress + t, kCountD);
+        // rows 0 .. B-2 of the next task's D block: global rows [r + B,
+        // r + 2B - 1), all inside the D block of the previous sweep's task
+        // k + 1 (published: this task waited for its D count), touched by no
+        // task that runs before the next one
+        // (lane l reads and writes only column l of S.Ds here, after its last
+        // read of this task's block)
+        have_pf = k + 1 < K;
+        if (have_pf) {
+          const int L1 = min(B, n - rn);
+          const double* rows1 = Br + (size_t)rn * LD + l;
+#pragma unroll
+          for (int i = 0; i < B - 1; ++i) S.Ds[i][l] = (i < L1 && l <= i) ? __ldcg(rows1 + (size_t)i * LD) : 0.0;
+        }
       } else {
         // ---- O <- O H;  next reflector from O[:, 0];  O <- H' O
         // band row rn + q holds O(q, j) at diagonal B + q - j: lane l reads j = B - 1 - l
