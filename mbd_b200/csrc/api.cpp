@@ -532,7 +532,14 @@ int plan_slots(mbd_ctx* ctx) {
   for (int g : ctx->order) ctx->geoms[g]->slot = slot_of[g];
   while ((int)ctx->slots.size() < S) {
     std::unique_ptr<RelaySlot> sl(new RelaySlot());
-    MBD_CUDA(cudaStreamCreateWithFlags(&sl->stream, cudaStreamNonBlocking));
+    // slot 0 takes the batch's largest geometry (longest first), whose
+    // stages set the batch's length: its stream runs at the device's highest
+    // priority, so the block scheduler serves its kernels before the other
+    // slots' (MBD_B200_PRIORITY=0: all at the default priority)
+    int least = 0, greatest = 0;
+    MBD_CUDA(cudaDeviceGetStreamPriorityRange(&least, &greatest));
+    const int prio = (ctx->priorities && ctx->slots.empty()) ? greatest : least;
+    MBD_CUDA(cudaStreamCreateWithPriority(&sl->stream, cudaStreamNonBlocking, prio));
     MBD_CUDA(cudaEventCreateWithFlags(&sl->done, cudaEventDisableTiming));
     MBD_CUDA(create_lookahead(&sl->la));
     ctx->slots.push_back(std::move(sl));
@@ -843,7 +850,8 @@ bool capture_batch(mbd_ctx* ctx, int mode) {
   const cudaError_t ec = cudaStreamEndCapture(ctx->stream, &graph);
   cudaGraphExec_t exec = nullptr;
   const bool ok = st == MBD_OK && ec == cudaSuccess && graph &&
-                  cudaGraphInstantiate(&exec, graph, 0) == cudaSuccess;
+                  cudaGraphInstantiate(&exec, graph,
+                                       ctx->priorities ? cudaGraphInstantiateFlagUseNodePriority : 0) == cudaSuccess;
   if (graph) cudaGraphDestroy(graph);
   if (!ok) {
     if (exec) cudaGraphExecDestroy(exec);
@@ -903,6 +911,10 @@ int mbd_rsscs_create(mbd_ctx** out, int device) {
     // previous panel's trailing update (MBD_B200_LOOKAHEAD=0: one stream)
     const char* la = std::getenv("MBD_B200_LOOKAHEAD");
     ctx->lookahead = !(la && la[0] == '0');
+    // stream priorities (the largest geometry's slot, the look-ahead QR),
+    // kept by captured graphs (MBD_B200_PRIORITY=0: default priority everywhere)
+    const char* pr = std::getenv("MBD_B200_PRIORITY");
+    ctx->priorities = !(pr && pr[0] == '0');
   }
   MBD_CUDA(init_device_constants());
   MBD_CUDA(init_chol_attributes());

@@ -154,6 +154,7 @@ struct mbd_ctx {
   mbd::HostBuf staging;   // download: every geometry's results in one pass
   mbd::Sy2sbLookAhead la_ctx{};   // look-ahead stream and events of the context-stream reductions
   bool lookahead = true;     // dense -> band look-ahead (MBD_B200_LOOKAHEAD=0: off)
+  bool priorities = true;    // stream and graph-node priorities (MBD_B200_PRIORITY=0: off)
   // standalone eigenvalue call: matrix, (d, e, eigenvalues, scratch), workspace
   mbd::DevBuf eig_a, eig_vec, eig_ws;
   mbd::DevBuf eigh_buf;   // mbd_rsscs_eigh: matrix, reflectors, vectors, Gram, scratch
