@@ -894,13 +894,14 @@ int mbd_rsscs_create(mbd_ctx** out, int device) {
     // timed: flag-synchronised (measured faster at every size on B200);
     // MBD_B200_CLUSTER_CHASE=1 makes it the cluster-resident one, =0 rules
     // the cluster-resident chase out even where the autotuner picks it
-    // MBD_B200_CG_FP32=1: the learned mode's block-CG runs its matrix passes
-    // on an FP32 copy of the relay matrices in two phases with an FP64
-    // restart between them (measured on B200 for the 2000-atom cluster:
-    // relay solve 15.7 ms against 17.4 ms for the one-phase FP64 passes, for
-    // 50 % more relay memory; off by default)
+    // the learned mode's block-CG runs its matrix passes on an FP32 copy of
+    // the relay matrices in two phases with an FP64 restart between them
+    // (measured on B200 for the 2000-atom cluster: relay solve 15.7 ms
+    // against 17.4 ms for the one-phase FP64 passes) wherever the copy (50 %
+    // more relay memory) fits in half the free device memory;
+    // MBD_B200_CG_FP32=1 always, =0 never
     const char* cf = std::getenv("MBD_B200_CG_FP32");
-    ctx->cg_fp32 = cf && cf[0] == '1';
+    ctx->cg_fp32_mode = (cf && cf[0] == '1') ? 1 : ((cf && cf[0] == '0') ? 0 : -1);
     const char* cc = std::getenv("MBD_B200_CLUSTER_CHASE");
     ctx->cluster_chase = !(cc && cc[0] == '0');
     if (cc && cc[0] == '1')

@@ -212,7 +212,8 @@ struct mbd_ctx {
   double wait_limit_s = 2.0;                   // bounded device waits (per device)
   int test_stall_wait = 0;                     // 1: the bulge-chasing launch's first wait runs out
   int f32_tensor_build = 0;                    // 1: mixed modes build the relay tensors in FP32 arithmetic
-  bool cg_fp32 = false;                        // learned mode: block-CG matrix passes on the FP32 copy
+  bool cg_fp32 = false;                        // learned mode: block-CG matrix passes on the FP32 copy (this batch)
+  int cg_fp32_mode = -1;                       // 1 always, 0 never, -1 where the copy fits (reserve_learned)
   mbd::TuneChoice tune[mbd::kTuneClasses];     // mbd_rsscs_autotune
   int panel_qr_default = 0;                    // MBD_B200_PANEL_QR=tsqr: 1
 };

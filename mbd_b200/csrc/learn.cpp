@@ -200,6 +200,26 @@ int reserve_learned(mbd_ctx* ctx) {
     if (st != MBD_OK) return st;
   }
   bool moved = false;
+  {
+    // the FP32 copy of the relay matrices for the two-phase block-CG: per
+    // slot n x ld x 21 floats of its largest geometry
+    bool fp32 = ctx->cg_fp32_mode == 1;
+    if (ctx->cg_fp32_mode < 0) {
+      size_t need = 0, held = 0, free_b = 0, total_b = 0;
+      for (int s = 0; s < ctx->n_slots; ++s) {
+        size_t r32 = 0;
+        for (int g : ctx->order)
+          if (ctx->geoms[g]->slot == s)
+            r32 = std::max(r32, sizeof(float) * (size_t)kNFreq * ctx->geoms[g]->plan.n * ctx->geoms[g]->plan.ld);
+        need += r32;
+        held += ctx->slots[s]->relay32.bytes;
+      }
+      MBD_CUDA(cudaMemGetInfo(&free_b, &total_b));
+      fp32 = (double)need <= 0.5 * (double)(free_b + held);
+    }
+    moved = fp32 != ctx->cg_fp32;   // the captured launches carry the choice
+    ctx->cg_fp32 = fp32;
+  }
   for (int s = 0; s < ctx->n_slots; ++s) {
     size_t cg = 0, gw = 0, res = 0;
     for (int g : ctx->order) {

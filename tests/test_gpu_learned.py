@@ -139,7 +139,8 @@ def test_network_graph_matches_oracle_neighbours(engine):
 def test_trained_network_saves_cg_iterations(engine, trained):
     """Held-out boxes: the network's warm start needs at least 4 % fewer
     block-CG iterations in total than a zero start, with the same energies
-    (measured on a B200: 133 against 140 over the six boxes).
+    (measured on a B200: 133 against 140 over the six boxes with FP64 passes,
+    142 against 152 counting both phases of the two-phase FP32 form).
 
     The bar is what a warm start of this accuracy can give: the iteration
     reduces the error by a roughly constant factor rho ~ 0.5 per step, so a

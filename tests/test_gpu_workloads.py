@@ -118,8 +118,9 @@ def test_headline_clusters_one_call_each_vs_oracle(engine):
 
 
 def test_two_phase_fp32_cg_headline_clusters():
-    """The opt-in mixed-precision block-CG of the learned mode
-    (MBD_B200_CG_FP32=1: matrix passes on an FP32 copy of the relay matrices,
+    """The mixed-precision block-CG of the learned mode, forced on
+    (MBD_B200_CG_FP32=1; by default it runs where its copy fits: matrix
+    passes on an FP32 copy of the relay matrices,
     products in FP32, a restart from the FP64 residual between its two
     phases) on the headline clusters, twice (the second compute replays the
     captured graph with the phase lengths of the first): the mixed forms'
