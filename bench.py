@@ -608,14 +608,15 @@ def main():
         sl = [s for _, s in geos]
         eng.energy_batch(gl, sl, args.mode)
         torch.cuda.synchronize()
-        t0 = time.perf_counter()
-        for _ in range(args.steps):
-            rr = eng.energy_batch(gl, sl, args.mode)
-        t_e2e = max_over_ranks(time.perf_counter() - t0)
+        with ClockSampler(local) as eclk:
+            t0 = time.perf_counter()
+            for _ in range(args.steps):
+                rr = eng.energy_batch(gl, sl, args.mode)
+            t_e2e = max_over_ranks(time.perf_counter() - t0)
         st2 = eng.stats()
         line["e2e"] = {"value": replica_rate(world, len(geos), args.steps, 1000.0 * t_e2e), "unit": "energies/s",
                        "h2d_bytes_per_step": st2["h2d_bytes"], "d2h_bytes_per_step": st2["d2h_bytes"],
-                       "status": [r.status for r in rr]}
+                       "status": [r.status for r in rr], "clocks": eclk.summary()}
     if WORKLOAD == "boxes":
         # one 200-atom box with these cut-offs already takes the oracle about
         # five minutes (its periodic image sums are numpy loops)
