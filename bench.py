@@ -571,7 +571,11 @@ def main():
                                              "(the reference's Cholesky, solves and Hamiltonian reduction) / "
                                              "device time of the whole step",
                               "peak_source": "nominal FP64 (148 SM x 64 DFMA/clk x 2 x 1965 MHz); "
-                                             "MEASURED_PEAKS.json has no FP64 entry"},
+                                             "MEASURED_PEAKS.json has no FP64 entry",
+                              # the same work against a split-precision (3xTF32) tensor-core rate:
+                              # the measured bf16 burst rate / 2 (TF32) / 3 (three products)
+                              "frac_of_tf32_split": step_tf / (load_peaks()[0].get("bf16_tflops", 1590.0) / 6.0),
+                              "tf32_split_peak": load_peaks()[0].get("bf16_tflops", 1590.0) / 6.0},
             "energies": [r.energy for r in res][:8],
             "refine_iters": [r.refine_iters for r in res][:8],
             "stage_ms": dict(stage)}
