@@ -5,7 +5,9 @@
 
 Objects go to mbd_b200/_build/, the library to mbd_b200/libmbd_b200.so.
 The CUDA runtime is linked statically (nvcc's default), so the library does
-not depend on which libcudart the host process loaded.
+not depend on which libcudart the host process loaded.  The pmbd.x front end
+(host/pmbd_b200.cpp) is linked against the library into mbd_b200/pmbd_b200,
+which finds libmbd_b200.so beside itself (rpath $ORIGIN).
 """
 from __future__ import annotations
 
@@ -21,6 +23,8 @@ ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 BUILD = os.path.join(HERE, "_build")
 LIB = os.path.join(HERE, "libmbd_b200.so")
+HOST = os.path.join(HERE, "host")
+EXE = os.path.join(HERE, "pmbd_b200")
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 COMMON = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompiler", "-Wall",
@@ -64,9 +68,26 @@ def build(force: bool = False, verbose: bool = True) -> str:
         res = subprocess.run(cmd, capture_output=True, text=True)
         if res.returncode != 0:
             raise RuntimeError(f"link failed:\n{res.stdout}\n{res.stderr}")
+    build_host(force)
     if verbose:
-        print(f"built {LIB}")
+        print(f"built {LIB} and {EXE}")
     return LIB
+
+
+def build_host(force: bool = False) -> str:
+    """Link the pmbd_b200 executable (plain C++, no device code) against
+    libmbd_b200.so."""
+    src = os.path.join(HOST, "pmbd_b200.cpp")
+    deps = [src, LIB, os.path.join(HOST, "pmbd_io.h"), os.path.join(ROOT, "include", "mbd_b200.h")]
+    if not force and os.path.exists(EXE) and os.path.getmtime(EXE) >= max(os.path.getmtime(d) for d in deps):
+        return EXE
+    cxx = shutil.which("g++") or "c++"
+    cmd = [cxx, "-std=c++17", "-O2", "-Wall", "-Wextra", "-I", os.path.join(ROOT, "include"), "-I", HOST, src,
+           "-o", EXE, "-L", HERE, "-lmbd_b200", "-Wl,-rpath,$ORIGIN", "-Wl,--allow-shlib-undefined"]
+    res = subprocess.run(cmd, capture_output=True, text=True)
+    if res.returncode != 0:
+        raise RuntimeError(f"host link failed:\n{res.stdout}\n{res.stderr}")
+    return EXE
 
 
 if __name__ == "__main__":

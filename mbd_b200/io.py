@@ -85,8 +85,11 @@ def parse_geometry(text: str) -> Geometry:
         if len(tok) < 5:
             raise InputError(f"geometry: atom record {i + 1} needs name x y z hirshfeld")
         names.append(tok[0][:2])                 # CHARACTER*2
-        xyz.append([_real(t) for t in tok[1:4]])
-        hv.append(_real(tok[4]))
+        try:
+            xyz.append([_real(t) for t in tok[1:4]])
+            hv.append(_real(tok[4]))
+        except ValueError as exc:
+            raise InputError(f"geometry: atom record {i + 1}: {exc}") from exc
     geo = Geometry(names, np.array(xyz, dtype=np.float64), np.array(hv, dtype=np.float64))
     if k < len(lines) and "lattice_vector" in lines[k]:
         geo.n_periodic = 3
@@ -95,7 +98,12 @@ def parse_geometry(text: str) -> Geometry:
             if k + i >= len(lines):
                 raise InputError("geometry: three lattice_vector records required")
             tok = lines[k + i].replace(",", " ").split()
-            lat[i] = [_real(t) for t in tok[1:4]]
+            if len(tok) < 4:
+                raise InputError("geometry: lattice_vector needs three components")
+            try:
+                lat[i] = [_real(t) for t in tok[1:4]]
+            except ValueError as exc:
+                raise InputError(f"geometry: lattice_vector: {exc}") from exc
         geo.lattice = lat
     return geo
 

@@ -1,8 +1,9 @@
-"""The command line on the GPU: `python -m mbd_b200 run` prints the MBD
-section of pmbd.x's report for the reference's examples/C6H6.in byte for byte
-as examples/C6H6.out prints it; `train` writes a network checkpoint that
-`run --mode mixed_learned --network` loads, with the energy within the mixed
-forms' 1e-6 Ha of the printed one."""
+"""The command lines on the GPU: `python -m mbd_b200 run` and the C++
+executable mbd_b200/pmbd_b200 print the MBD section of pmbd.x's report for
+the reference's examples/C6H6.in byte for byte as examples/C6H6.out prints
+it; `train` writes a network checkpoint that both load with `--mode
+mixed_learned --network`, with the energy within the mixed forms' 1e-6 Ha of
+the printed one."""
 import json
 import os
 import subprocess
@@ -39,16 +40,44 @@ def test_cli_run_prints_reference_report(tmp_path):
     assert out.stdout.splitlines() == fix["printed"]["report_lines"]
 
 
-def test_cli_train_then_run_learned(tmp_path):
-    fix, g, s = _c6h6(tmp_path)
-    net = tmp_path / "net.bin"
+@pytest.fixture(scope="module")
+def network(tmp_path_factory):
+    net = tmp_path_factory.mktemp("net") / "net.bin"
     tr = subprocess.run([sys.executable, "-m", "mbd_b200", "train", "--out", str(net), "--geoms", "12",
                          "--epochs", "2"], capture_output=True, text=True, cwd=ROOT, timeout=600)
     assert tr.returncode == 0, tr.stderr
+    return str(net)
+
+
+@pytest.fixture(scope="module")
+def pmbd():
+    from mbd_b200 import build
+    return build.build_host()
+
+
+def test_cli_train_then_run_learned(tmp_path, network):
+    fix, g, s = _c6h6(tmp_path)
     out = subprocess.run([sys.executable, "-m", "mbd_b200", "run", g, s, "--mode", "mixed_learned", "--network",
-                          str(net)], capture_output=True, text=True, cwd=ROOT, timeout=600)
+                          network], capture_output=True, text=True, cwd=ROOT, timeout=600)
     assert out.returncode == 0, out.stderr
     assert abs(_energy(out.stdout) - fix["printed"]["energy"]) <= 1e-6
+
+
+def test_pmbd_b200_prints_reference_report(tmp_path, pmbd):
+    fix, g, s = _c6h6(tmp_path)
+    out = subprocess.run([pmbd, g, s], capture_output=True, text=True, timeout=600)
+    assert out.returncode == 0, out.stderr
+    assert out.stdout.splitlines() == fix["printed"]["report_lines"]
+
+
+def test_pmbd_b200_modes(tmp_path, pmbd, network):
+    """mixed, and mixed_learned from zero and from the trained network: the
+    report's energy within 1e-6 Ha of the printed one."""
+    fix, g, s = _c6h6(tmp_path)
+    for extra in (["--mode", "mixed"], ["--mode", "mixed_learned"], ["--mode", "mixed_learned", "--network", network]):
+        out = subprocess.run([pmbd, g, s] + extra, capture_output=True, text=True, timeout=600)
+        assert out.returncode == 0, (extra, out.stderr)
+        assert abs(_energy(out.stdout) - fix["printed"]["energy"]) <= 1e-6, extra
 
 
 def test_cli_run_reports_unknown_element(tmp_path):
@@ -58,3 +87,11 @@ def test_cli_run_reports_unknown_element(tmp_path):
                          cwd=ROOT, timeout=600)
     assert out.returncode == 1
     assert "VdW parameters not defined" in out.stderr
+
+
+def test_pmbd_b200_reports_unknown_element(tmp_path, pmbd):
+    g = tmp_path / "bad.in"
+    g.write_text("1\n\nXx 0 0 0 1.0\n")
+    out = subprocess.run([pmbd, str(g)], capture_output=True, text=True, timeout=600)
+    assert out.returncode == 1
+    assert "VdW parameters not defined" in out.stderr and "(status 2)" in out.stderr
