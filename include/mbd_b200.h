@@ -154,10 +154,11 @@ int mbd_rsscs_eigh(mbd_ctx* ctx, const double* H, int n, int ld, double* w, doub
  *   w      DEVICE pointer, n doubles: eigenvalues in ascending order.
  *   stream cudaStream_t (NULL = legacy default stream); the call returns
  *          after the work on it has finished.
- * n must not exceed MBD_NOALLOC_MAX_N (else MBD_ERR_TOO_LARGE).  The first
- * call on a device looks up the scratch address with cudaGetSymbolAddress;
- * make that first call before any stream capture.  Calls share the scratch:
- * calls that overlap on the GPU (other streams or threads, same device) race. */
+ * n must not exceed MBD_NOALLOC_MAX_N (else MBD_ERR_TOO_LARGE).  Every call
+ * synchronises `stream` (it reads the kernels' error flag back before it
+ * returns), so no call may be made while a stream is being captured.  Calls
+ * share the scratch: calls that overlap on the GPU (other streams or
+ * threads, same device) race. */
 #define MBD_NOALLOC_MAX_N 2048
 int mbd_rsscs_eigvalsh_noalloc(double* H, int n, int ld, double* w, void* stream);
 

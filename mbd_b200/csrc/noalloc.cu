@@ -12,9 +12,10 @@
 // The array is a __device__ variable: every GPU that loads this library
 // holds kScratchBytes of it until the process exits.  Host code cannot use
 // its name as a device address, so the first call on each device (with that
-// device current) looks the address up once with cudaGetSymbolAddress.  That
-// first call should therefore come before any stream capture.  All calls
-// share the one array and it keeps the last call's contents: the parts that
+// device current) looks the address up once with cudaGetSymbolAddress.
+// Every call ends by reading the error flag back and synchronising the
+// caller's stream, so no call may be made while a stream is being captured.
+// All calls share the one array and it keeps the last call's contents: the parts that
 // must start at zero are cleared on every call, and calls that overlap on
 // the GPU (different streams, or host threads on the same device) race on it.
 #include <cuda_runtime.h>
