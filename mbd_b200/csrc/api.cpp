@@ -324,12 +324,24 @@ int relay_mixed(mbd_ctx* ctx, GeomDev* gd, RelaySlot& sl, size_t mstride, cudaEv
 
 }  // namespace
 
-void drop_graphs(mbd_ctx* ctx) {
-  for (auto& g : ctx->graph)
-    if (g) {
+void drop_graphs(mbd_ctx* ctx, bool keep_first) {
+  for (int m = 0; m < 3; ++m) {
+    cudaGraphExec_t& g = ctx->graph[m];
+    cudaGraphExec_t& prev = ctx->graph_prev[m];
+    if (g && keep_first && ctx->graph_first[m]) {
+      if (prev) cudaGraphExecDestroy(prev);
+      prev = g;
+    } else if (g) {
       cudaGraphExecDestroy(g);
-      g = nullptr;
     }
+    g = nullptr;
+    ctx->graph_first[m] = false;
+    if (!keep_first && prev) {
+      cudaGraphExecDestroy(prev);
+      prev = nullptr;
+      ctx->graph_sig[m].clear();
+    }
+  }
   // the next compute of each mode launches directly again (and reads back
   // the CG iterations), the one after it captures
   for (auto& gd : ctx->geoms) gd->cg_iters_seen = gd->cg_iters_seen1 = 0;
@@ -551,7 +563,7 @@ int plan_slots(mbd_ctx* ctx) {
 // Plain-path slot buffers, per-geometry Hamiltonians, the tridiagonal plan and
 // the device job tables of the uploaded batch.
 int prepare_batch(mbd_ctx* ctx, bool eigen) {
-  drop_graphs(ctx);
+  drop_graphs(ctx, true);
   ctx->order.clear();
   for (size_t g = 0; g < ctx->geoms.size(); ++g)
     if (ctx->geoms[g]->status_host == MBD_OK) ctx->order.push_back((int)g);
@@ -765,7 +777,7 @@ int reserve_mixed(mbd_ctx* ctx) {
     MBD_CUDA(grow(sl.mixv, vec));
     MBD_CUDA(grow(sl.res_ws, res));
     MBD_CUDA(grow(sl.solve_sync, sync));
-    if (moved) drop_graphs(ctx);
+    if (moved) drop_graphs(ctx, true);
   }
   return MBD_OK;
 }
@@ -837,8 +849,12 @@ int enqueue_batch(mbd_ctx* ctx, int mode) {
 }
 
 // Captures enqueue_batch into a graph for `mode`; false when capture is not
-// possible (the caller then enqueues directly).
-bool capture_batch(mbd_ctx* ctx, int mode) {
+// possible (the caller then enqueues directly).  first: the batch's first
+// compute in the mode (the full CG schedule); its graph updates the one kept
+// from an earlier batch when the launch sequences match (same kernels and
+// dependencies: cudaGraphExecUpdate then rewrites only the launch arguments,
+// far cheaper than instantiating), else it is instantiated.
+bool capture_batch(mbd_ctx* ctx, int mode, bool first) {
   cudaGraph_t graph = nullptr;
   if (cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
     cudaGetLastError();
@@ -849,9 +865,21 @@ bool capture_batch(mbd_ctx* ctx, int mode) {
   ctx->capturing = false;
   const cudaError_t ec = cudaStreamEndCapture(ctx->stream, &graph);
   cudaGraphExec_t exec = nullptr;
-  const bool ok = st == MBD_OK && ec == cudaSuccess && graph &&
-                  cudaGraphInstantiate(&exec, graph,
-                                       ctx->priorities ? cudaGraphInstantiateFlagUseNodePriority : 0) == cudaSuccess;
+  bool ok = st == MBD_OK && ec == cudaSuccess && graph;
+  if (ok && first && ctx->graph_prev[mode]) {
+    cudaGraphExecUpdateResultInfo info{};
+    if (cudaGraphExecUpdate(ctx->graph_prev[mode], graph, &info) == cudaSuccess) {
+      exec = ctx->graph_prev[mode];
+      ctx->graph_updates += 1;
+    } else {
+      cudaGetLastError();
+      cudaGraphExecDestroy(ctx->graph_prev[mode]);
+    }
+    ctx->graph_prev[mode] = nullptr;
+  }
+  if (ok && !exec)
+    ok = cudaGraphInstantiate(&exec, graph, ctx->priorities ? cudaGraphInstantiateFlagUseNodePriority : 0) ==
+         cudaSuccess;
   if (graph) cudaGraphDestroy(graph);
   if (!ok) {
     if (exec) cudaGraphExecDestroy(exec);
@@ -859,8 +887,26 @@ bool capture_batch(mbd_ctx* ctx, int mode) {
     return false;
   }
   ctx->graph[mode] = exec;
+  ctx->graph_first[mode] = first;
   ctx->graph_launches[mode] = ctx->launches;
   return true;
+}
+
+// What fixes a batch's launch sequence in `mode`, as far as the host knows
+// it before enqueueing: the geometries' sizes, image counts, slots and
+// reduction paths.  A first compute is captured only when this matches the
+// batch whose graph is kept (or the batch before it), so batches of changing
+// shape keep launching kernel by kernel instead of instantiating every time.
+std::vector<long long> batch_signature(const mbd_ctx* ctx, int mode) {
+  std::vector<long long> sig{mode, ctx->n_slots, (long long)ctx->order.size(), ctx->two_stage_batch ? 1 : 0};
+  for (int g : ctx->order) {
+    const GeomDev& gd = *ctx->geoms[g];
+    const GeomPlan& p = gd.plan;
+    sig.insert(sig.end(), {p.N, p.nsl, p.nH, gd.slot, (long long)p.scs_shifts.size(),
+                           (long long)p.cfdm_shifts.size(), (long long)p.diff_shift.size(),
+                           two_stage(ctx, p.nH) ? 1 : 0});
+  }
+  return sig;
 }
 
 }  // namespace
@@ -890,6 +936,8 @@ int mbd_rsscs_create(mbd_ctx** out, int device) {
   {
     const char* ng = std::getenv("MBD_B200_NO_GRAPHS");
     ctx->use_graphs = !(ng && ng[0] && ng[0] != '0');
+    const char* gu = std::getenv("MBD_B200_GRAPH_UPDATE");
+    ctx->graph_update = !(gu && gu[0] == '0');
     // the band -> tridiagonal chase of size classes the autotuner has not
     // timed: flag-synchronised (measured faster at every size on B200);
     // MBD_B200_CLUSTER_CHASE=1 makes it the cluster-resident one, =0 rules
@@ -1016,14 +1064,39 @@ int mbd_rsscs_compute(mbd_ctx* ctx, int mode) {
   // From the second compute of a batch in a mode on, capture the batch into a
   // CUDA graph once and replay it; a batch computed once (energy_batch, an
   // upload per call) is launched directly and does not pay for the capture.
+  //   A context that uploads batch after batch of one shape (a trajectory,
+  // the same structures re-submitted) runs each batch's first compute as a
+  // graph as well: captured, then written into the graph kept from the
+  // previous batch with cudaGraphExecUpdate, which costs a fraction of the
+  // gaps between kernels launched one by one.  The learned mode's graph of
+  // a first compute runs the full CG schedule; its second compute captures
+  // the iterations seen instead and the first graph is kept for the next
+  // batch.
   const bool repeat = ctx->mode_runs[mode]++ > 0;
-  if (ctx->use_graphs && repeat && !ctx->graph[mode] && !capture_batch(ctx, mode)) ctx->use_graphs = false;
+  if (ctx->use_graphs && repeat && ctx->graph[mode] && ctx->graph_first[mode] &&
+      mode == MBD_MODE_MIXED_LEARNED) {
+    if (ctx->graph_prev[mode]) cudaGraphExecDestroy(ctx->graph_prev[mode]);
+    ctx->graph_prev[mode] = ctx->graph[mode];
+    ctx->graph[mode] = nullptr;
+    ctx->graph_first[mode] = false;
+  }
+  if (ctx->use_graphs && !ctx->graph[mode]) {
+    if (repeat) {
+      if (!capture_batch(ctx, mode, false)) ctx->use_graphs = false;
+    } else if (ctx->graph_update) {
+      std::vector<long long> sig = batch_signature(ctx, mode);
+      const bool same = sig == ctx->graph_sig[mode] || sig == ctx->last_sig[mode];
+      ctx->last_sig[mode] = sig;
+      // a failed capture launches directly below
+      if (same && capture_batch(ctx, mode, true)) ctx->graph_sig[mode] = std::move(sig);
+    }
+  }
   if (ctx->use_graphs && ctx->graph[mode]) {
     ctx->launches = ctx->graph_launches[mode];
-    ctx->graph_replayed = true;
+    ctx->graph_kind = repeat ? 1 : 2;
     return cuda_status(cudaGraphLaunch(ctx->graph[mode], ctx->stream));
   }
-  ctx->graph_replayed = false;
+  ctx->graph_kind = 0;
   return enqueue_batch(ctx, mode);
 }
 
@@ -1408,12 +1481,13 @@ int mbd_rsscs_last_stats(mbd_ctx* ctx, double* out, int n) {
   out[0] = ctx->launches;
   out[1] = ctx->h2d_bytes;
   out[2] = ctx->d2h_bytes;
-  if (n >= 4) out[3] = ctx->graph_replayed ? 1.0 : 0.0;
+  if (n >= 4) out[3] = ctx->graph_kind;
   if (n >= 5) {
     double edges = 0.0;
     for (const auto& gd : ctx->geoms) edges += std::max(gd->n_edges, 0);
     out[4] = edges;
   }
+  if (n >= 6) out[5] = ctx->graph_updates;
   return MBD_OK;
 }
 

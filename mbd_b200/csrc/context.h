@@ -194,8 +194,22 @@ struct mbd_ctx {
   // upload or workspace reallocation
   cudaGraphExec_t graph[3] = {nullptr, nullptr, nullptr};
   double graph_launches[3] = {0, 0, 0};
+  // graph[mode] was captured at the batch's first compute (full CG schedule)
+  bool graph_first[3] = {false, false, false};
+  // a first-compute graph of an earlier batch, kept so that the next batch's
+  // first compute can update it (cudaGraphExecUpdate) instead of launching
+  // kernel by kernel or instantiating anew
+  cudaGraphExec_t graph_prev[3] = {nullptr, nullptr, nullptr};
+  // batch_signature of the batch whose first-compute graph is kept, and of
+  // the last batch computed for the first time, per mode
+  std::vector<long long> graph_sig[3], last_sig[3];
+  double graph_updates = 0;                  // first-compute graphs written by cudaGraphExecUpdate
   bool use_graphs = true;
-  bool graph_replayed = false;               // the last compute ran as a graph replay
+  bool graph_update = true;                  // MBD_B200_GRAPH_UPDATE=0: first computes launch directly
+  // how the last compute ran: 0 kernel by kernel, 1 replay of the batch's
+  // graph, 2 a graph captured at the batch's first compute (updated from an
+  // earlier batch's where the launch sequence matched)
+  int graph_kind = 0;
   int two_stage_max_n = 0;                   // largest matrix the two-stage reduction takes on this device
   bool two_stage_batch = false;              // two-stage reduction for the matrices it can take
   int two_stage_force = -1;                  // 1 / 0: forced on / off; -1: policy
@@ -281,7 +295,10 @@ inline int tuned_panel_qr(const mbd_ctx* ctx, int n) {
 }
 inline int tuned_chase_c(const mbd_ctx* ctx, int n) { return ctx->tune[tune_class(n)].chase_c; }
 // api.cpp
-void drop_graphs(mbd_ctx* ctx);
+// Destroys the captured graphs (they hold the launch arguments of the
+// uploaded batch and its buffers).  keep_first: a graph captured at a first
+// compute is kept for the next batch's first compute to update.
+void drop_graphs(mbd_ctx* ctx, bool keep_first = false);
 int run_front(mbd_ctx* ctx, GeomDev* gd, int gi, int mode, bool relay_only = false);
 int upload_batch(mbd_ctx* ctx, int n_geom, const mbd_geom* geoms, bool eigen);
 // learn.cpp

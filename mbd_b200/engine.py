@@ -469,10 +469,11 @@ class Engine:
         return S.reshape(M, 3, 3), grad, loss
 
     def stats(self) -> dict:
-        buf = (ctypes.c_double * 5)()
-        self.lib.mbd_rsscs_last_stats(self.ctx, buf, 5)
+        buf = (ctypes.c_double * 6)()
+        self.lib.mbd_rsscs_last_stats(self.ctx, buf, 6)
         return {"launches": int(buf[0]), "h2d_bytes": int(buf[1]), "d2h_bytes": int(buf[2]),
-                "graph_replayed": bool(buf[3]), "network_edges": int(buf[4])}
+                "graph_replayed": buf[3] == 1.0, "first_compute_graph": buf[3] == 2.0,
+                "network_edges": int(buf[4]), "graph_updates": int(buf[5])}
 
     def stream_handle(self) -> int:
         """cudaStream_t of this context (for recording caller-side events)."""

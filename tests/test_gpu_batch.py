@@ -138,6 +138,42 @@ def test_graph_replay_matches_direct_launches(engine, mode, monkeypatch):
             np.testing.assert_array_equal(a.alpha_iw, b.alpha_iw)
 
 
+@pytest.mark.parametrize("mode", ["plain", "mixed", "mixed_learned"])
+def test_first_compute_graph_across_batches(mode, monkeypatch):
+    """Batches of one shape uploaded one after another (the structures
+    change, the sizes do not): the first batch launches kernel by kernel, the
+    second's first compute is captured into a graph, and every later batch's
+    first compute is written into that graph by cudaGraphExecUpdate.  Every
+    batch's results equal a context that always launches directly, bit for
+    bit; a batch of another shape launches directly again."""
+    from mbd_b200 import Engine
+    from mbd_b200 import synthetic as sy
+    sizes = (25, 140, 60)
+    batches = [[sy.cluster(n, seed=1000 * b + n) for n in sizes] for b in range(4)]
+    batches.append([sy.cluster(n, seed=77 + n) for n in (30, 90)])
+    kinds, updates, runs = [], [], []
+    with Engine(0) as eng:
+        eng.use_network(False)
+        for items in batches:
+            res = eng.energy_batch([g for g, _ in items], [s for _, s in items], mode)
+            st = eng.stats()
+            kinds.append(2 if st["first_compute_graph"] else (1 if st["graph_replayed"] else 0))
+            updates.append(st["graph_updates"])
+            runs.append(res)
+    assert kinds == [0, 2, 2, 2, 0], kinds
+    assert updates == [0, 0, 1, 2, 2], updates
+    monkeypatch.setenv("MBD_B200_NO_GRAPHS", "1")
+    with Engine(0) as direct:
+        direct.use_network(False)
+        for items, res in zip(batches, runs):
+            ref = direct.energy_batch([g for g, _ in items], [s for _, s in items], mode)
+            for a, b in zip(res, ref):
+                assert a.status == 0 and b.status == 0
+                assert a.energy == b.energy
+                assert a.refine_iters == b.refine_iters
+                np.testing.assert_array_equal(a.alpha_iw, b.alpha_iw)
+
+
 @pytest.mark.parametrize("sizes", [(25, 140, 60, 300, 12), tuple(range(20, 20 + 7 * 40, 7))])
 def test_one_stage_reduction_matches_two_stage(engine, sizes, monkeypatch):
     """The grouped one-stage tridiagonalisation (MBD_B200_TWO_STAGE=0; the
