@@ -23,9 +23,7 @@ mixed_direct / learned_no_network : the 3xTF32 direct relay solve and the
         block-CG without the network, timed the same way.
 e2e   : the headline mode through mbd_rsscs_energy_batch with host buffers
         (upload + compute + download every step), wall clock.  Each step
-        uploads the batch anew; its compute runs as a CUDA graph written into
-        the previous step's graph (cudaGraphExecUpdate), as for any caller
-        that submits batches of one shape one after another.
+        uploads the batch anew, so its compute launches kernel by kernel.
 Multi-GPU: replicas only (each rank runs the whole workload on its GPU;
 value = all ranks' energies / max time).
 """
@@ -624,8 +622,8 @@ def main():
         line["e2e"] = {"value": replica_rate(world, len(geos), args.steps, 1000.0 * t_e2e), "unit": "energies/s",
                        "h2d_bytes_per_step": st2["h2d_bytes"], "d2h_bytes_per_step": st2["d2h_bytes"],
                        "status": [r.status for r in rr], "clocks": eclk.summary(),
-                       # how the last step's compute ran: a graph written into the previous
-                       # step's by cudaGraphExecUpdate, or kernel by kernel
+                       # how the last step's compute ran: kernel by kernel, or (with
+                       # MBD_B200_GRAPH_UPDATE=1) as a graph of the batch's shape
                        "first_compute_graph": st2["first_compute_graph"], "graph_updates": st2["graph_updates"]}
     if WORKLOAD == "boxes":
         # one 200-atom box with these cut-offs already takes the oracle about

@@ -194,17 +194,20 @@ int mbd_rsscs_last_timings(mbd_ctx* ctx, double* ms, int n);
  * [2] device->host bytes copied by mbd_rsscs_download, [3] (n >= 4) how the
  * last compute ran: 1 replay of the batch's captured CUDA graph, 0 the
  * kernels launched one by one, 2 the batch's first compute in the mode as a
- * graph.  The first compute of an uploaded batch launches directly unless
- * the context's previous batch had the same shape (sizes, image counts,
- * slots), in which case it is captured and written into the graph kept from
- * that batch (cudaGraphExecUpdate; MBD_B200_GRAPH_UPDATE=0 turns this off);
- * the second compute captures the graph if needed and replays it from then
- * on; a change of network, option or device buffers starts over,
+ * graph.  The first compute of an uploaded batch launches directly (with
+ * MBD_B200_GRAPH_UPDATE=1 set, not when the context's previous batch had the
+ * same shape: then it is captured and written into the graph kept from that
+ * batch by cudaGraphExecUpdate, or instantiated where the update is
+ * refused); the second compute captures the graph if needed and replays it
+ * from then on; a change of network, option or device buffers starts over,
  * [4] (n >= 5) the edges of the MIXED_LEARNED network's neighbour lists over
  * the batch's geometries (pairs within 5 A, periodic images included, both
  * directions; 0 until a learned compute or training has built them),
  * [5] (n >= 6) first-compute graphs this context has written by
- * cudaGraphExecUpdate since it was created.  n must be >= 3. */
+ * cudaGraphExecUpdate since it was created, [6] (n >= 7) the last such
+ * update's cudaGraphExecUpdateResult (0 success), [7] (n >= 8) the
+ * cudaGraphNodeType of the node a refused update names (-1 none).
+ * n must be >= 3. */
 int mbd_rsscs_last_stats(mbd_ctx* ctx, double* out, int n);
 
 /* The CUDA stream (cudaStream_t) every kernel of this context runs on, so a

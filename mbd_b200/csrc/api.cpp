@@ -868,7 +868,12 @@ bool capture_batch(mbd_ctx* ctx, int mode, bool first) {
   bool ok = st == MBD_OK && ec == cudaSuccess && graph;
   if (ok && first && ctx->graph_prev[mode]) {
     cudaGraphExecUpdateResultInfo info{};
-    if (cudaGraphExecUpdate(ctx->graph_prev[mode], graph, &info) == cudaSuccess) {
+    const cudaError_t eu = cudaGraphExecUpdate(ctx->graph_prev[mode], graph, &info);
+    ctx->graph_update_result = (int)info.result;
+    ctx->graph_update_node = -1;
+    cudaGraphNodeType nt;
+    if (info.errorNode && cudaGraphNodeGetType(info.errorNode, &nt) == cudaSuccess) ctx->graph_update_node = (int)nt;
+    if (eu == cudaSuccess) {
       exec = ctx->graph_prev[mode];
       ctx->graph_updates += 1;
     } else {
@@ -937,7 +942,7 @@ int mbd_rsscs_create(mbd_ctx** out, int device) {
     const char* ng = std::getenv("MBD_B200_NO_GRAPHS");
     ctx->use_graphs = !(ng && ng[0] && ng[0] != '0');
     const char* gu = std::getenv("MBD_B200_GRAPH_UPDATE");
-    ctx->graph_update = !(gu && gu[0] == '0');
+    ctx->graph_update = gu && gu[0] == '1';
     // the band -> tridiagonal chase of size classes the autotuner has not
     // timed: flag-synchronised (measured faster at every size on B200);
     // MBD_B200_CLUSTER_CHASE=1 makes it the cluster-resident one, =0 rules
@@ -1488,6 +1493,8 @@ int mbd_rsscs_last_stats(mbd_ctx* ctx, double* out, int n) {
     out[4] = edges;
   }
   if (n >= 6) out[5] = ctx->graph_updates;
+  if (n >= 7) out[6] = ctx->graph_update_result;
+  if (n >= 8) out[7] = ctx->graph_update_node;
   return MBD_OK;
 }
 

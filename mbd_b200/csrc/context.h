@@ -204,8 +204,11 @@ struct mbd_ctx {
   // the last batch computed for the first time, per mode
   std::vector<long long> graph_sig[3], last_sig[3];
   double graph_updates = 0;                  // first-compute graphs written by cudaGraphExecUpdate
+  // the last update's cudaGraphExecUpdateResult and, where it names one, the
+  // cudaGraphNodeType of the node it refused (-1 none)
+  int graph_update_result = 0, graph_update_node = -1;
   bool use_graphs = true;
-  bool graph_update = true;                  // MBD_B200_GRAPH_UPDATE=0: first computes launch directly
+  bool graph_update = false;                 // MBD_B200_GRAPH_UPDATE=1: first computes of repeated shapes as graphs
   // how the last compute ran: 0 kernel by kernel, 1 replay of the batch's
   // graph, 2 a graph captured at the batch's first compute (updated from an
   // earlier batch's where the launch sequence matched)

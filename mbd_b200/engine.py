@@ -469,11 +469,12 @@ class Engine:
         return S.reshape(M, 3, 3), grad, loss
 
     def stats(self) -> dict:
-        buf = (ctypes.c_double * 6)()
-        self.lib.mbd_rsscs_last_stats(self.ctx, buf, 6)
+        buf = (ctypes.c_double * 8)()
+        self.lib.mbd_rsscs_last_stats(self.ctx, buf, 8)
         return {"launches": int(buf[0]), "h2d_bytes": int(buf[1]), "d2h_bytes": int(buf[2]),
                 "graph_replayed": buf[3] == 1.0, "first_compute_graph": buf[3] == 2.0,
-                "network_edges": int(buf[4]), "graph_updates": int(buf[5])}
+                "network_edges": int(buf[4]), "graph_updates": int(buf[5]),
+                "graph_update_result": int(buf[6]), "graph_update_node": int(buf[7])}
 
     def stream_handle(self) -> int:
         """cudaStream_t of this context (for recording caller-side events)."""

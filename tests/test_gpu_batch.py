@@ -140,18 +140,21 @@ def test_graph_replay_matches_direct_launches(engine, mode, monkeypatch):
 
 @pytest.mark.parametrize("mode", ["plain", "mixed", "mixed_learned"])
 def test_first_compute_graph_across_batches(mode, monkeypatch):
-    """Batches of one shape uploaded one after another (the structures
-    change, the sizes do not): the first batch launches kernel by kernel, the
-    second's first compute is captured into a graph, and every later batch's
-    first compute is written into that graph by cudaGraphExecUpdate.  Every
-    batch's results equal a context that always launches directly, bit for
-    bit; a batch of another shape launches directly again."""
+    """MBD_B200_GRAPH_UPDATE=1, batches of one shape uploaded one after
+    another (the structures change, the sizes do not): the first batch
+    launches kernel by kernel, every later batch's first compute runs as a
+    graph (captured, then written into the previous batch's graph by
+    cudaGraphExecUpdate, or instantiated where the driver refuses the
+    update), and a batch of another shape launches kernel by kernel again.
+    Every batch's results equal a context that always launches directly, bit
+    for bit."""
     from mbd_b200 import Engine
     from mbd_b200 import synthetic as sy
     sizes = (25, 140, 60)
     batches = [[sy.cluster(n, seed=1000 * b + n) for n in sizes] for b in range(4)]
     batches.append([sy.cluster(n, seed=77 + n) for n in (30, 90)])
     kinds, updates, runs = [], [], []
+    monkeypatch.setenv("MBD_B200_GRAPH_UPDATE", "1")
     with Engine(0) as eng:
         eng.use_network(False)
         for items in batches:
@@ -161,7 +164,8 @@ def test_first_compute_graph_across_batches(mode, monkeypatch):
             updates.append(st["graph_updates"])
             runs.append(res)
     assert kinds == [0, 2, 2, 2, 0], kinds
-    assert updates == [0, 0, 1, 2, 2], updates
+    assert updates[:2] == [0, 0] and updates[4] == updates[3], updates
+    monkeypatch.setenv("MBD_B200_GRAPH_UPDATE", "0")
     monkeypatch.setenv("MBD_B200_NO_GRAPHS", "1")
     with Engine(0) as direct:
         direct.use_network(False)
