@@ -11,7 +11,11 @@ executable), checked on CPU.
   wrong-version file;
 * the linked pmbd_b200 answers a bad command line with status 2 and an
   unreadable input or a machine without an sm_100 GPU with status 1 and the
-  engine's message.
+  engine's message;
+* pmbd_b200 linked against a stub engine (tests/c/fake_mbd.c) hands the C
+  ABI exactly the atomic numbers, bohr coordinates, lattice, settings and
+  mode the Python host would, loads a network checkpoint, prints the
+  reference's report from the engine's results and reports engine errors.
 """
 import json
 import os
@@ -250,3 +254,134 @@ def test_pmbd_b200_without_a_gpu(pmbd, tmp_path):
     g.write_text("2\n\nC 0 0 0 0.8\nH 0 0 1.1 0.6\n")
     out = subprocess.run([pmbd, str(g)], capture_output=True, text=True, timeout=120)
     assert out.returncode == 1 and out.stderr.strip().endswith("(status 6)"), out.stderr
+
+
+@pytest.fixture(scope="module")
+def fake_pmbd(tmp_path_factory):
+    """pmbd_b200 linked against tests/c/fake_mbd.c built as libmbd_b200.so:
+    the executable's own code runs unchanged, the engine is a stub that
+    records what it is given and returns fixed values."""
+    d = tmp_path_factory.mktemp("fakembd")
+    inc = os.path.join(ROOT, "include")
+    subprocess.run(["gcc", "-std=c99", "-Wall", "-Werror", "-shared", "-fPIC", "-I", inc,
+                    os.path.join(ROOT, "tests", "c", "fake_mbd.c"), "-o", str(d / "libmbd_b200.so")], check=True)
+    exe = d / "pmbd_b200"
+    subprocess.run(["g++", "-std=c++17", "-O1", "-Wall", "-Wextra", "-Werror", "-I", inc, "-I",
+                    os.path.join(ROOT, "mbd_b200", "host"), os.path.join(ROOT, "mbd_b200", "host", "pmbd_b200.cpp"),
+                    "-L", str(d), "-lmbd_b200", "-Wl,-rpath," + str(d), "-o", str(exe)], check=True)
+    return str(exe)
+
+
+def _run_fake(exe, args, tmp_path, values, status=None):
+    vals = tmp_path / "values.txt"
+    vals.write_text(values)
+    rec = tmp_path / "record.txt"
+    if rec.exists():
+        rec.unlink()
+    env = dict(os.environ, FAKE_MBD_VALUES=str(vals), FAKE_MBD_RECORD=str(rec))
+    if status is not None:
+        env["FAKE_MBD_STATUS"] = str(status)
+    out = subprocess.run([exe] + list(args), capture_output=True, text=True, timeout=60, env=env)
+    lines = rec.read_text().splitlines() if rec.exists() else []
+    return out, lines
+
+
+def _record_fields(lines):
+    atoms = [ln.split()[1:] for ln in lines if ln.startswith("atom ")]
+    rec = {"atoms": [(int(a[0]), *[float.fromhex(t) for t in a[1:]]) for a in atoms],
+           "lattice": [float.fromhex(ln.split()[1]) for ln in lines if ln.startswith("lattice ")]}
+    for ln in lines:
+        key, *rest = ln.split()
+        if key in ("mode", "n_atoms", "n_periodic", "xc", "device", "use_network"):
+            rec[key] = int(rest[0])
+        elif key == "cuts":
+            rec[key] = [float.fromhex(t) for t in rest]
+        elif key == "vacuum":
+            rec[key] = [int(t) for t in rest]
+        elif key == "set_params":
+            rec[key] = (int(rest[0]), float.fromhex(rest[1]))
+    return rec
+
+
+@pytest.mark.parametrize("name", ["C6H6", "PBBA", "graphene_111", "H2O"])
+def test_pmbd_b200_host_with_a_stub_engine(fake_pmbd, tmp_path, name):
+    """What the executable hands the C ABI for the reference's inputs: atomic
+    numbers, coordinates and lattice vectors converted to bohr exactly as the
+    Python host converts them (MBD_rsSCS.f90:211-212), Hirshfeld ratios, the
+    settings' cut-offs, vacuum axes and xc, the mode; and the report it
+    prints from the engine's results (byte for byte the reference's report
+    where the fixture holds it, else the Python host's)."""
+    import types
+
+    from mbd_b200 import format_report, parse_geometry, parse_settings
+    from mbd_b200.engine import BOHR, element_z
+    from oracle import mbd_oracle as mo
+    with open(os.path.join(GOLDEN, name + ".json")) as fh:
+        fix = json.load(fh)
+    g = tmp_path / "geometry.in"
+    g.write_text(fix["geometry_in"])
+    s = tmp_path / "setting.in"
+    s.write_text(fix["settings_in"])
+    o = fix["oracle"]
+    out, lines = _run_fake(fake_pmbd, [str(g), str(s), "--device", "3"], tmp_path, _values(o, mo.CASIMIR_OMEGA))
+    assert out.returncode == 0, out.stderr
+    rec = _record_fields(lines)
+    geo = parse_geometry(fix["geometry_in"])
+    st = parse_settings(fix["settings_in"])
+    assert rec["device"] == 3 and rec["mode"] == 0 and "use_network" not in rec
+    assert rec["n_atoms"] == len(geo.names) and rec["n_periodic"] == geo.n_periodic
+    assert [a[0] for a in rec["atoms"]] == [element_z(nm) for nm in geo.names]
+    np.testing.assert_array_equal(np.array([a[1:4] for a in rec["atoms"]]), geo.coords / BOHR)
+    np.testing.assert_array_equal(np.array([a[4] for a in rec["atoms"]]), geo.hirshfeld)
+    np.testing.assert_array_equal(np.array(rec["lattice"]).reshape(3, 3), geo.lattice / BOHR)
+    assert rec["cuts"] == [st.mbd_scs_dip_cutoff, st.mbd_cfdm_dip_cutoff, st.mbd_supercell_cutoff]
+    assert rec["vacuum"] == [int(v) for v in st.mbd_scs_vacuum_axis] and rec["xc"] == st.xc
+    if "report_lines" in fix.get("printed", {}):
+        expect = fix["printed"]["report_lines"]
+    else:
+        res = types.SimpleNamespace(energy=o["energy"], c6_mol=o["c6_mol"], nimag=o["nimag"],
+                                    supercell=tuple(o["supercell"]), c6_eff=np.array(o["c6_eff"]),
+                                    alpha_eff=np.array(o["alpha_eff"]), mol_pol_eig=np.array(o["mol_pol_eig"]))
+        expect = format_report(geo, res, omega_grid=mo.CASIMIR_OMEGA).splitlines()
+    assert out.stdout.splitlines() == expect
+
+
+def test_pmbd_b200_modes_network_and_errors_with_a_stub_engine(fake_pmbd, tmp_path):
+    from mbd_b200.engine import write_network_file
+    from oracle import mbd_oracle as mo
+    with open(os.path.join(GOLDEN, "C6H6.json")) as fh:
+        fix = json.load(fh)
+    g = tmp_path / "geometry.in"
+    g.write_text(fix["geometry_in"])
+    vals = _values(fix["oracle"], mo.CASIMIR_OMEGA)
+    out, lines = _run_fake(fake_pmbd, [str(g), "--mode", "mixed"], tmp_path, vals)
+    rec = _record_fields(lines)
+    assert out.returncode == 0 and rec["mode"] == 1 and "use_network" not in rec
+    assert rec["cuts"] == [120.0, 100.0, 25.0] and rec["vacuum"] == [0, 0, 0] and rec["xc"] == 1
+    out, lines = _run_fake(fake_pmbd, [str(g), "--mode", "mixed_learned"], tmp_path, vals)
+    rec = _record_fields(lines)
+    assert out.returncode == 0 and rec["mode"] == 2 and rec["use_network"] == 0 and "set_params" not in rec
+    p = np.random.default_rng(4).standard_normal(16274).astype(np.float32)
+    net = tmp_path / "net.bin"
+    write_network_file(str(net), p)
+    out, lines = _run_fake(fake_pmbd, [str(g), "--mode", "mixed_learned", "--network", str(net)], tmp_path, vals)
+    rec = _record_fields(lines)
+    checksum = 0.0
+    for i, x in enumerate(p):
+        checksum += float(x) * (i % 7 + 1)
+    assert out.returncode == 0 and rec["mode"] == 2 and "use_network" not in rec
+    assert rec["set_params"] == (p.size, checksum)
+    # the network is read before the engine is touched
+    bad = bytearray(net.read_bytes())
+    bad[40] ^= 4
+    net.write_bytes(bytes(bad))
+    out, lines = _run_fake(fake_pmbd, [str(g), "--mode", "mixed_learned", "--network", str(net)], tmp_path, vals)
+    assert out.returncode == 1 and "SHA-256 mismatch" in out.stderr and lines == []
+    # an engine status: message and exit status 1, nothing on stdout
+    out, _ = _run_fake(fake_pmbd, [str(g)], tmp_path, vals, status=3)
+    assert out.returncode == 1 and out.stdout == ""
+    assert out.stderr.strip() == "pmbd_b200: fake error (status 3)"
+    x = tmp_path / "bad.in"
+    x.write_text("1\n\nXx 0 0 0 1.0\n")
+    out, _ = _run_fake(fake_pmbd, [str(x)], tmp_path, vals)
+    assert out.returncode == 1 and out.stderr.strip() == "pmbd_b200: fake: unknown element (status 2)"
