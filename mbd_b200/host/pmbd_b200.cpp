@@ -100,7 +100,13 @@ int main(int argc, char** argv) {
     const pmbd::Geometry g = pmbd::parse_geometry(slurp(a.geometry));
     const pmbd::Settings s = pmbd::parse_settings(a.settings.empty() ? std::string() : slurp(a.settings));
     std::vector<float> params;
-    if (a.mode == MBD_MODE_MIXED_LEARNED && !a.network.empty()) params = pmbd::read_network_file(a.network);
+    if (a.mode == MBD_MODE_MIXED_LEARNED && !a.network.empty()) {
+      params = pmbd::read_network_file(a.network);
+      const int want = mbd_rsscs_learned_param_count();
+      if ((long long)params.size() != want)
+        throw pmbd::InputError(a.network + ": " + std::to_string(params.size()) + " parameters, the engine's network has " +
+                               std::to_string(want));
+    }
 
     const int n = (int)g.names.size();
     std::vector<int> z(n);

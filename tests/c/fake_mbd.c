@@ -62,6 +62,8 @@ int mbd_rsscs_create(mbd_ctx** ctx, int device) {
 
 void mbd_rsscs_destroy(mbd_ctx* ctx) { free(ctx); }
 
+int mbd_rsscs_learned_param_count(void) { return 16274; }
+
 int mbd_rsscs_learned_use_network(mbd_ctx* ctx, int on) {
     (void)ctx;
     FILE* r = record();

@@ -377,6 +377,9 @@ def test_pmbd_b200_modes_network_and_errors_with_a_stub_engine(fake_pmbd, tmp_pa
     net.write_bytes(bytes(bad))
     out, lines = _run_fake(fake_pmbd, [str(g), "--mode", "mixed_learned", "--network", str(net)], tmp_path, vals)
     assert out.returncode == 1 and "SHA-256 mismatch" in out.stderr and lines == []
+    write_network_file(str(net), p[:100])
+    out, lines = _run_fake(fake_pmbd, [str(g), "--mode", "mixed_learned", "--network", str(net)], tmp_path, vals)
+    assert out.returncode == 1 and "100 parameters, the engine's network has 16274" in out.stderr and lines == []
     # an engine status: message and exit status 1, nothing on stdout
     out, _ = _run_fake(fake_pmbd, [str(g)], tmp_path, vals, status=3)
     assert out.returncode == 1 and out.stdout == ""
