@@ -384,6 +384,7 @@ int band_to_tridiag_single(mbd_ctx* ctx, double* Br, int n, double* d, double* e
 // frequency table, relay tensors, relay factorisation and solve (plain or
 // mixed), screened polarizabilities and C6, CFDM Hamiltonian into gd->hmat.
 int run_front(mbd_ctx* ctx, GeomDev* gd, int gi, int mode, bool relay_only) {
+  NvtxRange nvtx("mbd_b200 enqueue geometry");
   const GeomPlan& p = gd->plan;
   RelaySlot& sl = *ctx->slots[gd->slot];
   cudaStream_t s = sl.stream;
@@ -855,6 +856,7 @@ int enqueue_batch(mbd_ctx* ctx, int mode) {
 // dependencies: cudaGraphExecUpdate then rewrites only the launch arguments,
 // far cheaper than instantiating), else it is instantiated.
 bool capture_batch(mbd_ctx* ctx, int mode, bool first) {
+  NvtxRange nvtx(first ? "mbd_b200 capture first compute" : "mbd_b200 capture");
   cudaGraph_t graph = nullptr;
   if (cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
     cudaGetLastError();
@@ -1018,6 +1020,7 @@ void mbd_rsscs_destroy(mbd_ctx* ctx) {
 }
 
 int mbd_rsscs_upload(mbd_ctx* ctx, int n_geom, const mbd_geom* geoms) {
+  NvtxRange nvtx("mbd_b200 upload");
   if (!ctx || n_geom < 1 || !geoms) return MBD_ERR_ARG;
   return upload_batch(ctx, n_geom, geoms, true);
 }
@@ -1054,6 +1057,9 @@ int upload_batch(mbd_ctx* ctx, int n_geom, const mbd_geom* geoms, bool eigen) {
 extern "C" {
 
 int mbd_rsscs_compute(mbd_ctx* ctx, int mode) {
+  static const char* const kRange[3] = {"mbd_b200 compute plain", "mbd_b200 compute mixed",
+                                        "mbd_b200 compute mixed_learned"};
+  NvtxRange nvtx(mode >= 0 && mode < 3 ? kRange[mode] : "mbd_b200 compute");
   if (!ctx || !ctx->have_batch) return MBD_ERR_ARG;
   if (mode != MBD_MODE_PLAIN_FP64 && mode != MBD_MODE_MIXED && mode != MBD_MODE_MIXED_LEARNED) return MBD_ERR_ARG;
   if (mode == MBD_MODE_MIXED_LEARNED && ctx->use_net && !ctx->have_net) return MBD_ERR_NO_NETWORK;
@@ -1106,6 +1112,7 @@ int mbd_rsscs_compute(mbd_ctx* ctx, int mode) {
 }
 
 int mbd_rsscs_download(mbd_ctx* ctx, mbd_result* out) {
+  NvtxRange nvtx("mbd_b200 download");
   if (!ctx || !ctx->have_batch || !out) return MBD_ERR_ARG;
   MBD_CUDA(cudaSetDevice(ctx->device));
   // Every geometry's results in one pass into page-locked memory: the block
@@ -1292,6 +1299,7 @@ int mbd_rsscs_energy(mbd_ctx* ctx, const mbd_geom* geom, int mode, mbd_result* o
 }
 
 int mbd_rsscs_eigvalsh(mbd_ctx* ctx, const double* H, int n, int ld, double* w) {
+  NvtxRange nvtx("mbd_b200 eigvalsh");
   if (!ctx || !H || !w || n < 1 || ld < n) return MBD_ERR_ARG;
   MBD_CUDA(cudaSetDevice(ctx->device));
   cudaStream_t s = ctx->stream;
@@ -1331,6 +1339,7 @@ int mbd_rsscs_eigvalsh(mbd_ctx* ctx, const double* H, int n, int ld, double* w) 
 }
 
 int mbd_rsscs_eigh(mbd_ctx* ctx, const double* H, int n, int ld, double* w, double* Z, int ldz) {
+  NvtxRange nvtx("mbd_b200 eigh");
   if (!ctx || !H || !w || !Z || n < 1 || ld < n || ldz < n) return MBD_ERR_ARG;
   MBD_CUDA(cudaSetDevice(ctx->device));
   cudaStream_t s = ctx->stream;
@@ -1548,6 +1557,7 @@ int mbd_rsscs_set_option(mbd_ctx* ctx, int option, double value) {
 }
 
 int mbd_rsscs_autotune(mbd_ctx* ctx, int max_n) {
+  NvtxRange nvtx("mbd_b200 autotune");
   if (!ctx || max_n < 1) return MBD_ERR_ARG;
   MBD_CUDA(cudaSetDevice(ctx->device));
   MBD_CUDA(cudaDeviceSynchronize());

@@ -3,6 +3,7 @@
 #pragma once
 
 #include <cuda_runtime.h>
+#include <nvtx3/nvToolsExt.h>
 
 #include <memory>
 #include <vector>
@@ -12,6 +13,18 @@
 #include "mbd_internal.h"
 
 namespace mbd {
+
+// NVTX range over one scope of host code (upload, compute, capture, the
+// enqueue of one geometry, download, ...): a profiler that records NVTX shows
+// where the host time of a call goes; without one the calls return at once
+// (NVTX v3 is header-only and loads a tool's library only when one is
+// attached).
+struct NvtxRange {
+  explicit NvtxRange(const char* name) { nvtxRangePushA(name); }
+  ~NvtxRange() { nvtxRangePop(); }
+  NvtxRange(const NvtxRange&) = delete;
+  NvtxRange& operator=(const NvtxRange&) = delete;
+};
 
 // Refinement sweeps of the mixed relay solve and the residual gate
 // ||B - A X||_F / ||B||_F that accepts its result.

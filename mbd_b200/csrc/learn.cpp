@@ -83,6 +83,7 @@ GraphBox graph_box(const GeomPlan& p) {
 // lists.  Device copy of a graph: [off | nbr | src | species] ints,
 // [dvec | efeat | eproj] floats.
 int build_graphs(mbd_ctx* ctx, const std::vector<GeomDev*>& todo, cudaStream_t s) {
+  NvtxRange nvtx("mbd_b200 network neighbour lists");
   if (todo.empty()) return MBD_OK;
   const size_t K = todo.size();
   auto pad64 = [](size_t k) { return (k + 63) & ~size_t(63); };
@@ -366,6 +367,7 @@ int mbd_rsscs_learned_use_network(mbd_ctx* ctx, int on) {
 
 int mbd_rsscs_learned_train(mbd_ctx* ctx, int n_geom, const mbd_geom* geoms, int epochs, double lr, int seed,
                             double* epoch_loss) {
+  NvtxRange nvtx("mbd_b200 learned train");
   if (!ctx || !geoms || n_geom < 1 || epochs < 1 || !(lr > 0.0)) return MBD_ERR_ARG;
   MBD_CUDA(cudaSetDevice(ctx->device));
   int st = upload_batch(ctx, n_geom, geoms, false);
