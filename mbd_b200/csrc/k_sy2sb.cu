@@ -37,12 +37,6 @@ namespace {
 constexpr int B = kBand;            // 32
 constexpr int TL = 64;              // tile edge of symm / syr2k
 
-__device__ __forceinline__ double warp_sum(double v) {
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-  return v;
-}
-
 // The cluster barrier in its two halves: work a CTA does between its arrive
 // and its wait overlaps the other CTAs' arrival instead of delaying them.
 __device__ __forceinline__ void cluster_arrive() { asm volatile("barrier.cluster.arrive.release.aligned;" ::: "memory"); }

@@ -156,7 +156,6 @@ __global__ void __launch_bounds__(128, 2) tc3_gemm_kernel(const __grid_constant_
   uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
   __shared__ __align__(8) uint64_t full_bar[STAGES], empty_bar[STAGES], done_bar;
   __shared__ uint32_t tmem_base_sh;
-  __shared__ int abort_sh;
 
   const int warp = threadIdx.x / 32, lane = threadIdx.x % 32;
   const int b = blockIdx.y;
@@ -171,7 +170,6 @@ __global__ void __launch_bounds__(128, 2) tc3_gemm_kernel(const __grid_constant_
   const int iters = 3 * k_tiles;
 
   if (threadIdx.x == 0) {
-    abort_sh = 0;
     for (int s = 0; s < STAGES; ++s) {
       mbar_init(smem_u32(&full_bar[s]), 1);
       mbar_init(smem_u32(&empty_bar[s]), 1);
@@ -196,10 +194,7 @@ __global__ void __launch_bounds__(128, 2) tc3_gemm_kernel(const __grid_constant_
     for (int i = 0; i < iters; ++i) {
       const int s = i % STAGES;
       const uint32_t ph = (uint32_t)((i / STAGES) & 1);
-      if (i >= STAGES && !mbar_wait(smem_u32(&empty_bar[s]), ph ^ 1u, p.err)) {
-        abort_sh = 1;
-        break;
-      }
+      if (i >= STAGES && !mbar_wait(smem_u32(&empty_bar[s]), ph ^ 1u, p.err)) break;
       const int seg = i / k_tiles, kk = (i % k_tiles) * BK;
       const CUtensorMap* ma = (seg == 2) ? &maps.a_lo : &maps.a_hi;
       const CUtensorMap* mb = (seg == 1) ? &maps.b_lo : &maps.b_hi;
@@ -232,7 +227,6 @@ __global__ void __launch_bounds__(128, 2) tc3_gemm_kernel(const __grid_constant_
       umma_commit(smem_u32(&empty_bar[s]));
     }
     if (ok) umma_commit(smem_u32(&done_bar));
-    else abort_sh = 1;
   }
   __syncwarp();
   // ---------------- epilogue ----------------
@@ -240,6 +234,10 @@ __global__ void __launch_bounds__(128, 2) tc3_gemm_kernel(const __grid_constant_
   // pipeline shared memory -> one TMA bulk operation per 128x32 chunk:
   // reduce-add of -acc (SYRK) or plain stores of acc and its hi/lo split.
   // The tensor bounds clip rows/columns outside the matrix.
+  //   After a wait above gave up, done_bar is never committed: every thread
+  // then spends the bounded wait here, by whose end the copies and MMAs
+  // issued before the abort have completed, so TMEM is freed below only
+  // once nothing in flight can still write it.
   const bool ok = mbar_wait(smem_u32(&done_bar), 0, p.err);
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
   if (ok) {
