@@ -57,7 +57,7 @@ struct PairSmem {
   double s[B];
   double Ot[B][B + 1];   // O-warp: the O block, row-major (row l at Ot[l])
   double Ds[B][B];       // D-warp: band rows of D, Ds[i][d] = A(r + i, r + i - d)
-  int go;             // the O-warp's verdict after its wait, read by both warps
+  int go;             // the O-warp's decision after its wait, read by both warps
 };
 
 __device__ __forceinline__ void pair_sync(int pair) {
@@ -164,7 +164,7 @@ __global__ void __launch_bounds__(WARPS * 32) sb2st_kernel(const BandJob* jobs, 
     bool have_pf = false;
     for (int k = 0; k < K; ++k) {
       // the O-warp waits for the previous sweep and decides for the pair; the
-      // D-warp follows it through the barrier (one verdict, both warps leave
+      // D-warp follows it through the barrier (one decision, both warps leave
       // together)
       if (owarp) {
         bool ok;
