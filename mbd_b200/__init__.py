@@ -6,5 +6,5 @@ geometry.in / setting.in readers and report printer (``io``), the seeded
 synthetic workloads (``synthetic``) and the in-tree build (``build``).
 """
 from .io import (Geometry, InputError, Settings, format_report, parse_geometry, parse_settings, tile,  # noqa: F401
-                 write_geometry)
+                 write_geometry, write_settings)
 from .engine import EXPORTED, LIB_PATH, Engine, MbdError, Result, load_library  # noqa: F401

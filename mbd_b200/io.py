@@ -10,7 +10,8 @@
   and ignored: there is no process grid.
 * ``format_report`` prints the fields of MBD_at_rsSCS's report
   (UTILS.f90:223-331).
-* ``write_geometry`` writes a Geometry back in that format and ``tile``
+* ``write_geometry`` / ``write_settings`` write a Geometry / Settings back in
+  those formats and ``tile``
   replicates a periodic geometry into a supercell (the job of the
   reference's examples/process.py, which tiles the 60-atom graphene cell
   into graphene_<i><j>1.in), for any cell and along all three vectors.
@@ -120,6 +121,21 @@ def write_geometry(geo: Geometry) -> str:
         for a in geo.lattice:
             out.append(f"lattice_vector  {a[0]:.17g}  {a[1]:.17g}  {a[2]:.17g}")
     return "\n".join(out) + "\n"
+
+
+def write_settings(st: Settings) -> str:
+    """setting.in text for `st` as parse_settings (MBD_rsSCS.f90:98-135) reads
+    it: one keyword and its value(s) per line, reals in full double precision,
+    the vacuum axes as Fortran logicals (nprow / npcol are not written: no
+    process grid)."""
+    lg = lambda v: ".true." if v else ".false."
+    return "\n".join([
+        f"xc {int(st.xc)}",
+        f"mbd_supercell_cutoff {float(st.mbd_supercell_cutoff):.17g}",
+        f"mbd_cfdm_dip_cutoff {float(st.mbd_cfdm_dip_cutoff):.17g}",
+        f"mbd_scs_dip_cutoff {float(st.mbd_scs_dip_cutoff):.17g}",
+        "mbd_scs_vacuum_axis " + " ".join(lg(v) for v in st.mbd_scs_vacuum_axis),
+    ]) + "\n"
 
 
 def tile(geo: Geometry, reps) -> Geometry:

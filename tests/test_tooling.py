@@ -87,3 +87,54 @@ def test_cli_tile(tmp_path):
                    cwd=ROOT)
     t = parse_geometry(out.read_text())
     assert len(t.names) == 4 * 60 and t.n_periodic == 3
+
+
+def test_settings_round_trip():
+    from mbd_b200 import Settings, parse_settings, write_settings
+    st = Settings(xc=2, mbd_supercell_cutoff=12.5, mbd_cfdm_dip_cutoff=0.1 + 0.2, mbd_scs_dip_cutoff=90.0,
+                  mbd_scs_vacuum_axis=(False, True, True))
+    back = parse_settings(write_settings(st))
+    assert (back.xc, back.mbd_supercell_cutoff, back.mbd_cfdm_dip_cutoff, back.mbd_scs_dip_cutoff,
+            back.mbd_scs_vacuum_axis) == (2, 12.5, 0.1 + 0.2, 90.0, (False, True, True))
+    assert parse_settings(write_settings(Settings())).mbd_scs_vacuum_axis == (False, False, False)
+
+
+@pytest.mark.parametrize("kind,args", [("cluster", ["--atoms", "40", "--seed", "3"]),
+                                       ("box", ["--atoms", "30", "--seed", "2", "--scs-cut", "20", "--cfdm-cut",
+                                                "15", "--sc-cut", "5"]),
+                                       ("sheet", ["--reps", "3"]),
+                                       ("benzene", [])])
+def test_cli_generate_writes_the_generators_inputs(tmp_path, kind, args):
+    """`generate` writes the seeded generators' geometries and settings in
+    pmbd.x's formats; read back they are the generators' own, bit for bit."""
+    from mbd_b200 import parse_settings
+    from mbd_b200 import synthetic as sy
+    g, s = tmp_path / "geometry.in", tmp_path / "setting.in"
+    subprocess.run([sys.executable, "-m", "mbd_b200", "generate", kind] + args + ["-o", str(g), "--settings", str(s)],
+                   check=True, cwd=ROOT)
+    ref_g, ref_s = {"cluster": lambda: sy.cluster(40, seed=3),
+                    "box": lambda: sy.periodic_box(30, seed=2, scs_cut=20.0, cfdm_cut=15.0, sc_cut=5.0),
+                    "sheet": lambda: sy.graphene_sheet(3),
+                    "benzene": lambda: sy.benzene()}[kind]()
+    geo, st = parse_geometry(g.read_text()), parse_settings(s.read_text())
+    assert geo.names == list(ref_g.names) and geo.n_periodic == ref_g.n_periodic
+    assert np.array_equal(geo.coords, ref_g.coords) and np.array_equal(geo.hirshfeld, ref_g.hirshfeld)
+    assert np.array_equal(geo.lattice, ref_g.lattice)
+    assert (st.xc, st.mbd_supercell_cutoff, st.mbd_cfdm_dip_cutoff, st.mbd_scs_dip_cutoff,
+            tuple(st.mbd_scs_vacuum_axis)) == (ref_s.xc, ref_s.mbd_supercell_cutoff, ref_s.mbd_cfdm_dip_cutoff,
+                                               ref_s.mbd_scs_dip_cutoff, tuple(bool(v) for v in ref_s.mbd_scs_vacuum_axis))
+
+
+def test_cli_generate_batch_and_errors(tmp_path):
+    from mbd_b200 import synthetic as sy
+    out = tmp_path / "batch"
+    subprocess.run([sys.executable, "-m", "mbd_b200", "generate", "batch", "--count", "5", "--seed", "4", "-o",
+                    str(out)], check=True, cwd=ROOT)
+    ref = sy.cluster_batch(count=5, seed=4)
+    assert sorted(p.name for p in out.iterdir()) == [f"geometry_{k}.in" for k in range(5)] + ["setting.in"]
+    for k, (rg, _) in enumerate(ref):
+        geo = parse_geometry((out / f"geometry_{k}.in").read_text())
+        assert np.array_equal(geo.coords, rg.coords) and geo.names == list(rg.names)
+    bad = subprocess.run([sys.executable, "-m", "mbd_b200", "generate", "cluster", "-o", str(tmp_path / "x.in")],
+                         capture_output=True, text=True, cwd=ROOT)
+    assert bad.returncode == 1 and "--atoms N" in bad.stderr
