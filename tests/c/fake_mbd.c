@@ -9,7 +9,8 @@
  *   FAKE_MBD_STATUS  status mbd_rsscs_energy returns instead (optional);
  *   FAKE_MBD_RECORD  file that receives every argument the executable
  *                    passed: the mbd_geom fields, the mode, the network
- *                    switch and the parameters it set. */
+ *                    switch and the parameters it set.
+ * mbd_rsscs_energy_batch runs mbd_rsscs_energy on each geometry in turn. */
 #include <stdio.h>
 #include <stdlib.h>
 #include <string.h>
@@ -134,4 +135,13 @@ int mbd_rsscs_energy(mbd_ctx* ctx, const mbd_geom* g, int mode, mbd_result* out)
         for (int k = 0; k < 63; ++k) out->molpol_eig[k] = v[6 + 2 * N + k];
     out->status = MBD_OK;
     return MBD_OK;
+}
+
+int mbd_rsscs_energy_batch(mbd_ctx* ctx, int n_geom, const mbd_geom* geoms, int mode, mbd_result* out) {
+    int first = MBD_OK;
+    for (int g = 0; g < n_geom; ++g) {
+        const int st = mbd_rsscs_energy(ctx, &geoms[g], mode, &out[g]);
+        if (st != MBD_OK && first == MBD_OK) first = st;
+    }
+    return first;
 }

@@ -95,3 +95,35 @@ def test_pmbd_b200_reports_unknown_element(tmp_path, pmbd):
     out = subprocess.run([pmbd, str(g)], capture_output=True, text=True, timeout=600)
     assert out.returncode == 1
     assert "VdW parameters not defined" in out.stderr and "(status 2)" in out.stderr
+
+
+def test_pmbd_b200_batch_reports(tmp_path, pmbd):
+    """--batch: C6H6 and PBBA in one energy_batch call, one report file each
+    with the reference's lines (numbers to the last printed digit, which a
+    batch's different summation order may move by one)."""
+    lst = tmp_path / "list.txt"
+    fixes = {}
+    for name in ("C6H6", "PBBA"):
+        with open(os.path.join(GOLDEN, name + ".json")) as fh:
+            fixes[name] = json.load(fh)
+        (tmp_path / f"{name}.in").write_text(fixes[name]["geometry_in"])
+        (tmp_path / f"{name}.set").write_text(fixes[name]["settings_in"])
+    lst.write_text("C6H6.in C6H6.set\nPBBA.in PBBA.set\n")
+    out_dir = tmp_path / "reports"
+    out_dir.mkdir()
+    out = subprocess.run([pmbd, "--batch", str(lst), "--out-dir", str(out_dir)], capture_output=True, text=True,
+                         timeout=600)
+    assert out.returncode == 0, out.stderr
+    for name, fix in fixes.items():
+        got = (out_dir / f"{name}.out").read_text().splitlines()
+        want = fix["printed"]["report_lines"]
+        assert len(got) == len(want)
+        for a, b in zip(got, want):
+            ta, tb = a.split(), b.split()
+            assert len(ta) == len(tb), (a, b)
+            for x, y in zip(ta, tb):
+                if x != y:
+                    fx, fy = float(x), float(y)
+                    assert abs(fx - fy) <= 1.01 * 10.0 ** -(len(y.split(".")[1].split("E")[0])) * \
+                        (10.0 ** int(y.split("E")[1]) if "E" in y else 1.0), (a, b)
+        assert abs(_energy("\n".join(got)) - fix["printed"]["energy"]) <= 2e-9

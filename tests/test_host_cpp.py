@@ -388,3 +388,46 @@ def test_pmbd_b200_modes_network_and_errors_with_a_stub_engine(fake_pmbd, tmp_pa
     x.write_text("1\n\nXx 0 0 0 1.0\n")
     out, _ = _run_fake(fake_pmbd, [str(x)], tmp_path, vals)
     assert out.returncode == 1 and out.stderr.strip() == "pmbd_b200: fake: unknown element (status 2)"
+
+
+def test_pmbd_b200_batch_with_a_stub_engine(fake_pmbd, tmp_path):
+    """--batch: every listed geometry in one energy_batch call, a report file
+    per geometry (byte for byte the reference's for C6H6), a failing geometry
+    reported on stderr while the others are still written; relative paths in
+    the list are taken from the list's directory."""
+    from oracle import mbd_oracle as mo
+    with open(os.path.join(GOLDEN, "C6H6.json")) as fh:
+        fix = json.load(fh)
+    d = tmp_path / "inputs"
+    (d / "sub").mkdir(parents=True)
+    (d / "benzene.in").write_text(fix["geometry_in"])
+    (d / "sub" / "second.in").write_text(fix["geometry_in"])
+    (d / "setting.in").write_text(fix["settings_in"])
+    (d / "bad.in").write_text("1\n\nXx 0 0 0 1.0\n")
+    lst = d / "list.txt"
+    lst.write_text("# three geometries\nbenzene.in setting.in\n\nsub/second.in\n" + str(d / "bad.in") + "\n")
+    out_dir = tmp_path / "reports"
+    out_dir.mkdir()
+    vals = _values(fix["oracle"], mo.CASIMIR_OMEGA)
+    out, lines = _run_fake(fake_pmbd, ["--batch", str(lst), "--out-dir", str(out_dir), "--mode", "mixed"], tmp_path,
+                           vals)
+    assert out.returncode == 1 and out.stdout == ""
+    assert out.stderr.strip() == f"pmbd_b200: {d / 'bad.in'}: fake: unknown element (status 2)"
+    assert sorted(p.name for p in out_dir.iterdir()) == ["benzene.out", "second.out"]
+    for name in ("benzene.out", "second.out"):
+        assert (out_dir / name).read_text().splitlines() == fix["printed"]["report_lines"]
+    rec = _record_fields(lines)
+    assert rec["mode"] == 1 and len(rec["atoms"]) == 12 + 12 + 1
+    assert sum(1 for ln in lines if ln.startswith("mode ")) == 3
+    # two geometries that would write the same report, and a bad list line
+    lst.write_text("benzene.in\nsub/benzene.in\n")
+    (d / "sub" / "benzene.in").write_text(fix["geometry_in"])
+    out, _ = _run_fake(fake_pmbd, ["--batch", str(lst), "--out-dir", str(out_dir)], tmp_path, vals)
+    assert out.returncode == 1 and "would both write" in out.stderr
+    lst.write_text("benzene.in setting.in extra\n")
+    out, _ = _run_fake(fake_pmbd, ["--batch", str(lst), "--out-dir", str(out_dir)], tmp_path, vals)
+    assert out.returncode == 1 and "expected geometry.in [setting.in]" in out.stderr
+    for args in (["--batch", str(lst)], ["--out-dir", str(out_dir), str(d / "benzene.in")],
+                 ["--batch", str(lst), "--out-dir", str(out_dir), str(d / "benzene.in")]):
+        out, _ = _run_fake(fake_pmbd, args, tmp_path, vals)
+        assert out.returncode == 2 and out.stderr.startswith("usage: pmbd_b200"), args
