@@ -82,6 +82,9 @@ def build_host(force: bool = False) -> str:
     if not force and os.path.exists(EXE) and os.path.getmtime(EXE) >= max(os.path.getmtime(d) for d in deps):
         return EXE
     cxx = shutil.which("g++") or "c++"
+    # --allow-shlib-undefined: the library's own references into the CUDA
+    # driver resolve when it is loaded on a GPU machine; a build machine
+    # without a driver cannot resolve them at link time
     cmd = [cxx, "-std=c++17", "-O2", "-Wall", "-Wextra", "-I", os.path.join(ROOT, "include"), "-I", HOST, src,
            "-o", EXE, "-L", HERE, "-lmbd_b200", "-Wl,-rpath,$ORIGIN", "-Wl,--allow-shlib-undefined"]
     res = subprocess.run(cmd, capture_output=True, text=True)
