@@ -17,7 +17,8 @@
 // method without the network).  Exit status 0 on success; 1, with the
 // engine's message on stderr, when an input cannot be read or a geometry
 // fails (unknown element, relay matrix not positive definite, ...; in a
-// batch the other geometries' reports are still written); 2 for a bad
+// batch the other geometries' reports are still written, while an input
+// that cannot be read stops the batch before the GPU is used); 2 for a bad
 // command line.
 #include <cstdio>
 #include <cstring>
