@@ -424,6 +424,9 @@ def test_pmbd_b200_batch_with_a_stub_engine(fake_pmbd, tmp_path):
     (d / "sub" / "benzene.in").write_text(fix["geometry_in"])
     out, _ = _run_fake(fake_pmbd, ["--batch", str(lst), "--out-dir", str(out_dir)], tmp_path, vals)
     assert out.returncode == 1 and "would both write" in out.stderr
+    lst.write_text("benzene.in\nmissing.in\n")
+    out, lines = _run_fake(fake_pmbd, ["--batch", str(lst), "--out-dir", str(out_dir)], tmp_path, vals)
+    assert out.returncode == 1 and "missing.in: cannot open" in out.stderr and lines == []
     lst.write_text("benzene.in setting.in extra\n")
     out, _ = _run_fake(fake_pmbd, ["--batch", str(lst), "--out-dir", str(out_dir)], tmp_path, vals)
     assert out.returncode == 1 and "expected geometry.in [setting.in]" in out.stderr
