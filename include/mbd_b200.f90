@@ -175,11 +175,28 @@ MODULE mbd_b200_c
       INTEGER(c_int), VALUE :: n
     END FUNCTION mbd_rsscs_last_timings
 
+    ! counters of the last upload / compute / download (launches, bytes,
+    ! graph kind, network edges, graph updates): stats(n), n >= 3
+    INTEGER(c_int) FUNCTION mbd_rsscs_last_stats(ctx, stats, n) BIND(C, NAME='mbd_rsscs_last_stats')
+      IMPORT :: c_int, c_ptr, c_double
+      TYPE(c_ptr), VALUE :: ctx
+      REAL(c_double), INTENT(OUT) :: stats(*)
+      INTEGER(c_int), VALUE :: n
+    END FUNCTION mbd_rsscs_last_stats
+
     INTEGER(c_int) FUNCTION mbd_rsscs_autotune(ctx, max_n) BIND(C, NAME='mbd_rsscs_autotune')
       IMPORT :: c_int, c_ptr
       TYPE(c_ptr), VALUE :: ctx
       INTEGER(c_int), VALUE :: max_n
     END FUNCTION mbd_rsscs_autotune
+
+    ! the autotuner's choices, 8 values per size class: tuning(n), n >= 64
+    INTEGER(c_int) FUNCTION mbd_rsscs_tuning(ctx, tuning, n) BIND(C, NAME='mbd_rsscs_tuning')
+      IMPORT :: c_int, c_ptr, c_double
+      TYPE(c_ptr), VALUE :: ctx
+      REAL(c_double), INTENT(OUT) :: tuning(*)
+      INTEGER(c_int), VALUE :: n
+    END FUNCTION mbd_rsscs_tuning
 
     INTEGER(c_int) FUNCTION mbd_rsscs_learned_param_count() BIND(C, NAME='mbd_rsscs_learned_param_count')
       IMPORT :: c_int
